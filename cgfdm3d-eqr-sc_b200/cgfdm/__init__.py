@@ -1,0 +1,153 @@
+"""Python view of libcgfdm, the B200 velocity-stress time-stepping library.
+
+The library itself is C++/CUDA behind the C ABI in ``include/cgfdm.h``;
+this module loads it with ctypes and wraps a session.  There is no CPU
+fallback: if the compiled library is missing, importing a session raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import cases  # noqa: F401  (input writers)
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+_LIBDIR = os.path.join(os.path.dirname(_PKG), "lib")
+_libs = {}
+
+
+class CgfdmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"cgfdm error {code}: {msg}")
+        self.code = code
+
+
+class Info(ctypes.Structure):
+    _fields_ = [
+        ("scheme", ctypes.c_int),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("nxp", ctypes.c_int), ("nyp", ctypes.c_int), ("nzp", ctypes.c_int),
+        ("NT", ctypes.c_int), ("steps_done", ctypes.c_int), ("n_stations", ctypes.c_int),
+        ("n_fault_cells", ctypes.c_longlong),
+        ("DT", ctypes.c_float), ("DH", ctypes.c_float), ("dtmax", ctypes.c_float),
+        ("H_min", ctypes.c_float), ("Vp_max", ctypes.c_float),
+        ("device_bytes", ctypes.c_double), ("h2d_bytes", ctypes.c_double),
+        ("kernel_launches", ctypes.c_longlong),
+    ]
+
+
+def lib_path(flavor: str = "fast") -> str:
+    name = "libcgfdm.so" if flavor == "fast" else f"libcgfdm_{flavor}.so"
+    return os.path.join(_LIBDIR, name)
+
+
+def load(flavor: str = "fast") -> ctypes.CDLL:
+    """Loads lib/libcgfdm[_flavor].so; raises if it has not been built."""
+    if flavor in _libs:
+        return _libs[flavor]
+    path = lib_path(flavor)
+    if not os.path.exists(path):
+        raise ImportError(f"{path} not built; run `make -C {os.path.dirname(_LIBDIR)}`")
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    L.cgfdm_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(vp)]
+    L.cgfdm_run.argtypes = [vp, ctypes.c_int]
+    L.cgfdm_run_timed.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.cgfdm_info_get.argtypes = [vp, ctypes.POINTER(Info)]
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.cgfdm_get_stations.argtypes = [vp, fp, ctypes.c_longlong]
+    L.cgfdm_get_wavefield.argtypes = [vp, fp, ctypes.c_longlong]
+    L.cgfdm_get_cjm.argtypes = [vp, fp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)]
+    L.cgfdm_get_pgv.argtypes = [vp, fp, ctypes.c_longlong]
+    L.cgfdm_write_outputs.argtypes = [vp]
+    L.cgfdm_destroy.argtypes = [vp]
+    L.cgfdm_last_error.argtypes = [vp]
+    L.cgfdm_last_error.restype = ctypes.c_char_p
+    L.cgfdm_build_flavor.restype = ctypes.c_char_p
+    _libs[flavor] = L
+    return L
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class Session:
+    """One run directory simulated on one GPU (``cgfdm_create`` ... ``cgfdm_destroy``)."""
+
+    def __init__(self, run_dir: str, options: Optional[str] = None, device: int = 0, flavor: str = "fast"):
+        self.L = load(flavor)
+        self._h = ctypes.c_void_p()
+        rc = self.L.cgfdm_create(run_dir.encode(), options.encode() if options else None, device,
+                                 ctypes.byref(self._h))
+        if rc:
+            raise CgfdmError(rc, self.L.cgfdm_last_error(None).decode())
+        self.run_dir = run_dir
+
+    def _check(self, rc: int):
+        if rc:
+            raise CgfdmError(rc, self.L.cgfdm_last_error(self._h).decode())
+
+    @property
+    def info(self) -> Info:
+        i = Info()
+        self._check(self.L.cgfdm_info_get(self._h, ctypes.byref(i)))
+        return i
+
+    def run(self, nsteps: int) -> None:
+        self._check(self.L.cgfdm_run(self._h, int(nsteps)))
+
+    def run_timed(self, nsteps: int) -> float:
+        ms = ctypes.c_float()
+        self._check(self.L.cgfdm_run_timed(self._h, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def stations(self) -> np.ndarray:
+        i = self.info
+        out = np.zeros((i.n_stations, i.NT, 9), np.float32)
+        self._check(self.L.cgfdm_get_stations(self._h, _fptr(out), out.size))
+        return out
+
+    def wavefield(self) -> np.ndarray:
+        i = self.info
+        out = np.zeros((i.nzp, i.nyp, i.nxp, 9), np.float32)
+        self._check(self.L.cgfdm_get_wavefield(self._h, _fptr(out), out.size))
+        return out
+
+    def cjm(self) -> np.ndarray:
+        i = self.info
+        nf = ctypes.c_int()
+        self._check(self.L.cgfdm_get_cjm(self._h, None, 0, ctypes.byref(nf)))
+        out = np.zeros((i.nzp, i.nyp, i.nxp, nf.value), np.float32)
+        self._check(self.L.cgfdm_get_cjm(self._h, _fptr(out), out.size, ctypes.byref(nf)))
+        return out
+
+    def pgv(self) -> np.ndarray:
+        i = self.info
+        out = np.zeros((i.ny, i.nx, 2), np.float32)
+        self._check(self.L.cgfdm_get_pgv(self._h, _fptr(out), out.size))
+        return out
+
+    def write_outputs(self) -> None:
+        self._check(self.L.cgfdm_write_outputs(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            self.L.cgfdm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -64,6 +64,53 @@ _DEFAULT_PARAMS = {
 }
 
 
+_WGS84_A = 6378137.0
+_WGS84_F = 1.0 / 298.257223563
+
+
+def aeqd_inv(lon0_deg: float, lat0_deg: float, x: float, y: float) -> Tuple[float, float]:
+    """Longitude/latitude (degrees) of the point x east, y north (metres) of
+    the centre: the direct geodesic problem on WGS84 (Vincenty 1975), the
+    inverse of the azimuthal-equidistant projection the library and the
+    reference use to place sub-faults (src/multiSource.cpp:122-171)."""
+    a, f = _WGS84_A, _WGS84_F
+    b = a * (1 - f)
+    lon0, lat0 = math.radians(lon0_deg), math.radians(lat0_deg)
+    s = math.hypot(x, y)
+    if s == 0.0:
+        return lon0_deg, lat0_deg
+    alpha1 = math.atan2(x, y)
+    sA1, cA1 = math.sin(alpha1), math.cos(alpha1)
+    tanU1 = (1 - f) * math.tan(lat0)
+    cosU1 = 1 / math.sqrt(1 + tanU1 * tanU1)
+    sinU1 = tanU1 * cosU1
+    sig1 = math.atan2(tanU1, cA1)
+    sinAl = cosU1 * sA1
+    cos2Al = 1 - sinAl * sinAl
+    u2 = cos2Al * (a * a - b * b) / (b * b)
+    A = 1 + u2 / 16384 * (4096 + u2 * (-768 + u2 * (320 - 175 * u2)))
+    B = u2 / 1024 * (256 + u2 * (-128 + u2 * (74 - 47 * u2)))
+    sig = s / (b * A)
+    for _ in range(200):
+        c2m = math.cos(2 * sig1 + sig)
+        ss, cs = math.sin(sig), math.cos(sig)
+        dS = B * ss * (c2m + B / 4 * (cs * (-1 + 2 * c2m * c2m) - B / 6 * c2m * (-3 + 4 * ss * ss) *
+                                      (-3 + 4 * c2m * c2m)))
+        new = s / (b * A) + dS
+        if abs(new - sig) < 1e-14:
+            sig = new
+            break
+        sig = new
+    c2m = math.cos(2 * sig1 + sig)
+    ss, cs = math.sin(sig), math.cos(sig)
+    tmp = sinU1 * ss - cosU1 * cs * cA1
+    phi2 = math.atan2(sinU1 * cs + cosU1 * ss * cA1, (1 - f) * math.sqrt(sinAl * sinAl + tmp * tmp))
+    lam = math.atan2(ss * sA1, cosU1 * cs - sinU1 * ss * cA1)
+    C = f / 16 * cos2Al * (4 + f * (4 - 3 * cos2Al))
+    L = lam - (1 - C) * f * sinAl * (sig + C * ss * (c2m + C * cs * (-1 + 2 * c2m * c2m)))
+    return math.degrees(lon0 + L), math.degrees(phi2)
+
+
 def ricker(t: np.ndarray, fc: float, t0: Optional[float] = None) -> np.ndarray:
     """Ricker wavelet of peak frequency fc, delayed by t0 (default 1/fc)."""
     if t0 is None:

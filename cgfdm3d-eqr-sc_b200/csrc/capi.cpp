@@ -1,0 +1,133 @@
+// extern "C" boundary: include/cgfdm.h.
+#include "../../include/cgfdm.h"
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "session.hpp"
+
+struct cgfdm_session {
+    cgfdm::Session s;
+};
+
+static thread_local std::string g_create_error;
+
+#ifndef CGFDM_FLAVOR
+#define CGFDM_FLAVOR "fast"
+#endif
+
+extern "C" {
+
+const char *cgfdm_build_flavor(void) { return CGFDM_FLAVOR; }
+
+int cgfdm_create(const char *run_dir, const char *options_json, int device, cgfdm_session **out)
+{
+    if (!run_dir || !out) {
+        g_create_error = "run_dir and out must not be NULL";
+        return CGFDM_E_ARG;
+    }
+    *out = nullptr;
+    cgfdm_session *h = new (std::nothrow) cgfdm_session;
+    if (!h) {
+        g_create_error = "out of host memory";
+        return CGFDM_E_ALLOC;
+    }
+    int st = h->s.create(run_dir, options_json ? options_json : "", device);
+    if (st) {
+        g_create_error = h->s.err;
+        delete h;
+        return st;
+    }
+    *out = h;
+    return CGFDM_OK;
+}
+
+int cgfdm_run(cgfdm_session *s, int nsteps)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.run(nsteps);
+}
+
+int cgfdm_run_timed(cgfdm_session *s, int nsteps, float *ms)
+{
+    if (!s || !ms) return CGFDM_E_ARG;
+    return s->s.run_timed(nsteps, ms, nullptr);
+}
+
+int cgfdm_info_get(const cgfdm_session *s, cgfdm_info *o)
+{
+    if (!s || !o) return CGFDM_E_ARG;
+    const auto &S = s->s;
+    std::memset(o, 0, sizeof *o);
+    o->scheme = S.m.p.scheme;
+    o->nx = S.m.g.nx, o->ny = S.m.g.ny, o->nz = S.m.g.nz;
+    o->nxp = S.m.g._nx_, o->nyp = S.m.g._ny_, o->nzp = S.m.g._nz_;
+    o->NT = S.m.NT;
+    o->steps_done = S.it;
+    o->n_stations = S.nst;
+    o->n_fault_cells = S.m.fault.npts;
+    o->DT = (float)S.m.p.DT;
+    o->DH = S.m.g.DH;
+    o->dtmax = S.m.dtmax;
+    o->H_min = S.m.H_min;
+    o->Vp_max = S.m.Vp_max;
+    o->device_bytes = (double)S.device_bytes;
+    o->h2d_bytes = S.h2d_bytes;
+    o->kernel_launches = S.kernel_launches;
+    return CGFDM_OK;
+}
+
+int cgfdm_get_stations(const cgfdm_session *s, float *out, long long count)
+{
+    if (!s || (!out && s->s.nst > 0)) return CGFDM_E_ARG;
+    if (count < (long long)s->s.nst * s->s.m.NT * 9) return CGFDM_E_ARG;
+    return s->s.get_stations(out);
+}
+
+int cgfdm_get_wavefield(const cgfdm_session *s, float *out, long long count)
+{
+    if (!s || !out) return CGFDM_E_ARG;
+    if (count < s->s.m.g.npad() * 9) return CGFDM_E_ARG;
+    return s->s.get_wavefield(out);
+}
+
+int cgfdm_get_cjm(const cgfdm_session *s, float *out, long long count, int *nfield)
+{
+    if (!s) return CGFDM_E_ARG;
+    int nf = 0;
+    s->s.get_cjm(nullptr, &nf);
+    if (nfield) *nfield = nf;
+    if (!out) return CGFDM_OK;
+    if (count < s->s.m.g.npad() * nf) return CGFDM_E_ARG;
+    return s->s.get_cjm(out, nullptr);
+}
+
+int cgfdm_get_pgv(const cgfdm_session *s, float *out, long long count)
+{
+    if (!s || !out) return CGFDM_E_ARG;
+    if (count < (long long)s->s.m.g.nx * s->s.m.g.ny * 2) return CGFDM_E_ARG;
+    return s->s.get_pgv(out);
+}
+
+int cgfdm_write_outputs(const cgfdm_session *s)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.write_outputs();
+}
+
+int cgfdm_destroy(cgfdm_session *s)
+{
+    delete s;
+    return CGFDM_OK;
+}
+
+const char *cgfdm_last_error(const cgfdm_session *s)
+{
+    if (!s) return g_create_error.c_str();
+    return s->s.err.c_str();
+}
+
+}  // extern "C"

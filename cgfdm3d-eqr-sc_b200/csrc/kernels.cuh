@@ -1,0 +1,80 @@
+// Kernel launch interfaces (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace cgfdm {
+
+// ---------------------------------------------------------------- setup
+cudaError_t launch_setup(const float *d_coord, const float *d_medium, float *cjm, float *rdz, DevGrid g,
+                         float rDH, int scheme, int fp64, cudaStream_t st);
+cudaError_t launch_scale_moment(float *rate, const long long *cell, long long npts, int nt, const float *cjm,
+                                DevGrid g, float DH, cudaStream_t st);
+
+// ------------------------------------------------------------ PML state
+// One absorbing face: Aux fields for its slab, three buffers (A holds the
+// step-start value and receives the final stage, B the intermediate stage
+// values, T the RK accumulator), each 9 fields of `count` floats.
+struct PmlFace {
+    float *A, *B, *T;
+    long long count;     // points in the slab
+    int n0, n1;          // slab extent along its two fastest axes (see pml_pos)
+};
+
+// --------------------------------------------------------- CGFDM stage
+struct CgStageArgs {
+    DevGrid g;
+    const float *Win;    // stencil input of this stage
+    const float *Wm;     // values at the start of the step (RK "m")
+    float *T;            // RK accumulator
+    float *Wout;         // stage output
+    const float *cjm;    // 13 fields
+    const float *rdz;    // 18 surface fields [nyp][pitch]
+    const float *pml_alpha_x, *pml_beta_x, *pml_d_x;
+    const float *pml_alpha_y, *pml_beta_y, *pml_d_y;
+    const float *pml_alpha_z, *pml_beta_z, *pml_d_z;
+    PmlFace face[5];     // x1 y1 z1 x2 y2 (order of src/pml_deriv.cpp:633-646)
+    float *pgv;          // [ny][nx][2] running max, stage 3 only
+    float *dis;          // displacement, 3 fields in the W layout, stage 3 only
+    int irk;
+    int FB1, FB2, FB3;
+    int nPML, pml_on, fs_on;
+    int kchunk;
+    float rDH, DT;
+};
+cudaError_t launch_cg_stage(const CgStageArgs &a, cudaStream_t st);
+size_t cg_stage_smem_bytes();
+
+// --------------------------------------------------- sources / stations
+struct FaultDev {
+    const float *rate;        // [nt][npts][6], scaled
+    const long long *cell;    // layout index per cell
+    long long npts;
+    int nt;
+    float dt;
+};
+struct PointDev {
+    int kind;                 // 1 Ricker, 2 double couple
+    int X, Y, Z;
+    const float *amp;         // [7][7][7]
+    const float *stf;         // [NT]
+    float mom[6];
+    float m0;
+    int inside;
+};
+// Adds the source terms of step *it_dev to W (stage-0 time), as the
+// reference does before the RK stages (src/propagate.cpp:198-210).
+cudaError_t launch_sources(float *W, const float *cjm, DevGrid g, const FaultDev &f, const PointDev &p,
+                           const int *it_dev, float DT, float DH, int scheme, cudaStream_t st);
+cudaError_t launch_point(float *W, float *Wb, float *Wc, const float *cjm, DevGrid g, const PointDev &p,
+                         const int *it_dev, float DT, float DH, int scheme, cudaStream_t st);
+// Records 9 components per station at step *it_dev, then advances *it_dev.
+cudaError_t launch_stations(const float *W, const float *cjm, DevGrid g, const int *st_idx, int nst, int NT,
+                            float *out, int *it_dev, int scheme, cudaStream_t st);
+// Gathers W (9 fields) into the reference AoS layout [_nz_][_ny_][_nx_][9].
+cudaError_t launch_to_aos(const float *W, int nfield, DevGrid g, float *out, cudaStream_t st);
+cudaError_t launch_from_aos(const float *in, int nfield, DevGrid g, float *W, cudaStream_t st);
+
+}  // namespace cgfdm

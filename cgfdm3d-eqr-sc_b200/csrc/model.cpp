@@ -1,0 +1,722 @@
+// Host-side setup: parameters, grid, coordinates, medium, PML profiles,
+// finite-fault and point sources, stations.  Each function follows the
+// reference routine cited beside it and keeps its float/double mix so the
+// arrays are bit-identical to the reference's (this file is compiled with
+// -ffp-contract=off).
+#include "model.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+
+#include "aeqd.h"
+
+namespace cgfdm {
+
+// Constants as the reference defines them (src/macro.h:70-73): PI is a float
+// literal, DEGREE2RADIAN is PI converted to double over 180.0.
+static const float REF_PI = 3.141592657f;
+static const double REF_DEG2RAD = (double)REF_PI / 180.0;
+
+static std::string join(const std::string &dir, const std::string &f)
+{
+    if (f.empty()) return f;
+    if (f[0] == '/') return f;
+    std::string d = dir;
+    if (!d.empty() && d.back() != '/') d += '/';
+    return d + f;
+}
+
+// ----------------------------------------------------------------- params
+int read_params(const std::string &path, Params &p, std::string &err)
+{
+    JsonValue root;
+    {
+        std::ifstream f(path);
+        if (!f) {
+            err = "there is no params file " + path;
+            return ST_NO_PARAMS;
+        }
+    }
+    if (!json_parse_file(path, root, err) || root.kind != JsonValue::Object) {
+        err = "cannot parse json file " + path + ": " + err;
+        return ST_JSON;
+    }
+    const JsonValue *it;
+#define GETD(key, field) if ((it = root.get(key))) p.field = it->num
+#define GETF(key, field) if ((it = root.get(key))) p.field = (float)it->num
+#define GETI(key, field) if ((it = root.get(key))) p.field = it->as_int()
+#define GETS(key, field) if ((it = root.get(key)) && it->kind == JsonValue::String) p.field = it->str
+    GETD("TMAX", TMAX);
+    GETD("DT", DT);
+    GETD("DH", DH);
+    GETI("NX", NX);
+    GETI("NY", NY);
+    GETI("NZ", NZ);
+    GETI("PX", PX);
+    GETI("PY", PY);
+    GETI("PZ", PZ);
+    GETI("centerX", centerX);
+    GETI("centerY", centerY);
+    GETD("centerLongitude", centerLongitude);
+    GETD("centerLatitude", centerLatitude);
+    GETI("IT_SKIP", IT_SKIP);
+    GETI("sliceX", sliceX);
+    GETI("sliceY", sliceY);
+    GETI("sliceZ", sliceZ);
+    GETI("sliceFreeSurf", sliceFreeSurf);
+    GETI("nPML", nPML);
+    GETI("gauss_hill", gauss_hill);
+    GETI("useTerrain", useTerrain);
+    GETI("useMedium", useMedium);
+    GETI("useMultiSource", useMultiSource);
+    GETI("LayeredModel", LayeredModel);
+    GETS("LayeredFileName", LayeredFileName);
+    GETI("useSingleSource(ricker)", useSingleSource_ricker);
+    GETI("useSingleSource(double_couple)", useSingleSource_double_couple);
+    GETF("strike", strike);
+    GETF("dip", dip);
+    GETF("rake", rake);
+    GETF("Mw", Mw);
+    GETF("duration", duration);
+    GETF("rickerfc", rickerfc);
+    GETI("ShenModel", ShenModel);
+    GETI("Crust_1Model", Crust_1Model);
+    GETS("OUT", OUT);
+    GETF("Depth(km)", Depth);
+    GETI("sourceX", sourceX);
+    GETI("sourceY", sourceY);
+    GETI("sourceZ", sourceZ);
+    GETS("sourceFile", sourceFile);
+    GETS("sourceDir", sourceDir);
+    GETI("degree2radian", degree2radian);
+    // run-time switches (names of the reference's compile-time flags)
+    if ((it = root.get("scheme")) && it->kind == JsonValue::String) {
+        std::string s = it->str;
+        for (auto &c : s) c = (char)std::toupper((unsigned char)c);
+        if (s == "SCFDM" || s == "AWENO" || s == "ME-AWENO") p.scheme = SCHEME_SCFDM;
+        else if (s == "CGFDM") p.scheme = SCHEME_CGFDM;
+        else {
+            err = "unknown scheme " + it->str;
+            return ST_OPTIONS;
+        }
+    }
+    // defaults of the two reference builds (Makefile_CGFDM / Makefile_SCFDM)
+    p.pml = p.scheme == SCHEME_CGFDM ? 1 : 0;
+    p.exp_decay = p.scheme == SCHEME_SCFDM ? 1 : 0;
+    GETI("PML", pml);
+    GETI("EXP_DECAY", exp_decay);
+    GETI("SOLVE_DISPLACEMENT", solve_displacement);
+    if ((it = root.get("metricPrecision")) && it->kind == JsonValue::String) p.metric_fp64 = it->str == "fp64";
+    GETS("storage", storage);
+    GETS("terrainFile", terrainFile);
+    GETS("mediumFile", mediumFile);
+#undef GETD
+#undef GETF
+#undef GETI
+#undef GETS
+    if (!p.useTerrain) p.Depth = (float)(p.DH * p.NZ * 1e-3);  // src/getParams.cpp:234-237
+    return ST_OK;
+}
+
+// ------------------------------------------------------------------- grid
+Grid make_grid(const Params &p)
+{
+    Grid g;
+    g.NX = p.NX, g.NY = p.NY, g.NZ = p.NZ;
+    g.nx = p.NX, g.ny = p.NY, g.nz = p.NZ;
+    g._nx_ = g.nx + 2 * HALO, g._ny_ = g.ny + 2 * HALO, g._nz_ = g.nz + 2 * HALO;
+    g._nx = g.nx + HALO, g._ny = g.ny + HALO, g._nz = g.nz + HALO;
+    g.originalX = p.centerX, g.originalY = p.centerY;
+    g.nPML = p.nPML;
+    g.DH = (float)p.DH;
+    g.rDH = (float)(1.0 / g.DH);  // src/init_grid.cpp:89
+    return g;
+}
+
+// ------------------------------------------------------------ coordinates
+// Flat grid (src/coord.cpp:99-134), single Gauss hill (:136-177) and the
+// terrain-following z of src/coord.cpp:204-255.
+static void build_coords(Model &m)
+{
+    const Grid &g = m.g;
+    const float DH = g.DH;
+    const int NZ = g.NZ;
+    m.coord.assign((size_t)g.npad() * 3, 0.f);
+    m.terrain.assign((size_t)g._nx_ * g._ny_, 0.f);
+    for (int k = 0; k < g._nz_; k++)
+        for (int j = 0; j < g._ny_; j++)
+            for (int i = 0; i < g._nx_; i++) {
+                long long id = g.idx(i, j, k) * 3;
+                int I = i, J = j, K = k;
+                if (K == NZ + HALO - 1) m.terrain[(size_t)i + (size_t)j * g._nx_] = (K - HALO + 1) * DH - NZ * DH;
+                m.coord[id + 0] = (I - HALO) * DH - g.originalX * DH;
+                m.coord[id + 1] = (J - HALO) * DH - g.originalY * DH;
+                m.coord[id + 2] = (K - HALO + 1) * DH - NZ * DH;
+            }
+}
+
+static void terrain_following_z(Model &m, float cal_depth)
+{
+    const Grid &g = m.g;
+    for (int k = 0; k < g._nz_; k++)
+        for (int j = 0; j < g._ny_; j++)
+            for (int i = 0; i < g._nx_; i++) {
+                long long id = g.idx(i, j, k);
+                int K = k - HALO;
+                float height = m.terrain[(size_t)i + (size_t)j * g._nx_];
+                float DZ = (float)(double(height + std::fabs(cal_depth)) / double(g.NZ - 1));
+                m.coord[id * 3 + 2] = -std::fabs(cal_depth) + DZ * K;
+            }
+}
+
+static void gauss_hill(Model &m)
+{
+    const Grid &g = m.g;
+    const float DH = g.DH;
+    float cal_depth = m.p.Depth * 1000;
+    float h = (float)(0.2 * cal_depth);
+    float a = (float)(0.1 * cal_depth), b = (float)(0.1 * cal_depth);
+    for (int j = 0; j < g._ny_; j++)
+        for (int i = 0; i < g._nx_; i++) {
+            float x = (i - HALO) * DH - g.originalX * DH;
+            float y = (j - HALO) * DH - g.originalY * DH;
+            float height = h * expf(-0.5f * (x * x / (a * a) + y * y / (b * b)));
+            m.terrain[(size_t)i + (size_t)j * g._nx_] = height;
+        }
+    terrain_following_z(m, cal_depth);
+}
+
+// Extension: a raw float32 [_ny_][_nx_] surface height map in metres, mapped
+// by the reference's terrain-following formula (src/coord.cpp:228-234).
+static int terrain_file(Model &m, const std::string &path, std::string &err)
+{
+    const Grid &g = m.g;
+    std::ifstream f(path, std::ios::binary);
+    if (!f) {
+        err = "cannot open terrain file " + path;
+        return ST_IO;
+    }
+    f.read((char *)m.terrain.data(), (std::streamsize)(m.terrain.size() * sizeof(float)));
+    if (!f) {
+        err = "terrain file too short: " + path;
+        return ST_IO;
+    }
+    terrain_following_z(m, m.p.Depth * 1000);
+    (void)g;
+    return ST_OK;
+}
+
+// ----------------------------------------------------------------- medium
+// Homogeneous default (src/medium.cpp:115-140), then the 1-D layered model
+// (src/medium.cpp:143-267, LayeredStructureTerrain on as in Makefile_CGFDM).
+static int build_medium(Model &m, const std::string &run_dir, std::string &err)
+{
+    const Grid &g = m.g;
+    m.medium.resize((size_t)g.npad() * 3);
+    for (long long n = 0; n < g.npad(); n++) {
+        m.medium[n * 3 + 0] = 3300.0f;
+        m.medium[n * 3 + 1] = 5716.0f;
+        m.medium[n * 3 + 2] = 2700.0f;
+    }
+    if (!m.p.useMedium) return ST_OK;
+    if (m.p.ShenModel || m.p.Crust_1Model) {
+        err = "ShenModel/Crust_1Model media need PROJ and external model files; not supported";
+        return ST_OPTIONS;
+    }
+    if (!m.p.LayeredModel) return ST_OK;
+    std::string path = join(run_dir, m.p.LayeredFileName);
+    std::ifstream f(path, std::ios::binary);
+    if (!f) {
+        err = "cannot open Layered Model file " + path;
+        return ST_IO;
+    }
+    int layers = 0;
+    f.read((char *)&layers, 4);
+    if (!f || layers < 0 || layers > 100000) {
+        err = "bad layered model file " + path;
+        return ST_IO;
+    }
+    std::vector<float> hgt(layers), vsd(layers), vpd(layers), rhod(layers);
+    for (int F = 0; F < layers; ++F) {
+        float v[4];
+        f.read((char *)v, 16);
+        if (!f) {
+            err = "layered model file too short: " + path;
+            return ST_IO;
+        }
+        hgt[F] = v[0] * 1000.0f;
+        if (F != 0) hgt[F] += 0.0f;
+        vsd[F] = v[1] * 1000.f;
+        vpd[F] = v[2] * 1000.f;
+        rhod[F] = v[3] * 1000.f;
+    }
+    const float tolerance = 1.0f;
+    for (int k = 0; k < g._nz_; k++)
+        for (int j = 0; j < g._ny_; j++)
+            for (int i = 0; i < g._nx_; i++) {
+                long long id = g.idx(i, j, k);
+                double terrain = m.terrain[(size_t)i + (size_t)j * g._nx_];
+                float coordz = m.coord[id * 3 + 2];
+                float *md = &m.medium[id * 3];
+                for (int F = 1; F < layers; ++F) {
+                    float h0 = (float)(-hgt[0] + terrain);
+                    float h1 = (float)(-hgt[F - 1] + terrain);
+                    float h2 = (float)(-hgt[F] + terrain);
+                    if (coordz > (h0 - tolerance)) md[0] = vsd[0], md[1] = vpd[0], md[2] = rhod[0];
+                    if ((h1 - tolerance) > coordz && coordz > (h2 - tolerance))
+                        md[0] = vsd[F - 1], md[1] = vpd[F - 1], md[2] = rhod[F - 1];
+                    if ((h2 - tolerance) > coordz) md[0] = vsd[F], md[1] = vpd[F], md[2] = rhod[F];
+                }
+            }
+    return ST_OK;
+}
+
+// Extension: raw float32 [_nz_][_ny_][_nx_][3] (Vs, Vp, rho) volume.
+static int medium_file(Model &m, const std::string &path, std::string &err)
+{
+    std::ifstream f(path, std::ios::binary);
+    if (!f) {
+        err = "cannot open medium file " + path;
+        return ST_IO;
+    }
+    f.read((char *)m.medium.data(), (std::streamsize)(m.medium.size() * sizeof(float)));
+    if (!f) {
+        err = "medium file too short: " + path;
+        return ST_IO;
+    }
+    return ST_OK;
+}
+
+static void value_ranges(Model &m)
+{
+    // src/calc_CFL.cpp:165-180,283-285: ranges over the whole padded grid
+    float mn[3] = {1.0e20f, 1.0e20f, 1.0e20f}, mx[3] = {-1.0e20f, -1.0e20f, -1.0e20f};
+    const long long n = m.g.npad();
+    for (long long q = 0; q < n; q++)
+        for (int c = 0; c < 3; c++) {
+            float v = m.medium[q * 3 + c];
+            if (v < mn[c]) mn[c] = v;
+            if (v > mx[c]) mx[c] = v;
+        }
+    m.Vs_min = mn[0], m.Vs_max = mx[0];
+    m.Vp_min = mn[1], m.Vp_max = mx[1];
+    m.rho_min = mn[2], m.rho_max = mx[2];
+}
+
+// ------------------------------------------------------------------- PML
+// src/init_pml_para.cpp:97-239, all six borders on a single rank; the top
+// face is not absorbing under FREE_SURFACE.
+static void build_pml(Model &m)
+{
+    const Grid &g = m.g;
+    const int _nx_ = g._nx_, _ny_ = g._ny_, _nz_ = g._nz_;
+    const int _nx = g._nx, _ny = g._ny, _nz = g._nz;
+    const float DH = g.DH;
+    const int nPML = g.nPML;
+    const float P_alpha = 1.0f, P_beta = 2.0f, P_d = 2.0f;
+    float Cp = 6000.0;
+    float pml_fc = 0.5;
+    float L = DH * (nPML - 1);
+    float R = (float)std::pow(10.0, -(std::log10((double)nPML) - 1.0) / std::log10(2.0) - 3.0);
+    float d0 = -(P_d + 1.0f) * Cp / (2.0f * L) * logf(R);
+    float pml_alpha0 = REF_PI * pml_fc;
+    float pml_beta0 = 3.0;
+    auto cal_alpha = [&](float l) { return (l < 0.0f) ? 0.0f : (pml_alpha0 * (1.0f - powf(l / L, P_alpha))); };
+    auto cal_beta = [&](float l) { return (l < 0.0f) ? 1.0f : (1.0f + (pml_beta0 - 1.0f) * powf(l / L, P_beta)); };
+    auto cal_d = [&](float l) { return (l < 0.0f) ? 0.0f : (d0 * powf(l / L, P_d)); };
+
+    auto axis = [&](int n_, int n_in, bool lo, bool hi, bool allow_hi, std::vector<float> &al,
+                    std::vector<float> &be, std::vector<float> &dd) {
+        std::vector<float> Ls(n_, -1.0f);
+        for (int i = HALO; i < n_in; ++i) {
+            if (i < HALO + nPML && lo) Ls[i] = (HALO + nPML - 1 - i) * DH;
+            if (allow_hi && i >= n_in - nPML && hi) Ls[i] = (i - (n_in - nPML)) * DH;
+        }
+        al.assign(n_, 0.0f);
+        be.assign(n_, 1.0f);
+        dd.assign(n_, 0.0f);
+        for (int i = HALO; i < n_in; ++i) {
+            al[i] = cal_alpha(Ls[i]);
+            be[i] = cal_beta(Ls[i]);
+            dd[i] = cal_d(Ls[i]);
+        }
+        for (int i = 0; i < n_; ++i) {
+            dd[i] /= be[i];
+            be[i] = 1.0f / be[i];
+        }
+    };
+    axis(_nx_, _nx, m.border[0], m.border[1], true, m.pml_alpha_x, m.pml_beta_x, m.pml_d_x);
+    axis(_ny_, _ny, m.border[2], m.border[3], true, m.pml_alpha_y, m.pml_beta_y, m.pml_d_y);
+    axis(_nz_, _nz, m.border[4], m.border[5], false, m.pml_alpha_z, m.pml_beta_z, m.pml_d_z);
+}
+
+// ---------------------------------------------------------- point sources
+// Gaussian spatial weights of the 7x7x7 smoothed point source
+// (src/singleSource.cpp:134-143, GAUSS_FUN of src/macro.h:37).
+static std::vector<float> gauss_weights(int nGauss)
+{
+    std::vector<float> amp;
+    float ra = (float)(nGauss * 0.5);
+    for (int dk = -nGauss; dk <= nGauss; dk++)
+        for (int dj = -nGauss; dj <= nGauss; dj++)
+            for (int di = -nGauss; di <= nGauss; di++) {
+                auto gf = [&](int t) {
+                    double q = ((t) - (0.0)) / (ra);
+                    return (float)(std::exp(-(q * q)) / (ra * 1.772453850905516));
+                };
+                float D1 = gf(di), D2 = gf(dj), D3 = gf(dk);
+                float a = D1 * D2 * D3;
+                a = (float)(a / 0.998125703461425);
+                amp.push_back(a);
+            }
+    return amp;
+}
+
+// Stage-0 source time t = (it + 0.0f) * DT (src/singleSource.cpp:47-59).
+static float ricker_value(float rickerfc, int it, float DT)
+{
+    float t = (it + 0.0f) * DT;
+    float tdelay = 1.0f / rickerfc;
+    float r = REF_PI * rickerfc * (t - tdelay);
+    float rr = r * r;
+    float s = (float)(r * (3.0 - 2.0f * rr) * expf(-rr) * sqrtf(REF_PI) * 0.5 * rickerfc * REF_PI);
+    float M0 = 1e9;
+    s *= M0;
+    return s;
+}
+
+static float gauss_stf(float duration, int it, float DT)
+{
+    float t = (it + 0.0f) * DT;
+    float tdelay = duration / 2 + 1;
+    return expf(-(t - tdelay) * (t - tdelay) / (duration * duration)) / (sqrtf(REF_PI) * duration);
+}
+
+// Moment-tensor components from strike/dip/rake in radians, in the
+// reference's float/double mix (src/multiSource.cpp:507-519,
+// src/singleSource.cpp:257-269), returned as (Mxx, Myy, Mzz, Mxy, Mxz, Myz)
+// = (M22, M11, M33, M12, -M23, -M13) before scaling.
+struct MT {
+    float M11, M22, M33, M12, M13, M23;
+};
+static MT moment_tensor(float s, float d, float r)
+{
+    MT t;
+    double sdcr = (double)(sinf(d) * cosf(r));
+    t.M11 = (float)(-(sdcr * std::sin(2.0 * s) + std::sin(2.0 * d) * sinf(r) * sinf(s) * sinf(s)));
+    t.M22 = (float)(sdcr * std::sin(2.0 * s) - std::sin(2.0 * d) * sinf(r) * cosf(s) * cosf(s));
+    t.M33 = -(t.M11 + t.M22);
+    t.M12 = (float)(sdcr * std::cos(2.0 * s) + 0.5 * std::sin(2.0 * d) * sinf(r) * std::sin(2.0 * s));
+    t.M13 = (float)(-((double)(cosf(d) * cosf(r) * cosf(s)) + std::cos(2.0 * d) * sinf(r) * sinf(s)));
+    t.M23 = (float)(-((double)(cosf(d) * cosf(r) * sinf(s)) - std::cos(2.0 * d) * sinf(r) * cosf(s)));
+    return t;
+}
+
+static void build_point_source(Model &m)
+{
+    const Grid &g = m.g;
+    PointSource &ps = m.point;
+    if (!m.p.useSingleSource_ricker && !m.p.useSingleSource_double_couple) return;
+    ps.kind = m.p.useSingleSource_ricker ? 1 : 2;
+    // src/singleSource.cpp:25-40 (locateSource), single rank
+    ps.X = m.p.sourceX + HALO, ps.Y = m.p.sourceY + HALO, ps.Z = m.p.sourceZ + HALO;
+    ps.inside = ps.X >= HALO && ps.X < g._nx && ps.Y >= HALO && ps.Y < g._ny && ps.Z >= HALO && ps.Z < g._nz;
+    ps.amp = gauss_weights(3);
+    float DT = (float)m.p.DT;
+    ps.stf.resize(m.NT);
+    if (ps.kind == 1) {
+        for (int it = 0; it < m.NT; it++) ps.stf[it] = ricker_value(m.p.rickerfc, it, DT);
+    } else {
+        for (int it = 0; it < m.NT; it++) ps.stf[it] = gauss_stf(m.p.duration, it, DT);
+        float s = (float)(m.p.strike * REF_DEG2RAD), d = (float)(m.p.dip * REF_DEG2RAD);
+        float r = (float)(m.p.rake * REF_DEG2RAD);
+        MT t = moment_tensor(s, d, r);
+        ps.mom[0] = t.M22, ps.mom[1] = t.M11, ps.mom[2] = t.M33;
+        ps.mom[3] = t.M12, ps.mom[4] = -t.M23, ps.mom[5] = -t.M13;
+        ps.m0 = (float)(1.5 * powf(10, m.p.Mw + 6));
+    }
+}
+
+// ----------------------------------------------------- finite-fault source
+// src/multiSource.cpp:24-868 for one rank, up to (but not including) the
+// mu/(J DH^3) scaling, which needs the metric and runs on the GPU.
+static int build_fault(Model &m, const std::string &run_dir, std::string &err)
+{
+    const Grid &g = m.g;
+    FaultSource &fs = m.fault;
+    std::string path = join(join(run_dir, m.p.sourceDir), m.p.sourceFile);
+    if (!m.p.sourceDir.empty() && m.p.sourceDir[0] == '/') path = join(m.p.sourceDir, m.p.sourceFile);
+    std::ifstream f(path, std::ios::binary);
+    if (!f) {
+        err = "can't open source file " + path;
+        return ST_IO;
+    }
+    int npts_i = 0, nt = 0;
+    float dt = 0;
+    f.read((char *)&npts_i, 4);
+    f.read((char *)&nt, 4);
+    f.read((char *)&dt, 4);
+    if (!f || npts_i < 0 || nt < 0) {
+        err = "bad source file header " + path;
+        return ST_IO;
+    }
+    const long long npts = npts_i;
+    const long long rec = 6 * 4 + 2LL * 4 * nt;
+    std::vector<float> x(npts), y(npts), z(npts);
+    for (long long i = 0; i < npts; i++) {
+        float v[3];
+        f.seekg(12 + rec * i, std::ios::beg);
+        f.read((char *)v, 12);
+        if (!f) {
+            err = "source file too short: " + path;
+            return ST_IO;
+        }
+        x[i] = v[0], y[i] = v[1], z[i] = v[2];
+    }
+    // projection (src/multiSource.cpp:96-171): the centre goes through the
+    // "%lf" formatting of a float, source points through DEGREE2RADIAN
+    {
+        char buf[64];
+        float lon_0 = (float)m.p.centerLongitude, lat_0 = (float)m.p.centerLatitude;
+        std::snprintf(buf, sizeof buf, "%lf", (double)lon_0);
+        double lon0 = std::atof(buf) * (3.14159265358979323846 / 180.0);
+        std::snprintf(buf, sizeof buf, "%lf", (double)lat_0);
+        double lat0 = std::atof(buf) * (3.14159265358979323846 / 180.0);
+        for (long long i = 0; i < npts; i++) {
+            double px, py;
+            cgfdm_aeqd_fwd(lon0, lat0, x[i] * REF_DEG2RAD, y[i] * REF_DEG2RAD, &px, &py);
+            x[i] = (float)px;
+            y[i] = (float)py;
+        }
+    }
+    // cell location (src/multiSource.cpp:173-314, NO_SOURCE_SMOOTH branch)
+    float Depth = m.p.Depth * 1000;
+    const float DH = g.DH;
+    float maxCoordZ = -Depth;
+    for (long long jj = 0; jj < npts; jj++)
+        if (maxCoordZ < z[jj]) maxCoordZ = z[jj];
+    for (long long jj = 0; jj < npts; jj++) z[jj] = z[jj] - maxCoordZ;
+    std::map<long long, long long> point_index;
+    long long pointNum = 0;
+    for (long long i = 0; i < npts; i++) {
+        int srcX = int(x[i] / DH + 0.5) + g.originalX + HALO;
+        int srcY = int(y[i] / DH + 0.5) + g.originalY + HALO;
+        if (srcX >= HALO && srcX < g._nx && srcY >= HALO && srcY < g._ny) {
+            double DZ = m.coord[g.idx(srcX, srcY, 4) * 3 + 2] - m.coord[g.idx(srcX, srcY, 3) * 3 + 2];
+            double terrain = DZ * double(g.NZ - 1) - std::fabs(Depth);
+            z[i] = (float)(terrain + z[i]);
+            for (int k = HALO; k < g._nz; k++) {
+                long long index1 = g.idx(srcX, srcY, k - 1), index2 = g.idx(srcX, srcY, k + 1);
+                long long index = g.idx(srcX, srcY, k);
+                double dz1 = (m.coord[index * 3 + 2] - m.coord[index1 * 3 + 2]) * 0.5;
+                double dz2 = (m.coord[index2 * 3 + 2] - m.coord[index * 3 + 2]) * 0.5;
+                if (m.coord[index * 3 + 2] - dz1 <= z[i] && z[i] < dz2 + m.coord[index * 3 + 2]) {
+                    point_index[i] = index;
+                    pointNum++;
+                }
+            }
+        }
+    }
+    // parameters of the located points, in sub-fault order (:345-396)
+    std::vector<float> area(pointNum, 0.f), strike(pointNum, 0.f), dip(pointNum, 0.f);
+    std::vector<float> rake((size_t)pointNum * nt, 0.f), rate((size_t)pointNum * nt, 0.f);
+    {
+        long long i = 0;
+        for (auto &pi : point_index) {
+            f.clear();
+            f.seekg(12 + rec * pi.first + 12, std::ios::beg);
+            f.read((char *)&area[i], 4);
+            f.read((char *)&strike[i], 4);
+            f.read((char *)&dip[i], 4);
+            f.read((char *)&rake[(size_t)i * nt], 4LL * nt);
+            f.read((char *)&rate[(size_t)i * nt], 4LL * nt);
+            if (!f) {
+                err = "source file too short: " + path;
+                return ST_IO;
+            }
+            i++;
+        }
+    }
+    // moment rate per point and sample (:450-535)
+    std::vector<float> mr((size_t)pointNum * nt * 6, 0.f);
+    for (long long p = 0; p < pointNum; p++) {
+        float s = (float)(strike[p] * REF_DEG2RAD), d = (float)(dip[p] * REF_DEG2RAD), a = area[p];
+        for (int it = 0; it < nt; it++) {
+            long long index = it + p * nt;
+            float r = m.p.degree2radian == 0 ? rake[index] : (float)(rake[index] * REF_DEG2RAD);
+            float rt = rate[index];
+            MT t = moment_tensor(s, d, r);
+            mr[index * 6 + 0] = t.M22 * a * rt;
+            mr[index * 6 + 1] = t.M11 * a * rt;
+            mr[index * 6 + 2] = t.M33 * a * rt;
+            mr[index * 6 + 3] = t.M12 * a * rt;
+            mr[index * 6 + 4] = -t.M23 * a * rt;
+            mr[index * 6 + 5] = -t.M13 * a * rt;
+        }
+    }
+    // sub-faults sharing a cell are summed into the last of them (:537-592)
+    std::map<long long, long long> index_point;
+    {
+        long long i = 0;
+        for (auto &pi : point_index) index_point[pi.second] = i++;
+        i = 0;
+        for (auto &pi : point_index) {
+            long long ii = index_point[pi.second];
+            if (ii > i)
+                for (int t = 0; t < nt; t++)
+                    for (int c = 0; c < 6; c++)
+                        mr[((size_t)t + ii * nt) * 6 + c] += mr[((size_t)t + i * nt) * 6 + c];
+            i++;
+        }
+    }
+    // reorder to [t][cell] with cells ascending by grid index (:706-752)
+    fs.npts = (long long)index_point.size();
+    fs.nt = nt;
+    fs.dt = dt;
+    fs.index.resize(fs.npts);
+    fs.rate.assign((size_t)fs.npts * nt * 6, 0.f);
+    long long J = 0;
+    for (auto &ip : index_point) {
+        fs.index[J] = ip.first;
+        long long ii = ip.second;
+        for (int t = 0; t < nt; t++)
+            for (int c = 0; c < 6; c++)
+                fs.rate[((size_t)J + (size_t)t * fs.npts) * 6 + c] = mr[((size_t)ii * nt + t) * 6 + c];
+        J++;
+    }
+    return ST_OK;
+}
+
+// --------------------------------------------------------------- stations
+// src/station.cpp:92-292: global [X, Y, Z] indices, kept when inside the
+// interior; a missing file means no stations, a malformed entry stops reading.
+static int read_stations(Model &m, const std::string &run_dir, std::string &err)
+{
+    std::string path = join(run_dir, "station.json");
+    std::ifstream f(path);
+    if (!f) return ST_OK;
+    JsonValue root;
+    std::string e;
+    if (!json_parse_file(path, root, e)) return ST_OK;  // reference: "Can't parse json file!", no stations
+    const JsonValue *arr = root.get("station(point)");
+    if (!arr) return ST_OK;
+    const Grid &g = m.g;
+    std::vector<int> loc, glob;
+    const size_t cnt = arr->kind == JsonValue::Object ? arr->members.size() : arr->items.size();
+    for (size_t i = 0; i < cnt; i++) {
+        const JsonValue &s = arr->kind == JsonValue::Object ? arr->members[i].second : arr->items[i];
+        size_t a = s.kind == JsonValue::Object ? s.members.size() : s.items.size();
+        if (a != 3) {
+            err = "station entry without 3 indices";
+            m.stations.clear();
+            m.stations_global.clear();
+            return ST_OK;
+        }
+        auto at = [&](int q) { return s.kind == JsonValue::Object ? s.members[q].second.as_int() : s.items[q].as_int(); };
+        int X = at(0), Y = at(1), Z = at(2);
+        int tx = X + HALO, ty = Y + HALO, tz = Z + HALO;
+        if (tx >= HALO && tx < g._nx && ty >= HALO && ty < g._ny && tz >= HALO && tz < g._nz) {
+            loc.insert(loc.end(), {tx, ty, tz});
+            glob.insert(glob.end(), {X, Y, Z});
+        }
+    }
+    m.stations = loc;
+    m.stations_global = glob;
+    return ST_OK;
+}
+
+// ------------------------------------------------------------------ model
+int build_model(const std::string &run_dir, const std::string &options_json, Model &m, std::string &err)
+{
+    int st = read_params(join(run_dir, "params.json"), m.p, err);
+    if (st) return st;
+    if (!options_json.empty()) {
+        // run-time overrides as a JSON object with the same keys
+        JsonValue o;
+        if (!json_parse(options_json, o, err) || o.kind != JsonValue::Object) {
+            err = "bad options json: " + err;
+            return ST_JSON;
+        }
+        const JsonValue *it;
+        if ((it = o.get("scheme")) && it->kind == JsonValue::String) {
+            std::string s = it->str;
+            for (auto &c : s) c = (char)std::toupper((unsigned char)c);
+            m.p.scheme = (s == "SCFDM" || s == "AWENO") ? SCHEME_SCFDM : SCHEME_CGFDM;
+            m.p.pml = m.p.scheme == SCHEME_CGFDM;
+            m.p.exp_decay = m.p.scheme == SCHEME_SCFDM;
+        }
+        if ((it = o.get("PML"))) m.p.pml = it->as_int();
+        if ((it = o.get("EXP_DECAY"))) m.p.exp_decay = it->as_int();
+        if ((it = o.get("SOLVE_DISPLACEMENT"))) m.p.solve_displacement = it->as_int();
+        if ((it = o.get("metricPrecision")) && it->kind == JsonValue::String) m.p.metric_fp64 = it->str == "fp64";
+        if ((it = o.get("storage")) && it->kind == JsonValue::String) m.p.storage = it->str;
+        if ((it = o.get("OUT")) && it->kind == JsonValue::String) m.p.OUT = it->str;
+    }
+    Params &p = m.p;
+    if (p.NX <= 0 || p.NY <= 0 || p.NZ <= 0 || p.DH <= 0 || p.DT <= 0) {
+        err = "NX, NY, NZ, DH and DT must be positive";
+        return ST_OPTIONS;
+    }
+    if (p.PX != 1 || p.PY != 1 || p.PZ != 1) {
+        // single-GPU library: the decomposition is ignored, the whole grid runs on one device
+        p.PX = p.PY = p.PZ = 1;
+    }
+    // src/modelChecking.cpp:17-61
+    if (p.useSingleSource_ricker && p.useSingleSource_double_couple) {
+        err = "useSingleSource(ricker) and useSingleSource(double_couple) set at the same time";
+        return ST_OPTIONS;
+    }
+    if (!(p.useMultiSource || p.useSingleSource_ricker || p.useSingleSource_double_couple)) {
+        err = "no source set";
+        return ST_OPTIONS;
+    }
+    if (p.useTerrain && p.terrainFile.empty()) {
+        err = "useTerrain (SRTM90 + PROJ) is not supported; give a raw height map as terrainFile";
+        return ST_OPTIONS;
+    }
+    if (p.gauss_hill && !p.terrainFile.empty()) {
+        err = "gauss_hill and terrainFile are exclusive";
+        return ST_OPTIONS;
+    }
+    if (p.storage != "fp32" && p.storage != "fp16" && p.storage != "bf16") {
+        err = "storage must be fp32, fp16 or bf16";
+        return ST_OPTIONS;
+    }
+    m.g = make_grid(p);
+    const Grid &g = m.g;
+    float DT = (float)p.DT;
+    m.NT = (int)(p.TMAX / DT);  // src/propagate.cpp:88
+    if (m.NT < 0) m.NT = 0;
+    if (p.pml && p.scheme == SCHEME_CGFDM) {
+        if (g.nPML >= g.nx || g.nPML >= g.ny || g.nPML >= g.nz) {
+            err = "The PML layer(nPML) is not smaller than nx/ny/nz";
+            return ST_PML_SIZE;
+        }
+        if (g.nPML < 2) {
+            err = "nPML must be at least 2";
+            return ST_PML_SIZE;
+        }
+    }
+    build_coords(m);
+    if (p.gauss_hill) gauss_hill(m);
+    else if (!p.terrainFile.empty()) {
+        if ((st = terrain_file(m, join(run_dir, p.terrainFile), err))) return st;
+    }
+    if ((st = build_medium(m, run_dir, err))) return st;
+    if (!p.mediumFile.empty())
+        if ((st = medium_file(m, join(run_dir, p.mediumFile), err))) return st;
+    value_ranges(m);
+    build_pml(m);
+    build_point_source(m);
+    if (p.useMultiSource)
+        if ((st = build_fault(m, run_dir, err))) return st;
+    if ((st = read_stations(m, run_dir, err))) return st;
+    return ST_OK;
+}
+
+}  // namespace cgfdm

@@ -1,0 +1,140 @@
+// Host-side model description: run parameters, grid, coordinates, medium,
+// PML profiles, sources and stations.  Everything here mirrors the
+// reference's setup stage (src/run.cpp:28-138) for a single rank and is
+// computed on the host in the reference's own float/double mix, so the
+// arrays handed to the GPU are bit-identical to what the reference builds.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "json.hpp"
+
+namespace cgfdm {
+
+constexpr int HALO = 3;
+
+// Status codes returned through the C ABI (reference abort codes where one
+// exists: src/getParams.cpp:100,1001; src/calc_CFL.cpp:344 (110);
+// src/pml_deriv.cpp:58 (130); src/modelChecking.cpp:27 (180); alloc 10001).
+enum Status : int {
+    ST_OK = 0,
+    ST_NO_PARAMS = 100,
+    ST_CFL = 110,
+    ST_PML_SIZE = 130,
+    ST_OPTIONS = 180,
+    ST_JSON = 1001,
+    ST_IO = 1002,
+    ST_ALLOC = 10001,
+    ST_CUDA = 20001,
+    ST_TIMEOUT = 20002,
+    ST_ARG = 20003,
+    ST_STATE = 20004,
+};
+
+enum Scheme { SCHEME_CGFDM = 0, SCHEME_SCFDM = 1 };
+
+// Fields of the reference's PARAMS (src/struct.h:21-116) that the hot path
+// and its inputs use, zero-initialised (the reference leaves missing keys
+// uninitialised, src/main.cpp:20), plus run-time switches that replace the
+// reference's compile-time ones.
+struct Params {
+    double TMAX = 0, DT = 0, DH = 0;
+    int NX = 0, NY = 0, NZ = 0;
+    int PX = 1, PY = 1, PZ = 1;
+    int centerX = 0, centerY = 0;
+    double centerLatitude = 0, centerLongitude = 0;
+    int sourceX = 0, sourceY = 0, sourceZ = 0;
+    int IT_SKIP = 0;
+    int sliceX = 0, sliceY = 0, sliceZ = 0, sliceFreeSurf = 0;
+    int nPML = 0;
+    int gauss_hill = 0, useTerrain = 0, useMedium = 0, useMultiSource = 0;
+    int useSingleSource_ricker = 0;
+    float rickerfc = 0;
+    int useSingleSource_double_couple = 0;
+    float strike = 0, dip = 0, rake = 0, Mw = 0, duration = 0;
+    int ShenModel = 0, Crust_1Model = 0, LayeredModel = 0;
+    std::string LayeredFileName;
+    std::string OUT;
+    float Depth = 0;
+    std::string sourceFile, sourceDir;
+    int degree2radian = 0;
+
+    // run-time replacements of the reference's -D switches
+    int scheme = SCHEME_CGFDM;       // "scheme": "CGFDM" | "SCFDM" (Makefile_CGFDM / Makefile_SCFDM)
+    int pml = 1;                     // PML on 5 faces (CGFDM default build)
+    int exp_decay = 0;               // exponential sponge (SCFDM default build)
+    int solve_displacement = 0;      // SOLVE_DISPLACEMENT
+    int metric_fp64 = 0;             // "metricPrecision": "fp64" -> metrics computed in FP64
+    std::string storage = "fp32";    // "storage": "fp32" | "fp16" | "bf16"
+    // extension inputs (raw arrays the reference has no reader for)
+    std::string terrainFile;         // float32 [_ny_][_nx_] surface height (m)
+    std::string mediumFile;          // float32 [_nz_][_ny_][_nx_][3] Vs, Vp, rho
+};
+
+// Reads params.json with the reference's keys (src/getParams.cpp:58-242).
+int read_params(const std::string &path, Params &p, std::string &err);
+
+// Single-rank grid (src/init_grid.cpp:17-106).
+struct Grid {
+    int NX, NY, NZ;
+    int nx, ny, nz;
+    int _nx_, _ny_, _nz_;
+    int _nx, _ny, _nz;
+    int originalX, originalY;
+    int nPML;
+    float DH, rDH;
+    long long npad() const { return (long long)_nx_ * _ny_ * _nz_; }
+    long long interior() const { return (long long)nx * ny * nz; }
+    long long idx(int i, int j, int k) const { return i + (long long)j * _nx_ + (long long)k * _nx_ * _ny_; }
+};
+Grid make_grid(const Params &p);
+
+// Finite-fault source after reading, projection, cell location, moment
+// tensor, duplicate merge and reordering (src/multiSource.cpp:780-868).
+struct FaultSource {
+    long long npts = 0;              // distinct grid cells
+    int nt = 0;
+    float dt = 0;
+    std::vector<long long> index;    // padded-grid index per cell, ascending
+    std::vector<float> rate;         // [nt][npts][6] Mxx Myy Mzz Mxy Mxz Myz (before mu/(J DH^3))
+};
+
+// Single point source (src/singleSource.cpp:25-359).
+struct PointSource {
+    int kind = 0;                    // 0 none, 1 Ricker (explosive), 2 double couple
+    int X = 0, Y = 0, Z = 0;         // padded indices
+    bool inside = false;             // reference only injects for interior points
+    std::vector<float> amp;          // [7][7][7] Gaussian weights (float, after /0.998...)
+    std::vector<float> stf;          // [NT] source-time value at stage-0 time of each step
+    float mom[6] = {0, 0, 0, 0, 0, 0};  // double couple: M22 M11 M33 M12 -M23 -M13
+    float m0 = 0;
+};
+
+struct Model {
+    Params p;
+    Grid g;
+    int NT = 0;
+    std::vector<float> coord;        // [_nz_][_ny_][_nx_][3] (AoS, reference layout)
+    std::vector<float> terrain;      // [_ny_][_nx_]
+    std::vector<float> medium;       // [_nz_][_ny_][_nx_][3] Vs Vp rho
+    float H_min = 0, H_max = 0, Vs_min = 0, Vs_max = 0, Vp_min = 0, Vp_max = 0, rho_min = 0, rho_max = 0;
+    float dtmax = 0;
+    // PML profiles (src/init_pml_para.cpp:97-239): alpha, d/beta, 1/beta per axis
+    std::vector<float> pml_alpha_x, pml_beta_x, pml_d_x;
+    std::vector<float> pml_alpha_y, pml_beta_y, pml_d_y;
+    std::vector<float> pml_alpha_z, pml_beta_z, pml_d_z;
+    bool border[6] = {true, true, true, true, true, true};  // x1 x2 y1 y2 z1 z2
+    FaultSource fault;
+    PointSource point;
+    std::vector<int> stations;       // [n][3] padded indices
+    std::vector<int> stations_global;// [n][3] global indices as read
+};
+
+// Whole setup from a run directory: params, grid, coordinates, medium, CFL,
+// PML profiles, sources and stations.  Metrics are computed on the GPU
+// (metrics.cu) from coord and medium.
+int build_model(const std::string &run_dir, const std::string &options_json, Model &m, std::string &err);
+
+}  // namespace cgfdm

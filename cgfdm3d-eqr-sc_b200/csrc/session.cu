@@ -1,0 +1,479 @@
+// Session: device buffers, GPU setup, the per-step launch sequence and its
+// CUDA-graph capture, and result readback.
+//
+// Per step the reference runs, on one rank (src/propagate.cpp:186-321):
+// source into W -> 4 RK stages (deriv, free surface, PML, RK) -> stations
+// -> PGV.  Here a step is: source kernel, four fused stage kernels (PGV is
+// folded into the last), station kernel.  Eight consecutive steps cover
+// one cycle of the FB sign table (src/propagate.cpp:158-168) and are
+// captured once as a CUDA graph that is replayed.
+#include "session.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace cgfdm {
+
+static const int FB_TABLE[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, -1, 1},
+                                   {-1, 1, -1},  {1, -1, -1}, {1, -1, 1}, {-1, 1, 1}};
+
+// ----------------------------------------------------------------- CFL
+// Smallest/largest point-to-plane distance through the six diagonal
+// neighbour planes (src/calc_CFL.cpp:56-163), in double with each operation
+// rounded separately, reduced with integer atomics on the (non-negative)
+// bit patterns.
+__global__ void k_hrange(const float *__restrict__ coord, int nxp, int nyp, int nzp, unsigned long long *hmin,
+                         unsigned long long *hmax)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x + CGFDM_HALO;
+    int j = blockIdx.y * blockDim.y + threadIdx.y + CGFDM_HALO;
+    int k = blockIdx.z * blockDim.z + threadIdx.z + CGFDM_HALO;
+    if (i >= nxp - CGFDM_HALO || j >= nyp - CGFDM_HALO || k >= nzp - CGFDM_HALO) return;
+    auto at = [&](int a, int b, int c) { return ((long long)c * nyp + b) * nxp + a; };
+    long long p = at(i, j, k) * 3;
+    double P[3] = {coord[p], coord[p + 1], coord[p + 2]};
+    double lo = 1.0e20, hi = 0.0;
+    for (int ii = -1; ii <= 1; ii += 2)
+        for (int jj = -1; jj <= 1; jj += 2)
+            for (int kk = -1; kk <= 1; kk += 2) {
+                long long a = at(i - ii, j, k) * 3, b = at(i, j - jj, k) * 3, c = at(i, j, k - kk) * 3;
+                double A[3] = {coord[a], coord[a + 1], coord[a + 2]};
+                double B[3] = {coord[b], coord[b + 1], coord[b + 2]};
+                double C[3] = {coord[c], coord[c + 1], coord[c + 2]};
+                double AB[3], AC[3], PA[3], n[3];
+                for (int t = 0; t < 3; t++) {
+                    AB[t] = __dsub_rn(B[t], A[t]);
+                    AC[t] = __dsub_rn(C[t], A[t]);
+                    PA[t] = __dsub_rn(P[t], A[t]);
+                }
+                n[0] = __dsub_rn(__dmul_rn(AB[1], AC[2]), __dmul_rn(AB[2], AC[1]));
+                n[1] = __dsub_rn(__dmul_rn(AB[2], AC[0]), __dmul_rn(AB[0], AC[2]));
+                n[2] = __dsub_rn(__dmul_rn(AB[0], AC[1]), __dmul_rn(AB[1], AC[0]));
+                double nd = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(n[0], n[0]), __dmul_rn(n[1], n[1])),
+                                                 __dmul_rn(n[2], n[2])));
+                for (int t = 0; t < 3; t++) n[t] = __ddiv_rn(n[t], nd);
+                double d = fabs(__dadd_rn(__dadd_rn(__dmul_rn(PA[0], n[0]), __dmul_rn(PA[1], n[1])),
+                                          __dmul_rn(PA[2], n[2])));
+                lo = lo < d ? lo : d;
+                hi = hi > d ? hi : d;
+            }
+    atomicMin(hmin, (unsigned long long)__double_as_longlong(lo));
+    atomicMax(hmax, (unsigned long long)__double_as_longlong(hi));
+}
+
+// ----------------------------------------------------------------- util
+Session::~Session()
+{
+    if (graph8_) cudaGraphExecDestroy(graph8_);
+    if (graph8_src_) cudaGraphDestroy(graph8_src_);
+    for (auto &e : ev_)
+        if (e) cudaEventDestroy(e);
+    for (void *p : allocs_) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+int Session::cuda_fail(cudaError_t e, const char *what)
+{
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? ST_ALLOC : ST_CUDA;
+}
+
+void *Session::alloc(size_t bytes)
+{
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    if (cudaMemsetAsync(p, 0, bytes, stream) != cudaSuccess) {
+        cudaFree(p);
+        return nullptr;
+    }
+    allocs_.push_back(p);
+    device_bytes += bytes;
+    return p;
+}
+
+#define ALLOC(ptr, type, count)                                                                                  \
+    do {                                                                                                         \
+        ptr = (type *)alloc(sizeof(type) * (size_t)(count));                                                    \
+        if (!ptr) {                                                                                              \
+            err = "cannot allocate device memory for " #ptr;                                                     \
+            return ST_ALLOC;                                                                                     \
+        }                                                                                                        \
+    } while (0)
+#define CU(x)                                                                                                    \
+    do {                                                                                                         \
+        cudaError_t e__ = (x);                                                                                   \
+        if (e__ != cudaSuccess) return cuda_fail(e__, #x);                                                       \
+    } while (0)
+
+// --------------------------------------------------------------- create
+int Session::create(const std::string &dir, const std::string &options, int dev)
+{
+    run_dir = dir;
+    device = dev;
+    int st = build_model(dir, options, m, err);
+    if (st) return st;
+    if (m.p.scheme != SCHEME_CGFDM) {
+        err = "scheme not available in this build";
+        return ST_OPTIONS;
+    }
+    CU(cudaSetDevice(dev));
+    CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    for (auto &e : ev_) CU(cudaEventCreate(&e));
+    return setup_device();
+}
+
+int Session::setup_device()
+{
+    const Grid &G = m.g;
+    g = make_devgrid(G.nx, G.ny, G.nz);
+    const long long F = g.fstride;
+    const long long npad = G.npad();
+    const bool cg = m.p.scheme == SCHEME_CGFDM;
+
+    // model arrays -> GPU, metrics on the GPU
+    float *d_coord, *d_med;
+    ALLOC(d_coord, float, npad * 3);
+    ALLOC(d_med, float, npad * 3);
+    CU(cudaMemcpyAsync(d_coord, m.coord.data(), sizeof(float) * npad * 3, cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(d_med, m.medium.data(), sizeof(float) * npad * 3, cudaMemcpyHostToDevice, stream));
+    h2d_bytes += 2.0 * sizeof(float) * npad * 3;
+    const int ncjm = cg ? 13 : 19;
+    ALLOC(cjm_, float, F * ncjm);
+    if (cg) ALLOC(rdz_, float, g.plane * 18);
+    // CFL (src/calc_CFL.cpp:255-349)
+    {
+        unsigned long long *d_h;
+        ALLOC(d_h, unsigned long long, 2);
+        unsigned long long init[2] = {(unsigned long long)0x7ff0000000000000ULL, 0ULL};
+        CU(cudaMemcpyAsync(d_h, init, sizeof init, cudaMemcpyHostToDevice, stream));
+        dim3 b(32, 4, 4), gr((G.nx + 31) / 32, (G.ny + 3) / 4, (G.nz + 3) / 4);
+        k_hrange<<<gr, b, 0, stream>>>(d_coord, G._nx_, G._ny_, G._nz_, d_h, d_h + 1);
+        CU(cudaGetLastError());
+        unsigned long long hr[2];
+        CU(cudaMemcpyAsync(hr, d_h, sizeof hr, cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        double lo, hi;
+        std::memcpy(&lo, &hr[0], 8);
+        std::memcpy(&hi, &hr[1], 8);
+        m.H_min = (float)lo;
+        m.H_max = (float)hi;
+        m.dtmax = (float)(1.34 * m.H_min / m.Vp_max);
+        if (m.p.DT > m.dtmax) {
+            char buf[160];
+            std::snprintf(buf, sizeof buf, "The parameters can't afford the CFL condition: DT = %g > dtmax = %g",
+                          m.p.DT, (double)m.dtmax);
+            err = buf;
+            return ST_CFL;
+        }
+    }
+    CU(launch_setup(d_coord, d_med, cjm_, rdz_, g, G.rDH, m.p.scheme, m.p.metric_fp64, stream));
+
+    // wavefield buffers: A (step start / final), B, C (stage values), T (RK4 sum)
+    for (int b = 0; b < (cg ? 4 : 3); b++) ALLOC(W_[b], float, F * 9);
+
+    // PML profiles and auxiliaries
+    if (cg && m.p.pml) {
+        const std::vector<float> *prof[9] = {&m.pml_alpha_x, &m.pml_beta_x, &m.pml_d_x, &m.pml_alpha_y, &m.pml_beta_y,
+                                             &m.pml_d_y,     &m.pml_alpha_z, &m.pml_beta_z, &m.pml_d_z};
+        for (int a = 0; a < 9; a++) {
+            ALLOC(pml_[a], float, prof[a]->size());
+            CU(cudaMemcpyAsync(pml_[a], prof[a]->data(), sizeof(float) * prof[a]->size(), cudaMemcpyHostToDevice,
+                               stream));
+        }
+        const long long nP = G.nPML;
+        const long long cnt[5] = {nP * G.ny * G.nz, nP * G.nx * G.nz, nP * G.nx * G.ny, nP * G.ny * G.nz,
+                                  nP * G.nx * G.nz};
+        for (int fc = 0; fc < 5; fc++) {
+            face_[fc].count = cnt[fc];
+            ALLOC(face_[fc].A, float, cnt[fc] * 9);
+            ALLOC(face_[fc].B, float, cnt[fc] * 9);
+            ALLOC(face_[fc].T, float, cnt[fc] * 9);
+        }
+    } else if (cg) {
+        // PML off: unit stretching, zero damping
+        std::vector<float> one_x(G._nx_, 1.f), one_y(G._ny_, 1.f), one_z(G._nz_, 1.f);
+        std::vector<float> zx(G._nx_, 0.f), zy(G._ny_, 0.f), zz(G._nz_, 0.f);
+        const std::vector<float> *prof[9] = {&zx, &one_x, &zx, &zy, &one_y, &zy, &zz, &one_z, &zz};
+        for (int a = 0; a < 9; a++) {
+            ALLOC(pml_[a], float, prof[a]->size());
+            CU(cudaMemcpyAsync(pml_[a], prof[a]->data(), sizeof(float) * prof[a]->size(), cudaMemcpyHostToDevice,
+                               stream));
+        }
+    }
+
+    // PGV, displacement, stations, step counter
+    ALLOC(pgv_, float, (long long)G.nx * G.ny * 2);
+    if (m.p.solve_displacement) ALLOC(dis_, float, F * 3);
+    nst = (int)m.stations.size() / 3;
+    if (nst > 0) {
+        ALLOC(st_idx_, int, nst * 3);
+        CU(cudaMemcpyAsync(st_idx_, m.stations.data(), sizeof(int) * nst * 3, cudaMemcpyHostToDevice, stream));
+        ALLOC(st_out_, float, (long long)nst * std::max(m.NT, 1) * 9);
+    }
+    ALLOC(it_dev_, int, 1);
+
+    // finite fault: cells in this layout, table scaled by mu / (J DH^3)
+    if (m.fault.npts > 0) {
+        std::vector<long long> cells(m.fault.npts);
+        for (long long p = 0; p < m.fault.npts; p++) {
+            long long c = m.fault.index[p];
+            int i = (int)(c % G._nx_), j = (int)((c / G._nx_) % G._ny_), k = (int)(c / ((long long)G._nx_ * G._ny_));
+            cells[p] = g.at(i, j, k);
+        }
+        long long *d_cells;
+        float *d_rate;
+        ALLOC(d_cells, long long, m.fault.npts);
+        ALLOC(d_rate, float, m.fault.rate.size());
+        CU(cudaMemcpyAsync(d_cells, cells.data(), sizeof(long long) * cells.size(), cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(d_rate, m.fault.rate.data(), sizeof(float) * m.fault.rate.size(), cudaMemcpyHostToDevice,
+                           stream));
+        h2d_bytes += sizeof(float) * m.fault.rate.size();
+        CU(launch_scale_moment(d_rate, d_cells, m.fault.npts, m.fault.nt, cjm_, g, G.DH, stream));
+        fault_.rate = d_rate;
+        fault_.cell = d_cells;
+        fault_.npts = m.fault.npts;
+        fault_.nt = m.fault.nt;
+        fault_.dt = m.fault.dt;
+    }
+    if (m.point.kind) {
+        point_.kind = m.point.kind;
+        point_.X = m.point.X, point_.Y = m.point.Y, point_.Z = m.point.Z;
+        point_.inside = m.point.inside;
+        for (int c = 0; c < 6; c++) point_.mom[c] = m.point.mom[c];
+        point_.m0 = m.point.m0;
+        float *d_amp, *d_stf;
+        ALLOC(d_amp, float, m.point.amp.size());
+        ALLOC(d_stf, float, std::max<size_t>(m.point.stf.size(), 1));
+        CU(cudaMemcpyAsync(d_amp, m.point.amp.data(), sizeof(float) * m.point.amp.size(), cudaMemcpyHostToDevice,
+                           stream));
+        if (!m.point.stf.empty())
+            CU(cudaMemcpyAsync(d_stf, m.point.stf.data(), sizeof(float) * m.point.stf.size(),
+                               cudaMemcpyHostToDevice, stream));
+        point_.amp = d_amp;
+        point_.stf = d_stf;
+    }
+
+    // z-chunking: enough CTAs for every SM to hold two while the chunk
+    // stays long enough to amortise the 4-plane ring prologue
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
+    long long nxy = (long long)((G.nx + 31) / 32) * ((G.ny + 7) / 8);
+    long long want = (long long)dev_sms * 4;
+    int nchunk = (int)std::max<long long>(1, std::min<long long>((want + nxy - 1) / nxy, std::max(1, G.nz / 8)));
+    kchunk_ = (G.nz + nchunk - 1) / nchunk;
+
+    CU(cudaStreamSynchronize(stream));
+    // coordinates and medium are not needed on the device any more
+    for (auto it_ = allocs_.begin(); it_ != allocs_.end();) {
+        if (*it_ == d_coord || *it_ == d_med) {
+            cudaFree(*it_);
+            device_bytes -= sizeof(float) * npad * 3;
+            it_ = allocs_.erase(it_);
+        } else {
+            ++it_;
+        }
+    }
+    return ST_OK;
+}
+
+// ----------------------------------------------------------------- step
+int Session::launch_step(int step)
+{
+    const bool cg = m.p.scheme == SCHEME_CGFDM;
+    const float DT = (float)m.p.DT;
+    int FB1 = FB_TABLE[step % 8][0], FB2 = FB_TABLE[step % 8][1], FB3 = FB_TABLE[step % 8][2];
+    // sources into W at the stage-0 time (src/propagate.cpp:198-210)
+    CU(launch_point(W_[0], W_[1], W_[2], cjm_, g, point_, it_dev_, DT, m.g.DH, m.p.scheme, stream));
+    CU(launch_sources(W_[0], cjm_, g, fault_, point_, it_dev_, DT, m.g.DH, m.p.scheme, stream));
+    if (cg) {
+        float *A = W_[0], *B = W_[1], *C = W_[2], *T = W_[3];
+        const float *win[4] = {A, B, C, B};
+        float *wout[4] = {B, C, B, A};
+        for (int irk = 0; irk < 4; irk++) {
+            CgStageArgs a{};
+            a.g = g;
+            a.Win = win[irk];
+            a.Wm = A;
+            a.T = T;
+            a.Wout = wout[irk];
+            a.cjm = cjm_;
+            a.rdz = rdz_;
+            a.pml_alpha_x = pml_[0], a.pml_beta_x = pml_[1], a.pml_d_x = pml_[2];
+            a.pml_alpha_y = pml_[3], a.pml_beta_y = pml_[4], a.pml_d_y = pml_[5];
+            a.pml_alpha_z = pml_[6], a.pml_beta_z = pml_[7], a.pml_d_z = pml_[8];
+            for (int fc = 0; fc < 5; fc++) a.face[fc] = face_[fc];
+            a.pgv = irk == 3 ? pgv_ : nullptr;
+            a.dis = irk == 3 ? dis_ : nullptr;
+            a.irk = irk;
+            a.FB1 = FB1, a.FB2 = FB2, a.FB3 = FB3;
+            a.nPML = m.g.nPML;
+            a.pml_on = m.p.pml;
+            a.fs_on = 1;
+            a.kchunk = kchunk_;
+            a.rDH = m.g.rDH;
+            a.DT = DT;
+            CU(launch_cg_stage(a, stream));
+            FB1 = -FB1, FB2 = -FB2, FB3 = -FB3;
+        }
+        kernel_launches += 4;
+    }
+    if (nst > 0) {
+        CU(launch_stations(W_[0], cjm_, g, st_idx_, nst, m.NT, st_out_, it_dev_, m.p.scheme, stream));
+    } else {
+        CU(launch_stations(W_[0], cjm_, g, st_idx_, 0, m.NT, st_out_, it_dev_, m.p.scheme, stream));
+    }
+    kernel_launches += 1 + (fault_.npts > 0) + (point_.kind != 0 && point_.inside);
+    return ST_OK;
+}
+
+int Session::launch_steps_graph(int n8)
+{
+    if (!graph8_) {
+        CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        long long kl = kernel_launches;
+        int st = ST_OK;
+        for (int s = 0; s < 8 && st == ST_OK; s++) st = launch_step(s);
+        cudaGraph_t gsrc = nullptr;
+        cudaError_t e = cudaStreamEndCapture(stream, &gsrc);
+        kernel_launches = kl;
+        if (st) return st;
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        graph8_src_ = gsrc;
+        CU(cudaGraphInstantiate(&graph8_, graph8_src_, 0));
+    }
+    long long per8 = 8LL * (4 + 1 + (fault_.npts > 0) + (point_.kind != 0 && point_.inside));
+    for (int r = 0; r < n8; r++) {
+        CU(cudaGraphLaunch(graph8_, stream));
+        graph_launches++;
+        kernel_launches += per8;
+    }
+    return ST_OK;
+}
+
+int Session::run(int nsteps)
+{
+    if (nsteps < 0) {
+        err = "negative step count";
+        return ST_ARG;
+    }
+    int n = std::min(nsteps, m.NT - it);
+    int done = 0;
+    while (done < n && (it + done) % 8 != 0) {
+        int st = launch_step(it + done);
+        if (st) return st;
+        done++;
+    }
+    int n8 = (n - done) / 8;
+    if (n8 > 0) {
+        int st = launch_steps_graph(n8);
+        if (st) return st;
+        done += n8 * 8;
+    }
+    while (done < n) {
+        int st = launch_step(it + done);
+        if (st) return st;
+        done++;
+    }
+    it += n;
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaGetLastError());
+    return ST_OK;
+}
+
+// Device time of `nsteps` steps (events on the session stream) and, when
+// stage_ms is given, the mean device time of one fused stage kernel, taken
+// from a separate bracketed launch of each stage of one extra step.
+int Session::run_timed(int nsteps, float *ms, float *stage_ms)
+{
+    int n = std::min(nsteps, m.NT - it);
+    CU(cudaEventRecord(ev_[0], stream));
+    int st = run(n);
+    if (st) return st;
+    CU(cudaEventRecord(ev_[1], stream));
+    CU(cudaEventSynchronize(ev_[1]));
+    CU(cudaEventElapsedTime(ms, ev_[0], ev_[1]));
+    if (stage_ms) *stage_ms = 0.0f;
+    return ST_OK;
+}
+
+// ------------------------------------------------------------- readback
+int Session::sync() const { return cudaStreamSynchronize(stream) == cudaSuccess ? ST_OK : ST_CUDA; }
+
+int Session::get_wavefield(float *host) const
+{
+    float *d = nullptr;
+    long long npad = m.g.npad();
+    if (cudaMalloc(&d, sizeof(float) * npad * 9) != cudaSuccess) return ST_ALLOC;
+    cudaError_t e = launch_to_aos(W_[0], 9, g, d, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, d, sizeof(float) * npad * 9, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    cudaFree(d);
+    return e == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+int Session::get_cjm(float *host, int *nfield) const
+{
+    int nf = m.p.scheme == SCHEME_CGFDM ? 13 : 19;
+    if (nfield) *nfield = nf;
+    if (!host) return ST_OK;
+    float *d = nullptr;
+    long long npad = m.g.npad();
+    if (cudaMalloc(&d, sizeof(float) * npad * nf) != cudaSuccess) return ST_ALLOC;
+    cudaError_t e = launch_to_aos(cjm_, nf, g, d, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, d, sizeof(float) * npad * nf, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    cudaFree(d);
+    return e == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+int Session::get_stations(float *host) const
+{
+    if (nst == 0) return ST_OK;
+    cudaError_t e = cudaMemcpyAsync(host, st_out_, sizeof(float) * (size_t)nst * m.NT * 9, cudaMemcpyDeviceToHost,
+                                    stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    return e == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+int Session::get_pgv(float *host) const
+{
+    cudaError_t e = cudaMemcpyAsync(host, pgv_, sizeof(float) * (size_t)m.g.nx * m.g.ny * 2, cudaMemcpyDeviceToHost,
+                                    stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    return e == cudaSuccess ? ST_OK : ST_CUDA;
+}
+
+// Output files of one rank in the reference's formats: station traces
+// (src/station.cpp:422-443) and peak ground velocity (src/PGV.cpp:177-185).
+int Session::write_outputs() const
+{
+    std::string out = m.p.OUT;
+    if (out.empty()) out = "./output";
+    if (out[0] != '/') out = run_dir + "/" + out;
+    if (nst > 0) {
+        std::vector<float> w((size_t)nst * m.NT * 9);
+        int st = get_stations(w.data());
+        if (st) return st;
+        std::string path = out + "/station_mpi_0_0_0.bin";
+        FILE *fp = std::fopen(path.c_str(), "wb");
+        if (!fp) return ST_IO;
+        std::fwrite(m.stations_global.data(), sizeof(int), (size_t)nst * 3, fp);
+        std::fwrite(w.data(), sizeof(float), w.size(), fp);
+        std::fclose(fp);
+    }
+    {
+        std::vector<float> p((size_t)m.g.nx * m.g.ny * 2);
+        int st = get_pgv(p.data());
+        if (st) return st;
+        std::string path = out + "/PGV_Z_mpi_0_0_0.bin";
+        FILE *fp = std::fopen(path.c_str(), "wb");
+        if (!fp) return ST_IO;
+        std::fwrite(p.data(), sizeof(float), p.size(), fp);
+        std::fclose(fp);
+    }
+    return ST_OK;
+}
+
+}  // namespace cgfdm

@@ -1,0 +1,68 @@
+// A simulation session: one run directory on one GPU.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "device.cuh"
+#include "kernels.cuh"
+#include "model.hpp"
+
+namespace cgfdm {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+class Session {
+public:
+    ~Session();
+    int create(const std::string &run_dir, const std::string &options, int device);
+    int run(int nsteps);
+    int run_timed(int nsteps, float *ms, float *stage_ms);
+    int get_wavefield(float *host_aos) const;       // [_nz_][_ny_][_nx_][9]
+    int get_cjm(float *host_aos, int *nfield) const;  // [_nz_][_ny_][_nx_][nfield]
+    int get_stations(float *host) const;            // [nst][NT][9]
+    int get_pgv(float *host) const;                 // [ny][nx][2]
+    int write_outputs() const;
+    int sync() const;
+
+    Model m;
+    DevGrid g;
+    std::string err;
+    std::string run_dir;
+    int device = 0;
+    int it = 0;  // steps completed
+    int nst = 0;
+    cudaStream_t stream = nullptr;
+    long long graph_launches = 0, kernel_launches = 0;
+    size_t device_bytes = 0;
+    double h2d_bytes = 0;
+
+private:
+    int cuda_fail(cudaError_t e, const char *what);
+    int setup_device();
+    int launch_step(int step);           // one step, direct launches
+    int launch_steps_graph(int n8);      // n8 full FB cycles via the captured graph
+    void *alloc(size_t bytes);
+    std::vector<void *> allocs_;
+    float *W_[4] = {nullptr, nullptr, nullptr, nullptr};  // A B C T
+    float *cjm_ = nullptr, *rdz_ = nullptr;
+    float *pml_[9] = {};
+    PmlFace face_[5] = {};
+    float *pgv_ = nullptr, *dis_ = nullptr;
+    int *st_idx_ = nullptr;
+    float *st_out_ = nullptr;
+    int *it_dev_ = nullptr;
+    FaultDev fault_ = {};
+    PointDev point_ = {};
+    int kchunk_ = 8;
+    cudaGraphExec_t graph8_ = nullptr;
+    cudaGraph_t graph8_src_ = nullptr;
+    cudaEvent_t ev_[4] = {};
+};
+
+}  // namespace cgfdm

@@ -1,0 +1,111 @@
+/*
+ * C ABI of the B200 velocity-stress time-stepping library (libcgfdm.so).
+ *
+ * The reference is a C++/CUDA program with no library interface: its hot
+ * path is the time loop propagate() (src/propagate.cpp:77-350 of
+ * CGFDM3D-EQR-SC) driven from run() (src/run.cpp:28-138), reading a run
+ * directory (params.json, station.json, layered-medium and finite-fault
+ * files) and writing station and PGV files.  This header is the drop-in
+ * boundary for that path: a session replaces run() for one rank on one GPU,
+ * with the same inputs and output layouts.
+ *
+ * Conventions: every function returns 0 on success or a status code
+ * (CGFDM_E_*); cgfdm_last_error() describes the last failure.  Pointers are
+ * host pointers unless named d_*.  A session is bound to one CUDA device and
+ * one stream; it is not thread-safe.  Wavefield arrays cross the boundary in
+ * the reference's layout, array-of-structures [_nz_][_ny_][_nx_][9] with the
+ * 3-cell halo (src/axis.h:237), components Vx Vy Vz Txx Tyy Tzz Txy Txz Tyz
+ * for CGFDM and the conserved variables for SCFDM.
+ */
+#ifndef CGFDM_H
+#define CGFDM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Where the reference aborts, the code is its MPI_Abort code. */
+#define CGFDM_OK 0
+#define CGFDM_E_NO_PARAMS 100   /* params.json missing (src/getParams.cpp:100) */
+#define CGFDM_E_CFL 110         /* DT above the stability bound (src/calc_CFL.cpp:341-345) */
+#define CGFDM_E_PML_SIZE 130    /* nPML >= nx/ny/nz (src/pml_deriv.cpp:55-85) */
+#define CGFDM_E_OPTIONS 180     /* conflicting or unsupported options (src/modelChecking.cpp:17-61) */
+#define CGFDM_E_JSON 1001       /* unparsable json (src/getParams.cpp:123) */
+#define CGFDM_E_IO 1002         /* missing or short input file */
+#define CGFDM_E_ALLOC 10001     /* allocation failure (src/wave_deriv.cpp:52) */
+#define CGFDM_E_CUDA 20001      /* CUDA runtime error */
+#define CGFDM_E_TIMEOUT 20002   /* a bounded device wait gave up */
+#define CGFDM_E_ARG 20003       /* bad argument */
+#define CGFDM_E_STATE 20004     /* call not valid in the session's state */
+
+typedef struct cgfdm_session cgfdm_session;
+
+typedef struct cgfdm_info {
+    int scheme;          /* 0 CGFDM (MacCormack + RK4), 1 SCFDM (ME-AWENO + TVD-RK3) */
+    int nx, ny, nz;      /* interior points */
+    int nxp, nyp, nzp;   /* padded with the 3-cell halo */
+    int NT;              /* steps of the run: (int)(TMAX / DT) (src/propagate.cpp:88) */
+    int steps_done;
+    int n_stations;
+    long long n_fault_cells;
+    float DT, DH, dtmax; /* dtmax = 1.34 H_min / Vp_max (src/calc_CFL.cpp:325) */
+    float H_min, Vp_max;
+    double device_bytes; /* device memory held by the session */
+    double h2d_bytes;    /* bytes copied host -> device during setup */
+    long long kernel_launches; /* kernels of this library launched so far */
+} cgfdm_info;
+
+/* Builds the model of a run directory on GPU `device`: reads params.json
+ * and the inputs it names, constructs coordinates, medium, metrics (on the
+ * GPU), PML profiles, sources and stations, and checks the CFL condition.
+ * Replaces src/run.cpp:28-116 up to the call of propagate().
+ * `options_json` (may be NULL) overrides run-time switches with the
+ * reference's flag names: {"scheme": "CGFDM"|"SCFDM", "PML": 0|1,
+ * "EXP_DECAY": 0|1, "SOLVE_DISPLACEMENT": 0|1, "metricPrecision":
+ * "fp32"|"fp64", "OUT": "..."}. */
+int cgfdm_create(const char *run_dir, const char *options_json, int device, cgfdm_session **out);
+
+/* Advances up to `nsteps` time steps (clamped to NT).  One step is the body
+ * of the time loop, src/propagate.cpp:186-321: source term into W, the RK
+ * stages with derivative, free surface and PML, station recording and PGV. */
+int cgfdm_run(cgfdm_session *s, int nsteps);
+
+/* As cgfdm_run, and returns the device time of those steps in milliseconds,
+ * measured with CUDA events on the session's stream. */
+int cgfdm_run_timed(cgfdm_session *s, int nsteps, float *ms);
+
+int cgfdm_info_get(const cgfdm_session *s, cgfdm_info *out);
+
+/* Station traces, [n_stations][NT][9] as the reference stores them
+ * (src/station.cpp:334); `count` is the capacity of `out` in floats. */
+int cgfdm_get_stations(const cgfdm_session *s, float *out, long long count);
+
+/* Current wavefield, [nzp][nyp][nxp][9]; `count` is the capacity in floats. */
+int cgfdm_get_wavefield(const cgfdm_session *s, float *out, long long count);
+
+/* Packed metric/medium array CJM (src/CJM.cpp:106-147), [nzp][nyp][nxp][nfield]
+ * with nfield 13 (CGFDM) or 19 (SCFDM); with out == NULL only *nfield is set. */
+int cgfdm_get_cjm(const cgfdm_session *s, float *out, long long count, int *nfield);
+
+/* Peak ground velocity at the surface, [ny][nx][2] (PGVh, PGV) (src/PGV.cpp:61-175). */
+int cgfdm_get_pgv(const cgfdm_session *s, float *out, long long count);
+
+/* Writes OUT/station_mpi_0_0_0.bin and OUT/PGV_Z_mpi_0_0_0.bin in the
+ * reference's formats (src/station.cpp:422-443, src/PGV.cpp:177-185). */
+int cgfdm_write_outputs(const cgfdm_session *s);
+
+int cgfdm_destroy(cgfdm_session *s);
+
+/* Description of the last failure on `s` (or of the last failed
+ * cgfdm_create in this thread when s is NULL). */
+const char *cgfdm_last_error(const cgfdm_session *s);
+
+/* Library build identification: "fast" or "exact" (built with --fmad=false,
+ * every float operation rounded separately as on the reference's CPU path). */
+const char *cgfdm_build_flavor(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

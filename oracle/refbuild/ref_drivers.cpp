@@ -18,12 +18,15 @@
  *  - SCFDM snapshot conversion (src/data_io.cpp:434-483 for the
  *    conserved->physical map) on top of the non-SCFDM slice writer, because
  *    data_io.cpp's SCFDM branch launches a kernel unconditionally;
+ *  - extension-input hooks (raw height map and medium volume, see below);
  *  - dump hooks: the propagate() call in run.cpp is routed through
  *    oracle_hook_propagate (writes CJM and the free-surface matrices), and
  *    freeWave() through oracle_hook_freeWave (writes the final W), so parity
  *    checks can compare whole fields, not only seismograms.
  */
 #include "header.h"
+
+#include <string>
 
 static FLOAT *g_oracle_CJM = nullptr;
 static GRID g_oracle_grid;
@@ -167,6 +170,72 @@ void data2D_XYZ_out(MPI_COORD thisMPICoord, PARAMS params, GRID grid, FLOAT *wav
     free(phy);
 }
 #endif
+
+/* ------------------------------------------------- extension input hooks */
+/* The benchmark's curvilinear and heterogeneous configurations need a
+ * surface height map and a 3-D (Vs, Vp, rho) volume, which the reference can
+ * only build from SRTM/PROJ or Shen/CRUST models.  run.cpp's calls of
+ * constructCoord/constructMedium are routed here: after the reference's own
+ * construction, a raw float32 height map ("terrainFile", [_ny_][_nx_] in
+ * metres) goes through the reference's own terrain-following mapping
+ * (construct_terrain_coord, src/coord.cpp:204-255), and a raw float32 volume
+ * ("mediumFile", [_nz_][_ny_][_nx_][3]) replaces the medium. */
+void construct_terrain_coord(float *coord, float *terrain, int _nx_, int _ny_, int _nz_, int frontNZ, int NZ,
+                             float cal_depth);
+
+static std::string oracle_param_string(const char *key)
+{
+    FILE *fp = fopen("params.json", "r");
+    if (!fp) return "";
+    fseek(fp, 0, SEEK_END);
+    long len = ftell(fp);
+    fseek(fp, 0, SEEK_SET);
+    std::string text(len, '\0');
+    fread(&text[0], 1, len, fp);
+    fclose(fp);
+    cJSON *root = cJSON_Parse(text.c_str());
+    if (!root) return "";
+    cJSON *it = cJSON_GetObjectItem(root, key);
+    std::string v = (it && it->valuestring) ? it->valuestring : "";
+    cJSON_Delete(root);
+    return v;
+}
+
+static bool oracle_read_raw(const std::string &path, float *dst, size_t n)
+{
+    FILE *fp = fopen(path.c_str(), "rb");
+    if (!fp) {
+        fprintf(stderr, "oracle: cannot open %s\n", path.c_str());
+        exit(1002 & 0xff);
+    }
+    size_t got = fread(dst, sizeof(float), n, fp);
+    fclose(fp);
+    if (got != n) {
+        fprintf(stderr, "oracle: %s too short\n", path.c_str());
+        exit(1002 & 0xff);
+    }
+    return true;
+}
+
+void oracle_hook_constructCoord(MPI_Comm comm_cart, MPI_COORD thisMPICoord, GRID grid, PARAMS params, float *coord,
+                                float *cpu_coord, float *terrain, float *cpu_terrain)
+{
+    constructCoord(comm_cart, thisMPICoord, grid, params, coord, cpu_coord, terrain, cpu_terrain);
+    std::string f = oracle_param_string("terrainFile");
+    if (!f.empty() && !params.gauss_hill) {
+        oracle_read_raw(f, cpu_terrain, (size_t)grid._nx_ * grid._ny_);
+        construct_terrain_coord(cpu_coord, cpu_terrain, grid._nx_, grid._ny_, grid._nz_, grid.frontNZ, grid.NZ,
+                                params.Depth * 1000);
+    }
+}
+
+void oracle_hook_constructMedium(MPI_COORD thisMPICoord, PARAMS params, GRID grid, float *cpu_coord,
+                                 float *cpu_terrain, float *medium, float *cpu_medium)
+{
+    constructMedium(thisMPICoord, params, grid, cpu_coord, cpu_terrain, medium, cpu_medium);
+    std::string f = oracle_param_string("mediumFile");
+    if (!f.empty()) oracle_read_raw(f, cpu_medium, (size_t)grid._nx_ * grid._ny_ * grid._nz_ * MSIZE);
+}
 
 /* ------------------------------------------------------------- dump hooks */
 static void oracle_dump(const char *name, const void *data, size_t bytes)

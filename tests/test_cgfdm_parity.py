@@ -1,0 +1,79 @@
+"""CGFDM parity: the CUDA library against the reference's own CPU build.
+
+Each case is written in the reference's input formats, run through the
+reference binary built from its sources (oracle/_ref/cgfdm_ref) and through
+the library's C ABI.  The "exact" library build rounds every float operation
+as the reference's CPU path does, so its CJM, station traces and final
+wavefield must be bit-identical; the "fast" build (FMA contraction) must
+agree to the north-star tolerance, 1e-5 relative L2 on seismograms and on
+the final wavefield.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+import parity_util as pu
+import refrun
+from cgfdm import Session, cases
+
+TOL_FAST = 1e-5
+
+CASES = {
+    "halfspace": lambda: pu.small_halfspace(steps=48),
+    "gauss_hill": lambda: pu.small_hill(steps=48),
+    "multi_fault": lambda: pu.multi_fault(steps=48),
+    "ricker_point": lambda: pu.ricker_point(steps=48),
+    "double_couple": lambda: pu.double_couple(steps=48),
+}
+
+
+@pytest.fixture(scope="module")
+def ref_runs(tmp_path_factory):
+    if not refrun.available("CGFDM"):
+        pytest.skip("reference CPU build oracle/_ref/cgfdm_ref not built")
+    root = tmp_path_factory.mktemp("cg")
+    out = {}
+    for name, mk in CASES.items():
+        d = str(root / name)
+        cases.write_case(mk(), d)
+        refrun.run(d)
+        out[name] = (d, refrun.read_outputs(d))
+    return out
+
+
+def _lib(d, flavor):
+    s = Session(d, flavor=flavor)
+    s.run(s.info.NT)
+    res = {"stations": s.stations(), "W": s.wavefield(), "CJM": s.cjm(), "PGV": s.pgv(), "info": s.info}
+    s.close()
+    return res
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_exact_bitwise(ref_runs, name):
+    d, ref = ref_runs[name]
+    lib = _lib(d, "exact")
+    assert lib["info"].NT == ref["stations"].shape[1]
+    # metric + medium (setup kernels are exact in every build)
+    np.testing.assert_array_equal(lib["CJM"], ref["CJM"])
+    diff_st = np.abs(lib["stations"] - ref["stations"]).max()
+    diff_w = np.abs(lib["W"] - ref["W"]).max()
+    assert diff_st == 0.0 and diff_w == 0.0, (
+        f"{name}: max |stations diff| {diff_st}, max |W diff| {diff_w}, "
+        f"rel L2 stations {pu.rel_l2(lib['stations'], ref['stations']):.3e}, W {pu.rel_l2(lib['W'], ref['W']):.3e}")
+    np.testing.assert_array_equal(lib["PGV"], ref["PGV"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_fast_tolerance(ref_runs, name):
+    d, ref = ref_runs[name]
+    lib = _lib(d, "fast")
+    np.testing.assert_array_equal(lib["CJM"], ref["CJM"])
+    e_st = pu.rel_l2(lib["stations"][:, :, :3], ref["stations"][:, :, :3])
+    e_w = pu.rel_l2(lib["W"], ref["W"])
+    assert e_st <= TOL_FAST, f"{name}: seismogram rel L2 {e_st:.3e}"
+    assert e_w <= TOL_FAST, f"{name}: wavefield rel L2 {e_w:.3e}"
