@@ -13,17 +13,25 @@
 // velocity (src/PGV.cpp:61-175) and, if enabled, the displacement
 // (src/solve_displacement.cpp:27-63).
 //
-// Tiling: a CTA owns a 32 x 8 column tile and marches up a chunk of z.  The
-// nine wavefield components of each z-plane, with the one-sided x/y halo
-// the stencil needs (1 cell behind, 3 ahead, per the FB signs), are staged
-// once into a six-slot shared-memory ring by cp.async; derivatives along
-// x, y and z all read the ring, so each value crosses HBM once per stage.
-// Everything else (metric, RK inputs, auxiliaries) is a coalesced
-// structure-of-arrays load at the point itself.
+// Tiling: a CTA owns a 32 x 8 column tile and marches up a chunk of z.  Each
+// z-plane of the nine stencil-input components, with the halo the one-sided
+// operators need, arrives as one TMA box (40 x 12 x 1 x 9 floats,
+// cp.async.bulk.tensor.4d) into a six-slot shared-memory ring, completion
+// tracked by one mbarrier per slot; one elected thread issues the copies one
+// plane ahead of use.  Derivatives along x, y and z all read the ring, so
+// each value crosses HBM once per stage.  The FB signs are template
+// parameters, so every stencil tap is a fixed shared-memory offset.  Metric,
+// medium and RK inputs are plain coalesced loads issued before the ring wait.
+//
+// Every wait on an mbarrier is bounded: on timeout the CTA records the fact
+// in a device error word, waits (bounded) for its copies in flight and exits.
 //
 // Arithmetic follows the reference's expression order term by term; built
 // with --fmad=false the stage reproduces the reference's FP32 results bit for
 // bit, built normally it differs only by FMA contraction.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "device.cuh"
 #include "kernels.cuh"
 
@@ -31,42 +39,63 @@ namespace cgfdm {
 
 #define TX 32
 #define TY 8
-#define HXW (TX + 4)
-#define HYW (TY + 4)
-#define PLANE_F (HXW * HYW)
-#define PLANE (9 * PLANE_F)
+#define BXW 40           // box width: columns i0-4 .. i0+35 (start 16-byte aligned)
+#define BYW 12           // box height: one-sided y halo (1 behind, 3 ahead)
+#define PF (BXW * BYW)   // floats per field in a slot
+#define SLOT_F (9 * PF)  // floats per slot
+#define SLOT_BYTES (SLOT_F * 4)
 #define NSLOT 6
 
-size_t cg_stage_smem_bytes() { return (size_t)NSLOT * PLANE * sizeof(float); }
+size_t cg_stage_smem_bytes() { return (size_t)NSLOT * SLOT_BYTES + NSLOT * 8; }
 
-__device__ __forceinline__ void cp_async4(float *sdst, const float *gsrc, bool valid)
+// ------------------------------------------------------------ TMA helpers
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
 {
-    unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-    int n = valid ? 4 : 0;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc), "r"(n) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// Stage plane k of the nine components into one ring slot: rows
-// j0-hyL .. j0-hyL+HYW-1, columns i0-hxL .. i0-hxL+HXW-1.  Cells beyond the
-// padded grid (last tile only) are zero-filled and never used.
-__device__ __forceinline__ void load_plane(float *slot, const float *__restrict__ W, const DevGrid &g, int i0,
-                                           int j0, int hxL, int hyL, int k, int tid)
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes)
 {
-    const long long kb = (long long)k * g.plane + g.xoff;
-    for (int e = tid; e < PLANE; e += TX * TY) {
-        int f = e / PLANE_F;
-        int r = e - f * PLANE_F;
-        int yy = r / HXW;
-        int xx = r - yy * HXW;
-        int x = i0 - hxL + xx, y = j0 - hyL + yy;
-        bool ok = (x < g.nxp) && (y < g.nyp);
-        const float *src = ok ? W + f * g.fstride + kb + (long long)y * g.pitch + x : W;
-        cp_async4(slot + e, src, ok);
-    }
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after ~2^31 clock cycles (about a second).
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > (1LL << 31)) return false;
+    return true;
+}
+__device__ __forceinline__ void tma_load_4d(unsigned dst, const void *tmap, int x, int y, int z, int f, unsigned bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n" ::"r"(dst),
+        "l"((unsigned long long)tmap), "r"(x), "r"(y), "r"(z), "r"(f), "r"(bar)
+        : "memory");
 }
 
+__device__ __forceinline__ void tma_prefetch_4d(const void *tmap, int x, int y, int z, int f)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];\n" ::"l"(
+                     (unsigned long long)tmap),
+                 "r"(x), "r"(y), "r"(z), "r"(f)
+                 : "memory");
+}
+
+// ------------------------------------------------------------- operators
 // Contribution of one grid direction to the RHS, given the metric row
 // (xi, eta or zeta gradient) and the nine scaled derivatives along it
 // (src/wave_deriv.cpp:244-272; the same form in pml_deriv and
@@ -112,34 +141,31 @@ __device__ __forceinline__ float lop(float wm, float w0, float w1, float w2, flo
     return ((float)FB * s) * rDH;
 }
 
-struct Ring {
-    const float *ring;
-    int base;  // (ty + hyL) * HXW + tx + hxL
-    __device__ __forceinline__ float at(int kk, int f, int dx, int dy) const
+// Stencil taps in the ring: zp[m] points at this thread's cell of plane
+// k + FB3*(m-1); pc = zp[1] is the current plane.
+template <int FB1, int FB2, int FB3>
+struct Taps {
+    const float *zp[5];
+    __device__ __forceinline__ float rx(int f, float rDH) const
     {
-        return ring[(kk % NSLOT) * PLANE + f * PLANE_F + base + dy * HXW + dx];
+        const float *c = zp[1] + f * PF;
+        return lop(c[-FB1], c[0], c[FB1], c[2 * FB1], c[3 * FB1], FB1, rDH);
     }
+    __device__ __forceinline__ float ry(int f, float rDH) const
+    {
+        const float *c = zp[1] + f * PF;
+        return lop(c[-FB2 * BXW], c[0], c[FB2 * BXW], c[2 * FB2 * BXW], c[3 * FB2 * BXW], FB2, rDH);
+    }
+    __device__ __forceinline__ float rz(int f, float rDH) const
+    {
+        return lop(zp[0][f * PF], zp[1][f * PF], zp[2][f * PF], zp[3][f * PF], zp[4][f * PF], FB3, rDH);
+    }
+    __device__ __forceinline__ float rdir(int dir, int f, float rDH) const
+    {
+        return dir == 0 ? rx(f, rDH) : dir == 1 ? ry(f, rDH) : rz(f, rDH);
+    }
+    __device__ __forceinline__ float c(int f) const { return zp[1][f * PF]; }
 };
-
-__device__ __forceinline__ float raw_x(const Ring &R, int k, int f, int FB, float rDH)
-{
-    return lop(R.at(k, f, -FB, 0), R.at(k, f, 0, 0), R.at(k, f, FB, 0), R.at(k, f, 2 * FB, 0),
-               R.at(k, f, 3 * FB, 0), FB, rDH);
-}
-__device__ __forceinline__ float raw_y(const Ring &R, int k, int f, int FB, float rDH)
-{
-    return lop(R.at(k, f, 0, -FB), R.at(k, f, 0, 0), R.at(k, f, 0, FB), R.at(k, f, 0, 2 * FB),
-               R.at(k, f, 0, 3 * FB), FB, rDH);
-}
-__device__ __forceinline__ float raw_z(const Ring &R, int k, int f, int FB, float rDH)
-{
-    return lop(R.at(k - FB, f, 0, 0), R.at(k, f, 0, 0), R.at(k + FB, f, 0, 0), R.at(k + 2 * FB, f, 0, 0),
-               R.at(k + 3 * FB, f, 0, 0), FB, rDH);
-}
-__device__ __forceinline__ float raw_dir(const Ring &R, int dir, int k, int f, int FB, float rDH)
-{
-    return dir == 0 ? raw_x(R, k, f, FB, rDH) : dir == 1 ? raw_y(R, k, f, FB, rDH) : raw_z(R, k, f, FB, rDH);
-}
 
 // J * (metric . traction) at a point, for the traction image
 // (src/freeSurface.cpp:358-395).  mdir: 0 xi, 1 eta, 2 zeta.
@@ -189,66 +215,158 @@ __device__ __forceinline__ void ljt_z(const float *__restrict__ W, const float *
     for (int c = 0; c < 3; c++) out[c] = lop(J[0][c], J[1][c], J[2][c], J[3][c], J[4][c], FB, rDH);
 }
 
-__global__ void __launch_bounds__(TX *TY, 2) k_cg_stage(const CgStageArgs a)
+// ------------------------------------------------------------- the stage
+// Persistent CTAs (two per SM) take work items -- one 32 x 8 column tile
+// over one z-chunk -- from an atomic counter, chunks of a tile adjacent in
+// the order, so concurrently running items share their halo and chunk-edge
+// planes through L2 and no launch ends on a partial wave.
+template <int FB1, int FB2, int FB3>
+__global__ void __launch_bounds__(TX *TY, 2)
+    k_cg_stage(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUtensorMap tmC,
+               const __grid_constant__ CUtensorMap tmM, const __grid_constant__ CUtensorMap tmT, const CgStageArgs a)
 {
-    extern __shared__ float ring[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float *ring = reinterpret_cast<float *>(smem_raw);
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + NSLOT * SLOT_BYTES);
+    __shared__ int s_abort, s_item;
+
     const DevGrid g = a.g;
     const long long F = g.fstride;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int i0 = CGFDM_HALO + blockIdx.x * TX, j0 = CGFDM_HALO + blockIdx.y * TY;
-    const int i = i0 + tx, j = j0 + ty;
     const int _nx = g.nxp - CGFDM_HALO, _ny = g.nyp - CGFDM_HALO, _nz = g.nzp - CGFDM_HALO;
-    const bool active = i < _nx && j < _ny;
-    const int kb = CGFDM_HALO + blockIdx.z * a.kchunk;
-    const int ke = min(kb + a.kchunk, _nz);
-    if (kb >= ke) return;
-    const int FB1 = a.FB1, FB2 = a.FB2, FB3 = a.FB3;
-    const int hxL = FB1 > 0 ? 1 : 3, hyL = FB2 > 0 ? 1 : 3, za = FB3 > 0 ? 1 : 3;
+    constexpr int hyL = FB2 > 0 ? 1 : 3;
+    constexpr int za = FB3 > 0 ? 1 : 3;
     const float rDH = a.rDH, DT = a.DT;
-    const Ring R{ring, (ty + hyL) * HXW + tx + hxL};
+    const int cell = (ty + hyL) * BXW + tx + 4;
+    const int nitems = a.ntiles_x * a.ntiles_y * a.nchunk;
+    const int nPML = a.nPML;
 
-    for (int q = 0; q < 5; q++) {
-        int kk = kb - za + q;
-        load_plane(ring + (kk % NSLOT) * PLANE, a.Win, g, i0, j0, hxL, hyL, kk, tid);
+    if (tid == 0) {
+        s_abort = 0;
+        for (int s = 0; s < NSLOT; s++) mbar_init(smem_u32(&bars[s]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    cp_async_commit();
+    unsigned seq0 = 0;  // fills issued by this CTA before the current item
+
+    for (;;) {
+    __syncthreads();
+    if (tid == 0) s_item = atomicAdd(&a.work[0], 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= nitems || s_abort) break;
+    const int tile = item / a.nchunk, chunk = item - tile * a.nchunk;
+    const int by_ = tile / a.ntiles_x, bx_ = tile - by_ * a.ntiles_x;
+    const int i0 = CGFDM_HALO + bx_ * TX, j0 = CGFDM_HALO + by_ * TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool active = i < _nx && j < _ny;
+    const int kb = CGFDM_HALO + chunk * a.kchunk;
+    const int ke = min(kb + a.kchunk, _nz);
+    if (kb >= ke) continue;
+    const int kf = kb - za;                 // first plane this item loads
+    const int tx0 = g.xoff + i0 - 4;        // halo box origin column: a multiple of 32
+    const int ty0 = j0 - hyL;
+    const int px0 = g.xoff + i0;            // point box origin column: 4 mod 32
+
+    // plane kk of this item is fill number seq0 + (kk - kf) of the CTA
+    auto slot_of = [&](int kk) { return (int)((seq0 + (unsigned)(kk - kf)) % NSLOT); };
+    auto parity_of = [&](int kk) { return ((seq0 + (unsigned)(kk - kf)) / NSLOT) & 1u; };
+    auto issue = [&](int kk) {
+        int s = slot_of(kk);
+        unsigned bar = smem_u32(&bars[s]);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(bar, SLOT_BYTES);
+        tma_load_4d(smem_u32(ring + s * SLOT_F), &tmW, tx0, ty0, kk, 0, bar);
+    };
+    // point operands of plane kk into L2 ahead of their plain loads
+    auto prefetch_points = [&](int kk) {
+        tma_prefetch_4d(&tmC, px0, j0, kk, 0);
+        if (a.irk == 1 || a.irk == 2) tma_prefetch_4d(&tmM, px0, j0, kk, 0);
+        if (a.irk != 0) tma_prefetch_4d(&tmT, px0, j0, kk, 0);
+    };
+
+    const int klast = ke - za + 3;          // last plane of the last window
+    if (tid == 0) {
+        for (int kk = kf; kk <= min(kf + NSLOT - 1, klast); kk++) issue(kk);
+        for (int kk = kb; kk < min(kb + 2, ke); kk++) prefetch_points(kk);
+    }
+    int issued = min(kf + NSLOT - 1, klast);  // same value in every thread
+    // the first window: planes kf .. kf+3 (kf+4 is waited for in the loop)
+    bool ok = true;
+    for (int kk = kf; kk < kf + 4; kk++) ok = ok && mbar_wait_bounded(smem_u32(&bars[slot_of(kk)]), parity_of(kk));
+    if (!ok) {
+        s_abort = 1;
+        atomicOr(a.err, 1);
+    }
 
     const float bx = active ? a.pml_beta_x[i] : 1.0f, by = active ? a.pml_beta_y[j] : 1.0f;
-    const int nPML = a.nPML;
     const bool inx1 = a.pml_on && i < CGFDM_HALO + nPML, inx2 = a.pml_on && i >= _nx - nPML;
     const bool iny1 = a.pml_on && j < CGFDM_HALO + nPML, iny2 = a.pml_on && j >= _ny - nPML;
 
     for (int k = kb; k < ke; k++) {
-        cp_async_wait_all();
-        __syncthreads();
-        if (k + 1 < ke) {
-            int kk = k - za + 5;
-            load_plane(ring + (kk % NSLOT) * PLANE, a.Win, g, i0, j0, hxL, hyL, kk, tid);
-            cp_async_commit();
+        __syncthreads();                    // every thread is done with plane k - za - 1's slot
+        if (s_abort) break;
+        // prefetch plane k - za + 5 into the slot plane k - za - 1 has left
+        const int want = k - za + 5;
+        if (want > issued && want <= klast) {
+            if (tid == 0) issue(want);
+            issued = want;
+        }
+        if (tid == 0) {
+            if (k + 2 < ke) prefetch_points(k + 2);
+            if (want + 2 <= klast) tma_prefetch_4d(&tmW, tx0, ty0, want + 2, 0);
+        }
+        const long long q = g.at(i, j, k);
+        // point-wise operands, loaded before the ring wait
+        float xi_x = 0, xi_y = 0, xi_z = 0, et_x = 0, et_y = 0, et_z = 0, zt_x = 0, zt_y = 0, zt_z = 0;
+        float mu = 0, lam = 0, buo = 0, bz = 1;
+        float mv[9], tv[9];
+        if (active) {
+            xi_x = a.cjm[C_XI_X * F + q], xi_y = a.cjm[C_XI_Y * F + q], xi_z = a.cjm[C_XI_Z * F + q];
+            et_x = a.cjm[C_ET_X * F + q], et_y = a.cjm[C_ET_Y * F + q], et_z = a.cjm[C_ET_Z * F + q];
+            zt_x = a.cjm[C_ZT_X * F + q], zt_y = a.cjm[C_ZT_Y * F + q], zt_z = a.cjm[C_ZT_Z * F + q];
+            mu = a.cjm[C_MU * F + q], lam = a.cjm[C_LAMBDA * F + q];
+            buo = a.cjm[C_BUOY * F + q] * 1.0f;  // buoyancy *= Crho (= 1)
+            bz = a.pml_beta_z[k];
+            if (a.irk == 1 || a.irk == 2)
+                for (int f = 0; f < 9; f++) mv[f] = a.Wm[f * F + q];
+            if (a.irk != 0)
+                for (int f = 0; f < 9; f++) tv[f] = a.T[f * F + q];
+        }
+        const int kk_new = k - za + 4;
+        if (!mbar_wait_bounded(smem_u32(&bars[slot_of(kk_new)]), parity_of(kk_new))) {
+            s_abort = 1;
+            atomicOr(a.err, 1);
+            continue;
         }
         if (!active) continue;
 
-        const long long q = g.at(i, j, k);
-        const float xi_x = a.cjm[C_XI_X * F + q], xi_y = a.cjm[C_XI_Y * F + q], xi_z = a.cjm[C_XI_Z * F + q];
-        const float et_x = a.cjm[C_ET_X * F + q], et_y = a.cjm[C_ET_Y * F + q], et_z = a.cjm[C_ET_Z * F + q];
-        const float zt_x = a.cjm[C_ZT_X * F + q], zt_y = a.cjm[C_ZT_Y * F + q], zt_z = a.cjm[C_ZT_Z * F + q];
-        const float mu = a.cjm[C_MU * F + q], lam = a.cjm[C_LAMBDA * F + q];
-        const float buo = a.cjm[C_BUOY * F + q] * 1.0f;  // buoyancy *= Crho (= 1)
-        const float bz = a.pml_beta_z[k];
+        Taps<FB1, FB2, FB3> T;
+        for (int m = 0; m < 5; m++) {
+            int kk = k + FB3 * (m - 1);
+            T.zp[m] = ring + slot_of(kk) * SLOT_F + cell;
+        }
+        if (a.irk == 0)
+            for (int f = 0; f < 9; f++) mv[f] = T.c(f);
 
         float h[9];
         const bool fs = a.fs_on && k >= _nz - 3;
         if (!fs) {
             // src/wave_deriv.cpp:214-282
             float d[9], c[9];
-            for (int f = 0; f < 9; f++) d[f] = raw_x(R, k, f, FB1, rDH) * bx;
+#pragma unroll
+            for (int f = 0; f < 9; f++) d[f] = T.rx(f, rDH) * bx;
             dir_rhs(xi_x, xi_y, xi_z, d, mu, lam, buo, c);
+#pragma unroll
             for (int f = 0; f < 9; f++) h[f] = c[f];
-            for (int f = 0; f < 9; f++) d[f] = raw_y(R, k, f, FB2, rDH) * by;
+#pragma unroll
+            for (int f = 0; f < 9; f++) d[f] = T.ry(f, rDH) * by;
             dir_rhs(et_x, et_y, et_z, d, mu, lam, buo, c);
+#pragma unroll
             for (int f = 0; f < 9; f++) h[f] = h[f] + c[f];
-            for (int f = 0; f < 9; f++) d[f] = raw_z(R, k, f, FB3, rDH) * bz;
+#pragma unroll
+            for (int f = 0; f < 9; f++) d[f] = T.rz(f, rDH) * bz;
             dir_rhs(zt_x, zt_y, zt_z, d, mu, lam, buo, c);
+#pragma unroll
             for (int f = 0; f < 9; f++) h[f] = (h[f] + c[f]) * DT;
         } else {
             // src/freeSurface.cpp:345-492
@@ -261,8 +379,8 @@ __global__ void __launch_bounds__(TX *TY, 2) k_cg_stage(const CgStageArgs a)
             const float bj = buo * jinv;
             for (int c = 0; c < 3; c++) h[c] = (bj * ((jx[c] * bx + jy[c] * by) + jz[c])) * DT;
             float vxi[3], vet[3], vzt[3];
-            for (int c = 0; c < 3; c++) vxi[c] = raw_x(R, k, c, FB1, rDH) * bx;
-            for (int c = 0; c < 3; c++) vet[c] = raw_y(R, k, c, FB2, rDH) * by;
+            for (int c = 0; c < 3; c++) vxi[c] = T.rx(c, rDH) * bx;
+            for (int c = 0; c < 3; c++) vet[c] = T.ry(c, rDH) * by;
             if (k == _nz - 1) {
                 const long long s = g.at2(i, j);
                 for (int r = 0; r < 3; r++) {
@@ -272,12 +390,13 @@ __global__ void __launch_bounds__(TX *TY, 2) k_cg_stage(const CgStageArgs a)
                              ((dy[0] * vet[0] + dy[g.plane] * vet[1]) + dy[2 * g.plane] * vet[2]);
                 }
             } else if (k == _nz - 2) {
-                for (int c = 0; c < 3; c++)
-                    vzt[c] = ((float)FB3 * (R.at(k + FB3, c, 0, 0) - R.at(k, c, 0, 0))) * rDH;
+                // L2: plane k + FB3 is tap m = 2
+                for (int c = 0; c < 3; c++) vzt[c] = ((float)FB3 * (T.zp[2][c * PF] - T.zp[1][c * PF])) * rDH;
             } else {
+                // L3: planes k, k + FB3, k + 2 FB3 are taps 1, 2, 3
                 for (int c = 0; c < 3; c++)
-                    vzt[c] = ((float)FB3 * ((CG_CF1 * R.at(k, c, 0, 0) + CG_CF2 * R.at(k + FB3, c, 0, 0)) +
-                                            CG_CF3 * R.at(k + 2 * FB3, c, 0, 0))) *
+                    vzt[c] = ((float)FB3 * ((CG_CF1 * T.zp[1][c * PF] + CG_CF2 * T.zp[2][c * PF]) +
+                                            CG_CF3 * T.zp[3][c * PF])) *
                              rDH;
             }
             float s1[9], s2[9], s3[9];
@@ -298,20 +417,24 @@ __global__ void __launch_bounds__(TX *TY, 2) k_cg_stage(const CgStageArgs a)
                 const int dir = fc == 0 || fc == 3 ? 0 : fc == 1 || fc == 4 ? 1 : 2;
                 const PmlFace &P = a.face[fc];
                 long long pos;
-                if (dir == 0) pos = (long long)(i0p - (fc == 3 ? nx - nPML : 0)) + (long long)j0p * nPML + (long long)k0p * nPML * ny;
-                else if (dir == 1) pos = (long long)i0p + (long long)(j0p - (fc == 4 ? ny - nPML : 0)) * nx + (long long)k0p * nx * nPML;
-                else pos = (long long)i0p + (long long)j0p * nx + (long long)k0p * nx * ny;
+                if (dir == 0)
+                    pos = (long long)(i0p - (fc == 3 ? nx - nPML : 0)) + (long long)j0p * nPML +
+                          (long long)k0p * nPML * ny;
+                else if (dir == 1)
+                    pos = (long long)i0p + (long long)(j0p - (fc == 4 ? ny - nPML : 0)) * nx +
+                          (long long)k0p * nx * nPML;
+                else
+                    pos = (long long)i0p + (long long)j0p * nx + (long long)k0p * nx * ny;
                 const float *al = dir == 0 ? a.pml_alpha_x : dir == 1 ? a.pml_alpha_y : a.pml_alpha_z;
                 const float *be = dir == 0 ? a.pml_beta_x : dir == 1 ? a.pml_beta_y : a.pml_beta_z;
                 const float *dd = dir == 0 ? a.pml_d_x : dir == 1 ? a.pml_d_y : a.pml_d_z;
                 const int ix = dir == 0 ? i : dir == 1 ? j : k;
-                const int FB = dir == 0 ? FB1 : dir == 1 ? FB2 : FB3;
                 const float dval = dd[ix], beta = be[ix], alpha_d = dval + al[ix];
                 const float m0 = dir == 0 ? xi_x : dir == 1 ? et_x : zt_x;
                 const float m1 = dir == 0 ? xi_y : dir == 1 ? et_y : zt_y;
                 const float m2 = dir == 0 ? xi_z : dir == 1 ? et_z : zt_z;
                 float d[9], rhs[9], aux[9], hA[9];
-                for (int f = 0; f < 9; f++) d[f] = raw_dir(R, dir, k, f, FB, rDH) * dval;
+                for (int f = 0; f < 9; f++) d[f] = T.rdir(dir, f, rDH) * dval;
                 dir_rhs(m0, m1, m2, d, mu, lam, buo, rhs);
                 const float *cur = a.irk == 0 ? P.A : P.B;
                 for (int f = 0; f < 9; f++) aux[f] = cur[f * P.count + pos];
@@ -350,21 +473,28 @@ __global__ void __launch_bounds__(TX *TY, 2) k_cg_stage(const CgStageArgs a)
         // ---- RK4 update of the wavefield (src/wave_rk.cpp:17-104)
         float wout[9];
         if (a.irk == 0) {
+#pragma unroll
             for (int f = 0; f < 9; f++) {
-                float m = a.Wm[f * F + q];
-                a.T[f * F + q] = m + RK_BETA1 * h[f];
-                wout[f] = m + RK_ALPHA2 * h[f];
+                a.T[f * F + q] = mv[f] + RK_BETA1 * h[f];
+                wout[f] = mv[f] + RK_ALPHA2 * h[f];
             }
-        } else if (a.irk == 1 || a.irk == 2) {
+        } else if (a.irk == 1) {
+#pragma unroll
             for (int f = 0; f < 9; f++) {
-                float m = a.Wm[f * F + q];
-                float t = a.T[f * F + q];
-                a.T[f * F + q] = t + (a.irk == 1 ? RK_BETA2 : RK_BETA3) * h[f];
-                wout[f] = a.irk == 1 ? m + RK_ALPHA3 * h[f] : m + h[f];
+                a.T[f * F + q] = tv[f] + RK_BETA2 * h[f];
+                wout[f] = mv[f] + RK_ALPHA3 * h[f];
+            }
+        } else if (a.irk == 2) {
+#pragma unroll
+            for (int f = 0; f < 9; f++) {
+                a.T[f * F + q] = tv[f] + RK_BETA3 * h[f];
+                wout[f] = mv[f] + h[f];
             }
         } else {
-            for (int f = 0; f < 9; f++) wout[f] = a.T[f * F + q] + RK_BETA4 * h[f];
+#pragma unroll
+            for (int f = 0; f < 9; f++) wout[f] = tv[f] + RK_BETA4 * h[f];
         }
+#pragma unroll
         for (int f = 0; f < 9; f++) a.Wout[f * F + q] = wout[f];
 
         if (a.irk == 3) {
@@ -380,20 +510,84 @@ __global__ void __launch_bounds__(TX *TY, 2) k_cg_stage(const CgStageArgs a)
             }
         }
     }
+    __syncthreads();
+    if (s_abort) {
+        // no copy may still be landing in shared memory when the CTA exits
+        if (tid == 0)
+            for (int kk = max(kf, issued - NSLOT + 1); kk <= issued; kk++)
+                if (!mbar_wait_bounded(smem_u32(&bars[slot_of(kk)]), parity_of(kk))) atomicOr(a.err, 2);
+        break;
+    }
+    seq0 += (unsigned)(issued - kf + 1);
+    }  // work items
+
+    // the last CTA out resets the work counter for the next launch
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        int done = atomicAdd(&a.work[1], 1);
+        if (done == (int)(gridDim.x * gridDim.y * gridDim.z) - 1) {
+            atomicExch(&a.work[0], 0);
+            atomicExch(&a.work[1], 0);
+            __threadfence();
+        }
+    }
 }
 
-cudaError_t launch_cg_stage(const CgStageArgs &a, cudaStream_t st)
+// ------------------------------------------------------------ host side
+int cg_stage_ctas_per_sm() { return 2; }
+
+template <int FB1, int FB2, int FB3>
+static cudaError_t launch_t(const CgStageArgs &a, const CgStageMaps &m, int ctas, cudaStream_t st)
 {
-    static bool attr_set = false;
-    if (!attr_set) {
-        CUDA_TRY(cudaFuncSetAttribute(k_cg_stage, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    static bool attr = false;
+    if (!attr) {
+        CUDA_TRY(cudaFuncSetAttribute(k_cg_stage<FB1, FB2, FB3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)cg_stage_smem_bytes()));
-        attr_set = true;
+        attr = true;
     }
-    dim3 block(TX, TY, 1);
-    dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, (a.g.nz + a.kchunk - 1) / a.kchunk);
-    k_cg_stage<<<grid, block, cg_stage_smem_bytes(), st>>>(a);
+    const CUtensorMap &w = *reinterpret_cast<const CUtensorMap *>(m.win);
+    const CUtensorMap &c = *reinterpret_cast<const CUtensorMap *>(m.cjm);
+    const CUtensorMap &mm = *reinterpret_cast<const CUtensorMap *>(m.wm);
+    const CUtensorMap &t = *reinterpret_cast<const CUtensorMap *>(m.t);
+    k_cg_stage<FB1, FB2, FB3><<<ctas, dim3(TX, TY, 1), cg_stage_smem_bytes(), st>>>(w, c, mm, t, a);
     return cudaGetLastError();
+}
+
+cudaError_t launch_cg_stage(const CgStageArgs &a, const CgStageMaps &maps, int ctas, cudaStream_t st)
+{
+    const int key = (a.FB1 > 0) * 4 + (a.FB2 > 0) * 2 + (a.FB3 > 0);
+    switch (key) {
+    case 0: return launch_t<-1, -1, -1>(a, maps, ctas, st);
+    case 1: return launch_t<-1, -1, 1>(a, maps, ctas, st);
+    case 2: return launch_t<-1, 1, -1>(a, maps, ctas, st);
+    case 3: return launch_t<-1, 1, 1>(a, maps, ctas, st);
+    case 4: return launch_t<1, -1, -1>(a, maps, ctas, st);
+    case 5: return launch_t<1, -1, 1>(a, maps, ctas, st);
+    case 6: return launch_t<1, 1, -1>(a, maps, ctas, st);
+    default: return launch_t<1, 1, 1>(a, maps, ctas, st);
+    }
+}
+
+cudaError_t make_field_tmap(void *out, const float *base, const DevGrid &g, int nf, bool halo_box)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void *fn = nullptr;
+        CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    cuuint64_t dims[4] = {(cuuint64_t)g.pitch, (cuuint64_t)g.nyp, (cuuint64_t)g.nzp, (cuuint64_t)nf};
+    cuuint64_t strides[3] = {(cuuint64_t)g.pitch * 4, (cuuint64_t)g.plane * 4, (cuuint64_t)g.fstride * 4};
+    cuuint32_t box[4] = {halo_box ? (cuuint32_t)BXW : (cuuint32_t)TX, halo_box ? (cuuint32_t)BYW : (cuuint32_t)TY, 1,
+                         (cuuint32_t)nf};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = encode(reinterpret_cast<CUtensorMap *>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)base, dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 }  // namespace cgfdm

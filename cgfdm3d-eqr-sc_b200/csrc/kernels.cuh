@@ -38,14 +38,31 @@ struct CgStageArgs {
     PmlFace face[5];     // x1 y1 z1 x2 y2 (order of src/pml_deriv.cpp:633-646)
     float *pgv;          // [ny][nx][2] running max, stage 3 only
     float *dis;          // displacement, 3 fields in the W layout, stage 3 only
+    int *err;            // device error word: bit 0 = a bounded wait gave up
+    int *work;           // persistent-CTA work counter pair, zero between launches
+    int ntiles_x, ntiles_y, nchunk;  // work items: tiles x tiles x z-chunks
     int irk;
     int FB1, FB2, FB3;
     int nPML, pml_on, fs_on;
     int kchunk;
     float rDH, DT;
 };
-cudaError_t launch_cg_stage(const CgStageArgs &a, cudaStream_t st);
+// TMA descriptors (CUtensorMap, 128 bytes each) used by one stage launch:
+// the stencil input with its halo box, and 32x8 point boxes of the metric,
+// the step-start state and the RK accumulator for L2 prefetch.
+struct CgStageMaps {
+    alignas(64) unsigned char win[128];
+    alignas(64) unsigned char cjm[128];
+    alignas(64) unsigned char wm[128];
+    alignas(64) unsigned char t[128];
+};
+cudaError_t launch_cg_stage(const CgStageArgs &a, const CgStageMaps &maps, int grid_ctas, cudaStream_t st);
 size_t cg_stage_smem_bytes();
+// Encodes the 4-D tensor map (x, y, z, field) of an nf-field buffer, with a
+// halo box (40 x 12 x 1 x nf) or a point box (32 x 8 x 1 x nf); out must hold
+// 128 bytes.
+cudaError_t make_field_tmap(void *out, const float *base, const DevGrid &g, int nf, bool halo_box);
+int cg_stage_ctas_per_sm();
 
 // --------------------------------------------------- sources / stations
 struct FaultDev {

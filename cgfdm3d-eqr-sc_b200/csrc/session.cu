@@ -172,6 +172,15 @@ int Session::setup_device()
 
     // wavefield buffers: A (step start / final), B, C (stage values), T (RK4 sum)
     for (int b = 0; b < (cg ? 4 : 3); b++) ALLOC(W_[b], float, F * 9);
+    ALLOC(err_dev_, int, 1);
+    ALLOC(work_dev_, int, 2);
+    if (cg)
+        for (int b = 0; b < 3; b++) {
+            CU(make_field_tmap(maps_[b].win, W_[b], g, 9, true));
+            CU(make_field_tmap(maps_[b].cjm, cjm_, g, 13, false));
+            CU(make_field_tmap(maps_[b].wm, W_[0], g, 9, false));
+            CU(make_field_tmap(maps_[b].t, W_[3], g, 9, false));
+        }
 
     // PML profiles and auxiliaries
     if (cg && m.p.pml) {
@@ -255,14 +264,20 @@ int Session::setup_device()
         point_.stf = d_stf;
     }
 
-    // z-chunking: enough CTAs for every SM to hold two while the chunk
-    // stays long enough to amortise the 4-plane ring prologue
+    // work items for the persistent stage kernel: 32 x 8 column tiles times
+    // z-chunks of about 32 planes, at least four items per resident CTA so
+    // the dynamic schedule ends evenly
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
-    long long nxy = (long long)((G.nx + 31) / 32) * ((G.ny + 7) / 8);
-    long long want = (long long)dev_sms * 4;
-    int nchunk = (int)std::max<long long>(1, std::min<long long>((want + nxy - 1) / nxy, std::max(1, G.nz / 8)));
-    kchunk_ = (G.nz + nchunk - 1) / nchunk;
+    ntx_ = (G.nx + 31) / 32;
+    nty_ = (G.ny + 7) / 8;
+    const long long tiles = (long long)ntx_ * nty_;
+    const int ctas = dev_sms * cg_stage_ctas_per_sm();
+    nchunk_ = std::max(1, (G.nz + 31) / 32);
+    while (tiles * nchunk_ < 4LL * ctas && G.nz / (nchunk_ + 1) >= 12) nchunk_++;
+    kchunk_ = (G.nz + nchunk_ - 1) / nchunk_;
+    nchunk_ = (G.nz + kchunk_ - 1) / kchunk_;
+    grid_ctas_ = (int)std::min<long long>(ctas, tiles * nchunk_);
 
     CU(cudaStreamSynchronize(stream));
     // coordinates and medium are not needed on the device any more
@@ -290,6 +305,7 @@ int Session::launch_step(int step)
     if (cg) {
         float *A = W_[0], *B = W_[1], *C = W_[2], *T = W_[3];
         const float *win[4] = {A, B, C, B};
+        const int win_map[4] = {0, 1, 2, 1};
         float *wout[4] = {B, C, B, A};
         for (int irk = 0; irk < 4; irk++) {
             CgStageArgs a{};
@@ -314,7 +330,10 @@ int Session::launch_step(int step)
             a.kchunk = kchunk_;
             a.rDH = m.g.rDH;
             a.DT = DT;
-            CU(launch_cg_stage(a, stream));
+            a.err = err_dev_;
+            a.work = work_dev_;
+            a.ntiles_x = ntx_, a.ntiles_y = nty_, a.nchunk = nchunk_;
+            CU(launch_cg_stage(a, maps_[win_map[irk]], grid_ctas_, stream));
             FB1 = -FB1, FB2 = -FB2, FB3 = -FB3;
         }
         kernel_launches += 4;
@@ -379,6 +398,18 @@ int Session::run(int nsteps)
     it += n;
     CU(cudaStreamSynchronize(stream));
     CU(cudaGetLastError());
+    return check_device_error();
+}
+
+// A stage kernel whose bounded wait gave up leaves a bit in the error word.
+int Session::check_device_error()
+{
+    int e = 0;
+    CU(cudaMemcpy(&e, err_dev_, sizeof e, cudaMemcpyDeviceToHost));
+    if (e) {
+        err = "a stage kernel's bounded wait for its plane copies gave up (device error word " + std::to_string(e) + ")";
+        return ST_TIMEOUT;
+    }
     return ST_OK;
 }
 

@@ -63,6 +63,11 @@ private:
     cudaGraphExec_t graph8_ = nullptr;
     cudaGraph_t graph8_src_ = nullptr;
     cudaEvent_t ev_[4] = {};
+    CgStageMaps maps_[3] = {};                       // TMA descriptors per stencil input A, B, C
+    int *work_dev_ = nullptr;                        // persistent-CTA work counters
+    int ntx_ = 1, nty_ = 1, nchunk_ = 1, grid_ctas_ = 1;
+    int *err_dev_ = nullptr;                         // device error word of the stage kernels
+    int check_device_error();
 };
 
 }  // namespace cgfdm
