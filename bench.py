@@ -1,0 +1,323 @@
+"""Benchmark of the velocity-stress time-stepping hot path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Workload (default ``terrain_fault``): the curvilinear CGFDM configuration,
+400 x 400 x 200 points, DH = 100 m, eight-hill terrain, perturbed layered
+medium, 40 x 20 finite fault, 400 surface stations (cgfdm.configs).  A step
+is one RK4 time step of the whole grid.  Metric: Mpts*step/s, interior
+points x steps / seconds.
+
+Our arm: W untimed steps, then K steps timed with CUDA events on the
+session's stream (barrier + device sync on both sides, max over ranks);
+inputs (7.3 GB of model and wavefield) are resident and larger than L2.
+``e2e`` is the same metric through the C ABI from host files: create the
+session from the run directory (model build, host->device copies), run K
+steps, read the station traces back, destroy.  ``roofline`` uses the mean
+device time of one fused stage launch (events around each launch) and the
+algorithmic bytes of a launch.  ``cpu_baseline`` runs the reference's own
+CPU build (oracle/_ref/cgfdm_ref) on a sample of the workload on the host
+cores.
+
+Reference arm (--impl reference): the reference's CPU build, one process per
+host core on the sample grid, timed steps differenced against a run with
+only the warm-up steps so set-up is excluded.
+
+With N > 1 (torchrun), every rank advances its own replica of the workload
+on its own GPU; there is no exchange between ranks ("scaling": "weak").
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cgfdm3d-eqr-sc_b200")
+for p in (PKG, os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "Mpts*step/s"
+WORK = os.environ.get("CGFDM_BENCH_DIR", os.path.join(tempfile.gettempdir(), "cgfdm_bench"))
+SAMPLE_GRID = (160, 160, 100)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_point():
+    """DRAM bytes per interior point and stage launch, from the committed ncu
+    summary (profiles/cg_stage_traffic.txt), or None."""
+    path = os.path.join(ROOT, "profiles", "cg_stage_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_point_per_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+def make_workload(name, steps, directory):
+    from cgfdm import cases, configs
+
+    marker = os.path.join(directory, f".done_{steps}")
+    if os.path.exists(marker):
+        return directory
+    if os.path.exists(directory):
+        shutil.rmtree(directory)
+    if name == "terrain_fault":
+        configs.terrain_fault(directory, steps=steps)
+    elif name.startswith("terrain_fault_"):
+        nx, ny, nz = (int(v) for v in name.split("_")[-1].split("x"))
+        configs.terrain_fault(directory, steps=steps, NX=nx, NY=ny, NZ=nz)
+    elif name == "halfspace":
+        cases.write_case(configs.halfspace(steps=steps), directory)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    open(marker, "w").close()
+    return directory
+
+
+def workload_desc(name):
+    if name == "terrain_fault":
+        return ("terrain_fault: CGFDM RK4, 400x400x200 (32.0 Mpts interior), DH=100 m, 8-hill terrain, "
+                "4 layers + half-space with +-3% correlated perturbation, 40x20 finite fault, 400 stations, "
+                "12-layer PML on 5 faces, FP32")
+    if name == "halfspace":
+        return "halfspace: CGFDM RK4, 128x128x96, DH=100 m, homogeneous half-space, Mxy point source, 16 stations"
+    return name
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return self
+
+        def reader():
+            for line in self.proc.stdout:
+                self.samples.append([v.strip() for v in line.split(",")])
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        smax = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for n, v in zip(names, s[4:8]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_reference_rate(name, warmup_steps, timed_steps, procs):
+    """Reference CPU build on the sample grid: `procs` concurrent processes,
+    wall time of (warmup + timed) steps minus (warmup) steps, aggregate rate."""
+    import refrun
+
+    if not refrun.available("CGFDM"):
+        return None, "reference CPU build (oracle/_ref/cgfdm_ref) not built"
+    nx, ny, nz = SAMPLE_GRID
+    sample_name = f"terrain_fault_{nx}x{ny}x{nz}" if name.startswith("terrain_fault") else name
+    base = os.path.join(WORK, "cpu_sample")
+    runs = {}
+    for nt in (warmup_steps, warmup_steps + timed_steps):
+        d = make_workload(sample_name, nt, os.path.join(base, f"{sample_name}_{nt}"))
+        copies = []
+        for p in range(procs):
+            c = os.path.join(base, f"run_{nt}_{p}")
+            if os.path.exists(c):
+                shutil.rmtree(c)
+            os.makedirs(os.path.join(c, "output"))
+            for f in os.listdir(d):
+                src = os.path.join(d, f)
+                if os.path.isfile(src):
+                    os.symlink(src, os.path.join(c, f))
+            copies.append(c)
+        t0 = time.perf_counter()
+        ps = [subprocess.Popen(["taskset", "-c", str(p % os.cpu_count()), refrun.ref_binary("CGFDM")], cwd=c,
+                               stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL) for p, c in enumerate(copies)]
+        rcs = [p.wait() for p in ps]
+        runs[nt] = time.perf_counter() - t0
+        if any(rcs):
+            return None, f"reference CPU build failed with exit codes {sorted(set(rcs))}"
+    dt = runs[warmup_steps + timed_steps] - runs[warmup_steps]
+    pts = nx * ny * nz
+    rate = procs * pts * timed_steps / max(dt, 1e-9) / 1e6
+    sample = (f"reference CPU build (g++ -O2, single-threaded as shipped), {procs} concurrent processes pinned "
+              f"one per core, each on the {nx}x{ny}x{nz} sub-grid of the workload (same generators), "
+              f"{timed_steps} steps timed as wall({warmup_steps + timed_steps} steps) - wall({warmup_steps} steps)")
+    return {"value": rate, "unit": METRIC, "cores": procs, "kind": "reference", "sample": sample}, None
+
+
+# ------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=8)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="terrain_fault")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        procs = min(os.cpu_count() or 1, 32)
+        timed = max(1, min(args.steps, 4))
+        cb, why = cpu_reference_rate(args.workload, args.warmup if args.warmup <= 4 else 2, timed, procs)
+        if cb is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return 0
+        line = {"metric": METRIC, "value": cb["value"], "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
+                "steps": timed, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": workload_desc(args.workload), "sample_grid": "x".join(map(str, SAMPLE_GRID))},
+                "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                                            "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    from cgfdm import Session
+
+    total = args.warmup + args.steps + 8
+    d = os.path.join(WORK, f"{args.workload}_{total}")
+    if rank == 0:
+        make_workload(args.workload, total, d)
+    if dist:
+        dist.barrier()
+
+    # ---- device-timed leg: inputs resident on the GPU
+    s = Session(d, device=local_rank)
+    info = s.info
+    pts = info.nx * info.ny * info.nz
+    s.run(args.warmup)
+    torch.cuda.synchronize(local_rank)
+    if dist:
+        dist.barrier()
+    l0 = s.info.kernel_launches
+    with ClockSampler(local_rank) as clk:
+        ms = s.run_timed(args.steps)
+    launches = s.info.kernel_launches - l0
+    torch.cuda.synchronize(local_rank)
+    if dist:
+        dist.barrier()
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    stage_ms = s.profile_stages(8)
+    algo_step = info.algo_bytes_per_step
+    algo_launch = algo_step / info.stage_kernels_per_step
+    s.close()
+
+    # ---- end-to-end leg: run directory on disk -> C ABI -> stations on the host
+    t0 = time.perf_counter()
+    s2 = Session(d, device=local_rank)
+    s2.run(args.steps)
+    st = s2.stations()
+    i2 = s2.info
+    s2.close()
+    e2e_s = time.perf_counter() - t0
+    e = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(e, op=dist.ReduceOp.MAX)
+    e2e_s = float(e.item())
+
+    value = world * pts * args.steps / (ms_max * 1e-3) / 1e6
+    hbm_peak, peak_kind = peaks()
+    achieved = algo_launch / (stage_ms * 1e-3) / 1e9
+    tpp = traffic_per_point()
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_desc(args.workload), "points": pts, "DT": info.DT,
+                   "l2": "inputs larger than L2 (model + wavefield %.1f GB resident)" % (info.device_bytes / 1e9),
+                   "parallelism": f"replicas x{world}"},
+        "hbm_gbs_algorithmic": algo_step * args.steps / (ms_max * 1e-3) / 1e9,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "peak_kind": peak_kind,
+                     "traffic": (tpp * pts if tpp else None), "kernel": "k_cg_stage",
+                     "algo_bytes_per_launch": algo_launch, "mean_launch_ms": stage_ms},
+        "e2e": {"value": world * pts * args.steps / e2e_s / 1e6, "unit": METRIC,
+                "h2d_bytes_per_step": i2.h2d_bytes / args.steps, "d2h_bytes_per_step": st.nbytes / args.steps,
+                "seconds": e2e_s, "path": "cgfdm_create(run dir) + cgfdm_run(K) + cgfdm_get_stations + destroy"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb, why = cpu_reference_rate(args.workload, 2, 4, min(os.cpu_count() or 1, 32))
+        line["cpu_baseline"] = cb if cb else {"unavailable": why}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -37,6 +37,8 @@ class Info(ctypes.Structure):
         ("H_min", ctypes.c_float), ("Vp_max", ctypes.c_float),
         ("device_bytes", ctypes.c_double), ("h2d_bytes", ctypes.c_double),
         ("kernel_launches", ctypes.c_longlong),
+        ("algo_bytes_per_step", ctypes.c_double),
+        ("stage_kernels_per_step", ctypes.c_int),
     ]
 
 
@@ -58,6 +60,7 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
     L.cgfdm_run.argtypes = [vp, ctypes.c_int]
     L.cgfdm_run_timed.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     L.cgfdm_info_get.argtypes = [vp, ctypes.POINTER(Info)]
+    L.cgfdm_profile_stages.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     fp = ctypes.POINTER(ctypes.c_float)
     L.cgfdm_get_stations.argtypes = [vp, fp, ctypes.c_longlong]
     L.cgfdm_get_wavefield.argtypes = [vp, fp, ctypes.c_longlong]
@@ -104,6 +107,11 @@ class Session:
     def run_timed(self, nsteps: int) -> float:
         ms = ctypes.c_float()
         self._check(self.L.cgfdm_run_timed(self._h, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def profile_stages(self, nsteps: int) -> float:
+        ms = ctypes.c_float()
+        self._check(self.L.cgfdm_profile_stages(self._h, int(nsteps), ctypes.byref(ms)))
         return ms.value
 
     def stations(self) -> np.ndarray:

@@ -77,7 +77,15 @@ int cgfdm_info_get(const cgfdm_session *s, cgfdm_info *o)
     o->device_bytes = (double)S.device_bytes;
     o->h2d_bytes = S.h2d_bytes;
     o->kernel_launches = S.kernel_launches;
+    o->algo_bytes_per_step = S.algo_bytes_per_step();
+    o->stage_kernels_per_step = S.m.p.scheme == 0 ? 4 : 3;
     return CGFDM_OK;
+}
+
+int cgfdm_profile_stages(cgfdm_session *s, int nsteps, float *mean_stage_ms)
+{
+    if (!s || !mean_stage_ms || nsteps <= 0) return CGFDM_E_ARG;
+    return s->s.profile_stages(nsteps, mean_stage_ms);
 }
 
 int cgfdm_get_stations(const cgfdm_session *s, float *out, long long count)

@@ -294,7 +294,7 @@ int Session::setup_device()
 }
 
 // ----------------------------------------------------------------- step
-int Session::launch_step(int step)
+int Session::launch_step(int step, bool timed_stages)
 {
     const bool cg = m.p.scheme == SCHEME_CGFDM;
     const float DT = (float)m.p.DT;
@@ -333,7 +333,16 @@ int Session::launch_step(int step)
             a.err = err_dev_;
             a.work = work_dev_;
             a.ntiles_x = ntx_, a.ntiles_y = nty_, a.nchunk = nchunk_;
+            if (timed_stages) CU(cudaEventRecord(ev_[2], stream));
             CU(launch_cg_stage(a, maps_[win_map[irk]], grid_ctas_, stream));
+            if (timed_stages) {
+                CU(cudaEventRecord(ev_[3], stream));
+                CU(cudaEventSynchronize(ev_[3]));
+                float ms = 0;
+                CU(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
+                stage_ms_sum_ += ms;
+                stage_ms_count_++;
+            }
             FB1 = -FB1, FB2 = -FB2, FB3 = -FB3;
         }
         kernel_launches += 4;
@@ -427,6 +436,36 @@ int Session::run_timed(int nsteps, float *ms, float *stage_ms)
     CU(cudaEventElapsedTime(ms, ev_[0], ev_[1]));
     if (stage_ms) *stage_ms = 0.0f;
     return ST_OK;
+}
+
+int Session::profile_stages(int nsteps, float *mean)
+{
+    int n = std::min(nsteps, m.NT - it);
+    stage_ms_sum_ = 0;
+    stage_ms_count_ = 0;
+    for (int s = 0; s < n; s++) {
+        int st = launch_step(it + s, true);
+        if (st) return st;
+    }
+    it += n;
+    CU(cudaStreamSynchronize(stream));
+    *mean = stage_ms_count_ ? (float)(stage_ms_sum_ / stage_ms_count_) : 0.0f;
+    return check_device_error();
+}
+
+// Minimum bytes a step moves (float fields of 4 bytes): RK4 stages read the
+// stencil input, 12 metric/medium fields and the RK state and write the stage
+// output and accumulator, 39 + 57 + 57 + 39 = 192 fields per interior point;
+// each absorbing face adds 27 + 45 + 45 + 27 = 144 auxiliary fields per slab
+// point.
+double Session::algo_bytes_per_step() const
+{
+    const Grid &G = m.g;
+    double n = (double)G.nx * G.ny * G.nz;
+    double faces = 0;
+    if (m.p.pml && m.p.scheme == SCHEME_CGFDM)
+        faces = (double)G.nPML * (2.0 * G.ny * G.nz + 2.0 * G.nx * G.nz + (double)G.nx * G.ny);
+    return 4.0 * (192.0 * n + 144.0 * faces);
 }
 
 // ------------------------------------------------------------- readback

@@ -23,6 +23,8 @@ public:
     int create(const std::string &run_dir, const std::string &options, int device);
     int run(int nsteps);
     int run_timed(int nsteps, float *ms, float *stage_ms);
+    int profile_stages(int nsteps, float *mean_stage_ms);
+    double algo_bytes_per_step() const;
     int get_wavefield(float *host_aos) const;       // [_nz_][_ny_][_nx_][9]
     int get_cjm(float *host_aos, int *nfield) const;  // [_nz_][_ny_][_nx_][nfield]
     int get_stations(float *host) const;            // [nst][NT][9]
@@ -45,7 +47,9 @@ public:
 private:
     int cuda_fail(cudaError_t e, const char *what);
     int setup_device();
-    int launch_step(int step);           // one step, direct launches
+    int launch_step(int step, bool timed_stages = false);  // one step, direct launches
+    double stage_ms_sum_ = 0;
+    long long stage_ms_count_ = 0;
     int launch_steps_graph(int n8);      // n8 full FB cycles via the captured graph
     void *alloc(size_t bytes);
     std::vector<void *> allocs_;

@@ -53,6 +53,8 @@ typedef struct cgfdm_info {
     double device_bytes; /* device memory held by the session */
     double h2d_bytes;    /* bytes copied host -> device during setup */
     long long kernel_launches; /* kernels of this library launched so far */
+    double algo_bytes_per_step; /* bytes a step must move at minimum (see cgfdm_profile_stages) */
+    int stage_kernels_per_step; /* fused stage launches per step (4 for RK4, 3 for TVD-RK3) */
 } cgfdm_info;
 
 /* Builds the model of a run directory on GPU `device`: reads params.json
@@ -75,6 +77,15 @@ int cgfdm_run(cgfdm_session *s, int nsteps);
 int cgfdm_run_timed(cgfdm_session *s, int nsteps, float *ms);
 
 int cgfdm_info_get(const cgfdm_session *s, cgfdm_info *out);
+
+/* Advances `nsteps` steps launching every kernel directly (no graph), with
+ * CUDA events around each fused stage kernel, and returns the mean device
+ * time of one stage launch in milliseconds.  Divide algo_bytes_per_step by
+ * stage_kernels_per_step for the algorithmic bytes of one launch: per
+ * interior point and step, the stencil input, metric and medium (12 fields),
+ * RK state and accumulator of every stage (192 float fields in all for
+ * RK4), plus 144 auxiliary fields per point of each absorbing face. */
+int cgfdm_profile_stages(cgfdm_session *s, int nsteps, float *mean_stage_ms);
 
 /* Station traces, [n_stations][NT][9] as the reference stores them
  * (src/station.cpp:334); `count` is the capacity of `out` in floats. */

@@ -20,12 +20,26 @@ from cgfdm import Session, cases
 
 TOL_FAST = 1e-5
 
+def _case(mk):
+    return lambda d: cases.write_case(mk(), d)
+
+
+def _terrain_fault(d):
+    # the benchmark workload's generators at a small size: raw height map and
+    # medium volume (routed into the reference through its oracle hooks),
+    # 40x20 finite fault, 400 stations
+    from cgfdm import configs
+
+    configs.terrain_fault(d, steps=60, NX=64, NY=60, NZ=40, nPML=6)
+
+
 CASES = {
-    "halfspace": lambda: pu.small_halfspace(steps=48),
-    "gauss_hill": lambda: pu.small_hill(steps=48),
-    "multi_fault": lambda: pu.multi_fault(steps=48),
-    "ricker_point": lambda: pu.ricker_point(steps=48),
-    "double_couple": lambda: pu.double_couple(steps=48),
+    "halfspace": _case(lambda: pu.small_halfspace(steps=48)),
+    "gauss_hill": _case(lambda: pu.small_hill(steps=48)),
+    "multi_fault": _case(lambda: pu.multi_fault(steps=48)),
+    "ricker_point": _case(lambda: pu.ricker_point(steps=48)),
+    "double_couple": _case(lambda: pu.double_couple(steps=48)),
+    "terrain_fault": _terrain_fault,
 }
 
 
@@ -35,9 +49,9 @@ def ref_runs(tmp_path_factory):
         pytest.skip("reference CPU build oracle/_ref/cgfdm_ref not built")
     root = tmp_path_factory.mktemp("cg")
     out = {}
-    for name, mk in CASES.items():
+    for name, write in CASES.items():
         d = str(root / name)
-        cases.write_case(mk(), d)
+        write(d)
         refrun.run(d)
         out[name] = (d, refrun.read_outputs(d))
     return out
