@@ -111,6 +111,31 @@ int cgfdm_destroy(cgfdm_session *s);
  * cgfdm_create in this thread when s is NULL). */
 const char *cgfdm_last_error(const cgfdm_session *s);
 
+/* Allocation-free grid-spacing reduction.  No counterpart in the reference:
+ * it offers the smallest and largest point-to-plane distance of the CFL
+ * check (the quantity cgfdm_create computes as H_min, after
+ * src/calc_CFL.cpp:94-163) to callers that cannot allocate device memory at
+ * that point, for example an application whose other streams carry a live
+ * simulation (cudaMalloc/cudaFree can synchronize the whole device) or an
+ * embedder whose own pool allocator owns the device memory.  It calls no
+ * cudaMalloc, cudaFree or allocating library routine.
+ *
+ * d_coord: device array [nz+6][ny+6][nx+6][3] of float x, y, z (the
+ * reference's coordinate layout, halo included).  d_out: device array of two
+ * doubles, receiving H_min and H_max.  stream: a cudaStream_t, or NULL for
+ * the default stream; the call only enqueues work on it.
+ *
+ * Scratch lives in a static device array of CGFDM_NOALLOC_MAX_BLOCKS (min,
+ * max) pairs, 1 MiB, one pair per block of 32 x 8 x 16 points; larger grids
+ * are rejected with CGFDM_E_ARG and a message from
+ * cgfdm_noalloc_last_error().  The array is shared by every call on a device
+ * and keeps the last call's contents, so calls that overlap on the GPU race.
+ * The first call on each device looks up the array's device address with
+ * that device current. */
+#define CGFDM_NOALLOC_MAX_BLOCKS 65536
+int cgfdm_hrange_noalloc(const float *d_coord, int nx, int ny, int nz, double *d_out, void *stream);
+const char *cgfdm_noalloc_last_error(void);
+
 /* Library build identification: "fast" or "exact" (built with --fmad=false,
  * every float operation rounded separately as on the reference's CPU path). */
 const char *cgfdm_build_flavor(void);
