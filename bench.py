@@ -60,14 +60,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_point():
-    """DRAM bytes per interior point and stage launch, from the committed ncu
-    summary (profiles/cg_stage_traffic.txt), or None."""
+def traffic_ratio():
+    """DRAM traffic of the stage kernel over its algorithmic bytes, from the
+    committed ncu summary (profiles/cg_stage_traffic.txt), or None."""
     path = os.path.join(ROOT, "profiles", "cg_stage_traffic.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith("dram_bytes_per_point_per_launch:"):
+        if line.startswith("dram_traffic_over_algorithmic:"):
             return float(line.split(":", 1)[1])
     return None
 
@@ -289,7 +289,7 @@ def main():
     value = world * pts * args.steps / (ms_max * 1e-3) / 1e6
     hbm_peak, peak_kind = peaks()
     achieved = algo_launch / (stage_ms * 1e-3) / 1e9
-    tpp = traffic_per_point()
+    tr = traffic_ratio()
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -300,7 +300,7 @@ def main():
         "hbm_gbs_algorithmic": algo_step * args.steps / (ms_max * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "peak_kind": peak_kind,
-                     "traffic": (tpp * pts if tpp else None), "kernel": "k_cg_stage",
+                     "traffic": (tr * algo_launch if tr else None), "traffic_source": "ncu ratio on terrain_fault_256x256x128 x algorithmic bytes of this launch", "kernel": "k_cg_stage",
                      "algo_bytes_per_launch": algo_launch, "mean_launch_ms": stage_ms},
         "e2e": {"value": world * pts * args.steps / e2e_s / 1e6, "unit": METRIC,
                 "h2d_bytes_per_step": i2.h2d_bytes / args.steps, "d2h_bytes_per_step": st.nbytes / args.steps,

@@ -27,40 +27,50 @@ static const int FB_TABLE[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, -1,
 __global__ void k_hrange(const float *__restrict__ coord, int nxp, int nyp, int nzp, unsigned long long *hmin,
                          unsigned long long *hmax)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x + CGFDM_HALO;
-    int j = blockIdx.y * blockDim.y + threadIdx.y + CGFDM_HALO;
-    int k = blockIdx.z * blockDim.z + threadIdx.z + CGFDM_HALO;
-    if (i >= nxp - CGFDM_HALO || j >= nyp - CGFDM_HALO || k >= nzp - CGFDM_HALO) return;
-    auto at = [&](int a, int b, int c) { return ((long long)c * nyp + b) * nxp + a; };
-    long long p = at(i, j, k) * 3;
-    double P[3] = {coord[p], coord[p + 1], coord[p + 2]};
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + CGFDM_HALO;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + CGFDM_HALO;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + CGFDM_HALO;
     double lo = 1.0e20, hi = 0.0;
-    for (int ii = -1; ii <= 1; ii += 2)
-        for (int jj = -1; jj <= 1; jj += 2)
-            for (int kk = -1; kk <= 1; kk += 2) {
-                long long a = at(i - ii, j, k) * 3, b = at(i, j - jj, k) * 3, c = at(i, j, k - kk) * 3;
-                double A[3] = {coord[a], coord[a + 1], coord[a + 2]};
-                double B[3] = {coord[b], coord[b + 1], coord[b + 2]};
-                double C[3] = {coord[c], coord[c + 1], coord[c + 2]};
-                double AB[3], AC[3], PA[3], n[3];
-                for (int t = 0; t < 3; t++) {
-                    AB[t] = __dsub_rn(B[t], A[t]);
-                    AC[t] = __dsub_rn(C[t], A[t]);
-                    PA[t] = __dsub_rn(P[t], A[t]);
+    if (i < nxp - CGFDM_HALO && j < nyp - CGFDM_HALO && k < nzp - CGFDM_HALO) {
+        auto at = [&](int a, int b, int c) { return ((long long)c * nyp + b) * nxp + a; };
+        long long p = at(i, j, k) * 3;
+        double P[3] = {coord[p], coord[p + 1], coord[p + 2]};
+        for (int ii = -1; ii <= 1; ii += 2)
+            for (int jj = -1; jj <= 1; jj += 2)
+                for (int kk = -1; kk <= 1; kk += 2) {
+                    long long a = at(i - ii, j, k) * 3, b = at(i, j - jj, k) * 3, c = at(i, j, k - kk) * 3;
+                    double A[3] = {coord[a], coord[a + 1], coord[a + 2]};
+                    double B[3] = {coord[b], coord[b + 1], coord[b + 2]};
+                    double C[3] = {coord[c], coord[c + 1], coord[c + 2]};
+                    double AB[3], AC[3], PA[3], n[3];
+                    for (int t = 0; t < 3; t++) {
+                        AB[t] = __dsub_rn(B[t], A[t]);
+                        AC[t] = __dsub_rn(C[t], A[t]);
+                        PA[t] = __dsub_rn(P[t], A[t]);
+                    }
+                    n[0] = __dsub_rn(__dmul_rn(AB[1], AC[2]), __dmul_rn(AB[2], AC[1]));
+                    n[1] = __dsub_rn(__dmul_rn(AB[2], AC[0]), __dmul_rn(AB[0], AC[2]));
+                    n[2] = __dsub_rn(__dmul_rn(AB[0], AC[1]), __dmul_rn(AB[1], AC[0]));
+                    double nd = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(n[0], n[0]), __dmul_rn(n[1], n[1])),
+                                                     __dmul_rn(n[2], n[2])));
+                    for (int t = 0; t < 3; t++) n[t] = __ddiv_rn(n[t], nd);
+                    double d = fabs(__dadd_rn(__dadd_rn(__dmul_rn(PA[0], n[0]), __dmul_rn(PA[1], n[1])),
+                                              __dmul_rn(PA[2], n[2])));
+                    lo = lo < d ? lo : d;
+                    hi = hi > d ? hi : d;
                 }
-                n[0] = __dsub_rn(__dmul_rn(AB[1], AC[2]), __dmul_rn(AB[2], AC[1]));
-                n[1] = __dsub_rn(__dmul_rn(AB[2], AC[0]), __dmul_rn(AB[0], AC[2]));
-                n[2] = __dsub_rn(__dmul_rn(AB[0], AC[1]), __dmul_rn(AB[1], AC[0]));
-                double nd = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(n[0], n[0]), __dmul_rn(n[1], n[1])),
-                                                 __dmul_rn(n[2], n[2])));
-                for (int t = 0; t < 3; t++) n[t] = __ddiv_rn(n[t], nd);
-                double d = fabs(__dadd_rn(__dadd_rn(__dmul_rn(PA[0], n[0]), __dmul_rn(PA[1], n[1])),
-                                          __dmul_rn(PA[2], n[2])));
-                lo = lo < d ? lo : d;
-                hi = hi > d ? hi : d;
-            }
-    atomicMin(hmin, (unsigned long long)__double_as_longlong(lo));
-    atomicMax(hmax, (unsigned long long)__double_as_longlong(hi));
+    }
+    // Warp reduction first, then one atomic pair per warp: a per-thread atomic
+    // on the same two words serialises the whole grid in L2.
+    for (int o = 16; o > 0; o >>= 1) {
+        double l2 = __shfl_xor_sync(0xffffffffu, lo, o), h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+        lo = lo < l2 ? lo : l2;
+        hi = hi > h2 ? hi : h2;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(hmin, (unsigned long long)__double_as_longlong(lo));
+        atomicMax(hmax, (unsigned long long)__double_as_longlong(hi));
+    }
 }
 
 // ----------------------------------------------------------------- util
