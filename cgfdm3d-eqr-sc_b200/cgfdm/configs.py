@@ -169,8 +169,13 @@ def halfspace(steps: int = 1000) -> cases.Case:
 
 
 def terrain_fault(directory: str, steps: int = 3000, NX: int = 400, NY: int = 400, NZ: int = 200,
-                  DH: float = 100.0, nPML: int = 12, seed: int = 2, courant: float = 0.8) -> Tuple[cases.Case, dict]:
-    """Writes the curvilinear finite-fault workload into ``directory``."""
+                  DH: float = 100.0, nPML: int = 12, seed: int = 2, courant: float = 0.8,
+                  scheme: str = "CGFDM", source: str = "fault") -> Tuple[cases.Case, dict]:
+    """Writes the curvilinear finite-fault workload into ``directory``.
+
+    ``source="double_couple"`` replaces the finite fault by a point double
+    couple 8 cells below the centre of the surface (for small grids, where
+    the rupture would not reach the grid within a short run)."""
     rng = np.random.default_rng(seed)
     os.makedirs(directory, exist_ok=True)
     terrain = gaussian_hills(NX, NY, DH, rng)
@@ -185,5 +190,9 @@ def terrain_fault(directory: str, steps: int = 3000, NX: int = 400, NY: int = 40
     c = cases.Case(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=DT, steps=steps, nPML=nPML, layers=(),
                    fault=fault, stations=surface_stations(NX, NY, NZ, nPML, 20),
                    extra={"terrainFile": "terrain.bin", "mediumFile": "medium.bin", "useMedium": 1})
-    cases.write_case(c, directory)
+    if source == "double_couple":
+        c.fault = []
+        c.double_couple = dict(X=NX // 2, Y=NY // 2, Z=NZ - 8, strike=30.0, dip=60.0, rake=90.0, Mw=4.0,
+                               duration=0.3)
+    cases.write_case(c, directory, scheme=scheme)
     return c, {"hmin": hmin, "vp_max": vp_max, "DT": DT}

@@ -64,6 +64,37 @@ size_t cg_stage_smem_bytes();
 cudaError_t make_field_tmap(void *out, const float *base, const DevGrid &g, int nf, bool halo_box);
 int cg_stage_ctas_per_sm();
 
+// ------------------------------------------------ SCFDM (ME-AWENO) stage
+// One directional pass of a TVD stage: x stores the RHS in H, y adds to it,
+// z adds its part and writes the TVD-RK3 update to Wout.
+struct ScDirArgs {
+    DevGrid g;
+    const float *W;      // stencil input of this stage
+    const float *Wm;     // values at the start of the step (stages 1, 2)
+    float *Wout;         // stage output (z pass)
+    float *H;            // RHS accumulator, 9 fields
+    const float *cjm;    // 19 fields
+    const float *sjac;   // DT * rDH / J per point
+    const float *decay;  // sponge factors G[0..ndecay] (z pass of the last stage), or null
+    int ndecay;
+    int irk;
+    int copy_halo;       // z pass of stages 0 and 1: carry the halo above the surface to Wout
+    float alpha;         // Lax-Friedrichs speed (largest Vp)
+    int npos, nl;        // tile shape, set by launch_sc_dir
+};
+struct ScTiling {
+    int npos[3], nl[3], ntiles[3];
+};
+ScTiling sc_tiling(const DevGrid &g);
+size_t sc_dir_smem_bytes(const ScTiling &t, int dir);
+cudaError_t sc_dir_prepare();
+cudaError_t launch_sc_dir(int dir, ScDirArgs a, const ScTiling &t, cudaStream_t st);
+// Characteristic free surface, halo extrapolation, sponge of the top layers
+// and peak ground velocity, after the third stage of a step.
+cudaError_t launch_sc_surface(float *W, const float *cjm, DevGrid g, const float *decayG, int ndecay, float *pgv,
+                              cudaStream_t st);
+cudaError_t launch_sc_sjac(const float *cjm, DevGrid g, float DT, float rDH, float *sjac, cudaStream_t st);
+
 // --------------------------------------------------- sources / stations
 struct FaultDev {
     const float *rate;        // [nt][npts][6], scaled

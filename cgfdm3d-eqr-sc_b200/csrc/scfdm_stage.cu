@@ -1,0 +1,578 @@
+// ME-AWENO (SCFDM) time stepping for sm_100a: alternative-flux WENO5
+// finite differences, TVD-RK3, characteristic free surface and
+// exponential-decay sponge.
+//
+// A TVD stage is three pencil kernels, one per grid direction.  Each CTA
+// owns a tile of `npos` consecutive positions along its direction (the tile's
+// points plus the 3 + 3 neighbours their flux differences reach) times `nl`
+// lanes across it, and runs three phases through shared memory:
+//
+//   A  every position m computes, per variable, both WENO5-JS states that
+//      are upwinded from the cell centred at m: the left state of face m+1/2
+//      and the right state of face m-1/2 (src/alternative_flux_FD.cpp:42-59
+//      called at 137-141).  The two states share their three smoothness
+//      indicators, so they are computed once per position.
+//   B  every face m+1/2 combines the left state of position m with the
+//      right state of position m+1 into the Lax-Friedrichs flux, with the
+//      metric and medium of point m (src/alternative_flux_FD.cpp:144-169).
+//   C  every point takes the flux difference with the fourth- and
+//      sixth-order corrections (cal_du_x/y/z, src/alternative_flux_FD.cpp:
+//      1215-1435), or in the top three layers the variant built from point
+//      fluxes (1257-1277).
+//
+// The x pass stores the RHS, the y pass adds to it and the z pass adds its
+// part and applies the TVD-RK3 update (src/wave_rk_tvd.cpp:17-78), so the
+// RHS accumulates in the reference's order.  After the third stage one
+// kernel per surface column applies the characteristic free surface and
+// extrapolates into the halo above it (src/freeSurface.cpp:40-194), the
+// sponge factor of the top layers (src/exp_decay_absorb.cpp:19-106; the z
+// pass of the last stage applies it below them) and the peak ground velocity
+// (src/PGV.cpp:61-175).
+//
+// Faces the reference never writes -- along each direction those before
+// index 2 and from _n on -- have zero flux, exactly as its zero-initialised
+// flux buffer gives.  Halo points keep their values through a TVD stage, so
+// stage buffers only need the top halo planes copied across.
+//
+// Built with CGFDM_EXACT (and --fmad=false) every float and double operation
+// of phases A-C and of the RK update follows the reference's expression
+// order, so the result is bit-identical.  The default build shares the
+// smoothness indicators between the two states of a position, combines the
+// two fluxes of a face before applying the (linear) flux function, and folds
+// the flux-difference corrections into one six-tap filter.
+#include "device.cuh"
+#include "kernels.cuh"
+
+namespace cgfdm {
+
+namespace {
+
+constexpr int SC_THREADS = 256;
+
+// ------------------------------------------------------------ WENO5-JS
+#ifdef CGFDM_EXACT
+// The reference's WENO5_JS term by term (src/alternative_flux_FD.cpp:42-59):
+// float polynomials, double (beta + 1e-6)^2 and the division by it.
+__device__ __forceinline__ float weno5_ref(float u1, float u2, float u3, float u4, float u5)
+{
+    float b1 = 10.0f * u3 * u3 - 31.0f * u3 * u4 + 25.0f * u4 * u4 + 11.0f * u3 * u5 - 19.0f * u4 * u5 +
+               4.0f * u5 * u5;
+    float b2 = 4.0f * u2 * u2 - 13.0f * u2 * u3 + 13.0f * u3 * u3 + 5.0f * u2 * u4 - 13.0f * u3 * u4 +
+               4.0f * u4 * u4;
+    float b3 = 4.0f * u1 * u1 - 19.0f * u1 * u2 + 25.0f * u2 * u2 + 11.0f * u1 * u3 - 31.0f * u2 * u3 +
+               10.0f * u3 * u3;
+    b1 = 0.3333333333f * b1;
+    b2 = 0.3333333333f * b2;
+    b3 = 0.3333333333f * b3;
+    double e1 = __dadd_rn((double)b1, 1e-6), e2 = __dadd_rn((double)b2, 1e-6), e3 = __dadd_rn((double)b3, 1e-6);
+    b1 = __double2float_rn(__ddiv_rn(0.3125, __dmul_rn(e1, e1)));
+    b2 = __double2float_rn(__ddiv_rn(0.625, __dmul_rn(e2, e2)));
+    b3 = __double2float_rn(__ddiv_rn(0.0625, __dmul_rn(e3, e3)));
+    float tw = __fdiv_rn(1.0f, b1 + b2 + b3);
+    return (b1 * tw) * (0.375f * u3 + 0.75f * u4 - 0.125f * u5) +
+           (b2 * tw) * (-0.125f * u2 + 0.75f * u3 + 0.375f * u4) +
+           (b3 * tw) * (0.375f * u1 - 1.25f * u2 + 1.875f * u3);
+}
+#else
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+#endif
+
+// Both states upwinded from the cell centred at c, window a b c d e:
+// uL at the face c+1/2, uR at the face c-1/2.
+__device__ __forceinline__ void weno_pair(float a, float b, float c, float d, float e, float &uL, float &uR)
+{
+#ifdef CGFDM_EXACT
+    uL = weno5_ref(a, b, c, d, e);
+    uR = weno5_ref(e, d, c, b, a);
+#else
+    // Jiang-Shu indicators over the cell of c for the sub-stencils
+    // (a,b,c), (b,c,d), (c,d,e): 13/12 (second difference)^2 + 1/4 (slope)^2
+    const float k13 = 13.0f / 12.0f;
+    const float s0 = (a - 2.0f * b) + c, t0 = (a - 4.0f * b) + 3.0f * c;
+    const float s1 = (b - 2.0f * c) + d, t1 = b - d;
+    const float s2 = (c - 2.0f * d) + e, t2 = (3.0f * c - 4.0f * d) + e;
+    const float B0 = k13 * s0 * s0 + 0.25f * t0 * t0 + 1e-6f;
+    const float B1 = k13 * s1 * s1 + 0.25f * t1 * t1 + 1e-6f;
+    const float B2 = k13 * s2 * s2 + 0.25f * t2 * t2 + 1e-6f;
+    const float r0 = rcp_approx(B0 * B0), r1 = rcp_approx(B1 * B1), r2 = rcp_approx(B2 * B2);
+    // linear weights 5/16, 10/16, 1/16 for the sub-stencil on the face side,
+    // the centred one and the far one (the common 1/16 cancels)
+    {
+        const float wa = 5.0f * r2, wb = 10.0f * r1, wc = r0;
+        const float qa = 0.375f * c + 0.75f * d - 0.125f * e;
+        const float qb = -0.125f * b + 0.75f * c + 0.375f * d;
+        const float qc = 0.375f * a - 1.25f * b + 1.875f * c;
+        uL = (wa * qa + wb * qb + wc * qc) * rcp_approx(wa + wb + wc);
+    }
+    {
+        const float wa = 5.0f * r0, wb = 10.0f * r1, wc = r2;
+        const float qa = 0.375f * c + 0.75f * b - 0.125f * a;
+        const float qb = -0.125f * d + 0.75f * c + 0.375f * b;
+        const float qc = 0.375f * e - 1.25f * d + 1.875f * c;
+        uR = (wa * qa + wb * qb + wc * qc) * rcp_approx(wa + wb + wc);
+    }
+#endif
+}
+
+// Physical flux along the metric row (n0, n1, n2) of the state u
+// (src/alternative_flux_FD.cpp:146-154; the same form is hu at 1259-1268).
+__device__ __forceinline__ void point_flux(float n0, float n1, float n2, float lam, float mu, float buo,
+                                           const float u[9], float f[9])
+{
+    f[0] = -(n0 * (lam * u[4] + lam * u[5] + u[3] * (lam + 2.0f * mu)) + mu * n1 * u[8] + mu * n2 * u[7]);
+    f[1] = -(n1 * (lam * u[3] + lam * u[5] + u[4] * (lam + 2.0f * mu)) + mu * n0 * u[8] + mu * n2 * u[6]);
+    f[2] = -(n2 * (lam * u[3] + lam * u[4] + u[5] * (lam + 2.0f * mu)) + mu * n0 * u[7] + mu * n1 * u[6]);
+    f[3] = -((n0 * u[0]) * buo);
+    f[4] = -((n1 * u[1]) * buo);
+    f[5] = -((n2 * u[2]) * buo);
+    f[6] = -((n1 * u[2]) * buo + (n2 * u[1]) * buo);
+    f[7] = -((n0 * u[2]) * buo + (n2 * u[0]) * buo);
+    f[8] = -((n0 * u[1]) * buo + (n1 * u[0]) * buo);
+}
+
+// Lax-Friedrichs flux of a face from its left (uL) and right (uR) states.
+__device__ __forceinline__ void lf_flux(float n0, float n1, float n2, float lam, float mu, float buo, float alpha,
+                                        const float uL[9], const float uR[9], float F[9])
+{
+#ifdef CGFDM_EXACT
+    float fL[9], fR[9];
+    point_flux(n0, n1, n2, lam, mu, buo, uL, fL);
+    point_flux(n0, n1, n2, lam, mu, buo, uR, fR);
+#pragma unroll
+    for (int v = 0; v < 9; v++) F[v] = 0.5f * (fR[v] + fL[v] - alpha * (uR[v] - uL[v]));
+#else
+    // the flux is linear in the state: f(uL) + f(uR) = f(uL + uR)
+    float s[9], fs[9];
+#pragma unroll
+    for (int v = 0; v < 9; v++) s[v] = uL[v] + uR[v];
+    const float tr = s[3] + s[4] + s[5], m2 = 2.0f * mu;
+    fs[0] = n0 * (lam * tr + m2 * s[3]) + mu * (n1 * s[8] + n2 * s[7]);
+    fs[1] = n1 * (lam * tr + m2 * s[4]) + mu * (n0 * s[8] + n2 * s[6]);
+    fs[2] = n2 * (lam * tr + m2 * s[5]) + mu * (n0 * s[7] + n1 * s[6]);
+    fs[3] = buo * (n0 * s[0]);
+    fs[4] = buo * (n1 * s[1]);
+    fs[5] = buo * (n2 * s[2]);
+    fs[6] = buo * (n1 * s[2] + n2 * s[1]);
+    fs[7] = buo * (n0 * s[2] + n2 * s[0]);
+    fs[8] = buo * (n0 * s[1] + n1 * s[0]);
+    const float ha = 0.5f * alpha;
+#pragma unroll
+    for (int v = 0; v < 9; v++) F[v] = -0.5f * fs[v] - ha * (uR[v] - uL[v]);
+#endif
+}
+
+// Exponential-decay factor product of an interior point, in the
+// reference's order x-low, x-high, y-low, y-high, z-low
+// (src/exp_decay_absorb.cpp:36-92; free surface on, so no z-high layer).
+__device__ __forceinline__ float decay_apply(float w, int i, int j, int k, const DevGrid &g, const float *G, int nl)
+{
+    const int X = i - CGFDM_HALO, Y = j - CGFDM_HALO, Z = k - CGFDM_HALO;
+    if (X <= nl) w = w * G[nl - X];
+    if (X >= g.nx - nl) w = w * G[nl - (g.nx - X)];
+    if (Y <= nl) w = w * G[nl - Y];
+    if (Y >= g.ny - nl) w = w * G[nl - (g.ny - Y)];
+    if (Z <= nl) w = w * G[nl - Z];
+    return w;
+}
+
+}  // namespace
+
+// ------------------------------------------------------- direction pass
+// DIR 0: tiles along x, lanes are rows j (grid: x tiles, row groups, k).
+// DIR 1: tiles along y, lanes are columns i (grid: column groups, y tiles, k).
+// DIR 2: tiles along z, lanes are columns i (grid: column groups, j, z tiles).
+template <int DIR>
+__global__ void __launch_bounds__(SC_THREADS) k_sc_dir(const ScDirArgs a)
+{
+    extern __shared__ __align__(16) float sm[];
+    const DevGrid g = a.g;
+    const long long F = g.fstride;
+    const int npos = a.npos, nl = a.nl, P = npos - 6;
+    float *sL = sm, *sR = sm + 9 * npos * nl;
+    const int _nx = g.nxp - CGFDM_HALO, _ny = g.nyp - CGFDM_HALO, _nz = g.nzp - CGFDM_HALO;
+    const int nd = DIR == 0 ? _nx : DIR == 1 ? _ny : _nz;  // points along DIR end before nd
+    const long long stride = DIR == 0 ? 1 : DIR == 1 ? (long long)g.pitch : g.plane;
+    const int tile = DIR == 0 ? blockIdx.x : DIR == 1 ? blockIdx.y : blockIdx.z;
+    const int p0 = CGFDM_HALO + tile * P;
+    // the fixed coordinate(s) and the lane base
+    const int lane0 = CGFDM_HALO + (DIR == 0 ? blockIdx.y : blockIdx.x) * nl;
+    const int lane_end = DIR == 0 ? _ny : _nx;
+    const int jfix = DIR == 2 ? CGFDM_HALO + (int)blockIdx.y : 0;
+    const int kfix = DIR == 2 ? 0 : CGFDM_HALO + (int)blockIdx.z;
+    const int mc0 = DIR == 0 ? C_XI_X : DIR == 1 ? C_ET_X : C_ZT_X;  // metric row of this direction
+
+    auto coords = [&](int m, int lane, int &i, int &j, int &k) {
+        if (DIR == 0) i = m, j = lane0 + lane, k = kfix;
+        else if (DIR == 1) i = lane0 + lane, j = m, k = kfix;
+        else i = lane0 + lane, j = jfix, k = m;
+    };
+    auto sidx = [&](int v, int mi, int lane) {
+        return DIR == 0 ? (v * nl + lane) * npos + mi : (v * npos + mi) * nl + lane;
+    };
+    auto split = [&](int it, int n_along, int &mi, int &lane) {
+        if (DIR == 0) mi = it % n_along, lane = it / n_along;
+        else lane = it % nl, mi = it / nl;
+    };
+
+    // ---- phase A: both WENO states of every position
+    for (int it = threadIdx.x; it < npos * nl; it += SC_THREADS) {
+        int mi, lane;
+        split(it, npos, mi, lane);
+        const int m = p0 - CGFDM_HALO + mi;
+        if (lane0 + lane >= lane_end || m < 2 || m > nd) continue;
+        int i, j, k;
+        coords(m, lane, i, j, k);
+        const float *w = a.W + g.at(i, j, k);
+#pragma unroll 1
+        for (int v = 0; v < 9; v++) {
+            const float *wv = w + v * F;
+            float uL, uR;
+            weno_pair(wv[-2 * stride], wv[-stride], wv[0], wv[stride], wv[2 * stride], uL, uR);
+            sL[sidx(v, mi, lane)] = uL;
+            sR[sidx(v, mi, lane)] = uR;
+        }
+    }
+    __syncthreads();
+
+    // ---- phase B: Lax-Friedrichs flux of face m+1/2, stored over the left state
+    for (int it = threadIdx.x; it < npos * nl; it += SC_THREADS) {
+        int mi, lane;
+        split(it, npos, mi, lane);
+        const int m = p0 - CGFDM_HALO + mi;
+        if (lane0 + lane >= lane_end || mi == npos - 1) continue;
+        float Fv[9];
+        if (m >= 2 && m < nd) {
+            int i, j, k;
+            coords(m, lane, i, j, k);
+            const long long q = g.at(i, j, k);
+            const float n0 = a.cjm[(mc0 + 0) * F + q], n1 = a.cjm[(mc0 + 1) * F + q], n2 = a.cjm[(mc0 + 2) * F + q];
+            const float mu = a.cjm[C_MU * F + q], lam = a.cjm[C_LAMBDA * F + q], buo = a.cjm[C_BUOY * F + q];
+            float uL[9], uR[9];
+#pragma unroll
+            for (int v = 0; v < 9; v++) uL[v] = sL[sidx(v, mi, lane)], uR[v] = sR[sidx(v, mi + 1, lane)];
+            lf_flux(n0, n1, n2, lam, mu, buo, a.alpha, uL, uR, Fv);
+        } else {
+#pragma unroll
+            for (int v = 0; v < 9; v++) Fv[v] = 0.0f;
+        }
+#pragma unroll
+        for (int v = 0; v < 9; v++) sL[sidx(v, mi, lane)] = Fv[v];
+    }
+    __syncthreads();
+
+    // ---- phase C: flux difference at the tile's points, then the pass's epilogue
+    const float c24 = 1.0f / 24, c7 = 7.0f / 5760;
+    for (int it = threadIdx.x; it < P * nl; it += SC_THREADS) {
+        int pi, lane;
+        split(it, P, pi, lane);
+        const int p = p0 + pi;
+        if (lane0 + lane >= lane_end || p >= nd) continue;
+        int i, j, k;
+        coords(p, lane, i, j, k);
+        const long long q = g.at(i, j, k);
+        const float coef = a.sjac[q];  // DT * rDH / J
+        float val[9];
+        if (k >= _nz - 3) {
+            // top three layers: corrections from point fluxes at p-3 .. p+3
+            // (src/alternative_flux_FD.cpp:1253-1279)
+            float o2A[9], o4A[9], o2B[9], o4B[9];
+            const float c2[6] = {-5.0f, 39.0f, -34.0f, -34.0f, 39.0f, -5.0f};
+            const float c4[6] = {1.0f, -3.0f, 2.0f, 2.0f, -3.0f, 1.0f};
+#pragma unroll 1
+            for (int n = 0; n < 7; n++) {
+                const long long qn = q + (n - 3) * stride;
+                float u[9], hu[9];
+#pragma unroll
+                for (int v = 0; v < 9; v++) u[v] = a.W[v * F + qn];
+                point_flux(a.cjm[(mc0 + 0) * F + qn], a.cjm[(mc0 + 1) * F + qn], a.cjm[(mc0 + 2) * F + qn],
+                           a.cjm[C_LAMBDA * F + qn], a.cjm[C_MU * F + qn], a.cjm[C_BUOY * F + qn], u, hu);
+#pragma unroll
+                for (int v = 0; v < 9; v++) {
+                    if (n <= 5) {  // B: hu[0..5]
+                        if (n == 0) o2B[v] = c2[0] * hu[v], o4B[v] = hu[v];
+                        else if (c2[n] < 0.0f) o2B[v] = o2B[v] - (-c2[n]) * hu[v];
+                        else o2B[v] = o2B[v] + c2[n] * hu[v];
+                        if (n > 0) {
+                            if (c4[n] < 0.0f) o4B[v] = o4B[v] - (-c4[n]) * hu[v];
+                            else if (n == 5) o4B[v] = o4B[v] + hu[v];
+                            else o4B[v] = o4B[v] + c4[n] * hu[v];
+                        }
+                    }
+                    if (n >= 1) {  // A: hu[1..6]
+                        const int t = n - 1;
+                        if (t == 0) o2A[v] = c2[0] * hu[v], o4A[v] = hu[v];
+                        else {
+                            if (c2[t] < 0.0f) o2A[v] = o2A[v] - (-c2[t]) * hu[v];
+                            else o2A[v] = o2A[v] + c2[t] * hu[v];
+                            if (c4[t] < 0.0f) o4A[v] = o4A[v] - (-c4[t]) * hu[v];
+                            else if (t == 5) o4A[v] = o4A[v] + hu[v];
+                            else o4A[v] = o4A[v] + c4[t] * hu[v];
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < 9; v++) {
+                const float Fp = sL[sidx(v, pi + 3, lane)], Fm = sL[sidx(v, pi + 2, lane)];
+                const float A = Fp - c24 * ((1.0f / 48) * o2A[v]) + c7 * ((1.0f / 2) * o4A[v]);
+                const float B = Fm - c24 * ((1.0f / 48) * o2B[v]) + c7 * ((1.0f / 2) * o4B[v]);
+                val[v] = coef * (-(A - B));
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < 9; v++) {
+                float f[6];
+#pragma unroll
+                for (int t = 0; t < 6; t++) f[t] = sL[sidx(v, pi + t, lane)];  // faces p-3 .. p+2
+#ifdef CGFDM_EXACT
+                // src/alternative_flux_FD.cpp:1283
+                const float A = f[3] - c24 * ((1.0f / 12) * ((((-f[1] + 16.0f * f[2]) - 30.0f * f[3]) + 16.0f * f[4]) - f[5])) +
+                                c7 * ((((f[1] - 4.0f * f[2]) + 6.0f * f[3]) - 4.0f * f[4]) + f[5]);
+                const float B = f[2] - c24 * ((1.0f / 12) * ((((-f[0] + 16.0f * f[1]) - 30.0f * f[2]) + 16.0f * f[3]) - f[4])) +
+                                c7 * ((((f[0] - 4.0f * f[1]) + 6.0f * f[2]) - 4.0f * f[3]) + f[4]);
+                val[v] = coef * (-(A - B));
+#else
+                // corrected face flux Fh = c2 F-2 + c1 F-1 + c0 F0 + c1 F+1 + c2 F+2 with
+                // c0 = 6402/5760, c1 = -348/5760, c2 = 27/5760; val = -coef (Fh[p] - Fh[p-1])
+                // = coef (c2 (F[p-3] - F[p+2]) + (c1 - c2) (F[p-2] - F[p+1]) + (c0 - c1) (F[p-1] - F[p]))
+                constexpr float e0 = 27.0f / 5760, e1 = (-348.0f - 27.0f) / 5760, e2 = (6402.0f + 348.0f) / 5760;
+                const float d = e0 * (f[0] - f[5]) + e1 * (f[1] - f[4]) + e2 * (f[2] - f[3]);
+                val[v] = coef * d;
+#endif
+            }
+        }
+
+        // ---- epilogue
+        if (DIR == 0) {
+#pragma unroll
+            for (int v = 0; v < 9; v++) a.H[v * F + q] = val[v];
+        } else if (DIR == 1) {
+#pragma unroll
+            for (int v = 0; v < 9; v++) a.H[v * F + q] = a.H[v * F + q] + val[v];
+        } else {
+            const bool decay = a.decay != nullptr && k < _nz - 4;
+#pragma unroll
+            for (int v = 0; v < 9; v++) {
+                const float h = a.H[v * F + q] + val[v];
+                const float w = a.W[v * F + q];
+                float o;
+                if (a.irk == 0) {
+                    o = w + h;  // src/wave_rk_tvd.cpp:26-33
+                } else if (a.irk == 1) {
+                    const double m = a.Wm[v * F + q];
+                    o = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.75, m), __dmul_rn(0.25, (double)w)),
+                                                    __dmul_rn(0.25, (double)h)));
+                } else {
+                    const double m = a.Wm[v * F + q];
+                    o = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(1.0 / 3.0, m), __dmul_rn(2.0 / 3.0, (double)w)),
+                                                    __dmul_rn(2.0 / 3.0, (double)h)));
+                }
+                if (decay) o = decay_apply(o, i, j, k, g, a.decay, a.ndecay);
+                a.Wout[v * F + q] = o;
+            }
+            // stage buffers take the halo above the surface along (src/wave_rk_tvd.cpp runs over
+            // every point and halo points have a zero RHS, so they keep their value)
+            if (a.copy_halo && k == _nz - 1)
+                for (int h = 1; h <= CGFDM_HALO; h++)
+                    for (int v = 0; v < 9; v++) a.Wout[v * F + q + h * g.plane] = a.W[v * F + q + h * g.plane];
+        }
+    }
+}
+
+// --------------------------------------------------------- free surface
+// One thread per surface column (src/freeSurface.cpp:40-194).  The
+// characteristic condition is restated with the inverse of the basis
+// B = [n s t]: T = B^-1 sigma B^-T and v' = B^-1 v are the stress and
+// velocity in that basis; after the condition, sigma = B T B^T, v = B v'.
+// Evaluated in double from the float fields and rounded once.
+__global__ void k_sc_surface(float *W, const float *__restrict__ cjm, DevGrid g, const float *__restrict__ decayG,
+                             int ndecay, float *pgv)
+{
+    const int i = CGFDM_HALO + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = CGFDM_HALO + blockIdx.y * blockDim.y + threadIdx.y;
+    const int _nx = g.nxp - CGFDM_HALO, _ny = g.nyp - CGFDM_HALO, _nz = g.nzp - CGFDM_HALO;
+    if (i >= _nx || j >= _ny) return;
+    const long long F = g.fstride;
+    const long long q = g.at(i, j, _nz - 1);
+    const float mu = cjm[C_MU * F + q], lam = cjm[C_LAMBDA * F + q], buo = cjm[C_BUOY * F + q];
+    const float rho = 1.0f / buo;
+    const float vs = sqrtf(mu * buo), vp = sqrtf((lam + 2.0f * mu) * buo);
+
+    // orthonormalised surface normal and the two tangent directions
+    const double jac = cjm[C_JAC * F + q];
+    double n[3] = {cjm[C_ZT_X * F + q] / jac, cjm[C_ZT_Y * F + q] / jac, cjm[C_ZT_Z * F + q] / jac};
+    double s[3] = {cjm[C_X_XI * F + q], cjm[C_Y_XI * F + q], cjm[C_Z_XI * F + q]};
+    double t[3] = {cjm[C_X_ET * F + q], cjm[C_Y_ET * F + q], cjm[C_Z_ET * F + q]};
+    auto normalise = [](double *x) {
+        double r = 1.0 / sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+        x[0] *= r, x[1] *= r, x[2] *= r;
+    };
+    normalise(n), normalise(s), normalise(t);
+    auto cross = [](const double *x, const double *y, double *o) {
+        o[0] = x[1] * y[2] - x[2] * y[1];
+        o[1] = x[2] * y[0] - x[0] * y[2];
+        o[2] = x[0] * y[1] - x[1] * y[0];
+    };
+    // rows of B^-1: (s x t, t x n, n x s) / det
+    double R[3][3];
+    cross(s, t, R[0]), cross(t, n, R[1]), cross(n, s, R[2]);
+    const double det = n[0] * R[0][0] + n[1] * R[0][1] + n[2] * R[0][2];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) R[r][c] /= det;
+
+    // conservative -> physical: stress from strain, velocity from momentum
+    double u[9];
+    for (int v = 0; v < 9; v++) u[v] = W[v * F + q];
+    const double L = lam, M = mu, Bu = buo;
+    const double tr = u[3] + u[4] + u[5];
+    double S[3][3];
+    S[0][0] = L * tr + 2.0 * M * u[3];
+    S[1][1] = L * tr + 2.0 * M * u[4];
+    S[2][2] = L * tr + 2.0 * M * u[5];
+    S[0][1] = S[1][0] = M * u[8];
+    S[0][2] = S[2][0] = M * u[7];
+    S[1][2] = S[2][1] = M * u[6];
+    const double vel[3] = {u[0] * Bu, u[1] * Bu, u[2] * Bu};
+
+    // into the (n, s, t) basis
+    double RS[3][3], T[3][3], vb[3];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) RS[r][c] = R[r][0] * S[0][c] + R[r][1] * S[1][c] + R[r][2] * S[2][c];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) T[r][c] = RS[r][0] * R[c][0] + RS[r][1] * R[c][1] + RS[r][2] * R[c][2];
+    for (int r = 0; r < 3; r++) vb[r] = R[r][0] * vel[0] + R[r][1] * vel[1] + R[r][2] * vel[2];
+
+    // characteristic free-surface condition (src/freeSurface.cpp:142-150)
+    const double rho_d = rho, vs_d = vs, vp_d = vp;
+    const double ratio = L / (L + 2.0 * M);
+    T[1][1] -= T[0][0] * ratio;
+    T[2][2] -= T[0][0] * ratio;
+    vb[1] -= T[0][1] / (vs_d * rho_d);
+    vb[2] -= T[0][2] / (vs_d * rho_d);
+    vb[0] -= T[0][0] / (vp_d * rho_d);
+    T[0][0] = 0.0, T[0][1] = T[1][0] = 0.0, T[0][2] = T[2][0] = 0.0;
+
+    // back: sigma = B T B^T, v = B v'
+    const double Bm[3][3] = {{n[0], s[0], t[0]}, {n[1], s[1], t[1]}, {n[2], s[2], t[2]}};
+    double BT[3][3], Sg[3][3], v2[3];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) BT[r][c] = Bm[r][0] * T[0][c] + Bm[r][1] * T[1][c] + Bm[r][2] * T[2][c];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) Sg[r][c] = BT[r][0] * Bm[c][0] + BT[r][1] * Bm[c][1] + BT[r][2] * Bm[c][2];
+    for (int r = 0; r < 3; r++) v2[r] = Bm[r][0] * vb[0] + Bm[r][1] * vb[1] + Bm[r][2] * vb[2];
+
+    // physical -> conservative: momentum, and strain by the isotropic compliance
+    const double comp = 1.0 / (2.0 * M * (3.0 * L + 2.0 * M));
+    const double strace = Sg[0][0] + Sg[1][1] + Sg[2][2];
+    double o[9];
+    o[0] = v2[0] * rho_d, o[1] = v2[1] * rho_d, o[2] = v2[2] * rho_d;
+    for (int d = 0; d < 3; d++) o[3 + d] = (2.0 * (L + M) * Sg[d][d] - L * (strace - Sg[d][d])) * comp;
+    o[6] = Sg[1][2] / M, o[7] = Sg[0][2] / M, o[8] = Sg[0][1] / M;
+    for (int v = 0; v < 9; v++) W[v * F + q] = (float)o[v];
+
+    // cubic extrapolation into the three halo layers above
+    // (src/freeSurface.cpp:180-190: extrap3 = 4 k1 - 6 k2 + 4 k3 - k4)
+    for (int v = 0; v < 9; v++) {
+        float *c = W + v * F + q;
+        for (int h = 1; h <= CGFDM_HALO; h++) {
+            const long long P = g.plane;
+            c[h * P] = 4.0f * c[(h - 1) * P] - 6.0f * c[(h - 2) * P] + 4.0f * c[(h - 3) * P] - c[(h - 4) * P];
+        }
+    }
+
+    // sponge factors of the top four layers (the z pass of the last stage
+    // did the layers below; the extrapolation above used values before it)
+    if (decayG)
+        for (int k = max(CGFDM_HALO, _nz - 4); k < _nz; k++) {
+            const long long qk = g.at(i, j, k);
+            for (int v = 0; v < 9; v++) W[v * F + qk] = decay_apply(W[v * F + qk], i, j, k, g, decayG, ndecay);
+        }
+
+    // peak ground velocity of the surface layer (src/PGV.cpp:115-137)
+    if (pgv) {
+        const float Vx = __fmul_rn(W[0 * F + q], buo), Vy = __fmul_rn(W[1 * F + q], buo),
+                    Vz = __fmul_rn(W[2 * F + q], buo);
+        const float Vh = __fsqrt_rn(__fadd_rn(__fmul_rn(Vx, Vx), __fmul_rn(Vy, Vy)));
+        const float V = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(Vx, Vx), __fmul_rn(Vy, Vy)), __fmul_rn(Vz, Vz)));
+        const long long pp = (long long)(i - CGFDM_HALO) + (long long)(j - CGFDM_HALO) * g.nx;
+        if (pgv[pp * 2 + 0] < Vh) pgv[pp * 2 + 0] = Vh;
+        if (pgv[pp * 2 + 1] < V) pgv[pp * 2 + 1] = V;
+    }
+}
+
+// DT * rDH / J per interior point, as cal_du forms it (jac = 1.0 / CJM[9]
+// in double, stored float; src/alternative_flux_FD.cpp:1251, 1283).
+__global__ void k_sc_sjac(const float *__restrict__ cjm, DevGrid g, float DT, float rDH, float *sjac)
+{
+    const int i = CGFDM_HALO + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = CGFDM_HALO + blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = CGFDM_HALO + blockIdx.z;
+    if (i >= g.nxp - CGFDM_HALO || j >= g.nyp - CGFDM_HALO) return;
+    const long long q = g.at(i, j, k);
+    const float jac = __double2float_rn(__ddiv_rn(1.0, (double)cjm[C_JAC * g.fstride + q]));
+    sjac[q] = __fmul_rn(__fmul_rn(DT, rDH), jac);
+}
+
+// ------------------------------------------------------------ launchers
+ScTiling sc_tiling(const DevGrid &g)
+{
+    ScTiling t;
+    // x: 64 positions x 4 rows; y, z: 80 positions x 16 columns
+    t.npos[0] = 64, t.nl[0] = 4;
+    t.npos[1] = 80, t.nl[1] = 16;
+    t.npos[2] = 80, t.nl[2] = 16;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    for (int d = 0; d < 3; d++) t.ntiles[d] = (n[d] + t.npos[d] - 7) / (t.npos[d] - 6);
+    return t;
+}
+
+size_t sc_dir_smem_bytes(const ScTiling &t, int dir) { return sizeof(float) * 18 * t.npos[dir] * t.nl[dir]; }
+
+cudaError_t sc_dir_prepare()
+{
+    size_t mx = 18 * 80 * 16 * sizeof(float);
+    CUDA_TRY(cudaFuncSetAttribute(k_sc_dir<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx));
+    CUDA_TRY(cudaFuncSetAttribute(k_sc_dir<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx));
+    CUDA_TRY(cudaFuncSetAttribute(k_sc_dir<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx));
+    return cudaSuccess;
+}
+
+cudaError_t launch_sc_dir(int dir, ScDirArgs a, const ScTiling &t, cudaStream_t st)
+{
+    const DevGrid &g = a.g;
+    a.npos = t.npos[dir], a.nl = t.nl[dir];
+    const size_t smem = sc_dir_smem_bytes(t, dir);
+    if (dir == 0) {
+        dim3 gr(t.ntiles[0], (g.ny + a.nl - 1) / a.nl, g.nz);
+        k_sc_dir<0><<<gr, SC_THREADS, smem, st>>>(a);
+    } else if (dir == 1) {
+        dim3 gr((g.nx + a.nl - 1) / a.nl, t.ntiles[1], g.nz);
+        k_sc_dir<1><<<gr, SC_THREADS, smem, st>>>(a);
+    } else {
+        dim3 gr((g.nx + a.nl - 1) / a.nl, g.ny, t.ntiles[2]);
+        k_sc_dir<2><<<gr, SC_THREADS, smem, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sc_surface(float *W, const float *cjm, DevGrid g, const float *decayG, int ndecay, float *pgv,
+                              cudaStream_t st)
+{
+    dim3 b(32, 4), gr((g.nx + 31) / 32, (g.ny + 3) / 4);
+    k_sc_surface<<<gr, b, 0, st>>>(W, cjm, g, decayG, ndecay, pgv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sc_sjac(const float *cjm, DevGrid g, float DT, float rDH, float *sjac, cudaStream_t st)
+{
+    dim3 b(32, 8), gr((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
+    k_sc_sjac<<<gr, b, 0, st>>>(cjm, g, DT, rDH, sjac);
+    return cudaGetLastError();
+}
+
+}  // namespace cgfdm

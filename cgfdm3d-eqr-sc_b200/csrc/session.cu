@@ -124,8 +124,23 @@ int Session::create(const std::string &dir, const std::string &options, int dev)
     device = dev;
     int st = build_model(dir, options, m, err);
     if (st) return st;
-    if (m.p.scheme != SCHEME_CGFDM) {
-        err = "scheme not available in this build";
+    // the reference builds that exist: CGFDM with PML (Makefile_CGFDM), SCFDM
+    // with the exponential sponge (Makefile_SCFDM); exp_decay_absorb.cpp only
+    // compiles under SCFDM and the SCFDM flux kernels take no PML terms
+    if (m.p.scheme == SCHEME_SCFDM && m.p.pml) {
+        err = "PML is not available with the SCFDM scheme (use EXP_DECAY)";
+        return ST_OPTIONS;
+    }
+    if (m.p.scheme == SCHEME_CGFDM && m.p.exp_decay) {
+        err = "EXP_DECAY is only available with the SCFDM scheme";
+        return ST_OPTIONS;
+    }
+    if (m.p.scheme == SCHEME_SCFDM && m.p.solve_displacement) {
+        err = "SOLVE_DISPLACEMENT is not available with the SCFDM scheme in this library";
+        return ST_OPTIONS;
+    }
+    if (m.p.scheme == SCHEME_SCFDM && m.g.nz < 8) {
+        err = "the SCFDM scheme needs NZ >= 8";
         return ST_OPTIONS;
     }
     CU(cudaSetDevice(dev));
@@ -191,6 +206,27 @@ int Session::setup_device()
             CU(make_field_tmap(maps_[b].wm, W_[0], g, 9, false));
             CU(make_field_tmap(maps_[b].t, W_[3], g, 9, false));
         }
+
+    // SCFDM: RHS accumulator, DT * rDH / J, sponge factors, pass tiling
+    if (!cg) {
+        ALLOC(h_, float, F * 9);
+        ALLOC(sjac_, float, F);
+        CU(launch_sc_sjac(cjm_, g, (float)m.p.DT, m.g.rDH, sjac_, stream));
+        CU(sc_dir_prepare());
+        sct_ = sc_tiling(g);
+        if (m.p.exp_decay) {
+            // G[p] = exp(-(alpha p)^2), p = 0 .. 20, in float as
+            // src/exp_decay_absorb.cpp:45,110-111 evaluates it
+            const float alpha = (float)0.015;
+            float G[SC_DECAY_LAYERS + 1];
+            for (int p = 0; p <= SC_DECAY_LAYERS; p++) {
+                const float x = alpha * (float)p;
+                G[p] = std::exp(-x * x);
+            }
+            ALLOC(decay_, float, SC_DECAY_LAYERS + 1);
+            CU(cudaMemcpyAsync(decay_, G, sizeof G, cudaMemcpyHostToDevice, stream));
+        }
+    }
 
     // PML profiles and auxiliaries
     if (cg && m.p.pml) {
@@ -356,6 +392,39 @@ int Session::launch_step(int step, bool timed_stages)
             FB1 = -FB1, FB2 = -FB2, FB3 = -FB3;
         }
         kernel_launches += 4;
+    } else {
+        // TVD-RK3: A -> B, (A, B) -> C, (A, C) -> A (src/propagate.cpp:212-244)
+        float *A = W_[0], *B = W_[1], *C = W_[2];
+        const float *win[3] = {A, B, C};
+        float *wout[3] = {B, C, A};
+        for (int irk = 0; irk < 3; irk++) {
+            ScDirArgs a{};
+            a.g = g;
+            a.W = win[irk];
+            a.Wm = A;
+            a.Wout = wout[irk];
+            a.H = h_;
+            a.cjm = cjm_;
+            a.sjac = sjac_;
+            a.decay = irk == 2 ? decay_ : nullptr;
+            a.ndecay = SC_DECAY_LAYERS;
+            a.irk = irk;
+            a.copy_halo = irk < 2;
+            a.alpha = m.Vp_max;
+            if (timed_stages) CU(cudaEventRecord(ev_[2], stream));
+            for (int dir = 0; dir < 3; dir++) CU(launch_sc_dir(dir, a, sct_, stream));
+            if (timed_stages) {
+                CU(cudaEventRecord(ev_[3], stream));
+                CU(cudaEventSynchronize(ev_[3]));
+                float ms = 0;
+                CU(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
+                stage_ms_sum_ += ms;
+                stage_ms_count_++;
+            }
+        }
+        // characteristic free surface, halo, top-layer sponge, PGV (src/propagate.cpp:245-290)
+        CU(launch_sc_surface(A, cjm_, g, decay_, SC_DECAY_LAYERS, pgv_, stream));
+        kernel_launches += 10;
     }
     if (nst > 0) {
         CU(launch_stations(W_[0], cjm_, g, st_idx_, nst, m.NT, st_out_, it_dev_, m.p.scheme, stream));
@@ -381,7 +450,8 @@ int Session::launch_steps_graph(int n8)
         graph8_src_ = gsrc;
         CU(cudaGraphInstantiate(&graph8_, graph8_src_, 0));
     }
-    long long per8 = 8LL * (4 + 1 + (fault_.npts > 0) + (point_.kind != 0 && point_.inside));
+    const int stage_launches = m.p.scheme == SCHEME_CGFDM ? 4 : 10;
+    long long per8 = 8LL * (stage_launches + 1 + (fault_.npts > 0) + (point_.kind != 0 && point_.inside));
     for (int r = 0; r < n8; r++) {
         CU(cudaGraphLaunch(graph8_, stream));
         graph_launches++;
@@ -473,6 +543,9 @@ double Session::algo_bytes_per_step() const
     const Grid &G = m.g;
     double n = (double)G.nx * G.ny * G.nz;
     double faces = 0;
+    // SCFDM: W_n + 13 metric/medium fields -> W1 (31 fields), then two stages
+    // reading the stage value, the metric and W_n and writing W (40 each)
+    if (m.p.scheme == SCHEME_SCFDM) return 4.0 * 111.0 * n;
     if (m.p.pml && m.p.scheme == SCHEME_CGFDM)
         faces = (double)G.nPML * (2.0 * G.ny * G.nz + 2.0 * G.nx * G.nz + (double)G.nx * G.ny);
     return 4.0 * (192.0 * n + 144.0 * faces);

@@ -71,6 +71,9 @@ private:
     int *work_dev_ = nullptr;                        // persistent-CTA work counters
     int ntx_ = 1, nty_ = 1, nchunk_ = 1, grid_ctas_ = 1;
     int *err_dev_ = nullptr;                         // device error word of the stage kernels
+    float *h_ = nullptr, *sjac_ = nullptr, *decay_ = nullptr;  // SCFDM RHS, DT*rDH/J, sponge factors
+    ScTiling sct_ = {};
+    static constexpr int SC_DECAY_LAYERS = 20;       // src/exp_decay_absorb.cpp:109
     int check_device_error();
 };
 

@@ -1,0 +1,88 @@
+"""ME-AWENO (SCFDM) parity: the CUDA library against the reference's own CPU
+build of the SCFDM scheme (oracle/_ref/scfdm_ref: WENO5-JS alternative-flux
+finite differences, Lax-Friedrichs flux, TVD-RK3, characteristic free
+surface, exponential-decay sponge).
+
+The metric and medium set-up must be bit-identical in both library builds.
+The time stepping is held to the north-star tolerance, 1e-5 relative L2 on
+the station seismograms (velocity components) and on the final wavefield:
+the library restates the characteristic free-surface rotation with the
+inverse of the surface basis in double precision instead of the
+reference's expanded float formulas, so neither build is bit-identical
+there, and the default build also shares the WENO smoothness indicators
+and folds the flux-difference corrections (different rounding, same
+arithmetic).
+"""
+
+import numpy as np
+import pytest
+
+import parity_util as pu
+import refrun
+from cgfdm import Session, cases
+
+TOL = 1e-5
+
+
+def _sc(mk):
+    return lambda d: cases.write_case(mk(), d, scheme="SCFDM")
+
+
+def _terrain_point(d):
+    from cgfdm import configs
+
+    # the benchmark's terrain and medium generators with a point double couple
+    configs.terrain_fault(d, steps=30, NX=40, NY=36, NZ=28, nPML=6, scheme="SCFDM", courant=0.5,
+                          source="double_couple")
+
+
+CASES = {
+    "halfspace": _sc(lambda: pu.small_halfspace(steps=40, courant=0.5)),
+    "gauss_hill": _sc(lambda: pu.small_hill(steps=40)),
+    "ricker_point": _sc(lambda: pu.ricker_point(steps=40, courant=0.5)),
+    "double_couple": _sc(lambda: pu.double_couple(steps=40, courant=0.5)),
+    "multi_fault": _sc(lambda: pu.multi_fault(steps=40, courant=0.5)),
+    "terrain_point": _terrain_point,
+}
+
+
+@pytest.fixture(scope="module")
+def ref_runs(tmp_path_factory):
+    if not refrun.available("SCFDM"):
+        pytest.skip("reference CPU build oracle/_ref/scfdm_ref not built")
+    root = tmp_path_factory.mktemp("sc")
+    out = {}
+    for name, write in CASES.items():
+        d = str(root / name)
+        write(d)
+        refrun.run(d, "SCFDM")
+        out[name] = (d, refrun.read_outputs(d, "SCFDM"))
+    return out
+
+
+def _lib(d, flavor):
+    s = Session(d, flavor=flavor)
+    assert s.info.scheme == 1
+    s.run(s.info.NT)
+    res = {"stations": s.stations(), "W": s.wavefield(), "CJM": s.cjm(), "PGV": s.pgv(), "info": s.info}
+    s.close()
+    return res
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flavor", ["exact", "fast"])
+@pytest.mark.parametrize("name", list(CASES))
+def test_scfdm_tolerance(ref_runs, name, flavor):
+    d, ref = ref_runs[name]
+    lib = _lib(d, flavor)
+    assert lib["info"].NT == ref["stations"].shape[1]
+    assert np.abs(ref["W"]).max() > 0.0 and np.abs(ref["stations"][:, :, :3]).max() > 0.0  # not a vacuous case
+    np.testing.assert_array_equal(lib["CJM"], ref["CJM"])
+    assert np.isfinite(lib["W"]).all()
+    e_st = pu.rel_l2(lib["stations"][:, :, :3], ref["stations"][:, :, :3])
+    e_w = pu.rel_l2(lib["W"], ref["W"])
+    e_pgv = pu.rel_l2(lib["PGV"], ref["PGV"])
+    print(f"{name} {flavor}: stations {e_st:.3e} W {e_w:.3e} PGV {e_pgv:.3e}")
+    assert e_st <= TOL, f"{name}: seismogram rel L2 {e_st:.3e}"
+    assert e_w <= TOL, f"{name}: wavefield rel L2 {e_w:.3e}"
+    assert e_pgv <= TOL, f"{name}: PGV rel L2 {e_pgv:.3e}"
