@@ -49,6 +49,7 @@ for p in (PKG, os.path.join(ROOT, "oracle")):
 METRIC = "Mpts*step/s"
 WORK = os.environ.get("CGFDM_BENCH_DIR", os.path.join(tempfile.gettempdir(), "cgfdm_bench"))
 SAMPLE_GRID = (160, 160, 100)
+SAMPLE_GRID_SC = (48, 48, 40)    # the reference's SCFDM CPU path is ~50x slower per point
 
 
 def peaks():
@@ -85,6 +86,11 @@ def make_workload(name, steps, directory):
     elif name.startswith("terrain_fault_"):
         nx, ny, nz = (int(v) for v in name.split("_")[-1].split("x"))
         configs.terrain_fault(directory, steps=steps, NX=nx, NY=ny, NZ=nz)
+    elif name == "aweno_basin":
+        configs.aweno_basin(directory, steps=steps)
+    elif name.startswith("aweno_basin_"):
+        nx, ny, nz = (int(v) for v in name.split("_")[-1].split("x"))
+        configs.aweno_basin(directory, steps=steps, NX=nx, NY=ny, NZ=nz)
     elif name == "halfspace":
         cases.write_case(configs.halfspace(steps=steps), directory)
     else:
@@ -100,7 +106,15 @@ def workload_desc(name):
                 "12-layer PML on 5 faces, FP32")
     if name == "halfspace":
         return "halfspace: CGFDM RK4, 128x128x96, DH=100 m, homogeneous half-space, Mxy point source, 16 stations"
+    if name == "aweno_basin":
+        return ("aweno_basin: ME-AWENO (SCFDM) TVD-RK3, 512x512x256 (67.1 Mpts interior), DH=50 m, 8-hill terrain, "
+                "6 dipping planar interfaces (Vs 1200-3600 m/s) + ellipsoidal basin Vs=400 m/s, 5 Hz Ricker point "
+                "source, 100 stations, exponential sponge, characteristic free surface, FP32")
     return name
+
+
+def is_scfdm(name):
+    return name.startswith("aweno")
 
 
 class ClockSampler:
@@ -163,10 +177,17 @@ def cpu_reference_rate(name, warmup_steps, timed_steps, procs):
     wall time of (warmup + timed) steps minus (warmup) steps, aggregate rate."""
     import refrun
 
-    if not refrun.available("CGFDM"):
-        return None, "reference CPU build (oracle/_ref/cgfdm_ref) not built"
-    nx, ny, nz = SAMPLE_GRID
-    sample_name = f"terrain_fault_{nx}x{ny}x{nz}" if name.startswith("terrain_fault") else name
+    if not refrun.available("SCFDM" if is_scfdm(name) else "CGFDM"):
+        return None, "reference CPU build (oracle/_ref) not built"
+    sc = is_scfdm(name)
+    nx, ny, nz = SAMPLE_GRID_SC if sc else SAMPLE_GRID
+    if name.startswith("terrain_fault"):
+        sample_name = f"terrain_fault_{nx}x{ny}x{nz}"
+    elif sc:
+        sample_name = f"aweno_basin_{nx}x{ny}x{nz}"
+    else:
+        sample_name = name
+    scheme = "SCFDM" if sc else "CGFDM"
     base = os.path.join(WORK, "cpu_sample")
     runs = {}
     for nt in (warmup_steps, warmup_steps + timed_steps):
@@ -183,7 +204,7 @@ def cpu_reference_rate(name, warmup_steps, timed_steps, procs):
                     os.symlink(src, os.path.join(c, f))
             copies.append(c)
         t0 = time.perf_counter()
-        ps = [subprocess.Popen(["taskset", "-c", str(p % os.cpu_count()), refrun.ref_binary("CGFDM")], cwd=c,
+        ps = [subprocess.Popen(["taskset", "-c", str(p % os.cpu_count()), refrun.ref_binary(scheme)], cwd=c,
                                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL) for p, c in enumerate(copies)]
         rcs = [p.wait() for p in ps]
         runs[nt] = time.perf_counter() - t0
@@ -192,7 +213,8 @@ def cpu_reference_rate(name, warmup_steps, timed_steps, procs):
     dt = runs[warmup_steps + timed_steps] - runs[warmup_steps]
     pts = nx * ny * nz
     rate = procs * pts * timed_steps / max(dt, 1e-9) / 1e6
-    sample = (f"reference CPU build (g++ -O2, single-threaded as shipped), {procs} concurrent processes pinned "
+    sample = (f"reference CPU build ({scheme}, g++ {'-O3' if sc else '-O2'}, single-threaded as shipped), "
+              f"{procs} concurrent processes pinned "
               f"one per core, each on the {nx}x{ny}x{nz} sub-grid of the workload (same generators), "
               f"{timed_steps} steps timed as wall({warmup_steps + timed_steps} steps) - wall({warmup_steps} steps)")
     return {"value": rate, "unit": METRIC, "cores": procs, "kind": "reference", "sample": sample}, None
@@ -226,7 +248,8 @@ def main():
         line = {"metric": METRIC, "value": cb["value"], "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
                 "steps": timed, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": workload_desc(args.workload), "sample_grid": "x".join(map(str, SAMPLE_GRID))},
+                "config": {"workload": workload_desc(args.workload),
+                           "sample_grid": "x".join(map(str, SAMPLE_GRID_SC if is_scfdm(args.workload) else SAMPLE_GRID))},
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
                                             "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -290,17 +313,21 @@ def main():
     hbm_peak, peak_kind = peaks()
     achieved = algo_launch / (stage_ms * 1e-3) / 1e9
     tr = traffic_ratio()
+    sc = is_scfdm(args.workload)
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scheme": "SCFDM" if sc else "CGFDM",
         "config": {"workload": workload_desc(args.workload), "points": pts, "DT": info.DT,
                    "l2": "inputs larger than L2 (model + wavefield %.1f GB resident)" % (info.device_bytes / 1e9),
                    "parallelism": f"replicas x{world}"},
         "hbm_gbs_algorithmic": algo_step * args.steps / (ms_max * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "peak_kind": peak_kind,
-                     "traffic": (tr * algo_launch if tr else None), "traffic_source": "ncu ratio on terrain_fault_256x256x128 x algorithmic bytes of this launch", "kernel": "k_cg_stage",
+                     "traffic": (tr * algo_launch if tr and not sc else None),
+                     "traffic_source": None if sc else "ncu ratio on terrain_fault_256x256x128 x algorithmic bytes of this launch",
+                     "kernel": "k_sc_dir x3 (one TVD stage)" if sc else "k_cg_stage",
                      "algo_bytes_per_launch": algo_launch, "mean_launch_ms": stage_ms},
         "e2e": {"value": world * pts * args.steps / e2e_s / 1e6, "unit": METRIC,
                 "h2d_bytes_per_step": i2.h2d_bytes / args.steps, "d2h_bytes_per_step": st.nbytes / args.steps,

@@ -12,6 +12,14 @@
                      correlated perturbations (correlation length 1 km), a
                      40x20 finite fault (strike 30, dip 60, rake 90, k^-2 slip,
                      rupture at 0.8 Vs), 400 surface stations, 3000 steps.
+* ``aweno_basin``    the ME-AWENO (SCFDM, TVD-RK3, exponential sponge)
+                     workload: 512x512x256, DH = 50 m, terrain as above, a
+                     discontinuous medium of seven layers separated by six
+                     planar interfaces with seeded dips up to 20 degrees
+                     (Vs 1200-3600 m/s, a 3:1 contrast), an ellipsoidal
+                     low-velocity basin (Vs = 400 m/s, semi-axes 8 x 5 x 1 km)
+                     under the centre of the surface, one 5 Hz Ricker point
+                     source, 100 surface stations, 4000 steps.
 
 Everything is drawn from numpy ``default_rng(seed)``.  The terrain and the
 heterogeneous medium are raw arrays ("terrainFile", "mediumFile"), which the
@@ -195,4 +203,64 @@ def terrain_fault(directory: str, steps: int = 3000, NX: int = 400, NY: int = 40
         c.double_couple = dict(X=NX // 2, Y=NY // 2, Z=NZ - 8, strike=30.0, dip=60.0, rake=90.0, Mw=4.0,
                                duration=0.3)
     cases.write_case(c, directory, scheme=scheme)
+    return c, {"hmin": hmin, "vp_max": vp_max, "DT": DT}
+
+
+def dipping_layers_basin(z: np.ndarray, NX: int, NY: int, DH: float, rng: np.random.Generator,
+                         n_interfaces: int = 6, max_dip_deg: float = 20.0, vs_range=(1200.0, 3600.0),
+                         basin_vs: float = 400.0, basin_axes_m=(8000.0, 5000.0, 1000.0)) -> np.ndarray:
+    """(Vs, Vp, rho) volume [nzp][nyp][nxp][3] with sharp planar dipping
+    interfaces and an ellipsoidal basin.  Interface i passes through depth
+    d_i under the grid centre with a seeded dip (<= max_dip_deg) and dip
+    direction; Vs rises layer by layer from vs_range[0] to vs_range[1];
+    Vp = 1.73 Vs, Gardner rho = 310 Vp^0.25.  The basin is centred under the
+    centre of the free surface and measured from the local surface."""
+    nzp, nyp, nxp = z.shape
+    x = ((np.arange(nxp) - HALO - NX // 2) * DH).astype(np.float64)
+    y = ((np.arange(nyp) - HALO - NY // 2) * DH).astype(np.float64)
+    ztop_col = z[-HALO - 1].astype(np.float64)                  # surface height per column
+    depth_total = float(ztop_col.max() - z[HALO].min())
+    d0 = np.sort(rng.uniform(0.08, 0.85, n_interfaces)) * depth_total
+    dips = np.radians(rng.uniform(0.0, max_dip_deg, n_interfaces))
+    az = rng.uniform(0.0, 2.0 * np.pi, n_interfaces)
+    vs_layers = np.sort(rng.uniform(vs_range[0], vs_range[1], n_interfaces + 1))
+    vs_layers[0], vs_layers[-1] = vs_range
+    X, Y = np.meshgrid(x, y)
+    zref = float(ztop_col.max())
+    vs = np.full(z.shape, vs_layers[0], np.float32)
+    for n in range(n_interfaces):
+        # interface depth below zref, a plane dipping along azimuth az
+        dint = d0[n] + np.tan(dips[n]) * (np.cos(az[n]) * X + np.sin(az[n]) * Y)
+        below = (zref - z) > dint[None, :, :]
+        vs[below] = vs_layers[n + 1]
+    ax, ay, az_ = basin_axes_m
+    dsurf = ztop_col[None, :, :] - z
+    inside = (X[None] / ax) ** 2 + (Y[None] / ay) ** 2 + (dsurf / az_) ** 2 <= 1.0
+    vs[inside] = basin_vs
+    vp = (vs * 1.73).astype(np.float32)
+    rho = (310.0 * vp.astype(np.float64) ** 0.25).astype(np.float32)
+    return np.stack([vs, vp, rho], -1).astype(np.float32)
+
+
+def aweno_basin(directory: str, steps: int = 4000, NX: int = 512, NY: int = 512, NZ: int = 256,
+                DH: float = 50.0, seed: int = 3, courant: float = 0.5, fc: float = 5.0,
+                n_side: int = 10) -> Tuple[cases.Case, dict]:
+    """Writes the ME-AWENO basin workload (SCFDM scheme) into ``directory``."""
+    rng = np.random.default_rng(seed)
+    os.makedirs(directory, exist_ok=True)
+    # hills scaled with the model: heights 200-1500 m, widths 2-8 km
+    terrain = gaussian_hills(NX, NY, DH, rng)
+    z = _coords_z(terrain, NZ, DH)
+    med = dipping_layers_basin(z, NX, NY, DH, rng)
+    vp_max = float(med[..., 1].max())
+    hmin = hmin_terrain(terrain, NX, NY, NZ, DH, NX // 2, NY // 2)
+    DT = cases.cfl_dt(DH, vp_max, courant, hmin=hmin)
+    terrain.tofile(os.path.join(directory, "terrain.bin"))
+    med.tofile(os.path.join(directory, "medium.bin"))
+    c = cases.Case(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=DT, steps=steps, nPML=12, layers=(), fault=[],
+                   stations=surface_stations(NX, NY, NZ, 20, n_side),
+                   extra={"terrainFile": "terrain.bin", "mediumFile": "medium.bin", "useMedium": 1})
+    # 2 km below the surface, or half the model depth on small grids
+    c.ricker_point = (NX // 2, NY // 2, NZ - 1 - min(int(round(2000.0 / DH)), NZ // 2), fc)
+    cases.write_case(c, directory, scheme="SCFDM")
     return c, {"hmin": hmin, "vp_max": vp_max, "DT": DT}

@@ -266,6 +266,45 @@ void oracle_hook_propagate(MPI_Comm comm_cart, MPI_COORD thisMPICoord, MPI_NEIGH
     oracle_dump("oracle_rDZ.bin", mat_rDZ._rDZ_DX, sizeof(float) * 2 * MATSIZE * grid._nx_ * grid._ny_);
 #endif
 #endif
+    /* scalars of the run as propagate() sees them (src/propagate.cpp:86-90) and,
+       for the restated oracle, the finite-fault table before its scaling */
+    {
+        char path[1024];
+        snprintf(path, sizeof(path), "%s/oracle_meta.txt", params.OUT);
+        FILE *fp = fopen(path, "w");
+        if (fp) {
+            float DT = params.DT;
+            int NT = params.TMAX / DT;
+            fprintf(fp, "nx %d\nny %d\nnz %d\nDT %.9g\nDH %.9g\nrDH %.9g\nNT %d\nnPML %d\n", grid.nx, grid.ny,
+                    grid.nz, DT, grid.DH, grid.rDH, NT, params.nPML);
+            fprintf(fp, "sourceX %d\nsourceY %d\nsourceZ %d\nrickerfc %.9g\nstrike %.9g\ndip %.9g\nrake %.9g\n"
+                        "Mw %.9g\nduration %.9g\n",
+                    params.sourceX, params.sourceY, params.sourceZ, params.rickerfc, params.strike, params.dip,
+                    params.rake, params.Mw, params.duration);
+            int kind = params.useMultiSource ? 3 : params.useSingleSource_ricker ? 1
+                                                 : params.useSingleSource_double_couple ? 2 : 0;
+            fprintf(fp, "src_kind %d\n", kind);
+#ifdef SCFDM
+            extern float vp_max_for_SCFDM;
+            fprintf(fp, "vp_max %.9g\n", vp_max_for_SCFDM);
+#endif
+            fclose(fp);
+        }
+        if (params.useMultiSource) {
+            long long npts = src_in.npts, nt = src_in.nt;
+            float dt = src_in.dt;
+            snprintf(path, sizeof(path), "%s/oracle_src.bin", params.OUT);
+            fp = fopen(path, "wb");
+            if (fp) {
+                fwrite(&npts, 8, 1, fp);
+                fwrite(&nt, 8, 1, fp);
+                fwrite(&dt, 4, 1, fp);
+                fwrite(srcIndex, 8, npts, fp);
+                fwrite(momentRate, 4, npts * nt * MOMSIZE, fp);
+                fclose(fp);
+            }
+        }
+    }
     propagate(comm_cart, thisMPICoord, mpiNeighbor, grid, params, wave, mat_rDZ, CJM, src_in, srcIndex,
               momentRate, momentRateSlice, slice, sliceData, sliceDataCpu);
 }

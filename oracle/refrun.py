@@ -49,6 +49,17 @@ def run(run_dir: str, scheme: str = "CGFDM", timeout: float = 3600.0, log: Optio
     return time.perf_counter() - t0
 
 
+def run_many(run_dirs, scheme: str = "CGFDM", timeout: float = 3600.0) -> None:
+    """Runs the reference binary in several run directories at once, one
+    process each (at most one per host core)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    workers = max(1, min(len(run_dirs), os.cpu_count() or 1))
+    with ThreadPoolExecutor(workers) as ex:
+        for f in [ex.submit(run, d, scheme, timeout) for d in run_dirs]:
+            f.result()
+
+
 def read_outputs(run_dir: str, scheme: str = "CGFDM") -> Dict[str, np.ndarray]:
     p = _params(run_dir)
     NX, NY, NZ = p["nx"], p["ny"], p["nz"]

@@ -48,13 +48,12 @@ def ref_runs(tmp_path_factory):
     if not refrun.available("CGFDM"):
         pytest.skip("reference CPU build oracle/_ref/cgfdm_ref not built")
     root = tmp_path_factory.mktemp("cg")
-    out = {}
+    dirs = {}
     for name, write in CASES.items():
-        d = str(root / name)
-        write(d)
-        refrun.run(d)
-        out[name] = (d, refrun.read_outputs(d))
-    return out
+        dirs[name] = str(root / name)
+        write(dirs[name])
+    refrun.run_many(list(dirs.values()), "CGFDM")
+    return {name: (d, refrun.read_outputs(d)) for name, d in dirs.items()}
 
 
 def _lib(d, flavor):

@@ -36,6 +36,13 @@ def _terrain_point(d):
                           source="double_couple")
 
 
+def _aweno_basin(d):
+    # the ME-AWENO benchmark's generators (dipping interfaces, basin, terrain) at a small size
+    from cgfdm import configs
+
+    configs.aweno_basin(d, steps=20, NX=40, NY=40, NZ=32, n_side=4)
+
+
 CASES = {
     "halfspace": _sc(lambda: pu.small_halfspace(steps=40, courant=0.5)),
     "gauss_hill": _sc(lambda: pu.small_hill(steps=40)),
@@ -43,6 +50,7 @@ CASES = {
     "double_couple": _sc(lambda: pu.double_couple(steps=40, courant=0.5)),
     "multi_fault": _sc(lambda: pu.multi_fault(steps=40, courant=0.5)),
     "terrain_point": _terrain_point,
+    "aweno_basin": _aweno_basin,
 }
 
 
@@ -51,13 +59,12 @@ def ref_runs(tmp_path_factory):
     if not refrun.available("SCFDM"):
         pytest.skip("reference CPU build oracle/_ref/scfdm_ref not built")
     root = tmp_path_factory.mktemp("sc")
-    out = {}
+    dirs = {}
     for name, write in CASES.items():
-        d = str(root / name)
-        write(d)
-        refrun.run(d, "SCFDM")
-        out[name] = (d, refrun.read_outputs(d, "SCFDM"))
-    return out
+        dirs[name] = str(root / name)
+        write(dirs[name])
+    refrun.run_many(list(dirs.values()), "SCFDM")
+    return {name: (d, refrun.read_outputs(d, "SCFDM")) for name, d in dirs.items()}
 
 
 def _lib(d, flavor):
