@@ -43,6 +43,9 @@ class Info(ctypes.Structure):
 
 
 def lib_path(flavor: str = "fast") -> str:
+    """lib/libcgfdm.so ("fast"), lib/libcgfdm_<flavor>.so, or an explicit .so path."""
+    if flavor.endswith(".so"):
+        return os.path.abspath(flavor)
     name = "libcgfdm.so" if flavor == "fast" else f"libcgfdm_{flavor}.so"
     return os.path.join(_LIBDIR, name)
 
@@ -67,6 +70,9 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
     L.cgfdm_get_cjm.argtypes = [vp, fp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)]
     L.cgfdm_get_pgv.argtypes = [vp, fp, ctypes.c_longlong]
     L.cgfdm_write_outputs.argtypes = [vp]
+    L.cgfdm_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.cgfdm_checkpoint.argtypes = [vp, vp, ctypes.c_longlong]
+    L.cgfdm_restore.argtypes = [vp, vp, ctypes.c_longlong]
     L.cgfdm_destroy.argtypes = [vp]
     L.cgfdm_last_error.argtypes = [vp]
     L.cgfdm_last_error.restype = ctypes.c_char_p
@@ -113,6 +119,19 @@ class Session:
         ms = ctypes.c_float()
         self._check(self.L.cgfdm_profile_stages(self._h, int(nsteps), ctypes.byref(ms)))
         return ms.value
+
+    def checkpoint(self) -> np.ndarray:
+        """The time-stepping state at the current step boundary (cgfdm_checkpoint)."""
+        n = ctypes.c_longlong()
+        self._check(self.L.cgfdm_checkpoint_size(self._h, ctypes.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        self._check(self.L.cgfdm_checkpoint(self._h, buf.ctypes.data_as(ctypes.c_void_p), buf.size))
+        return buf
+
+    def restore(self, buf: np.ndarray) -> None:
+        """Loads a checkpoint of a session of the same run directory (cgfdm_restore)."""
+        buf = np.ascontiguousarray(buf, np.uint8)
+        self._check(self.L.cgfdm_restore(self._h, buf.ctypes.data_as(ctypes.c_void_p), buf.size))
 
     def stations(self) -> np.ndarray:
         i = self.info

@@ -126,6 +126,25 @@ int cgfdm_write_outputs(const cgfdm_session *s)
     return s->s.write_outputs();
 }
 
+int cgfdm_checkpoint_size(const cgfdm_session *s, long long *bytes)
+{
+    if (!s || !bytes) return CGFDM_E_ARG;
+    *bytes = (long long)s->s.checkpoint_bytes();
+    return CGFDM_OK;
+}
+
+int cgfdm_checkpoint(cgfdm_session *s, void *out, long long bytes)
+{
+    if (!s || !out || bytes < 0) return CGFDM_E_ARG;
+    return s->s.checkpoint(out, (size_t)bytes);
+}
+
+int cgfdm_restore(cgfdm_session *s, const void *in, long long bytes)
+{
+    if (!s || !in || bytes < 0) return CGFDM_E_ARG;
+    return s->s.restore(in, (size_t)bytes);
+}
+
 int cgfdm_destroy(cgfdm_session *s)
 {
     delete s;

@@ -203,6 +203,37 @@ __global__ void k_from_aos(const float *__restrict__ in, int nf, DevGrid g, floa
     for (int f = 0; f < nf; f++) W[f * g.fstride + q] = in[n * nf + f];
 }
 
+// One plane of one field for the snapshot files (pack_iodata_x/y/z,
+// src/data_io.cpp:96-250): axis 0 is the plane i = idx laid out [nz][ny],
+// axis 1 the plane j = idx as [nz][nx], axis 2 the plane k = idx as [ny][nx].
+// SCFDM snapshots hold the velocity, momentum times buoyancy
+// (src/data_io.cpp:434-483).
+__global__ void k_pack_slice(const float *__restrict__ W, int nf, const float *__restrict__ cjm, DevGrid g,
+                             int axis, int idx, int comp, int scheme, float *out)
+{
+    const int a0 = blockIdx.x * blockDim.x + threadIdx.x, a1 = blockIdx.y * blockDim.y + threadIdx.y;
+    const int n0 = axis == 0 ? g.ny : g.nx, n1 = axis == 2 ? g.ny : g.nz;
+    if (a0 >= n0 || a1 >= n1) return;
+    int i, j, k;
+    if (axis == 0) i = idx, j = a0 + CGFDM_HALO, k = a1 + CGFDM_HALO;
+    else if (axis == 1) i = a0 + CGFDM_HALO, j = idx, k = a1 + CGFDM_HALO;
+    else i = a0 + CGFDM_HALO, j = a1 + CGFDM_HALO, k = idx;
+    const long long q = g.at(i, j, k);
+    float v = W[comp * g.fstride + q];
+    if (scheme == 1 && cjm) v = __fmul_rn(v, cjm[C_BUOY * g.fstride + q]);
+    out[(long long)a1 * n0 + a0] = v;
+    (void)nf;
+}
+
+cudaError_t launch_pack_slice(const float *W, const float *cjm, DevGrid g, int axis, int idx, int comp, int scheme,
+                              float *out, cudaStream_t st)
+{
+    const int n0 = axis == 0 ? g.ny : g.nx, n1 = axis == 2 ? g.ny : g.nz;
+    dim3 b(32, 8), gr((n0 + 31) / 32, (n1 + 7) / 8);
+    k_pack_slice<<<gr, b, 0, st>>>(W, 9, cjm, g, axis, idx, comp, scheme, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_to_aos(const float *W, int nf, DevGrid g, float *out, cudaStream_t st)
 {
     long long npad = (long long)g.nxp * g.nyp * g.nzp;

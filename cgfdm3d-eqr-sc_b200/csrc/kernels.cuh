@@ -59,10 +59,11 @@ struct CgStageMaps {
 cudaError_t launch_cg_stage(const CgStageArgs &a, const CgStageMaps &maps, int grid_ctas, cudaStream_t st);
 size_t cg_stage_smem_bytes();
 // Encodes the 4-D tensor map (x, y, z, field) of an nf-field buffer, with a
-// halo box (40 x 12 x 1 x nf) or a point box (32 x 8 x 1 x nf); out must hold
+// halo box (40 x (tile rows + 4) x 1 x nf) or a point box (32 x tile rows x 1 x nf); out must hold
 // 128 bytes.
 cudaError_t make_field_tmap(void *out, const float *base, const DevGrid &g, int nf, bool halo_box);
 int cg_stage_ctas_per_sm();
+int cg_stage_tile_y();
 
 // ------------------------------------------------ SCFDM (ME-AWENO) stage
 // One directional pass of a TVD stage: x stores the RHS in H, y adds to it,
@@ -86,7 +87,7 @@ struct ScTiling {
     int npos[3], nl[3], ntiles[3];
 };
 ScTiling sc_tiling(const DevGrid &g);
-size_t sc_dir_smem_bytes(const ScTiling &t, int dir);
+
 cudaError_t sc_dir_prepare();
 cudaError_t launch_sc_dir(int dir, ScDirArgs a, const ScTiling &t, cudaStream_t st);
 // Characteristic free surface, halo extrapolation, sponge of the top layers
@@ -121,6 +122,11 @@ cudaError_t launch_point(float *W, float *Wb, float *Wc, const float *cjm, DevGr
 // Records 9 components per station at step *it_dev, then advances *it_dev.
 cudaError_t launch_stations(const float *W, const float *cjm, DevGrid g, const int *st_idx, int nst, int NT,
                             float *out, int *it_dev, int scheme, cudaStream_t st);
+// One slice of field `comp` of W for the snapshot files: axis 0/1/2 = the
+// plane i/j/k = idx, in the reference's [nz][ny] / [nz][nx] / [ny][nx]
+// order; SCFDM (scheme 1, cjm given) converts momentum to velocity.
+cudaError_t launch_pack_slice(const float *W, const float *cjm, DevGrid g, int axis, int idx, int comp, int scheme,
+                              float *out, cudaStream_t st);
 // Gathers W (9 fields) into the reference AoS layout [_nz_][_ny_][_nx_][9].
 cudaError_t launch_to_aos(const float *W, int nfield, DevGrid g, float *out, cudaStream_t st);
 cudaError_t launch_from_aos(const float *in, int nfield, DevGrid g, float *W, cudaStream_t st);

@@ -182,57 +182,193 @@ __device__ __forceinline__ float decay_apply(float w, int i, int j, int k, const
 
 }  // namespace
 
-// ------------------------------------------------------- direction pass
-// DIR 0: tiles along x, lanes are rows j (grid: x tiles, row groups, k).
-// DIR 1: tiles along y, lanes are columns i (grid: column groups, y tiles, k).
-// DIR 2: tiles along z, lanes are columns i (grid: column groups, j, z tiles).
-template <int DIR>
-__global__ void __launch_bounds__(SC_THREADS) k_sc_dir(const ScDirArgs a)
+// Flux difference of one point in the top three layers: the corrections
+// come from point fluxes at p-3 .. p+3 along the direction
+// (src/alternative_flux_FD.cpp:1253-1279).  Fp, Fm: fluxes of the faces
+// p+1/2 and p-1/2.  Only three layers take this path, so it reads its
+// operands from global memory.
+__device__ __noinline__ void surface_diff(const ScDirArgs &a, long long q, long long stride, int mc0, float coef,
+                                          const float *Fp, const float *Fm, float *val)
 {
+    const long long F = a.g.fstride;
+    const float c24 = 1.0f / 24, c7 = 7.0f / 5760;
+    float o2A[9], o4A[9], o2B[9], o4B[9];
+    const float c2[6] = {-5.0f, 39.0f, -34.0f, -34.0f, 39.0f, -5.0f};
+    const float c4[6] = {1.0f, -3.0f, 2.0f, 2.0f, -3.0f, 1.0f};
+    for (int n = 0; n < 7; n++) {
+        const long long qn = q + (n - 3) * stride;
+        float u[9], hu[9];
+#pragma unroll
+        for (int v = 0; v < 9; v++) u[v] = a.W[v * F + qn];
+        point_flux(a.cjm[(mc0 + 0) * F + qn], a.cjm[(mc0 + 1) * F + qn], a.cjm[(mc0 + 2) * F + qn],
+                   a.cjm[C_LAMBDA * F + qn], a.cjm[C_MU * F + qn], a.cjm[C_BUOY * F + qn], u, hu);
+#pragma unroll
+        for (int v = 0; v < 9; v++) {
+            // o2 = -5 u1 + 39 u2 - 34 u3 - 34 u4 + 39 u5 - 5 u6, o4 = u1 - 3 u2 + 2 u3 + 2 u4 - 3 u5 + u6,
+            // accumulated left to right: B over hu[0..5], A over hu[1..6]
+            if (n <= 5) {
+                if (n == 0) o2B[v] = c2[0] * hu[v], o4B[v] = hu[v];
+                else {
+                    o2B[v] = c2[n] < 0.0f ? o2B[v] - (-c2[n]) * hu[v] : o2B[v] + c2[n] * hu[v];
+                    o4B[v] = c4[n] < 0.0f ? o4B[v] - (-c4[n]) * hu[v] : (n == 5 ? o4B[v] + hu[v] : o4B[v] + c4[n] * hu[v]);
+                }
+            }
+            if (n >= 1) {
+                const int t = n - 1;
+                if (t == 0) o2A[v] = c2[0] * hu[v], o4A[v] = hu[v];
+                else {
+                    o2A[v] = c2[t] < 0.0f ? o2A[v] - (-c2[t]) * hu[v] : o2A[v] + c2[t] * hu[v];
+                    o4A[v] = c4[t] < 0.0f ? o4A[v] - (-c4[t]) * hu[v] : (t == 5 ? o4A[v] + hu[v] : o4A[v] + c4[t] * hu[v]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 9; v++) {
+        const float A = Fp[v] - c24 * ((1.0f / 48) * o2A[v]) + c7 * ((1.0f / 2) * o4A[v]);
+        const float B = Fm[v] - c24 * ((1.0f / 48) * o2B[v]) + c7 * ((1.0f / 2) * o4B[v]);
+        val[v] = coef * (-(A - B));
+    }
+}
+
+// Flux difference of an interior point from the fluxes f[0..5] of the faces
+// p-5/2 .. p+5/2 (src/alternative_flux_FD.cpp:1283).
+__device__ __forceinline__ float interior_diff(const float f[6], float coef)
+{
+#ifdef CGFDM_EXACT
+    const float c24 = 1.0f / 24, c7 = 7.0f / 5760;
+    const float A = f[3] - c24 * ((1.0f / 12) * ((((-f[1] + 16.0f * f[2]) - 30.0f * f[3]) + 16.0f * f[4]) - f[5])) +
+                    c7 * ((((f[1] - 4.0f * f[2]) + 6.0f * f[3]) - 4.0f * f[4]) + f[5]);
+    const float B = f[2] - c24 * ((1.0f / 12) * ((((-f[0] + 16.0f * f[1]) - 30.0f * f[2]) + 16.0f * f[3]) - f[4])) +
+                    c7 * ((((f[0] - 4.0f * f[1]) + 6.0f * f[2]) - 4.0f * f[3]) + f[4]);
+    return coef * (-(A - B));
+#else
+    // corrected face flux Fh = c2 F-2 + c1 F-1 + c0 F0 + c1 F+1 + c2 F+2 with
+    // c0 = 6402/5760, c1 = -348/5760, c2 = 27/5760; val = -coef (Fh[p] - Fh[p-1])
+    // = coef (c2 (F[p-3] - F[p+2]) + (c1 - c2) (F[p-2] - F[p+1]) + (c0 - c1) (F[p-1] - F[p]))
+    constexpr float e0 = 27.0f / 5760, e1 = (-348.0f - 27.0f) / 5760, e2 = (6402.0f + 348.0f) / 5760;
+    return coef * (e0 * (f[0] - f[5]) + e1 * (f[1] - f[4]) + e2 * (f[2] - f[3]));
+#endif
+}
+
+// The pass's use of the flux difference val of point q = (i, j, k): the x
+// pass stores the RHS, the y pass adds to it, the z pass adds its part and
+// applies the TVD-RK3 update (src/wave_rk_tvd.cpp:17-78), the sponge below
+// the top four layers in the last stage, and carries the halo above the
+// surface into the stage buffer in stages 0 and 1 (the reference's update
+// runs over every point; halo points have a zero RHS and keep their value).
+template <int DIR>
+__device__ __forceinline__ void epilogue(const ScDirArgs &a, long long q, int i, int j, int k, const float val[9])
+{
+    const long long F = a.g.fstride;
+    if (DIR == 0) {
+#pragma unroll
+        for (int v = 0; v < 9; v++) a.H[v * F + q] = val[v];
+    } else if (DIR == 1) {
+#pragma unroll
+        for (int v = 0; v < 9; v++) a.H[v * F + q] = a.H[v * F + q] + val[v];
+    } else {
+        const int _nz = a.g.nzp - CGFDM_HALO;
+        const bool decay = a.decay != nullptr && k < _nz - 4;
+#pragma unroll
+        for (int v = 0; v < 9; v++) {
+            const float h = a.H[v * F + q] + val[v];
+            const float w = a.W[v * F + q];
+            float o;
+            if (a.irk == 0) {
+                o = w + h;
+            } else if (a.irk == 1) {
+                const double m = a.Wm[v * F + q];
+                o = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.75, m), __dmul_rn(0.25, (double)w)),
+                                                __dmul_rn(0.25, (double)h)));
+            } else {
+                const double m = a.Wm[v * F + q];
+                o = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(1.0 / 3.0, m), __dmul_rn(2.0 / 3.0, (double)w)),
+                                                __dmul_rn(2.0 / 3.0, (double)h)));
+            }
+            if (decay) o = decay_apply(o, i, j, k, a.g, a.decay, a.ndecay);
+            a.Wout[v * F + q] = o;
+        }
+        if (a.copy_halo && k == _nz - 1)
+            for (int h = 1; h <= CGFDM_HALO; h++)
+                for (int v = 0; v < 9; v++) a.Wout[v * F + q + h * a.g.plane] = a.W[v * F + q + h * a.g.plane];
+    }
+}
+
+// ------------------------------------------------------------ tiled pass
+// Tiles of NPOS positions along the pass direction (the tile's NPOS - 6
+// points and the neighbours their differences reach) times NL lanes across
+// it: rows j for the x pass (grid: x tiles, row groups, k), columns i for
+// the y and z passes (grid: column groups, y tiles, k / column groups, j,
+// z tiles).  Three phases through shared memory:
+//   A  both WENO states upwinded from every position,
+//   B  the Lax-Friedrichs flux of every face, written over the left states,
+//   C  the flux difference of every point and the pass's epilogue.
+constexpr int SCX_NPOS = 64, SCX_NL = 4;
+// y and z tiles: 32 positions (26 points) x 16 columns, 37 KB of shared
+// memory, five CTAs per SM (register cap 48); on the 512 x 512 x 256 basin
+// workload this beat 80 x 16 at two CTAs by 1.4x and a one-warp-per-pencil
+// register-streaming variant by 1.7x: the passes are latency-bound and
+// occupancy pays.
+#ifndef SCY_NPOS
+#define SCY_NPOS 32
+#endif
+#ifndef SCY_NL
+#define SCY_NL 16
+#endif
+
+#ifndef SC_TILE_MIN_CTAS
+#define SC_TILE_MIN_CTAS 5
+#endif
+
+template <int DIR, int NPOS, int NL>
+__global__ void __launch_bounds__(SC_THREADS, SC_TILE_MIN_CTAS) k_sc_tile(const ScDirArgs a)
+{
+    constexpr int P = NPOS - 6;
     extern __shared__ __align__(16) float sm[];
+    float *sL = sm, *sR = sm + 9 * NPOS * NL;
     const DevGrid g = a.g;
     const long long F = g.fstride;
-    const int npos = a.npos, nl = a.nl, P = npos - 6;
-    float *sL = sm, *sR = sm + 9 * npos * nl;
     const int _nx = g.nxp - CGFDM_HALO, _ny = g.nyp - CGFDM_HALO, _nz = g.nzp - CGFDM_HALO;
-    const int nd = DIR == 0 ? _nx : DIR == 1 ? _ny : _nz;  // points along DIR end before nd
+    const int nd = DIR == 0 ? _nx : DIR == 1 ? _ny : _nz;  // points along the pass end before nd
     const long long stride = DIR == 0 ? 1 : DIR == 1 ? (long long)g.pitch : g.plane;
     const int tile = DIR == 0 ? blockIdx.x : DIR == 1 ? blockIdx.y : blockIdx.z;
     const int p0 = CGFDM_HALO + tile * P;
-    // the fixed coordinate(s) and the lane base
-    const int lane0 = CGFDM_HALO + (DIR == 0 ? blockIdx.y : blockIdx.x) * nl;
+    const int lane0 = CGFDM_HALO + (DIR == 0 ? blockIdx.y : blockIdx.x) * NL;
     const int lane_end = DIR == 0 ? _ny : _nx;
     const int jfix = DIR == 2 ? CGFDM_HALO + (int)blockIdx.y : 0;
     const int kfix = DIR == 2 ? 0 : CGFDM_HALO + (int)blockIdx.z;
-    const int mc0 = DIR == 0 ? C_XI_X : DIR == 1 ? C_ET_X : C_ZT_X;  // metric row of this direction
+    constexpr int mc0 = DIR == 0 ? C_XI_X : DIR == 1 ? C_ET_X : C_ZT_X;  // metric row of this direction
 
     auto coords = [&](int m, int lane, int &i, int &j, int &k) {
         if (DIR == 0) i = m, j = lane0 + lane, k = kfix;
         else if (DIR == 1) i = lane0 + lane, j = m, k = kfix;
         else i = lane0 + lane, j = jfix, k = m;
     };
-    auto sidx = [&](int v, int mi, int lane) {
-        return DIR == 0 ? (v * nl + lane) * npos + mi : (v * npos + mi) * nl + lane;
+    // consecutive threads take consecutive x: positions for the x pass, lanes otherwise
+    auto sidx = [](int v, int mi, int lane) {
+        return DIR == 0 ? (v * NL + lane) * NPOS + mi : (v * NPOS + mi) * NL + lane;
     };
-    auto split = [&](int it, int n_along, int &mi, int &lane) {
+    auto split = [](int it, int n_along, int &mi, int &lane) {
         if (DIR == 0) mi = it % n_along, lane = it / n_along;
-        else lane = it % nl, mi = it / nl;
+        else lane = it % NL, mi = it / NL;
     };
 
     // ---- phase A: both WENO states of every position
-    for (int it = threadIdx.x; it < npos * nl; it += SC_THREADS) {
+    for (int it = threadIdx.x; it < NPOS * NL; it += SC_THREADS) {
         int mi, lane;
-        split(it, npos, mi, lane);
+        split(it, NPOS, mi, lane);
         const int m = p0 - CGFDM_HALO + mi;
         if (lane0 + lane >= lane_end || m < 2 || m > nd) continue;
         int i, j, k;
         coords(m, lane, i, j, k);
         const float *w = a.W + g.at(i, j, k);
-#pragma unroll 1
+#pragma unroll 3
         for (int v = 0; v < 9; v++) {
             const float *wv = w + v * F;
             float uL, uR;
-            weno_pair(wv[-2 * stride], wv[-stride], wv[0], wv[stride], wv[2 * stride], uL, uR);
+            weno_pair(__ldg(wv - 2 * stride), __ldg(wv - stride), __ldg(wv), __ldg(wv + stride), __ldg(wv + 2 * stride),
+                      uL, uR);
             sL[sidx(v, mi, lane)] = uL;
             sR[sidx(v, mi, lane)] = uR;
         }
@@ -240,11 +376,11 @@ __global__ void __launch_bounds__(SC_THREADS) k_sc_dir(const ScDirArgs a)
     __syncthreads();
 
     // ---- phase B: Lax-Friedrichs flux of face m+1/2, stored over the left state
-    for (int it = threadIdx.x; it < npos * nl; it += SC_THREADS) {
+    for (int it = threadIdx.x; it < NPOS * NL; it += SC_THREADS) {
         int mi, lane;
-        split(it, npos, mi, lane);
+        split(it, NPOS, mi, lane);
         const int m = p0 - CGFDM_HALO + mi;
-        if (lane0 + lane >= lane_end || mi == npos - 1) continue;
+        if (lane0 + lane >= lane_end || mi == NPOS - 1) continue;
         float Fv[9];
         if (m >= 2 && m < nd) {
             int i, j, k;
@@ -265,9 +401,8 @@ __global__ void __launch_bounds__(SC_THREADS) k_sc_dir(const ScDirArgs a)
     }
     __syncthreads();
 
-    // ---- phase C: flux difference at the tile's points, then the pass's epilogue
-    const float c24 = 1.0f / 24, c7 = 7.0f / 5760;
-    for (int it = threadIdx.x; it < P * nl; it += SC_THREADS) {
+    // ---- phase C: flux difference at the tile's points
+    for (int it = threadIdx.x; it < P * NL; it += SC_THREADS) {
         int pi, lane;
         split(it, P, pi, lane);
         const int p = p0 + pi;
@@ -278,109 +413,20 @@ __global__ void __launch_bounds__(SC_THREADS) k_sc_dir(const ScDirArgs a)
         const float coef = a.sjac[q];  // DT * rDH / J
         float val[9];
         if (k >= _nz - 3) {
-            // top three layers: corrections from point fluxes at p-3 .. p+3
-            // (src/alternative_flux_FD.cpp:1253-1279)
-            float o2A[9], o4A[9], o2B[9], o4B[9];
-            const float c2[6] = {-5.0f, 39.0f, -34.0f, -34.0f, 39.0f, -5.0f};
-            const float c4[6] = {1.0f, -3.0f, 2.0f, 2.0f, -3.0f, 1.0f};
-#pragma unroll 1
-            for (int n = 0; n < 7; n++) {
-                const long long qn = q + (n - 3) * stride;
-                float u[9], hu[9];
+            float Fp[9], Fm[9];
 #pragma unroll
-                for (int v = 0; v < 9; v++) u[v] = a.W[v * F + qn];
-                point_flux(a.cjm[(mc0 + 0) * F + qn], a.cjm[(mc0 + 1) * F + qn], a.cjm[(mc0 + 2) * F + qn],
-                           a.cjm[C_LAMBDA * F + qn], a.cjm[C_MU * F + qn], a.cjm[C_BUOY * F + qn], u, hu);
-#pragma unroll
-                for (int v = 0; v < 9; v++) {
-                    if (n <= 5) {  // B: hu[0..5]
-                        if (n == 0) o2B[v] = c2[0] * hu[v], o4B[v] = hu[v];
-                        else if (c2[n] < 0.0f) o2B[v] = o2B[v] - (-c2[n]) * hu[v];
-                        else o2B[v] = o2B[v] + c2[n] * hu[v];
-                        if (n > 0) {
-                            if (c4[n] < 0.0f) o4B[v] = o4B[v] - (-c4[n]) * hu[v];
-                            else if (n == 5) o4B[v] = o4B[v] + hu[v];
-                            else o4B[v] = o4B[v] + c4[n] * hu[v];
-                        }
-                    }
-                    if (n >= 1) {  // A: hu[1..6]
-                        const int t = n - 1;
-                        if (t == 0) o2A[v] = c2[0] * hu[v], o4A[v] = hu[v];
-                        else {
-                            if (c2[t] < 0.0f) o2A[v] = o2A[v] - (-c2[t]) * hu[v];
-                            else o2A[v] = o2A[v] + c2[t] * hu[v];
-                            if (c4[t] < 0.0f) o4A[v] = o4A[v] - (-c4[t]) * hu[v];
-                            else if (t == 5) o4A[v] = o4A[v] + hu[v];
-                            else o4A[v] = o4A[v] + c4[t] * hu[v];
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int v = 0; v < 9; v++) {
-                const float Fp = sL[sidx(v, pi + 3, lane)], Fm = sL[sidx(v, pi + 2, lane)];
-                const float A = Fp - c24 * ((1.0f / 48) * o2A[v]) + c7 * ((1.0f / 2) * o4A[v]);
-                const float B = Fm - c24 * ((1.0f / 48) * o2B[v]) + c7 * ((1.0f / 2) * o4B[v]);
-                val[v] = coef * (-(A - B));
-            }
+            for (int v = 0; v < 9; v++) Fp[v] = sL[sidx(v, pi + 3, lane)], Fm[v] = sL[sidx(v, pi + 2, lane)];
+            surface_diff(a, q, stride, mc0, coef, Fp, Fm, val);
         } else {
 #pragma unroll
             for (int v = 0; v < 9; v++) {
                 float f[6];
 #pragma unroll
-                for (int t = 0; t < 6; t++) f[t] = sL[sidx(v, pi + t, lane)];  // faces p-3 .. p+2
-#ifdef CGFDM_EXACT
-                // src/alternative_flux_FD.cpp:1283
-                const float A = f[3] - c24 * ((1.0f / 12) * ((((-f[1] + 16.0f * f[2]) - 30.0f * f[3]) + 16.0f * f[4]) - f[5])) +
-                                c7 * ((((f[1] - 4.0f * f[2]) + 6.0f * f[3]) - 4.0f * f[4]) + f[5]);
-                const float B = f[2] - c24 * ((1.0f / 12) * ((((-f[0] + 16.0f * f[1]) - 30.0f * f[2]) + 16.0f * f[3]) - f[4])) +
-                                c7 * ((((f[0] - 4.0f * f[1]) + 6.0f * f[2]) - 4.0f * f[3]) + f[4]);
-                val[v] = coef * (-(A - B));
-#else
-                // corrected face flux Fh = c2 F-2 + c1 F-1 + c0 F0 + c1 F+1 + c2 F+2 with
-                // c0 = 6402/5760, c1 = -348/5760, c2 = 27/5760; val = -coef (Fh[p] - Fh[p-1])
-                // = coef (c2 (F[p-3] - F[p+2]) + (c1 - c2) (F[p-2] - F[p+1]) + (c0 - c1) (F[p-1] - F[p]))
-                constexpr float e0 = 27.0f / 5760, e1 = (-348.0f - 27.0f) / 5760, e2 = (6402.0f + 348.0f) / 5760;
-                const float d = e0 * (f[0] - f[5]) + e1 * (f[1] - f[4]) + e2 * (f[2] - f[3]);
-                val[v] = coef * d;
-#endif
+                for (int t = 0; t < 6; t++) f[t] = sL[sidx(v, pi + t, lane)];  // faces p-5/2 .. p+5/2
+                val[v] = interior_diff(f, coef);
             }
         }
-
-        // ---- epilogue
-        if (DIR == 0) {
-#pragma unroll
-            for (int v = 0; v < 9; v++) a.H[v * F + q] = val[v];
-        } else if (DIR == 1) {
-#pragma unroll
-            for (int v = 0; v < 9; v++) a.H[v * F + q] = a.H[v * F + q] + val[v];
-        } else {
-            const bool decay = a.decay != nullptr && k < _nz - 4;
-#pragma unroll
-            for (int v = 0; v < 9; v++) {
-                const float h = a.H[v * F + q] + val[v];
-                const float w = a.W[v * F + q];
-                float o;
-                if (a.irk == 0) {
-                    o = w + h;  // src/wave_rk_tvd.cpp:26-33
-                } else if (a.irk == 1) {
-                    const double m = a.Wm[v * F + q];
-                    o = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.75, m), __dmul_rn(0.25, (double)w)),
-                                                    __dmul_rn(0.25, (double)h)));
-                } else {
-                    const double m = a.Wm[v * F + q];
-                    o = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(1.0 / 3.0, m), __dmul_rn(2.0 / 3.0, (double)w)),
-                                                    __dmul_rn(2.0 / 3.0, (double)h)));
-                }
-                if (decay) o = decay_apply(o, i, j, k, g, a.decay, a.ndecay);
-                a.Wout[v * F + q] = o;
-            }
-            // stage buffers take the halo above the surface along (src/wave_rk_tvd.cpp runs over
-            // every point and halo points have a zero RHS, so they keep their value)
-            if (a.copy_halo && k == _nz - 1)
-                for (int h = 1; h <= CGFDM_HALO; h++)
-                    for (int v = 0; v < 9; v++) a.Wout[v * F + q + h * g.plane] = a.W[v * F + q + h * g.plane];
-        }
+        epilogue<DIR>(a, q, i, j, k, val);
     }
 }
 
@@ -522,23 +568,26 @@ __global__ void k_sc_sjac(const float *__restrict__ cjm, DevGrid g, float DT, fl
 ScTiling sc_tiling(const DevGrid &g)
 {
     ScTiling t;
-    // x: 64 positions x 4 rows; y, z: 80 positions x 16 columns
-    t.npos[0] = 64, t.nl[0] = 4;
-    t.npos[1] = 80, t.nl[1] = 16;
-    t.npos[2] = 80, t.nl[2] = 16;
-    const int n[3] = {g.nx, g.ny, g.nz};
-    for (int d = 0; d < 3; d++) t.ntiles[d] = (n[d] + t.npos[d] - 7) / (t.npos[d] - 6);
+    t.npos[0] = SCX_NPOS, t.nl[0] = SCX_NL;
+    t.ntiles[0] = (g.nx + SCX_NPOS - 7) / (SCX_NPOS - 6);
+    t.npos[1] = t.npos[2] = SCY_NPOS, t.nl[1] = t.nl[2] = SCY_NL;
+    t.ntiles[1] = (g.ny + SCY_NPOS - 7) / (SCY_NPOS - 6);
+    t.ntiles[2] = (g.nz + SCY_NPOS - 7) / (SCY_NPOS - 6);
     return t;
 }
 
-size_t sc_dir_smem_bytes(const ScTiling &t, int dir) { return sizeof(float) * 18 * t.npos[dir] * t.nl[dir]; }
+template <int DIR, int NPOS, int NL>
+static cudaError_t tile_attr()
+{
+    return cudaFuncSetAttribute(k_sc_tile<DIR, NPOS, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(float) * 18 * NPOS * NL));
+}
 
 cudaError_t sc_dir_prepare()
 {
-    size_t mx = 18 * 80 * 16 * sizeof(float);
-    CUDA_TRY(cudaFuncSetAttribute(k_sc_dir<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx));
-    CUDA_TRY(cudaFuncSetAttribute(k_sc_dir<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx));
-    CUDA_TRY(cudaFuncSetAttribute(k_sc_dir<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx));
+    CUDA_TRY((tile_attr<0, SCX_NPOS, SCX_NL>()));
+    CUDA_TRY((tile_attr<1, SCY_NPOS, SCY_NL>()));
+    CUDA_TRY((tile_attr<2, SCY_NPOS, SCY_NL>()));
     return cudaSuccess;
 }
 
@@ -546,16 +595,18 @@ cudaError_t launch_sc_dir(int dir, ScDirArgs a, const ScTiling &t, cudaStream_t 
 {
     const DevGrid &g = a.g;
     a.npos = t.npos[dir], a.nl = t.nl[dir];
-    const size_t smem = sc_dir_smem_bytes(t, dir);
     if (dir == 0) {
-        dim3 gr(t.ntiles[0], (g.ny + a.nl - 1) / a.nl, g.nz);
-        k_sc_dir<0><<<gr, SC_THREADS, smem, st>>>(a);
-    } else if (dir == 1) {
-        dim3 gr((g.nx + a.nl - 1) / a.nl, t.ntiles[1], g.nz);
-        k_sc_dir<1><<<gr, SC_THREADS, smem, st>>>(a);
+        dim3 gr(t.ntiles[0], (g.ny + SCX_NL - 1) / SCX_NL, g.nz);
+        k_sc_tile<0, SCX_NPOS, SCX_NL><<<gr, SC_THREADS, sizeof(float) * 18 * SCX_NPOS * SCX_NL, st>>>(a);
     } else {
-        dim3 gr((g.nx + a.nl - 1) / a.nl, g.ny, t.ntiles[2]);
-        k_sc_dir<2><<<gr, SC_THREADS, smem, st>>>(a);
+        const size_t smem = sizeof(float) * 18 * SCY_NPOS * SCY_NL;
+        if (dir == 1) {
+            dim3 gr((g.nx + SCY_NL - 1) / SCY_NL, t.ntiles[1], g.nz);
+            k_sc_tile<1, SCY_NPOS, SCY_NL><<<gr, SC_THREADS, smem, st>>>(a);
+        } else {
+            dim3 gr((g.nx + SCY_NL - 1) / SCY_NL, g.ny, t.ntiles[2]);
+            k_sc_tile<2, SCY_NPOS, SCY_NL><<<gr, SC_THREADS, smem, st>>>(a);
+        }
     }
     return cudaGetLastError();
 }

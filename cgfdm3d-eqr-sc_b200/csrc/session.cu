@@ -310,13 +310,13 @@ int Session::setup_device()
         point_.stf = d_stf;
     }
 
-    // work items for the persistent stage kernel: 32 x 8 column tiles times
+    // work items for the persistent stage kernel: 32-column tiles times
     // z-chunks of about 32 planes, at least four items per resident CTA so
     // the dynamic schedule ends evenly
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
     ntx_ = (G.nx + 31) / 32;
-    nty_ = (G.ny + 7) / 8;
+    nty_ = (G.ny + cg_stage_tile_y() - 1) / cg_stage_tile_y();
     const long long tiles = (long long)ntx_ * nty_;
     const int ctas = dev_sms * cg_stage_ctas_per_sm();
     nchunk_ = std::max(1, (G.nz + 31) / 32);
@@ -460,13 +460,10 @@ int Session::launch_steps_graph(int n8)
     return ST_OK;
 }
 
-int Session::run(int nsteps)
+// n steps from `it` without synchronizing: direct launches up to the next
+// multiple of 8, the captured 8-step graph, direct launches for the rest.
+int Session::run_plain(int n)
 {
-    if (nsteps < 0) {
-        err = "negative step count";
-        return ST_ARG;
-    }
-    int n = std::min(nsteps, m.NT - it);
     int done = 0;
     while (done < n && (it + done) % 8 != 0) {
         int st = launch_step(it + done);
@@ -485,6 +482,33 @@ int Session::run(int nsteps)
         done++;
     }
     it += n;
+    return ST_OK;
+}
+
+int Session::run(int nsteps)
+{
+    if (nsteps < 0) {
+        err = "negative step count";
+        return ST_ARG;
+    }
+    int n = std::min(nsteps, m.NT - it);
+    if (!snapshots_on()) {
+        int st = run_plain(n);
+        if (st) return st;
+    } else {
+        // snapshots after every step s with s % IT_SKIP == 0 (src/propagate.cpp:289-309)
+        const int end = it + n;
+        while (it < end) {
+            int next = (it + m.p.IT_SKIP - 1) / m.p.IT_SKIP * m.p.IT_SKIP;  // first snapshot step >= it
+            int stop = std::min(end, next + 1);
+            int st = run_plain(stop - it);
+            if (st) return st;
+            if (stop == next + 1) {
+                st = write_snapshots(next);
+                if (st) return st;
+            }
+        }
+    }
     CU(cudaStreamSynchronize(stream));
     CU(cudaGetLastError());
     return check_device_error();
@@ -600,11 +624,119 @@ int Session::get_pgv(float *host) const
 
 // Output files of one rank in the reference's formats: station traces
 // (src/station.cpp:422-443) and peak ground velocity (src/PGV.cpp:177-185).
-int Session::write_outputs() const
+std::string Session::out_dir() const
 {
     std::string out = m.p.OUT;
     if (out.empty()) out = "./output";
     if (out[0] != '/') out = run_dir + "/" + out;
+    return out;
+}
+
+// ---------------------------------------------------------------- snapshots
+bool Session::snapshots_on() const
+{
+    if (m.p.IT_SKIP <= 0) return false;
+    const int sx = m.p.sliceX + HALO, sy = m.p.sliceY + HALO, sz = m.p.sliceZ + HALO;
+    return m.p.sliceFreeSurf || (sx >= HALO && sx < m.g._nx) || (sy >= HALO && sy < m.g._ny) ||
+           (sz >= HALO && sz < m.g._nz);
+}
+
+// Velocity slices after step `step` (data2D_XYZ_out, src/data_io.cpp:485-560):
+// OUT/V{x,y,z}_<step>_{X,Y,Z}_mpi_0_0_0.bin at the configured slices and,
+// with sliceFreeSurf, OUT/FreeSurfV{x,y,z}_<step>_Z_mpi_0_0_0.bin of the top
+// layer; with displacement on, OUT/FreeSurfU{x,y,z}_<step>_Z_... as well
+// (src/data_io.cpp:613-626).
+int Session::write_snapshots(int step)
+{
+    const Grid &G = m.g;
+    const size_t maxn = (size_t)std::max({(long long)G.nx * G.ny, (long long)G.nx * G.nz, (long long)G.ny * G.nz});
+    if (!slice_dev_) ALLOC(slice_dev_, float, maxn);
+    std::vector<float> host(maxn);
+    const std::string out = out_dir();
+    auto one = [&](const float *src, int scheme, int axis, int idx, int comp, const std::string &name) -> int {
+        const int n0 = axis == 0 ? G.ny : G.nx, n1 = axis == 2 ? G.ny : G.nz;
+        CU(launch_pack_slice(src, cjm_, g, axis, idx, comp, scheme, slice_dev_, stream));
+        CU(cudaMemcpyAsync(host.data(), slice_dev_, sizeof(float) * n0 * n1, cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        const char ax = "XYZ"[axis];
+        std::string path = out + "/" + name + "_" + ax + "_mpi_0_0_0.bin";
+        FILE *fp = std::fopen(path.c_str(), "wb");
+        if (!fp) {
+            err = "cannot write " + path;
+            return ST_IO;
+        }
+        std::fwrite(host.data(), sizeof(float), (size_t)n0 * n1, fp);
+        std::fclose(fp);
+        return ST_OK;
+    };
+    const int idx[3] = {m.p.sliceX + HALO, m.p.sliceY + HALO, m.p.sliceZ + HALO};
+    const int lim[3] = {G._nx, G._ny, G._nz};
+    const char *comp_name[3] = {"Vx", "Vy", "Vz"};
+    const std::string s = std::to_string(step);
+    for (int c = 0; c < 3; c++)
+        for (int axis = 0; axis < 3; axis++)
+            if (idx[axis] >= HALO && idx[axis] < lim[axis]) {
+                int st = one(W_[0], m.p.scheme, axis, idx[axis], c, std::string(comp_name[c]) + "_" + s);
+                if (st) return st;
+            }
+    if (m.p.sliceFreeSurf) {
+        for (int c = 0; c < 3; c++) {
+            int st = one(W_[0], m.p.scheme, 2, G._nz - 1, c, std::string("FreeSurf") + comp_name[c] + "_" + s);
+            if (st) return st;
+        }
+        if (dis_) {
+            const char *un[3] = {"FreeSurfUx", "FreeSurfUy", "FreeSurfUz"};
+            for (int c = 0; c < 3; c++) {
+                int st = one(dis_, 0, 2, G._nz - 1, c, std::string(un[c]) + "_" + s);
+                if (st) return st;
+            }
+        }
+    }
+    return ST_OK;
+}
+
+// Model slices (data2D_Model_out, src/data_io.cpp:585-610, written by
+// src/run.cpp:70 before the time loop): coordX/Y/Z and Vs/Vp/rho at the
+// configured slices, from the host copies of the coordinates and medium.
+static int write_model_slices(const Model &m, const std::string &out)
+{
+    const Grid &G = m.g;
+    const int idx[3] = {m.p.sliceX + HALO, m.p.sliceY + HALO, m.p.sliceZ + HALO};
+    const int lim[3] = {G._nx, G._ny, G._nz};
+    const char *names[6] = {"coordX", "coordY", "coordZ", "Vs", "Vp", "rho"};
+    for (int v = 0; v < 6; v++) {
+        const std::vector<float> &src = v < 3 ? m.coord : m.medium;
+        if (src.empty()) continue;
+        for (int axis = 0; axis < 3; axis++) {
+            if (!(idx[axis] >= HALO && idx[axis] < lim[axis])) continue;
+            const int n0 = axis == 0 ? G.ny : G.nx, n1 = axis == 2 ? G.ny : G.nz;
+            std::vector<float> buf((size_t)n0 * n1);
+            for (int a1 = 0; a1 < n1; a1++)
+                for (int a0 = 0; a0 < n0; a0++) {
+                    int i, j, k;
+                    if (axis == 0) i = idx[0], j = a0 + HALO, k = a1 + HALO;
+                    else if (axis == 1) i = a0 + HALO, j = idx[1], k = a1 + HALO;
+                    else i = a0 + HALO, j = a1 + HALO, k = idx[2];
+                    const long long p = ((long long)k * G._ny_ + j) * G._nx_ + i;
+                    buf[(size_t)a1 * n0 + a0] = src[p * 3 + (v % 3)];
+                }
+            std::string path = out + "/" + names[v] + "_" + "XYZ"[axis] + "_mpi_0_0_0.bin";
+            FILE *fp = std::fopen(path.c_str(), "wb");
+            if (!fp) return ST_IO;
+            std::fwrite(buf.data(), sizeof(float), buf.size(), fp);
+            std::fclose(fp);
+        }
+    }
+    return ST_OK;
+}
+
+int Session::write_outputs() const
+{
+    const std::string out = out_dir();
+    {
+        int st = write_model_slices(m, out);
+        if (st) return st;
+    }
     if (nst > 0) {
         std::vector<float> w((size_t)nst * m.NT * 9);
         int st = get_stations(w.data());
@@ -626,6 +758,91 @@ int Session::write_outputs() const
         std::fwrite(p.data(), sizeof(float), p.size(), fp);
         std::fclose(fp);
     }
+    return ST_OK;
+}
+
+// ------------------------------------------------------ checkpointing
+// The state a step depends on: the step counter, the wavefield at the step
+// boundary (buffer A; the other buffers are stage temporaries), the PML
+// auxiliaries at the step boundary (A of each face), and the running outputs
+// (PGV, displacement, station traces recorded so far).  Layout: a header of
+// 8 + P int64 (magic, version, scheme, nx, ny, nz, steps done, P, then the
+// byte size of each of the P parts listed by ckpt_parts), then the parts.
+namespace {
+constexpr long long CKPT_MAGIC = 0x314b434d44464743LL;  // "CGFDMCK1"
+}
+
+void Session::ckpt_parts(std::vector<std::pair<void *, size_t>> &parts) const
+{
+    const long long F = g.fstride;
+    parts.clear();
+    parts.push_back({W_[0], sizeof(float) * F * 9});
+    if (m.p.scheme == SCHEME_CGFDM && m.p.pml)
+        for (int fc = 0; fc < 5; fc++) parts.push_back({face_[fc].A, sizeof(float) * face_[fc].count * 9});
+    parts.push_back({pgv_, sizeof(float) * (size_t)m.g.nx * m.g.ny * 2});
+    if (dis_) parts.push_back({dis_, sizeof(float) * F * 3});
+    if (nst > 0) parts.push_back({st_out_, sizeof(float) * (size_t)nst * std::max(m.NT, 1) * 9});
+}
+
+size_t Session::checkpoint_bytes() const
+{
+    std::vector<std::pair<void *, size_t>> parts;
+    ckpt_parts(parts);
+    size_t n = sizeof(long long) * (8 + parts.size());
+    for (auto &p : parts) n += p.second;
+    return n;
+}
+
+int Session::checkpoint(void *host, size_t bytes)
+{
+    if (bytes < checkpoint_bytes()) {
+        err = "checkpoint buffer too small";
+        return ST_ARG;
+    }
+    std::vector<std::pair<void *, size_t>> parts;
+    ckpt_parts(parts);
+    long long *h = (long long *)host;
+    h[0] = CKPT_MAGIC, h[1] = 1, h[2] = m.p.scheme, h[3] = m.g.nx, h[4] = m.g.ny, h[5] = m.g.nz, h[6] = it;
+    h[7] = (long long)parts.size();
+    for (size_t i = 0; i < parts.size(); i++) h[8 + i] = (long long)parts[i].second;
+    char *o = (char *)(h + 8 + parts.size());
+    CU(cudaStreamSynchronize(stream));
+    for (auto &p : parts) {
+        CU(cudaMemcpyAsync(o, p.first, p.second, cudaMemcpyDeviceToHost, stream));
+        o += p.second;
+    }
+    CU(cudaStreamSynchronize(stream));
+    return ST_OK;
+}
+
+int Session::restore(const void *host, size_t bytes)
+{
+    std::vector<std::pair<void *, size_t>> parts;
+    ckpt_parts(parts);
+    const long long *h = (const long long *)host;
+    if (bytes < sizeof(long long) * 8 || h[0] != CKPT_MAGIC || h[1] != 1) {
+        err = "not a checkpoint of this library";
+        return ST_ARG;
+    }
+    if (h[2] != m.p.scheme || h[3] != m.g.nx || h[4] != m.g.ny || h[5] != m.g.nz || h[6] < 0 || h[6] > m.NT ||
+        h[7] != (long long)parts.size() || bytes < checkpoint_bytes()) {
+        err = "checkpoint does not match this session (scheme, grid, options or NT differ)";
+        return ST_ARG;
+    }
+    for (size_t i = 0; i < parts.size(); i++)
+        if (h[8 + i] != (long long)parts[i].second) {
+            err = "checkpoint does not match this session (array sizes differ)";
+            return ST_ARG;
+        }
+    const char *o = (const char *)(h + 8 + parts.size());
+    CU(cudaStreamSynchronize(stream));
+    for (auto &p : parts) {
+        CU(cudaMemcpyAsync(p.first, o, p.second, cudaMemcpyHostToDevice, stream));
+        o += p.second;
+    }
+    it = (int)h[6];
+    CU(cudaMemcpyAsync(it_dev_, &it, sizeof(int), cudaMemcpyHostToDevice, stream));
+    CU(cudaStreamSynchronize(stream));
     return ST_OK;
 }
 

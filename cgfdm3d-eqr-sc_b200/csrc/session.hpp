@@ -31,6 +31,9 @@ public:
     int get_pgv(float *host) const;                 // [ny][nx][2]
     int write_outputs() const;
     int sync() const;
+    size_t checkpoint_bytes() const;
+    int checkpoint(void *host, size_t bytes);       // state at the current step boundary
+    int restore(const void *host, size_t bytes);    // from a checkpoint of an identical session
 
     Model m;
     DevGrid g;
@@ -75,6 +78,12 @@ private:
     ScTiling sct_ = {};
     static constexpr int SC_DECAY_LAYERS = 20;       // src/exp_decay_absorb.cpp:109
     int check_device_error();
+    void ckpt_parts(std::vector<std::pair<void *, size_t>> &parts) const;
+    int run_plain(int n);                 // n steps from `it`, graphs where aligned
+    bool snapshots_on() const;
+    int write_snapshots(int step);        // slices after step `step`
+    std::string out_dir() const;
+    float *slice_dev_ = nullptr;
 };
 
 }  // namespace cgfdm

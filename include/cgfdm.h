@@ -105,6 +105,18 @@ int cgfdm_get_pgv(const cgfdm_session *s, float *out, long long count);
  * reference's formats (src/station.cpp:422-443, src/PGV.cpp:177-185). */
 int cgfdm_write_outputs(const cgfdm_session *s);
 
+/* Checkpoint of the time-stepping state at the current step boundary: the
+ * step counter, the wavefield, the PML auxiliaries, and the running outputs
+ * (PGV, displacement, station traces so far), in a host buffer of
+ * cgfdm_checkpoint_size bytes.  cgfdm_restore loads one into a session
+ * created from the same run directory and options; stepping on from there
+ * gives bit-identical results to an uninterrupted run.  The reference keeps
+ * no restart files; this replaces re-running it from step 0 (it has no
+ * counterpart in src/). */
+int cgfdm_checkpoint_size(const cgfdm_session *s, long long *bytes);
+int cgfdm_checkpoint(cgfdm_session *s, void *out, long long bytes);
+int cgfdm_restore(cgfdm_session *s, const void *in, long long bytes);
+
 int cgfdm_destroy(cgfdm_session *s);
 
 /* Description of the last failure on `s` (or of the last failed
