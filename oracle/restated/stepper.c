@@ -469,25 +469,50 @@ static void cg_deriv(int FB1, int FB2, int FB3)
 
 /* RK4 of the wavefield over every point (src/wave_rk.cpp:17-104; halo
  * points have a zero RHS) and of the PML auxiliaries (src/pml_rk.cpp:18-73) */
+/* Storage-precision experiment (STORE_MANT_BITS, see Makefile): every
+ * value written to the stored state (wavefield, RK sum, step start, PML
+ * auxiliaries) is rounded to that many significand bits (11 = FP16, 8 =
+ * BF16), with the float exponent range kept: 16-bit storage with ideal
+ * per-field scaling.  Off by default. */
+#ifndef STORE_MANT_BITS
+#define STORE_MANT_BITS 0
+#endif
+static real store(real x)
+{
+#if STORE_MANT_BITS > 0
+    float f = (float)x;
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    const int drop = 24 - STORE_MANT_BITS;
+    const uint32_t half = 1u << (drop - 1), mask = (1u << drop) - 1;
+    const uint32_t lsb = (u >> drop) & 1u;
+    u = (u + half - 1 + lsb) & ~mask; /* round to nearest, ties to even */
+    memcpy(&f, &u, 4);
+    return (real)f;
+#else
+    return x;
+#endif
+}
+
 static void rk4(int irk)
 {
     const float b1 = 0.16666667f, b2 = 0.33333333f, b3 = 0.33333333f, b4 = 0.16666667f, a2 = 0.5f, a3 = 0.5f;
     for (long long n = 0; n < np_pad * 9; n++) {
         real h = Wh[n];
-        if (irk == 0) Wm[n] = W[n], Wt[n] = Wm[n] + b1 * h, W[n] = Wm[n] + a2 * h;
-        else if (irk == 1) Wt[n] = Wt[n] + b2 * h, W[n] = Wm[n] + a3 * h;
-        else if (irk == 2) Wt[n] = Wt[n] + b3 * h, W[n] = Wm[n] + h;
-        else W[n] = Wt[n] + b4 * h;
+        if (irk == 0) Wm[n] = W[n], Wt[n] = store(Wm[n] + b1 * h), W[n] = store(Wm[n] + a2 * h);
+        else if (irk == 1) Wt[n] = store(Wt[n] + b2 * h), W[n] = store(Wm[n] + a3 * h);
+        else if (irk == 2) Wt[n] = store(Wt[n] + b3 * h), W[n] = store(Wm[n] + h);
+        else W[n] = store(Wt[n] + b4 * h);
     }
     if (pml_on)
         for (int fc = 0; fc < 5; fc++) {
             Face *F = &FACE[fc];
             for (long long n = 0; n < F->n * 9; n++) {
                 real h = F->h[n];
-                if (irk == 0) F->m[n] = F->A[n], F->t[n] = F->m[n] + b1 * h, F->A[n] = F->m[n] + a2 * h;
-                else if (irk == 1) F->t[n] = F->t[n] + b2 * h, F->A[n] = F->m[n] + a3 * h;
-                else if (irk == 2) F->t[n] = F->t[n] + b3 * h, F->A[n] = F->m[n] + h;
-                else F->A[n] = F->t[n] + b4 * h;
+                if (irk == 0) F->m[n] = F->A[n], F->t[n] = store(F->m[n] + b1 * h), F->A[n] = store(F->m[n] + a2 * h);
+                else if (irk == 1) F->t[n] = store(F->t[n] + b2 * h), F->A[n] = store(F->m[n] + a3 * h);
+                else if (irk == 2) F->t[n] = store(F->t[n] + b3 * h), F->A[n] = store(F->m[n] + h);
+                else F->A[n] = store(F->t[n] + b4 * h);
             }
         }
 }
@@ -593,9 +618,9 @@ static void tvd(int irk)
 {
     for (long long n = 0; n < np_pad * 9; n++) {
         real h = Wh[n];
-        if (irk == 0) Wm[n] = W[n], W[n] = Wm[n] + h;
-        else if (irk == 1) W[n] = (real)(0.75 * Wm[n] + 0.25 * W[n] + 0.25 * h);
-        else W[n] = (real)((1.0 / 3.0) * Wm[n] + (2.0 / 3.0) * W[n] + (2.0 / 3.0) * h);
+        if (irk == 0) Wm[n] = W[n], W[n] = store(Wm[n] + h);
+        else if (irk == 1) W[n] = store((real)(0.75 * Wm[n] + 0.25 * W[n] + 0.25 * h));
+        else W[n] = store((real)((1.0 / 3.0) * Wm[n] + (2.0 / 3.0) * W[n] + (2.0 / 3.0) * h));
     }
 }
 
