@@ -220,6 +220,78 @@ def cpu_reference_rate(name, warmup_steps, timed_steps, procs):
     return {"value": rate, "unit": METRIC, "cores": procs, "kind": "reference", "sample": sample}, None
 
 
+# ---------------------------------------------------------------- batches
+def bench_batch(args, world, rank, local_rank):
+    """``--workload batchN``: N independent CGFDM shots of uneven sizes
+    (cgfdm.configs.batch_shots: 64-256 x 64-256 x 64-128, layered media,
+    terrain up to 1 km, random moment tensors, 32 stations each) advanced
+    together, one persistent stage launch per RK stage, 8 steps per graph
+    replay.  Also times each shot alone for comparison.  One GPU."""
+    import torch
+    from cgfdm import Batch, Session, configs
+
+    n = int(args.workload[len("batch"):] or 32)
+    total = args.warmup + 2 * args.steps + 8  # batched steps, then the same number per shot alone
+    root = os.path.join(WORK, f"{args.workload}_{total}")
+    marker = os.path.join(root, ".done")
+    if not os.path.exists(marker):
+        if os.path.exists(root):
+            shutil.rmtree(root)
+        configs.batch_shots(root, n=n, steps=total)
+        open(marker, "w").close()
+    dirs = sorted(os.path.join(root, d) for d in os.listdir(root) if d.startswith("shot_"))
+    sessions = [Session(d, device=local_rank) for d in dirs]
+    pts = sum(s.info.nx * s.info.ny * s.info.nz for s in sessions)
+    algo = sum(s.info.algo_bytes_per_step for s in sessions)
+    b = Batch(sessions)
+    b.run(args.warmup)
+    torch.cuda.synchronize(local_rank)
+    with ClockSampler(local_rank) as clk:
+        ms = b.run_timed(args.steps)
+    b.close()
+    # each shot alone, same number of steps
+    alone_ms = 0.0
+    for s in sessions:
+        alone_ms += s.run_timed(args.steps)
+    for s in sessions:
+        s.close()
+    # end to end: run directories on disk -> sessions -> batch -> traces on the host
+    t0 = time.perf_counter()
+    ss = [Session(d, device=local_rank) for d in dirs]
+    b2 = Batch(ss)
+    b2.run(args.steps)
+    st_bytes = sum(s.stations().nbytes for s in ss)
+    h2d = sum(s.info.h2d_bytes for s in ss)
+    b2.close()
+    for s in ss:
+        s.close()
+    e2e_s = time.perf_counter() - t0
+    value = pts * args.steps / (ms * 1e-3) / 1e6
+    hbm_peak, peak_kind = peaks()
+    achieved = algo * args.steps / (ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "scheme": "CGFDM",
+        "config": {"workload": f"{n} CGFDM shots of uneven sizes (64-256 x 64-256 x 64-128, DH=100 m), layered "
+                               "media, terrain <= 1 km, random moment tensors, 32 stations each, one persistent "
+                               "stage launch per RK stage for all shots, 8-step CUDA graphs",
+                   "points": pts, "shots": n,
+                   "alone_Mpts_step_s": pts * args.steps / (alone_ms * 1e-3) / 1e6,
+                   "l2": "inputs larger than L2", "parallelism": "batch x1"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,
+                     "kernel": "k_cg_stage (batched; whole step incl. sources and stations)"},
+        "e2e": {"value": pts * args.steps / e2e_s / 1e6, "unit": METRIC, "h2d_bytes_per_step": h2d / args.steps,
+                "d2h_bytes_per_step": st_bytes / args.steps, "seconds": e2e_s},
+        "gpu_launches": int(args.steps * (4 + 2 * n)),
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 # ------------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -256,6 +328,9 @@ def main():
         return 0
 
     import torch
+
+    if args.workload.startswith("batch"):
+        return bench_batch(args, world, rank, local_rank)
 
     dist = None
     if world > 1:

@@ -74,6 +74,12 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
     L.cgfdm_checkpoint.argtypes = [vp, vp, ctypes.c_longlong]
     L.cgfdm_restore.argtypes = [vp, vp, ctypes.c_longlong]
     L.cgfdm_destroy.argtypes = [vp]
+    L.cgfdm_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
+    L.cgfdm_batch_run.argtypes = [vp, ctypes.c_int]
+    L.cgfdm_batch_run_timed.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.cgfdm_batch_destroy.argtypes = [vp]
+    L.cgfdm_batch_last_error.argtypes = [vp]
+    L.cgfdm_batch_last_error.restype = ctypes.c_char_p
     L.cgfdm_last_error.argtypes = [vp]
     L.cgfdm_last_error.restype = ctypes.c_char_p
     L.cgfdm_build_flavor.restype = ctypes.c_char_p
@@ -165,6 +171,50 @@ class Session:
     def close(self) -> None:
         if self._h:
             self.L.cgfdm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """CGFDM sessions advanced together, one persistent stage launch for all
+    (``cgfdm_batch_create`` ... ``cgfdm_batch_destroy``).  The sessions stay
+    owned by the caller and must outlive the batch."""
+
+    def __init__(self, sessions):
+        self.sessions = list(sessions)
+        self.L = self.sessions[0].L
+        arr = (ctypes.c_void_p * len(self.sessions))(*[s._h.value for s in self.sessions])
+        self._h = ctypes.c_void_p()
+        rc = self.L.cgfdm_batch_create(arr, len(self.sessions), ctypes.byref(self._h))
+        if rc:
+            raise CgfdmError(rc, self.L.cgfdm_batch_last_error(None).decode())
+
+    def _check(self, rc: int):
+        if rc:
+            raise CgfdmError(rc, self.L.cgfdm_batch_last_error(self._h).decode())
+
+    def run(self, nsteps: int) -> None:
+        self._check(self.L.cgfdm_batch_run(self._h, int(nsteps)))
+
+    def run_timed(self, nsteps: int) -> float:
+        ms = ctypes.c_float()
+        self._check(self.L.cgfdm_batch_run_timed(self._h, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def close(self) -> None:
+        if self._h:
+            self.L.cgfdm_batch_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __enter__(self):

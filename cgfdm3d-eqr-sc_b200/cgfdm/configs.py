@@ -264,3 +264,51 @@ def aweno_basin(directory: str, steps: int = 4000, NX: int = 512, NY: int = 512,
     c.ricker_point = (NX // 2, NY // 2, NZ - 1 - min(int(round(2000.0 / DH)), NZ // 2), fc)
     cases.write_case(c, directory, scheme="SCFDM")
     return c, {"hmin": hmin, "vp_max": vp_max, "DT": DT}
+
+
+def batch_shots(root: str, n: int = 32, steps: int = 1500, seed: int = 5, sizes=((64, 256), (64, 256), (64, 128)),
+                DH: float = 100.0, nPML: int = 12, n_stations: int = 32, courant: float = 0.8) -> list:
+    """Writes ``n`` independent CGFDM run directories root/shot_<i> for the
+    batched workload: grid sizes drawn from ``sizes`` (NX, NY, NZ ranges),
+    a random layered medium (3-6 layers, Vs 1500-4500 m/s increasing with
+    depth, Vp = 1.73 Vs, Gardner density), Gaussian-hill terrain of random
+    amplitude up to 1 km, one point moment tensor (random strike, dip, rake;
+    M0 = 1e16 N m with a Ricker moment rate of 1-4 Hz) at 30 % of the model
+    depth, ``n_stations`` surface stations.  Returns the directories."""
+    rng = np.random.default_rng(seed)
+    dirs = []
+    for s in range(n):
+        NX = int(rng.integers(sizes[0][0], sizes[0][1] + 1))
+        NY = int(rng.integers(sizes[1][0], sizes[1][1] + 1))
+        NZ = int(rng.integers(sizes[2][0], sizes[2][1] + 1))
+        d = os.path.join(root, f"shot_{s:02d}")
+        os.makedirs(d, exist_ok=True)
+        terrain = gaussian_hills(NX, NY, DH, rng)
+        amp = float(rng.uniform(0.0, 1000.0))
+        terrain = (terrain * (amp / max(float(terrain.max()), 1e-6))).astype(np.float32)
+        nl = int(rng.integers(3, 7))
+        depth_total = NZ * DH
+        tops = np.concatenate([[0.0], np.sort(rng.uniform(0.1, 0.9, nl - 1)) * depth_total]) / 1000.0
+        vs = np.sort(rng.uniform(1500.0, 4500.0, nl))
+        vp = 1.73 * vs
+        rho = 310.0 * vp ** 0.25
+        layers = tuple((float(tops[i]), float(vs[i] / 1000), float(vp[i] / 1000), float(rho[i] / 1000))
+                       for i in range(nl))
+        vp_max = float(vp.max())
+        hmin = hmin_terrain(terrain, NX, NY, NZ, DH, NX // 2, NY // 2)
+        DT = cases.cfl_dt(DH, vp_max, courant, hmin=hmin)
+        depth_src = 0.3 * depth_total
+        li = int(np.searchsorted(tops * 1000.0, depth_src, side="right") - 1)
+        mu = float(rho[li] * vs[li] ** 2)
+        fault, _ = cases.moment_fault(steps, DT, 0.01, 100.0, 30.0, depth_src, 1e16, float(rng.uniform(1.0, 4.0)),
+                                      mu, strike=float(rng.uniform(0, 360)), dip=float(rng.uniform(10, 90)),
+                                      rake=float(rng.uniform(-180, 180)))
+        xs = rng.integers(nPML + 4, NX - nPML - 4, n_stations)
+        ys = rng.integers(nPML + 4, NY - nPML - 4, n_stations)
+        stations = [(int(x), int(y), NZ - 1) for x, y in zip(xs, ys)]
+        terrain.tofile(os.path.join(d, "terrain.bin"))
+        c = cases.Case(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=DT, steps=steps, nPML=nPML, layers=layers, fault=fault,
+                       stations=stations, extra={"terrainFile": "terrain.bin"})
+        cases.write_case(c, d)
+        dirs.append(d)
+    return dirs

@@ -6,11 +6,17 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
+#include "batch.hpp"
 #include "session.hpp"
 
 struct cgfdm_session {
     cgfdm::Session s;
+};
+
+struct cgfdm_batch {
+    cgfdm::Batch b;
 };
 
 static thread_local std::string g_create_error;
@@ -144,6 +150,56 @@ int cgfdm_restore(cgfdm_session *s, const void *in, long long bytes)
     if (!s || !in || bytes < 0) return CGFDM_E_ARG;
     return s->s.restore(in, (size_t)bytes);
 }
+
+int cgfdm_batch_create(cgfdm_session *const *sessions, int n, cgfdm_batch **out)
+{
+    if (!sessions || n <= 0 || !out) {
+        g_create_error = "sessions, n > 0 and out are required";
+        return CGFDM_E_ARG;
+    }
+    *out = nullptr;
+    std::vector<cgfdm::Session *> v;
+    for (int i = 0; i < n; i++) {
+        if (!sessions[i]) {
+            g_create_error = "NULL session in batch";
+            return CGFDM_E_ARG;
+        }
+        v.push_back(&sessions[i]->s);
+    }
+    cgfdm_batch *h = new (std::nothrow) cgfdm_batch;
+    if (!h) {
+        g_create_error = "out of host memory";
+        return CGFDM_E_ALLOC;
+    }
+    int st = h->b.create(v);
+    if (st) {
+        g_create_error = h->b.err;
+        delete h;
+        return st;
+    }
+    *out = h;
+    return CGFDM_OK;
+}
+
+int cgfdm_batch_run(cgfdm_batch *b, int nsteps)
+{
+    if (!b) return CGFDM_E_ARG;
+    return b->b.run(nsteps);
+}
+
+int cgfdm_batch_run_timed(cgfdm_batch *b, int nsteps, float *ms)
+{
+    if (!b || !ms) return CGFDM_E_ARG;
+    return b->b.run(nsteps, ms);
+}
+
+int cgfdm_batch_destroy(cgfdm_batch *b)
+{
+    delete b;
+    return CGFDM_OK;
+}
+
+const char *cgfdm_batch_last_error(const cgfdm_batch *b) { return b ? b->b.err.c_str() : g_create_error.c_str(); }
 
 int cgfdm_destroy(cgfdm_session *s)
 {

@@ -231,26 +231,28 @@ __device__ __forceinline__ void ljt_z(const float *__restrict__ W, const float *
 // over one z-chunk -- from an atomic counter, chunks of a tile adjacent in
 // the order, so concurrently running items share their halo and chunk-edge
 // planes through L2 and no launch ends on a partial wave.
-template <int FB1, int FB2, int FB3>
+//
+// BATCH = false: one session, its descriptor a kernel parameter (arguments
+// and tensor maps in parameter space).  BATCH = true: the work items of
+// nsess sessions, their descriptors in global memory; a CTA copies the
+// arguments of the session its current item belongs to into shared memory.
+template <int FB1, int FB2, int FB3, bool BATCH>
 __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
-    k_cg_stage(const __grid_constant__ CUtensorMap tmW, const __grid_constant__ CUtensorMap tmC,
-               const __grid_constant__ CUtensorMap tmM, const __grid_constant__ CUtensorMap tmT, const CgStageArgs a)
+    k_cg_stage(const __grid_constant__ CgStageDesc d1, const CgStageDesc *__restrict__ descs,
+               const int *__restrict__ item_start, int nsess, int *work)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float *ring = reinterpret_cast<float *>(smem_raw);
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + NSLOT * SLOT_BYTES);
     __shared__ int s_abort, s_item;
-
-    const DevGrid g = a.g;
-    const long long F = g.fstride;
+    __shared__ __align__(16) CgStageArgs s_args;
+    const CgStageArgs &a = BATCH ? s_args : d1.a;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int _nx = g.nxp - CGFDM_HALO, _ny = g.nyp - CGFDM_HALO, _nz = g.nzp - CGFDM_HALO;
     constexpr int hyL = FB2 > 0 ? 1 : 3;
     constexpr int za = FB3 > 0 ? 1 : 3;
-    const float rDH = a.rDH, DT = a.DT;
     const int cell = (ty + hyL) * BXW + tx + 4;
-    const int nitems = a.ntiles_x * a.ntiles_y * a.nchunk;
-    const int nPML = a.nPML;
+    const int total = BATCH ? item_start[nsess] : d1.a.ntiles_x * d1.a.ntiles_y * d1.a.nchunk;
+    int sess = -1;
 
     if (tid == 0) {
         s_abort = 0;
@@ -261,10 +263,35 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
 
     for (;;) {
     __syncthreads();
-    if (tid == 0) s_item = atomicAdd(&a.work[0], 1);
+    if (tid == 0) s_item = atomicAdd(&work[0], 1);
     __syncthreads();
-    const int item = s_item;
-    if (item >= nitems || s_abort) break;
+    const int gitem = s_item;
+    if (gitem >= total || s_abort) break;
+    if (BATCH) {
+        // items of one session are consecutive; find this one's session
+        int ns = 0;
+        while (ns + 1 < nsess && gitem >= item_start[ns + 1]) ns++;
+        if (ns != sess) {
+            sess = ns;
+            const int *src = reinterpret_cast<const int *>(&descs[sess].a);
+            int *dst = reinterpret_cast<int *>(&s_args);
+            for (int w = tid; w < (int)(sizeof(CgStageArgs) / 4); w += TX * TY) dst[w] = src[w];
+            __syncthreads();
+        }
+    } else {
+        sess = 0;
+    }
+    const CgStageDesc &D = BATCH ? descs[sess] : d1;
+    const CUtensorMap *tmW = reinterpret_cast<const CUtensorMap *>(D.tmW);
+    const CUtensorMap *tmC = reinterpret_cast<const CUtensorMap *>(D.tmC);
+    const CUtensorMap *tmM = reinterpret_cast<const CUtensorMap *>(D.tmM);
+    const CUtensorMap *tmT = reinterpret_cast<const CUtensorMap *>(D.tmT);
+    const DevGrid g = a.g;
+    const long long F = g.fstride;
+    const int _nx = g.nxp - CGFDM_HALO, _ny = g.nyp - CGFDM_HALO, _nz = g.nzp - CGFDM_HALO;
+    const float rDH = a.rDH, DT = a.DT;
+    const int nPML = a.nPML;
+    const int item = BATCH ? gitem - item_start[sess] : gitem;
     const int tile = item / a.nchunk, chunk = item - tile * a.nchunk;
     const int by_ = tile / a.ntiles_x, bx_ = tile - by_ * a.ntiles_x;
     const int i0 = CGFDM_HALO + bx_ * TX, j0 = CGFDM_HALO + by_ * TY;
@@ -286,13 +313,13 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         unsigned bar = smem_u32(&bars[s]);
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         mbar_expect_tx(bar, SLOT_BYTES);
-        tma_load_4d(smem_u32(ring + s * SLOT_F), &tmW, tx0, ty0, kk, 0, bar);
+        tma_load_4d(smem_u32(ring + s * SLOT_F), tmW, tx0, ty0, kk, 0, bar);
     };
     // point operands of plane kk into L2 ahead of their plain loads
     auto prefetch_points = [&](int kk) {
-        tma_prefetch_4d(&tmC, px0, j0, kk, 0);
-        if (a.irk == 1 || a.irk == 2) tma_prefetch_4d(&tmM, px0, j0, kk, 0);
-        if (a.irk != 0) tma_prefetch_4d(&tmT, px0, j0, kk, 0);
+        tma_prefetch_4d(tmC, px0, j0, kk, 0);
+        if (a.irk == 1 || a.irk == 2) tma_prefetch_4d(tmM, px0, j0, kk, 0);
+        if (a.irk != 0) tma_prefetch_4d(tmT, px0, j0, kk, 0);
     };
 
     const int klast = ke - za + 3;          // last plane of the last window
@@ -324,7 +351,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         }
         if (tid == 0) {
             if (k + 2 < ke) prefetch_points(k + 2);
-            if (want + 2 <= klast) tma_prefetch_4d(&tmW, tx0, ty0, want + 2, 0);
+            if (want + 2 <= klast) tma_prefetch_4d(tmW, tx0, ty0, want + 2, 0);
         }
         const long long q = g.at(i, j, k);
         // point-wise operands, loaded before the ring wait
@@ -536,10 +563,10 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     __syncthreads();
     if (tid == 0) {
         __threadfence();
-        int done = atomicAdd(&a.work[1], 1);
+        int done = atomicAdd(&work[1], 1);
         if (done == (int)(gridDim.x * gridDim.y * gridDim.z) - 1) {
-            atomicExch(&a.work[0], 0);
-            atomicExch(&a.work[1], 0);
+            atomicExch(&work[0], 0);
+            atomicExch(&work[1], 0);
             __threadfence();
         }
     }
@@ -549,36 +576,48 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
 int cg_stage_ctas_per_sm() { return CG_CTAS_PER_SM; }
 int cg_stage_tile_y() { return TY; }
 
-template <int FB1, int FB2, int FB3>
-static cudaError_t launch_t(const CgStageArgs &a, const CgStageMaps &m, int ctas, cudaStream_t st)
+template <int FB1, int FB2, int FB3, bool BATCH>
+static cudaError_t launch_t(const CgStageDesc &d1, const CgStageDesc *descs, const int *item_start, int nsess,
+                            int *work, int ctas, cudaStream_t st)
 {
     static bool attr = false;
     if (!attr) {
-        CUDA_TRY(cudaFuncSetAttribute(k_cg_stage<FB1, FB2, FB3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CUDA_TRY(cudaFuncSetAttribute(k_cg_stage<FB1, FB2, FB3, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)cg_stage_smem_bytes()));
         attr = true;
     }
-    const CUtensorMap &w = *reinterpret_cast<const CUtensorMap *>(m.win);
-    const CUtensorMap &c = *reinterpret_cast<const CUtensorMap *>(m.cjm);
-    const CUtensorMap &mm = *reinterpret_cast<const CUtensorMap *>(m.wm);
-    const CUtensorMap &t = *reinterpret_cast<const CUtensorMap *>(m.t);
-    k_cg_stage<FB1, FB2, FB3><<<ctas, dim3(TX, TY, 1), cg_stage_smem_bytes(), st>>>(w, c, mm, t, a);
+    k_cg_stage<FB1, FB2, FB3, BATCH>
+        <<<ctas, dim3(TX, TY, 1), cg_stage_smem_bytes(), st>>>(d1, descs, item_start, nsess, work);
     return cudaGetLastError();
 }
 
-cudaError_t launch_cg_stage(const CgStageArgs &a, const CgStageMaps &maps, int ctas, cudaStream_t st)
+template <bool BATCH>
+static cudaError_t launch_b(int FB1, int FB2, int FB3, const CgStageDesc &d1, const CgStageDesc *descs,
+                            const int *item_start, int nsess, int *work, int ctas, cudaStream_t st)
 {
-    const int key = (a.FB1 > 0) * 4 + (a.FB2 > 0) * 2 + (a.FB3 > 0);
+    const int key = (FB1 > 0) * 4 + (FB2 > 0) * 2 + (FB3 > 0);
     switch (key) {
-    case 0: return launch_t<-1, -1, -1>(a, maps, ctas, st);
-    case 1: return launch_t<-1, -1, 1>(a, maps, ctas, st);
-    case 2: return launch_t<-1, 1, -1>(a, maps, ctas, st);
-    case 3: return launch_t<-1, 1, 1>(a, maps, ctas, st);
-    case 4: return launch_t<1, -1, -1>(a, maps, ctas, st);
-    case 5: return launch_t<1, -1, 1>(a, maps, ctas, st);
-    case 6: return launch_t<1, 1, -1>(a, maps, ctas, st);
-    default: return launch_t<1, 1, 1>(a, maps, ctas, st);
+    case 0: return launch_t<-1, -1, -1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
+    case 1: return launch_t<-1, -1, 1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
+    case 2: return launch_t<-1, 1, -1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
+    case 3: return launch_t<-1, 1, 1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
+    case 4: return launch_t<1, -1, -1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
+    case 5: return launch_t<1, -1, 1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
+    case 6: return launch_t<1, 1, -1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
+    default: return launch_t<1, 1, 1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
     }
+}
+
+cudaError_t launch_cg_stage(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int ctas, cudaStream_t st)
+{
+    return launch_b<false>(FB1, FB2, FB3, d, nullptr, nullptr, 1, work, ctas, st);
+}
+
+cudaError_t launch_cg_stage_batch(int FB1, int FB2, int FB3, const CgStageDesc *descs, const int *item_start,
+                                  int nsess, int *work, int ctas, cudaStream_t st)
+{
+    static const CgStageDesc unused{};
+    return launch_b<true>(FB1, FB2, FB3, unused, descs, item_start, nsess, work, ctas, st);
 }
 
 cudaError_t make_field_tmap(void *out, const float *base, const DevGrid &g, int nf, bool halo_box)

@@ -39,7 +39,6 @@ struct CgStageArgs {
     float *pgv;          // [ny][nx][2] running max, stage 3 only
     float *dis;          // displacement, 3 fields in the W layout, stage 3 only
     int *err;            // device error word: bit 0 = a bounded wait gave up
-    int *work;           // persistent-CTA work counter pair, zero between launches
     int ntiles_x, ntiles_y, nchunk;  // work items: tiles x tiles x z-chunks
     int irk;
     int FB1, FB2, FB3;
@@ -56,7 +55,21 @@ struct CgStageMaps {
     alignas(64) unsigned char wm[128];
     alignas(64) unsigned char t[128];
 };
-cudaError_t launch_cg_stage(const CgStageArgs &a, const CgStageMaps &maps, int grid_ctas, cudaStream_t st);
+// Everything one stage launch needs for one session: the four tensor maps
+// (CUtensorMap, 128 bytes each, 64-byte aligned) and the arguments.
+// work: the launch's work-counter pair, zero between launches.
+struct alignas(64) CgStageDesc {
+    unsigned char tmW[128], tmC[128], tmM[128], tmT[128];
+    CgStageArgs a;
+};
+// One session's stage, its descriptor passed as a kernel parameter.
+cudaError_t launch_cg_stage(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,
+                            cudaStream_t st);
+// A batch: session s owns work items item_start[s] .. item_start[s+1]-1, its
+// descriptor is descs[s] in device memory; all advance with the same FB
+// signs and stage number.
+cudaError_t launch_cg_stage_batch(int FB1, int FB2, int FB3, const CgStageDesc *descs, const int *item_start,
+                                  int nsess, int *work, int grid_ctas, cudaStream_t st);
 size_t cg_stage_smem_bytes();
 // Encodes the 4-D tensor map (x, y, z, field) of an nf-field buffer, with a
 // halo box (40 x (tile rows + 4) x 1 x nf) or a point box (32 x tile rows x 1 x nf); out must hold

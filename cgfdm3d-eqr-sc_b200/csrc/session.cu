@@ -325,6 +325,11 @@ int Session::setup_device()
     nchunk_ = (G.nz + kchunk_ - 1) / kchunk_;
     grid_ctas_ = (int)std::min<long long>(ctas, tiles * nchunk_);
 
+    if (cg) {
+        int st = build_stage_descs();
+        if (st) return st;
+    }
+
     CU(cudaStreamSynchronize(stream));
     // coordinates and medium are not needed on the device any more
     for (auto it_ = allocs_.begin(); it_ != allocs_.end();) {
@@ -339,48 +344,64 @@ int Session::setup_device()
     return ST_OK;
 }
 
+// The four stage descriptors (RK4 stage irk reads win[irk] and writes
+// wout[irk]: A -> B, B -> C, C -> B, B -> A) with their tensor maps.
+void Session::stage_desc(int irk, CgStageDesc &d) const
+{
+    float *A = W_[0], *B = W_[1], *C = W_[2], *T = W_[3];
+    const float *win[4] = {A, B, C, B};
+    const int win_map[4] = {0, 1, 2, 1};
+    float *wout[4] = {B, C, B, A};
+    std::memset(&d, 0, sizeof d);
+    CgStageArgs &a = d.a;
+    a.g = g;
+    a.Win = win[irk];
+    a.Wm = A;
+    a.T = T;
+    a.Wout = wout[irk];
+    a.cjm = cjm_;
+    a.rdz = rdz_;
+    a.pml_alpha_x = pml_[0], a.pml_beta_x = pml_[1], a.pml_d_x = pml_[2];
+    a.pml_alpha_y = pml_[3], a.pml_beta_y = pml_[4], a.pml_d_y = pml_[5];
+    a.pml_alpha_z = pml_[6], a.pml_beta_z = pml_[7], a.pml_d_z = pml_[8];
+    for (int fc = 0; fc < 5; fc++) a.face[fc] = face_[fc];
+    a.pgv = irk == 3 ? pgv_ : nullptr;
+    a.dis = irk == 3 ? dis_ : nullptr;
+    a.irk = irk;
+    a.nPML = m.g.nPML;
+    a.pml_on = m.p.pml;
+    a.fs_on = 1;
+    a.kchunk = kchunk_;
+    a.rDH = m.g.rDH;
+    a.DT = (float)m.p.DT;
+    a.err = err_dev_;
+    a.ntiles_x = ntx_, a.ntiles_y = nty_, a.nchunk = nchunk_;
+    std::memcpy(d.tmW, maps_[win_map[irk]].win, 128);
+    std::memcpy(d.tmC, maps_[win_map[irk]].cjm, 128);
+    std::memcpy(d.tmM, maps_[win_map[irk]].wm, 128);
+    std::memcpy(d.tmT, maps_[win_map[irk]].t, 128);
+}
+
+int Session::stage_items() const { return ntx_ * nty_ * nchunk_; }
+
+int Session::build_stage_descs()
+{
+    for (int irk = 0; irk < 4; irk++) stage_desc(irk, desc_host_[irk]);
+    return ST_OK;
+}
+
 // ----------------------------------------------------------------- step
 int Session::launch_step(int step, bool timed_stages)
 {
     const bool cg = m.p.scheme == SCHEME_CGFDM;
     const float DT = (float)m.p.DT;
     int FB1 = FB_TABLE[step % 8][0], FB2 = FB_TABLE[step % 8][1], FB3 = FB_TABLE[step % 8][2];
-    // sources into W at the stage-0 time (src/propagate.cpp:198-210)
-    CU(launch_point(W_[0], W_[1], W_[2], cjm_, g, point_, it_dev_, DT, m.g.DH, m.p.scheme, stream));
-    CU(launch_sources(W_[0], cjm_, g, fault_, point_, it_dev_, DT, m.g.DH, m.p.scheme, stream));
+    (void)DT;
+    if (int st = launch_sources_on(stream)) return st;
     if (cg) {
-        float *A = W_[0], *B = W_[1], *C = W_[2], *T = W_[3];
-        const float *win[4] = {A, B, C, B};
-        const int win_map[4] = {0, 1, 2, 1};
-        float *wout[4] = {B, C, B, A};
         for (int irk = 0; irk < 4; irk++) {
-            CgStageArgs a{};
-            a.g = g;
-            a.Win = win[irk];
-            a.Wm = A;
-            a.T = T;
-            a.Wout = wout[irk];
-            a.cjm = cjm_;
-            a.rdz = rdz_;
-            a.pml_alpha_x = pml_[0], a.pml_beta_x = pml_[1], a.pml_d_x = pml_[2];
-            a.pml_alpha_y = pml_[3], a.pml_beta_y = pml_[4], a.pml_d_y = pml_[5];
-            a.pml_alpha_z = pml_[6], a.pml_beta_z = pml_[7], a.pml_d_z = pml_[8];
-            for (int fc = 0; fc < 5; fc++) a.face[fc] = face_[fc];
-            a.pgv = irk == 3 ? pgv_ : nullptr;
-            a.dis = irk == 3 ? dis_ : nullptr;
-            a.irk = irk;
-            a.FB1 = FB1, a.FB2 = FB2, a.FB3 = FB3;
-            a.nPML = m.g.nPML;
-            a.pml_on = m.p.pml;
-            a.fs_on = 1;
-            a.kchunk = kchunk_;
-            a.rDH = m.g.rDH;
-            a.DT = DT;
-            a.err = err_dev_;
-            a.work = work_dev_;
-            a.ntiles_x = ntx_, a.ntiles_y = nty_, a.nchunk = nchunk_;
             if (timed_stages) CU(cudaEventRecord(ev_[2], stream));
-            CU(launch_cg_stage(a, maps_[win_map[irk]], grid_ctas_, stream));
+            CU(launch_cg_stage(FB1, FB2, FB3, desc_host_[irk], work_dev_, grid_ctas_, stream));
             if (timed_stages) {
                 CU(cudaEventRecord(ev_[3], stream));
                 CU(cudaEventSynchronize(ev_[3]));
@@ -426,12 +447,24 @@ int Session::launch_step(int step, bool timed_stages)
         CU(launch_sc_surface(A, cjm_, g, decay_, SC_DECAY_LAYERS, pgv_, stream));
         kernel_launches += 10;
     }
-    if (nst > 0) {
-        CU(launch_stations(W_[0], cjm_, g, st_idx_, nst, m.NT, st_out_, it_dev_, m.p.scheme, stream));
-    } else {
-        CU(launch_stations(W_[0], cjm_, g, st_idx_, 0, m.NT, st_out_, it_dev_, m.p.scheme, stream));
-    }
+    if (int st = launch_stations_on(stream)) return st;
     kernel_launches += 1 + (fault_.npts > 0) + (point_.kind != 0 && point_.inside);
+    return ST_OK;
+}
+
+// Sources into W at the stage-0 time of the step *it_dev_ (src/propagate.cpp:198-210).
+int Session::launch_sources_on(cudaStream_t st)
+{
+    const float DT = (float)m.p.DT;
+    CU(launch_point(W_[0], W_[1], W_[2], cjm_, g, point_, it_dev_, DT, m.g.DH, m.p.scheme, st));
+    CU(launch_sources(W_[0], cjm_, g, fault_, point_, it_dev_, DT, m.g.DH, m.p.scheme, st));
+    return ST_OK;
+}
+
+// Station traces of the step just completed; advances *it_dev_.
+int Session::launch_stations_on(cudaStream_t st)
+{
+    CU(launch_stations(W_[0], cjm_, g, st_idx_, nst, m.NT, st_out_, it_dev_, m.p.scheme, st));
     return ST_OK;
 }
 

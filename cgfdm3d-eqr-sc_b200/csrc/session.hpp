@@ -71,6 +71,8 @@ private:
     cudaGraph_t graph8_src_ = nullptr;
     cudaEvent_t ev_[4] = {};
     CgStageMaps maps_[3] = {};                       // TMA descriptors per stencil input A, B, C
+    CgStageDesc desc_host_[4] = {};                  // stage descriptors, one per RK stage
+    int build_stage_descs();
     int *work_dev_ = nullptr;                        // persistent-CTA work counters
     int ntx_ = 1, nty_ = 1, nchunk_ = 1, grid_ctas_ = 1;
     int *err_dev_ = nullptr;                         // device error word of the stage kernels
@@ -78,9 +80,19 @@ private:
     ScTiling sct_ = {};
     static constexpr int SC_DECAY_LAYERS = 20;       // src/exp_decay_absorb.cpp:109
     int check_device_error();
+
+public:
+    // the stage descriptor of RK stage irk, and the stage's work items (batches use these)
+    void stage_desc(int irk, CgStageDesc &d) const;
+    int stage_items() const;
+    int launch_sources_on(cudaStream_t st);
+    int launch_stations_on(cudaStream_t st);
+    int check_errors() { return check_device_error(); }
+    bool snapshots_on() const;
+
+private:
     void ckpt_parts(std::vector<std::pair<void *, size_t>> &parts) const;
     int run_plain(int n);                 // n steps from `it`, graphs where aligned
-    bool snapshots_on() const;
     int write_snapshots(int step);        // slices after step `step`
     std::string out_dir() const;
     float *slice_dev_ = nullptr;

@@ -117,6 +117,25 @@ int cgfdm_checkpoint_size(const cgfdm_session *s, long long *bytes);
 int cgfdm_checkpoint(cgfdm_session *s, void *out, long long bytes);
 int cgfdm_restore(cgfdm_session *s, const void *in, long long bytes);
 
+/* Batches: several CGFDM sessions -- independent shots or media of uneven
+ * grid sizes -- advanced together, every RK stage of all of them in one
+ * persistent launch of the fused stage kernel, eight steps per replay of a
+ * captured CUDA graph.  The sessions must be CGFDM, on one device, at the
+ * same step, without snapshots; they stay owned by the caller and must
+ * outlive the batch, and while batched they are stepped only through it
+ * (cgfdm_batch_run advances each by min(nsteps, steps left to the shortest
+ * NT)).  Results per session are those of running it alone, bit for bit.
+ * The reference runs one model per program; this has no counterpart in src/. */
+typedef struct cgfdm_batch cgfdm_batch;
+int cgfdm_batch_create(cgfdm_session *const *sessions, int n, cgfdm_batch **out);
+int cgfdm_batch_run(cgfdm_batch *b, int nsteps);
+/* As cgfdm_batch_run, returning the device time of the steps in ms. */
+int cgfdm_batch_run_timed(cgfdm_batch *b, int nsteps, float *ms);
+int cgfdm_batch_destroy(cgfdm_batch *b);
+/* Last failure of b, or of the last failed cgfdm_batch_create in this
+ * thread when b is NULL. */
+const char *cgfdm_batch_last_error(const cgfdm_batch *b);
+
 int cgfdm_destroy(cgfdm_session *s);
 
 /* Description of the last failure on `s` (or of the last failed
