@@ -220,6 +220,17 @@ def cpu_reference_rate(name, warmup_steps, timed_steps, procs):
     return {"value": rate, "unit": METRIC, "cores": procs, "kind": "reference", "sample": sample}, None
 
 
+def max_over_ranks(value, dist, device):
+    """Largest per-rank value over all ranks (the value itself without a
+    process group).  Timings of a multi-GPU run are the slowest rank's."""
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------- batches
 def bench_batch(args, world, rank, local_rank):
     """``--workload batchN``: N independent CGFDM shots of uneven sizes
@@ -362,10 +373,7 @@ def main():
     torch.cuda.synchronize(local_rank)
     if dist:
         dist.barrier()
-    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, dist, f"cuda:{local_rank}")
     stage_ms = s.profile_stages(8)
     algo_step = info.algo_bytes_per_step
     algo_launch = algo_step / info.stage_kernels_per_step
@@ -379,10 +387,7 @@ def main():
     i2 = s2.info
     s2.close()
     e2e_s = time.perf_counter() - t0
-    e = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if dist:
-        dist.all_reduce(e, op=dist.ReduceOp.MAX)
-    e2e_s = float(e.item())
+    e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{local_rank}")
 
     value = world * pts * args.steps / (ms_max * 1e-3) / 1e6
     hbm_peak, peak_kind = peaks()
