@@ -309,7 +309,10 @@ constexpr int SCX_NPOS = 64, SCX_NL = 4;
 // memory, five CTAs per SM (register cap 48); on the 512 x 512 x 256 basin
 // workload this beat 80 x 16 at two CTAs by 1.4x and a one-warp-per-pencil
 // register-streaming variant by 1.7x: the passes are latency-bound and
-// occupancy pays.
+// occupancy pays (staging the W window in shared memory first, at three to
+// five CTAs per SM, was 1.5x slower than reading it through L1, and sliding
+// one thread's window over two positions 6 % slower than one position per
+// thread).
 #ifndef SCY_NPOS
 #define SCY_NPOS 32
 #endif
@@ -320,12 +323,8 @@ constexpr int SCX_NPOS = 64, SCX_NL = 4;
 #ifndef SC_TILE_MIN_CTAS
 #define SC_TILE_MIN_CTAS 5
 #endif
-#ifndef SC_STAGE_W
-#define SC_STAGE_W 0     // 1: stage the tile's W window in shared memory before phase A
-#endif
-// shared memory of a tile: left/right states (9 + 9 fields per position) and
-// optionally the W window (9 fields x (NPOS + 4) positions)
-constexpr size_t sc_tile_smem(int npos, int nl) { return sizeof(float) * (18 * npos + (SC_STAGE_W ? 9 * (npos + 4) : 0)) * nl; }
+// shared memory of a tile: left and right states, 9 + 9 fields per position
+constexpr size_t sc_tile_smem(int npos, int nl) { return sizeof(float) * 18 * npos * nl; }
 
 template <int DIR, int NPOS, int NL>
 __global__ void __launch_bounds__(SC_THREADS, SC_TILE_MIN_CTAS) k_sc_tile(const ScDirArgs a)
@@ -360,44 +359,12 @@ __global__ void __launch_bounds__(SC_THREADS, SC_TILE_MIN_CTAS) k_sc_tile(const 
         else lane = it % NL, mi = it / NL;
     };
 
-#if SC_STAGE_W
-    // ---- the tile's W window (positions p0-5 .. p0-5+NPOS+3) into shared memory
-    float *sW = sm + 18 * NPOS * NL;
-    constexpr int NW = NPOS + 4;
-    const int npd = DIR == 0 ? g.nxp : DIR == 1 ? g.nyp : g.nzp;
-    auto widx = [](int v, int r, int lane) { return DIR == 0 ? (v * NL + lane) * NW + r : (v * NW + r) * NL + lane; };
-    for (int it = threadIdx.x; it < NW * NL * 9; it += SC_THREADS) {
-        const int v = it / (NW * NL), rem = it - v * NW * NL;
-        int r, lane;
-        if (DIR == 0) r = rem % NW, lane = rem / NW;
-        else lane = rem % NL, r = rem / NL;
-        const int m = p0 - 5 + r;
-        float x = 0.0f;
-        if (lane0 + lane < lane_end && m >= 0 && m < npd) {
-            int i, j, k;
-            coords(m, lane, i, j, k);
-            x = __ldg(a.W + v * F + g.at(i, j, k));
-        }
-        sW[widx(v, r, lane)] = x;
-    }
-    __syncthreads();
-#endif
     // ---- phase A: both WENO states of every position
     for (int it = threadIdx.x; it < NPOS * NL; it += SC_THREADS) {
         int mi, lane;
         split(it, NPOS, mi, lane);
         const int m = p0 - CGFDM_HALO + mi;
         if (lane0 + lane >= lane_end || m < 2 || m > nd) continue;
-#if SC_STAGE_W
-#pragma unroll 3
-        for (int v = 0; v < 9; v++) {
-            float uL, uR;
-            weno_pair(sW[widx(v, mi, lane)], sW[widx(v, mi + 1, lane)], sW[widx(v, mi + 2, lane)],
-                      sW[widx(v, mi + 3, lane)], sW[widx(v, mi + 4, lane)], uL, uR);
-            sL[sidx(v, mi, lane)] = uL;
-            sR[sidx(v, mi, lane)] = uR;
-        }
-#else
         int i, j, k;
         coords(m, lane, i, j, k);
         const float *w = a.W + g.at(i, j, k);
@@ -410,7 +377,6 @@ __global__ void __launch_bounds__(SC_THREADS, SC_TILE_MIN_CTAS) k_sc_tile(const 
             sL[sidx(v, mi, lane)] = uL;
             sR[sidx(v, mi, lane)] = uR;
         }
-#endif
     }
     __syncthreads();
 

@@ -18,3 +18,11 @@ def hill_fault():
 
 
 CASES["cg_hill_fault"] = (hill_fault, "CGFDM")
+
+
+def sc_hill():
+    c = pu.small_hill(steps=24, NX=24, NY=22, NZ=18, nPML=5)
+    return c
+
+
+CASES["sc_hill"] = (sc_hill, "SCFDM")
