@@ -94,7 +94,6 @@ struct ScDirArgs {
     int irk;
     int copy_halo;       // z pass of stages 0 and 1: carry the halo above the surface to Wout
     float alpha;         // Lax-Friedrichs speed (largest Vp)
-    int npos, nl;        // tile shape, set by launch_sc_dir
 };
 struct ScTiling {
     int npos[3], nl[3], ntiles[3];
@@ -103,10 +102,11 @@ ScTiling sc_tiling(const DevGrid &g);
 
 cudaError_t sc_dir_prepare();
 cudaError_t launch_sc_dir(int dir, ScDirArgs a, const ScTiling &t, cudaStream_t st);
-// Characteristic free surface, halo extrapolation, sponge of the top layers
-// and peak ground velocity, after the third stage of a step.
+// Characteristic free surface, halo extrapolation, sponge of the top layers,
+// peak ground velocity and (dis given) the surface-layer displacement, after
+// the third stage of a step.
 cudaError_t launch_sc_surface(float *W, const float *cjm, DevGrid g, const float *decayG, int ndecay, float *pgv,
-                              cudaStream_t st);
+                              float *dis, float DT, cudaStream_t st);
 cudaError_t launch_sc_sjac(const float *cjm, DevGrid g, float DT, float rDH, float *sjac, cudaStream_t st);
 
 // --------------------------------------------------- sources / stations

@@ -3,8 +3,8 @@
 // exponential-decay sponge.
 //
 // A TVD stage is three pencil kernels, one per grid direction.  Each CTA
-// owns a tile of `npos` consecutive positions along its direction (the tile's
-// points plus the 3 + 3 neighbours their flux differences reach) times `nl`
+// owns a tile of NPOS consecutive positions along its direction (the tile's
+// points plus the 3 + 3 neighbours their flux differences reach) times NL
 // lanes across it, and runs three phases through shared memory:
 //
 //   A  every position m computes, per variable, both WENO5-JS states that
@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(SC_THREADS, SC_TILE_MIN_CTAS) k_sc_tile(const 
 // velocity in that basis; after the condition, sigma = B T B^T, v = B v'.
 // Evaluated in double from the float fields and rounded once.
 __global__ void k_sc_surface(float *W, const float *__restrict__ cjm, DevGrid g, const float *__restrict__ decayG,
-                             int ndecay, float *pgv)
+                             int ndecay, float *pgv, float *dis, float DT)
 {
     const int i = CGFDM_HALO + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = CGFDM_HALO + blockIdx.y * blockDim.y + threadIdx.y;
@@ -544,6 +544,14 @@ __global__ void k_sc_surface(float *W, const float *__restrict__ cjm, DevGrid g,
             for (int v = 0; v < 9; v++) W[v * F + qk] = decay_apply(W[v * F + qk], i, j, k, g, decayG, ndecay);
         }
 
+    // displacement, Dis += (momentum * buoyancy) * DT after the sponge
+    // (src/solve_displacement.cpp:45-62, called at src/propagate.cpp:264-266).
+    // Only the surface layer of Dis is ever read (the FreeSurfU files,
+    // src/data_io.cpp:619-633), so only that layer is integrated.
+    if (dis)
+        for (int c = 0; c < 3; c++)
+            dis[c * F + q] = __fadd_rn(dis[c * F + q], __fmul_rn(__fmul_rn(W[c * F + q], buo), DT));
+
     // peak ground velocity of the surface layer (src/PGV.cpp:115-137)
     if (pgv) {
         const float Vx = __fmul_rn(W[0 * F + q], buo), Vy = __fmul_rn(W[1 * F + q], buo),
@@ -599,7 +607,6 @@ cudaError_t sc_dir_prepare()
 cudaError_t launch_sc_dir(int dir, ScDirArgs a, const ScTiling &t, cudaStream_t st)
 {
     const DevGrid &g = a.g;
-    a.npos = t.npos[dir], a.nl = t.nl[dir];
     if (dir == 0) {
         dim3 gr(t.ntiles[0], (g.ny + SCX_NL - 1) / SCX_NL, g.nz);
         k_sc_tile<0, SCX_NPOS, SCX_NL><<<gr, SC_THREADS, sc_tile_smem(SCX_NPOS, SCX_NL), st>>>(a);
@@ -617,10 +624,10 @@ cudaError_t launch_sc_dir(int dir, ScDirArgs a, const ScTiling &t, cudaStream_t 
 }
 
 cudaError_t launch_sc_surface(float *W, const float *cjm, DevGrid g, const float *decayG, int ndecay, float *pgv,
-                              cudaStream_t st)
+                              float *dis, float DT, cudaStream_t st)
 {
     dim3 b(32, 4), gr((g.nx + 31) / 32, (g.ny + 3) / 4);
-    k_sc_surface<<<gr, b, 0, st>>>(W, cjm, g, decayG, ndecay, pgv);
+    k_sc_surface<<<gr, b, 0, st>>>(W, cjm, g, decayG, ndecay, pgv, dis, DT);
     return cudaGetLastError();
 }
 

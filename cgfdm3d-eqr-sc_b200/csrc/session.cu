@@ -135,10 +135,6 @@ int Session::create(const std::string &dir, const std::string &options, int dev)
         err = "EXP_DECAY is only available with the SCFDM scheme";
         return ST_OPTIONS;
     }
-    if (m.p.scheme == SCHEME_SCFDM && m.p.solve_displacement) {
-        err = "SOLVE_DISPLACEMENT is not available with the SCFDM scheme in this library";
-        return ST_OPTIONS;
-    }
     if (m.p.scheme == SCHEME_SCFDM && m.g.nz < 8) {
         err = "the SCFDM scheme needs NZ >= 8";
         return ST_OPTIONS;
@@ -396,7 +392,6 @@ int Session::launch_step(int step, bool timed_stages)
     const bool cg = m.p.scheme == SCHEME_CGFDM;
     const float DT = (float)m.p.DT;
     int FB1 = FB_TABLE[step % 8][0], FB2 = FB_TABLE[step % 8][1], FB3 = FB_TABLE[step % 8][2];
-    (void)DT;
     if (int st = launch_sources_on(stream)) return st;
     if (cg) {
         for (int irk = 0; irk < 4; irk++) {
@@ -444,7 +439,7 @@ int Session::launch_step(int step, bool timed_stages)
             }
         }
         // characteristic free surface, halo, top-layer sponge, PGV (src/propagate.cpp:245-290)
-        CU(launch_sc_surface(A, cjm_, g, decay_, SC_DECAY_LAYERS, pgv_, stream));
+        CU(launch_sc_surface(A, cjm_, g, decay_, SC_DECAY_LAYERS, pgv_, dis_, DT, stream));
         kernel_launches += 10;
     }
     if (int st = launch_stations_on(stream)) return st;

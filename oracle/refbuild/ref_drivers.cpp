@@ -315,3 +315,14 @@ void oracle_hook_freeWave(WAVE wave)
     oracle_dump("oracle_final_W.bin", wave.W, sizeof(FLOAT) * WSIZE * num);
     freeWave(wave);
 }
+
+#ifdef SOLVE_DISPLACEMENT
+/* ---------------------------------------------------- displacement driver */
+/* src/solve_displacement.cpp:65-74 launches its kernel with dim3 on the GPU
+ * only; on the CPU the kernel body is the loop nest itself. */
+void SolveDisplacementKernel(FLOAT *W, FLOAT *Dis, FLOAT *CJM, int _nx_, int _ny_, int _nz_, FLOAT dt);
+void SolveDisplacement(GRID grid, FLOAT *W, FLOAT *Dis, FLOAT *CJM, FLOAT dt)
+{
+    SolveDisplacementKernel(W, Dis, CJM, grid._nx_, grid._ny_, grid._nz_, dt);
+}
+#endif

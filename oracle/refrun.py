@@ -24,12 +24,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
 
-def ref_binary(scheme: str = "CGFDM") -> str:
-    return os.path.join(REF_DIR, "cgfdm_ref" if scheme.upper() == "CGFDM" else "scfdm_ref")
+def ref_binary(scheme: str = "CGFDM", displacement: bool = False) -> str:
+    """The build of one scheme; ``displacement`` picks the one compiled with
+    SOLVE_DISPLACEMENT (src/propagate.cpp:101-104, 264-266, 305-307), which
+    also writes FreeSurfUx/Uy/Uz with the free-surface snapshots."""
+    name = "cgfdm_ref" if scheme.upper() == "CGFDM" else "scfdm_ref"
+    return os.path.join(REF_DIR, name + ("_dis" if displacement else ""))
 
 
-def available(scheme: str = "CGFDM") -> bool:
-    return os.access(ref_binary(scheme), os.X_OK)
+def available(scheme: str = "CGFDM", displacement: bool = False) -> bool:
+    return os.access(ref_binary(scheme, displacement), os.X_OK)
 
 
 def _params(run_dir: str) -> dict:
@@ -38,13 +42,14 @@ def _params(run_dir: str) -> dict:
     return {k.lower(): v for k, v in p.items()}
 
 
-def run(run_dir: str, scheme: str = "CGFDM", timeout: float = 3600.0, log: Optional[str] = None) -> float:
+def run(run_dir: str, scheme: str = "CGFDM", timeout: float = 3600.0, log: Optional[str] = None,
+        displacement: bool = False) -> float:
     """Runs the reference binary in run_dir; returns wall seconds."""
     out = os.path.join(run_dir, _params(run_dir).get("out", "./output"))
     os.makedirs(out, exist_ok=True)
     t0 = time.perf_counter()
     with open(log or os.path.join(run_dir, "ref.log"), "w") as lf:
-        subprocess.run([ref_binary(scheme)], cwd=run_dir, stdout=lf, stderr=subprocess.STDOUT, check=True,
+        subprocess.run([ref_binary(scheme, displacement)], cwd=run_dir, stdout=lf, stderr=subprocess.STDOUT, check=True,
                        timeout=timeout)
     return time.perf_counter() - t0
 
