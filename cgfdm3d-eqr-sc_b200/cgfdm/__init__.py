@@ -74,6 +74,11 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
     L.cgfdm_checkpoint.argtypes = [vp, vp, ctypes.c_longlong]
     L.cgfdm_restore.argtypes = [vp, vp, ctypes.c_longlong]
     L.cgfdm_destroy.argtypes = [vp]
+    L.cgfdm_set_wavefield.argtypes = [vp, fp, ctypes.c_longlong]
+    L.cgfdm_set_medium.argtypes = [vp, fp, ctypes.c_longlong]
+    L.cgfdm_adjoint_apply.argtypes = [vp, ctypes.c_int, fp, ctypes.c_longlong]
+    L.cgfdm_gradient.argtypes = [vp, fp, ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(ctypes.c_double), fp,
+                                 ctypes.c_longlong]
     L.cgfdm_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
     L.cgfdm_batch_run.argtypes = [vp, ctypes.c_int]
     L.cgfdm_batch_run_timed.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
@@ -167,6 +172,36 @@ class Session:
 
     def write_outputs(self) -> None:
         self._check(self.L.cgfdm_write_outputs(self._h))
+
+    def set_wavefield(self, w: np.ndarray) -> None:
+        """Overwrites the wavefield, [nzp][nyp][nxp][9] (cgfdm_set_wavefield)."""
+        w = np.ascontiguousarray(w, np.float32)
+        self._check(self.L.cgfdm_set_wavefield(self._h, _fptr(w), w.size))
+
+    def set_medium(self, medium: np.ndarray) -> None:
+        """New (Vs, Vp, rho) medium, [nzp][nyp][nxp][3]; back to step 0 (cgfdm_set_medium)."""
+        medium = np.ascontiguousarray(medium, np.float32)
+        self._check(self.L.cgfdm_set_medium(self._h, _fptr(medium), medium.size))
+
+    def adjoint_apply(self, state: np.ndarray, nsteps: int) -> np.ndarray:
+        """Transpose of the last ``nsteps`` steps applied to ``state`` (cgfdm_adjoint_apply)."""
+        out = np.array(state, np.float32, copy=True, order="C")
+        self._check(self.L.cgfdm_adjoint_apply(self._h, int(nsteps), _fptr(out), out.size))
+        return out
+
+    def gradient(self, observed: np.ndarray, checkpoint_every: int = 100):
+        """Misfit J = 1/2 sum (v - d)^2 over the station velocities and its
+        gradient [3][nz][ny][nx] with respect to (Vp, Vs, rho) (cgfdm_gradient).
+        ``observed`` is [n_stations][NT][3]."""
+        i = self.info
+        obs = np.ascontiguousarray(observed, np.float32)
+        if obs.shape != (i.n_stations, i.NT, 3):
+            raise ValueError(f"observed must be ({i.n_stations}, {i.NT}, 3), got {obs.shape}")
+        grad = np.zeros((3, i.nz, i.ny, i.nx), np.float32)
+        J = ctypes.c_double()
+        self._check(self.L.cgfdm_gradient(self._h, _fptr(obs), obs.size, int(checkpoint_every), ctypes.byref(J),
+                                          _fptr(grad), grad.size))
+        return J.value, grad
 
     def close(self) -> None:
         if self._h:

@@ -151,6 +151,36 @@ int cgfdm_restore(cgfdm_session *s, const void *in, long long bytes)
     return s->s.restore(in, (size_t)bytes);
 }
 
+int cgfdm_set_wavefield(cgfdm_session *s, const float *in, long long count)
+{
+    if (!s || !in) return CGFDM_E_ARG;
+    if (count < s->s.m.g.npad() * 9) return CGFDM_E_ARG;
+    return s->s.set_wavefield(in);
+}
+
+int cgfdm_set_medium(cgfdm_session *s, const float *medium, long long count)
+{
+    if (!s || !medium) return CGFDM_E_ARG;
+    if (count < s->s.m.g.npad() * 3) return CGFDM_E_ARG;
+    return s->s.set_medium(medium);
+}
+
+int cgfdm_adjoint_apply(cgfdm_session *s, int nsteps, float *state, long long count)
+{
+    if (!s || !state) return CGFDM_E_ARG;
+    if (count < s->s.m.g.npad() * 9) return CGFDM_E_ARG;
+    return s->s.adjoint_apply(nsteps, state);
+}
+
+int cgfdm_gradient(cgfdm_session *s, const float *observed, long long obs_count, int checkpoint_every,
+                   double *misfit, float *grad, long long grad_count)
+{
+    if (!s || !grad || (!observed && s->s.nst > 0)) return CGFDM_E_ARG;
+    if (obs_count < (long long)s->s.nst * s->s.m.NT * 3) return CGFDM_E_ARG;
+    if (grad_count < 3LL * s->s.m.g.nx * s->s.m.g.ny * s->s.m.g.nz) return CGFDM_E_ARG;
+    return s->s.gradient(observed, checkpoint_every, misfit, grad);
+}
+
 int cgfdm_batch_create(cgfdm_session *const *sessions, int n, cgfdm_batch **out)
 {
     if (!sessions || n <= 0 || !out) {

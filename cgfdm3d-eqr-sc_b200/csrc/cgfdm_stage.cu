@@ -421,6 +421,11 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
             for (int c = 0; c < 3; c++) vet[c] = T.ry(c, rDH) * by;
             if (k == _nz - 1) {
                 const long long s = g.at2(i, j);
+                if (a.vdstore)
+                    for (int c = 0; c < 3; c++) {
+                        a.vdstore[c * g.plane + s] = vxi[c];
+                        a.vdstore[(3 + c) * g.plane + s] = vet[c];
+                    }
                 for (int r = 0; r < 3; r++) {
                     const float *dx = a.rdz + (long long)(r * 3) * g.plane + s;
                     const float *dy = a.rdz + (long long)(9 + r * 3) * g.plane + s;
@@ -507,6 +512,10 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
                 }
             }
         }
+
+        if (a.hstore)
+#pragma unroll
+            for (int f = 0; f < 9; f++) a.hstore[f * F + q] = h[f];
 
         // ---- RK4 update of the wavefield (src/wave_rk.cpp:17-104)
         float wout[9];

@@ -38,6 +38,8 @@ struct CgStageArgs {
     PmlFace face[5];     // x1 y1 z1 x2 y2 (order of src/pml_deriv.cpp:633-646)
     float *pgv;          // [ny][nx][2] running max, stage 3 only
     float *dis;          // displacement, 3 fields in the W layout, stage 3 only
+    float *hstore;       // or null: receives this stage's RHS h (9 fields, W layout) for the adjoint
+    float *vdstore;      // or null: receives the surface layer's xi/eta velocity derivatives (6 x plane)
     int *err;            // device error word: bit 0 = a bounded wait gave up
     int ntiles_x, ntiles_y, nchunk;  // work items: tiles x tiles x z-chunks
     int irk;
@@ -108,6 +110,45 @@ cudaError_t launch_sc_dir(int dir, ScDirArgs a, const ScTiling &t, cudaStream_t 
 cudaError_t launch_sc_surface(float *W, const float *cjm, DevGrid g, const float *decayG, int ndecay, float *pgv,
                               float *dis, float DT, cudaStream_t st);
 cudaError_t launch_sc_sjac(const float *cjm, DevGrid g, float DT, float rDH, float *sjac, cudaStream_t st);
+
+// ------------------------------------------------------ CGFDM adjoint
+// One RK4 stage of the transposed step (csrc/adjoint.cu).  Going back
+// through stage s = 3, 2, 1, 0 of step n, with lambda' the adjoint of
+// W_{n+1}, mu_s the adjoint of the stage's RHS h_s and nu_s = L_s^T mu_s:
+//   mu_3 = b4 lambda'; mu_2 = b3 lambda' + nu_3; mu_1 = b2 lambda' + a3 nu_2;
+//   mu_0 = b1 lambda' + a2 nu_1;  lambda_n = lambda' + nu_3 + nu_2 + nu_1 + nu_0,
+// for the wavefield and, point-wise, for the PML auxiliaries.
+struct AdjStageArgs {
+    DevGrid g;
+    const float *cjm, *rdz;
+    const float *drdz;   // d rdz / d mu (18 fields) then d rdz / d lambda (18), [36][plane], or null
+    const float *pml_alpha_x, *pml_beta_x, *pml_d_x;
+    const float *pml_alpha_y, *pml_beta_y, *pml_d_y;
+    const float *pml_alpha_z, *pml_beta_z, *pml_d_z;
+    const float *Lp;     // lambda' (9 fields)
+    float *M;            // mu_s in; mu_{s-1} out
+    float *Lam;          // running sum; lambda_n after stage 0
+    float *Phi;          // 27 fields: per direction, the adjoint of its one-sided differences
+    float *SF;           // surface layers L = 0..2 (k = _nz-1-L): 12 channels each, [3][12][plane]
+    PmlFace face[5];     // adjoint auxiliaries per face: A = lambda', B = mu, T = running sum
+    const float *h;      // stored RHS h_s of the forward stage (9 fields), or null: no gradient
+    const float *vd;     // stored surface xi/eta velocity derivatives (6 x plane) of the stage
+    float *grad;         // 3 fields: d J / d (mu, lambda, buoyancy), accumulated
+    int irk;
+    int FB1, FB2, FB3;
+    int nPML, pml_on, fs_on;
+    float rDH, DT;
+};
+cudaError_t launch_adj_stage(const AdjStageArgs &a, cudaStream_t st);
+// Adds the seismogram residual of sample n, res[station][n][3], to the
+// velocity of lambda (the misfit is 1/2 sum (v - d)^2).
+cudaError_t launch_adj_residual(float *Lp, DevGrid g, const int *st_idx, int nst, int NT, int n, const float *res,
+                                cudaStream_t st);
+// d rdz / d mu and d rdz / d lambda at the surface, in FP64 dual numbers.
+cudaError_t launch_surface_derivs(const float *cjm, DevGrid g, float *drdz, cudaStream_t st);
+// (mu, lambda, buoyancy) gradients -> (Vp, Vs, rho) on the interior,
+// out [3][nz][ny][nx]; medium [_nz_][_ny_][_nx_][3] as (Vs, Vp, rho).
+cudaError_t launch_grad_chain(const float *grad, const float *medium, DevGrid g, float *out, cudaStream_t st);
 
 // --------------------------------------------------- sources / stations
 struct FaultDev {

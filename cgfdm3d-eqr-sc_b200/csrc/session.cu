@@ -8,6 +8,7 @@
 // one cycle of the FB sign table (src/propagate.cpp:158-168) and are
 // captured once as a CUDA graph that is replayed.
 #include "session.hpp"
+#include "session_util.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -18,6 +19,11 @@ namespace cgfdm {
 
 static const int FB_TABLE[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, -1, 1},
                                    {-1, 1, -1},  {1, -1, -1}, {1, -1, 1}, {-1, 1, 1}};
+
+void fb_signs(int step, int fb[3])
+{
+    for (int c = 0; c < 3; c++) fb[c] = FB_TABLE[step % 8][c];
+}
 
 // ----------------------------------------------------------------- CFL
 // Smallest/largest point-to-plane distance through the six diagonal
@@ -102,20 +108,6 @@ void *Session::alloc(size_t bytes)
     device_bytes += bytes;
     return p;
 }
-
-#define ALLOC(ptr, type, count)                                                                                  \
-    do {                                                                                                         \
-        ptr = (type *)alloc(sizeof(type) * (size_t)(count));                                                    \
-        if (!ptr) {                                                                                              \
-            err = "cannot allocate device memory for " #ptr;                                                     \
-            return ST_ALLOC;                                                                                     \
-        }                                                                                                        \
-    } while (0)
-#define CU(x)                                                                                                    \
-    do {                                                                                                         \
-        cudaError_t e__ = (x);                                                                                   \
-        if (e__ != cudaSuccess) return cuda_fail(e__, #x);                                                       \
-    } while (0)
 
 // --------------------------------------------------------------- create
 int Session::create(const std::string &dir, const std::string &options, int dev)

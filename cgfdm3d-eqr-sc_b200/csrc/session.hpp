@@ -12,6 +12,10 @@
 
 namespace cgfdm {
 
+// FB signs of the first RK stage of a step (src/propagate.cpp:158-168);
+// each later stage flips all three.
+void fb_signs(int step, int fb[3]);
+
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
@@ -34,6 +38,11 @@ public:
     size_t checkpoint_bytes() const;
     int checkpoint(void *host, size_t bytes);       // state at the current step boundary
     int restore(const void *host, size_t bytes);    // from a checkpoint of an identical session
+    int set_wavefield(const float *host_aos);       // [_nz_][_ny_][_nx_][9]; PML auxiliaries kept
+    // CGFDM adjoint (csrc/gradient.cu)
+    int adjoint_apply(int nsteps, float *host_aos);  // transpose of the last nsteps steps, in place
+    int gradient(const float *obs, int ckpt_every, double *misfit, float *grad);
+    int set_medium(const float *host_medium);       // [_nz_][_ny_][_nx_][3] (Vs, Vp, rho); back to step 0
 
     Model m;
     DevGrid g;
@@ -91,6 +100,21 @@ public:
     bool snapshots_on() const;
 
 private:
+    // adjoint state: lambda', mu, running sum (9 fields each), the per-
+    // direction difference adjoints (27 fields), the surface channels, the
+    // auxiliaries' adjoints per face, the gradient and d rdz / d (mu, lambda)
+    struct Adjoint {
+        float *Lp = nullptr, *M = nullptr, *Lam = nullptr, *Phi = nullptr, *SF = nullptr;
+        PmlFace face[5] = {};
+        float *grad = nullptr, *drdz = nullptr;
+    } adj_;
+    int adj_prepare();
+    void adj_args(AdjStageArgs &a, int irk, const int FB[3]) const;
+    int adj_step(int n, float *const *h4, float *const *vd4);  // lambda_{n+1} -> lambda_n
+    void adj_swap();
+    size_t state_bytes() const;                                  // W_A and the faces' A
+    int save_state(char *dst);
+    int load_state(const char *src);
     void ckpt_parts(std::vector<std::pair<void *, size_t>> &parts) const;
     int run_plain(int n);                 // n steps from `it`, graphs where aligned
     int write_snapshots(int step);        // slices after step `step`

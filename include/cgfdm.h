@@ -117,6 +117,48 @@ int cgfdm_checkpoint_size(const cgfdm_session *s, long long *bytes);
 int cgfdm_checkpoint(cgfdm_session *s, void *out, long long bytes);
 int cgfdm_restore(cgfdm_session *s, const void *in, long long bytes);
 
+/* Overwrites the wavefield, [nzp][nyp][nxp][9] (halo included, held equal
+ * in every stage buffer as the point sources keep it); the PML auxiliaries
+ * and the step counter are kept.  No counterpart in src/ (an initial
+ * condition; the reference always starts from rest). */
+int cgfdm_set_wavefield(cgfdm_session *s, const float *in, long long count);
+
+/* Replaces the medium, [nzp][nyp][nxp][3] as (Vs, Vp, rho) in m/s and
+ * kg/m^3 -- the layout of a mediumFile -- and rebuilds the packed medium,
+ * the free-surface matrices and the finite-fault scaling from it as
+ * cgfdm_create does (src/CJM.cpp:52-77, src/contravariant.cpp:365-461); the
+ * session returns to step 0 at rest.  CFL is re-checked at the session's DT
+ * (CGFDM_E_CFL).  CGFDM only. */
+int cgfdm_set_medium(cgfdm_session *s, const float *medium, long long count);
+
+/* Discrete adjoint of the CGFDM time loop (no counterpart in src/).
+ *
+ * cgfdm_gradient: gradient of the seismogram misfit
+ *     J = 1/2 sum over stations, samples n < NT and components x, y, z of
+ *         (v - d)^2,
+ * v the velocity the run records at the stations (station file
+ * components 0..2), d = observed [n_stations][NT][3], with respect to Vp,
+ * Vs and rho at every interior grid point: grad [3][nz][ny][nx] (Vp, Vs,
+ * rho; zero inside the PML layers), *misfit = J.  The session must stand at
+ * step 0 (new, or after cgfdm_set_medium) and have point sources only; it
+ * runs the whole forward once keeping the state every `checkpoint_every`
+ * steps in device memory, then per segment, last first, re-runs it storing
+ * each RK stage's right-hand side and steps the transposed operator back
+ * through it.  Device memory: (NT / checkpoint_every + 1) states plus
+ * 36 * checkpoint_every wavefield-sized fields; CGFDM_E_ALLOC names the
+ * amount when it is not free.  The session ends at step NT with the forward
+ * run's state and station traces.
+ *
+ * cgfdm_adjoint_apply: applies the transpose of the last `nsteps` steps the
+ * session ran (without source and station terms) to `state`,
+ * [nzp][nyp][nxp][9] in and out; the PML auxiliaries' adjoints start from
+ * zero.  Halo entries are ignored on input and zero on output.  With x and
+ * y interior-only states, <A x, y> = <x, A^T y> for A the forward map from
+ * cgfdm_set_wavefield to cgfdm_get_wavefield (the dot-product test). */
+int cgfdm_gradient(cgfdm_session *s, const float *observed, long long obs_count, int checkpoint_every,
+                   double *misfit, float *grad, long long grad_count);
+int cgfdm_adjoint_apply(cgfdm_session *s, int nsteps, float *state, long long count);
+
 /* Batches: several CGFDM sessions -- independent shots or media of uneven
  * grid sizes -- advanced together, every RK stage of all of them in one
  * persistent launch of the fused stage kernel, eight steps per replay of a

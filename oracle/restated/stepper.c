@@ -18,9 +18,15 @@
  *   src.bin         finite fault: int64 npts, int64 nt, float dt,
  *                   int64 index[npts], float rate[nt][npts][6] (unscaled)
  *   stations.bin    int32 [n][3] padded-grid indices
+ *   perturb.txt     optional, lines "i j k dmu dlambda dbuoyancy": additions
+ *                   (in REAL) to the medium of padded-grid point (i, j, k)
+ *                   of the CGFDM stencil, the free-surface matrices of a
+ *                   perturbed surface point recomputed from it (finite
+ *                   differences of the misfit for the adjoint's tests)
  * Output (float32, in the bundle directory):
  *   out_stations.bin [n][NT][9], out_W.bin [_nz_][_ny_][_nx_][9],
- *   out_pgv.bin [ny][nx][2]
+ *   out_pgv.bin [ny][nx][2]; the FP64 build also writes
+ *   out_stations64.bin [n][NT][9] in float64
  *
  * Layout: the reference's array-of-structures, point (i, j, k) at
  * i + j*_nx_ + k*_nx_*_ny_ (src/axis.h:73), 9 fields per point.
@@ -55,12 +61,14 @@ static float vp_max;
 
 static float *CJM;    /* [np][ncjm] */
 static float *RDZ;    /* [2][nyp*nxp][9] */
+static real *CJMR;    /* CJM in REAL, with the perturbations of perturb.txt */
+static real *RDZR;    /* RDZ in REAL, recomputed at perturbed surface cells */
 static int nst;
 static int *ST;       /* [nst][3] */
 
 static long long np_pad;
 #define IDX(i, j, k) ((long long)(i) + (long long)(j) * nxp + (long long)(k) * nxp * nyp)
-#define C(idx, f) ((real)CJM[(idx) * ncjm + (f)])
+#define C(idx, f) (CJMR[(idx) * ncjm + (f)])
 
 static real *W, *Wh, *Wt, *Wm; /* state, RHS, RK accumulator, step start */
 static real *Ust;              /* stations [nst][NT][9] */
@@ -418,7 +426,7 @@ static void cg_deriv(int FB1, int FB2, int FB3)
                     }
                     if (k == _nz - 1) {
                         const long long s = (long long)j * nxp + i;
-                        const float *dx = RDZ + s * 9, *dy = RDZ + ((long long)nxp * nyp + s) * 9;
+                        const real *dx = RDZR + s * 9, *dy = RDZR + ((long long)nxp * nyp + s) * 9;
                         for (int r = 0; r < 3; r++)
                             vzt[r] = ((dx[r * 3] * vxi[0] + dx[r * 3 + 1] * vxi[1]) + dx[r * 3 + 2] * vxi[2]) +
                                      ((dy[r * 3] * vet[0] + dy[r * 3 + 1] * vet[1]) + dy[r * 3 + 2] * vet[2]);
@@ -455,7 +463,7 @@ static void cg_deriv(int FB1, int FB2, int FB3)
                         for (int f = 0; f < 9; f++) hA[f] = (rhs[f] - ad * aux[f]) * (real)DT;
                         if (k == _nz - 1 && a < 2) {
                             const long long s = (long long)j * nxp + i;
-                            const float *mr = RDZ + ((long long)a * nxp * nyp + s) * 9;
+                            const real *mr = RDZR + ((long long)a * nxp * nyp + s) * 9;
                             real vz[9] = {0}, t3[9];
                             for (int r = 0; r < 3; r++) vz[r] = (mr[r * 3] * d[0] + mr[r * 3 + 1] * d[1]) + mr[r * 3 + 2] * d[2];
                             dir_rhs(C(q, 6), C(q, 7), C(q, 8), vz, mu, lam, buo, t3);
@@ -762,6 +770,86 @@ static void pgv_update(void)
         }
 }
 
+/* ======================================================= perturbations
+ * The traction-free zeta derivative at the surface (src/contravariant.cpp:
+ * 365-461): V_zeta = rx V_xi + ry V_eta with rx = -DZ^-1 DX, ry = -DZ^-1 DY,
+ * DZ, DX, DY the 3x3 blocks of the surface traction from the zeta, xi and
+ * eta velocity derivatives.  m: xi_x .. zt_z at the point.
+ */
+static void surface_rdz(const real *m, real mu, real lam, real *rx, real *ry)
+{
+    const real *xi = m, *et = m + 3, *zt = m + 6;
+    const real chi = 2 * lam + mu, lm = lam + mu;
+    real DZ[9], DX[9], DY[9], A[9];
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++)
+            DZ[r * 3 + c] = r == c ? chi * zt[r] * zt[r] + mu * (zt[0] * zt[0] + zt[1] * zt[1] + zt[2] * zt[2] - zt[r] * zt[r])
+                                   : lm * zt[r] * zt[c];
+    for (int b = 0; b < 2; b++) {
+        const real *a = b == 0 ? xi : et;
+        real *D = b == 0 ? DX : DY;
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++)
+                D[r * 3 + c] = r == c ? chi * zt[r] * a[r] + mu * (zt[0] * a[0] + zt[1] * a[1] + zt[2] * a[2] - zt[r] * a[r])
+                                      : lam * zt[r] * a[c] + mu * zt[c] * a[r];
+    }
+    /* inverse of DZ by its adjugate */
+    const real det = DZ[0] * (DZ[4] * DZ[8] - DZ[5] * DZ[7]) - DZ[1] * (DZ[3] * DZ[8] - DZ[5] * DZ[6]) +
+                     DZ[2] * (DZ[3] * DZ[7] - DZ[4] * DZ[6]);
+    A[0] = (DZ[4] * DZ[8] - DZ[5] * DZ[7]) / det, A[1] = (DZ[2] * DZ[7] - DZ[1] * DZ[8]) / det;
+    A[2] = (DZ[1] * DZ[5] - DZ[2] * DZ[4]) / det, A[3] = (DZ[5] * DZ[6] - DZ[3] * DZ[8]) / det;
+    A[4] = (DZ[0] * DZ[8] - DZ[2] * DZ[6]) / det, A[5] = (DZ[2] * DZ[3] - DZ[0] * DZ[5]) / det;
+    A[6] = (DZ[3] * DZ[7] - DZ[4] * DZ[6]) / det, A[7] = (DZ[1] * DZ[6] - DZ[0] * DZ[7]) / det;
+    A[8] = (DZ[0] * DZ[4] - DZ[1] * DZ[3]) / det;
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) {
+            real vx = 0, vy = 0;
+            for (int t = 0; t < 3; t++) vx += A[r * 3 + t] * DX[t * 3 + c], vy += A[r * 3 + t] * DY[t * 3 + c];
+            rx[r * 3 + c] = -vx, ry[r * 3 + c] = -vy;
+        }
+}
+
+static void load_model(const char *dir)
+{
+    CJMR = malloc(sizeof(real) * np_pad * ncjm);
+    for (long long n = 0; n < np_pad * ncjm; n++) CJMR[n] = (real)CJM[n];
+    if (scheme != 0) return;
+    RDZR = malloc(sizeof(real) * 18 * nxp * nyp);
+    for (long long n = 0; n < 18LL * nxp * nyp; n++) RDZR[n] = (real)RDZ[n];
+    char p[4096];
+    snprintf(p, sizeof p, "%s/perturb.txt", dir);
+    FILE *f = fopen(p, "r");
+    if (!f) return;
+    int i, j, k;
+    double dm, dl, db;
+    while (fscanf(f, "%d %d %d %lf %lf %lf", &i, &j, &k, &dm, &dl, &db) == 6) {
+        if (i < 0 || j < 0 || k < 0 || i >= nxp || j >= nyp || k >= nzp) die("perturbation outside the grid", p);
+        const long long q = IDX(i, j, k);
+        CJMR[q * ncjm + 10] += (real)dm;
+        CJMR[q * ncjm + 11] += (real)dl;
+        CJMR[q * ncjm + 12] += (real)db;
+        if (k == nzp - HALO - 1) {
+            const long long s = (long long)j * nxp + i;
+            surface_rdz(CJMR + q * ncjm, CJMR[q * ncjm + 10], CJMR[q * ncjm + 11], RDZR + s * 9,
+                        RDZR + ((long long)nxp * nyp + s) * 9);
+        }
+    }
+    fclose(f);
+}
+
+static void write_f64(const char *dir, const char *name, const real *x, long long n)
+{
+    char p[4096];
+    snprintf(p, sizeof p, "%s/%s", dir, name);
+    FILE *f = fopen(p, "wb");
+    if (!f) die("cannot write", p);
+    for (long long o = 0; o < n; o++) {
+        double v = (double)x[o];
+        fwrite(&v, 8, 1, f);
+    }
+    fclose(f);
+}
+
 /* ================================================================ main */
 int main(int argc, char **argv)
 {
@@ -775,6 +863,7 @@ int main(int argc, char **argv)
         RDZ = read_file(dir, "rdz.bin", &nb);
         if (!RDZ || nb != sizeof(float) * 18 * nxp * nyp) die("bad rdz.bin in", dir);
     }
+    load_model(dir);
     ST = read_file(dir, "stations.bin", &nb);
     nst = ST ? (int)(nb / 12) : 0;
     if (src_kind == 3) {
@@ -837,6 +926,7 @@ int main(int argc, char **argv)
         pgv_update();
     }
     write_f32(dir, "out_stations.bin", Ust, (long long)nst * NT * 9);
+    if (!IS_F32) write_f64(dir, "out_stations64.bin", Ust, (long long)nst * NT * 9);
     write_f32(dir, "out_W.bin", W, np_pad * 9);
     write_f32(dir, "out_pgv.bin", PGV, (long long)nx * ny * 2);
     return 0;
