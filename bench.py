@@ -303,6 +303,112 @@ def bench_batch(args, world, rank, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------- adjoint
+ADJ_BYTES_PER_POINT_STAGE = 4 * (9 + 9 + 9 + 12 + 18 + 9 + 6)
+
+
+def bench_adjoint(args, world, rank, local_rank):
+    """``--workload adjoint[_STEPS]``: the misfit gradient with respect to
+    Vp, Vs and rho (cgfdm_gradient) on the 192 x 192 x 128 layered model
+    with a 2 km, +8 % Vs ball in the true medium (cgfdm.configs.adjoint_shots):
+    four shots (2 Hz Ricker point sources), 64 surface stations, NT = 2000
+    steps each (or STEPS), checkpoints every 100 steps.  The observed data
+    are the true medium's seismograms; the gradient is taken at the starting
+    medium (no ball) and summed over the shots.  Reports gradient throughput
+    (shots x points x NT / seconds) and the adjoint/forward cost: wall time
+    of the gradient over that of a forward run of the same shot (both from
+    step 0, medium set, traces read back).  One GPU; --steps/--warmup do
+    not apply (a shot is one unit)."""
+    import numpy as np
+    import torch
+    from cgfdm import Session, configs
+
+    NT = int(args.workload.split("_")[1]) if "_" in args.workload else 2000
+    root = os.path.join(WORK, f"adjoint_{NT}")
+    marker = os.path.join(root, ".done")
+    if not os.path.exists(marker):
+        if os.path.exists(root):
+            shutil.rmtree(root)
+        configs.adjoint_shots(root, steps=NT)
+        open(marker, "w").close()
+    dirs = sorted(os.path.join(root, d) for d in os.listdir(root) if d.startswith("shot_"))
+    NX, NY, NZ, DH = 192, 192, 128, 100.0
+    true = configs.adjoint_layers(NX, NY, NZ, DH, True)
+    start = configs.adjoint_layers(NX, NY, NZ, DH, False)
+    K = 100
+    t_fwd = t_grad = 0.0
+    phases = np.zeros(3)
+    grad_sum = None
+    J_sum = 0.0
+    with ClockSampler(local_rank) as clk:
+        for d in dirs:
+            s = Session(d, device=local_rank)
+            info = s.info
+            s.set_medium(true)
+            s.run(info.NT)
+            obs = s.stations()[:, :, :3].copy()
+            # forward run alone (second forward of the shot: warm)
+            s.set_medium(start)
+            torch.cuda.synchronize(local_rank)
+            t0 = time.perf_counter()
+            s.run(info.NT)
+            s.stations()
+            torch.cuda.synchronize(local_rank)
+            t_fwd += time.perf_counter() - t0
+            s.set_medium(start)
+            torch.cuda.synchronize(local_rank)
+            t0 = time.perf_counter()
+            J, g = s.gradient(obs, K)
+            torch.cuda.synchronize(local_rank)
+            t_grad += time.perf_counter() - t0
+            phases += np.array(s.gradient_profile())
+            J_sum += J
+            grad_sum = g if grad_sum is None else grad_sum + g
+            pts = info.nx * info.ny * info.nz
+            dev_gb = info.device_bytes / 1e9
+            s.close()
+    n = len(dirs)
+    steps_adj = n * NT
+    adj_ms_step = phases[2] / steps_adj
+    algo = ADJ_BYTES_PER_POINT_STAGE * 4 * pts
+    achieved = algo / (adj_ms_step * 1e-3) / 1e9
+    hbm_peak, peak_kind = peaks()
+    # the gradient should see the ball: its Vs gradient there against elsewhere
+    kk, jj, ii = np.meshgrid(np.arange(NZ), np.arange(NY), np.arange(NX), indexing="ij")
+    zc = (NZ - 1) - 0.4 * NZ
+    inside = np.sqrt((ii - (NX - 1) / 2) ** 2 + (jj - (NY - 1) / 2) ** 2 + (kk - zc) ** 2) * DH < 2000.0
+    gvs = grad_sum[1]
+    line = {
+        "metric": METRIC, "value": n * pts * NT / t_grad / 1e6, "unit": METRIC, "n_gpus": 1, "steps": NT,
+        "warmup": 0, "ms_per_step": t_grad * 1e3 / steps_adj, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "scheme": "CGFDM",
+        "config": {"workload": "adjoint: CGFDM misfit gradient w.r.t. Vp, Vs, rho, 192x192x128, DH=100 m, 4 layers "
+                               "+ half-space, true model with a 2 km-radius +8% Vs ball, 4 shots (2 Hz Ricker "
+                               "point sources), 64 surface stations, checkpoint every 100 steps, FP32",
+                   "points": pts, "shots": n, "NT": NT, "checkpoint_every": K,
+                   "l2": "inputs larger than L2 (%.1f GB resident per session)" % dev_gb,
+                   "parallelism": "replicas x1"},
+        "adjoint_over_forward": t_grad / t_fwd,
+        "forward_s": t_fwd, "gradient_s": t_grad,
+        "phases_ms": {"forward_with_checkpoints": phases[0], "segment_reruns_storing_rhs": phases[1],
+                      "adjoint_steps": phases[2]},
+        "misfit": J_sum,
+        "grad_vs_ball_over_outside": float(np.abs(gvs[inside]).mean() / max(np.abs(gvs[~inside]).mean(), 1e-300)),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,
+                     "kernel": "k_adj_pre + k_adj_gather (one adjoint step = 4 stages x 2 launches)",
+                     "algo_bytes_per_step": algo, "mean_step_ms": adj_ms_step},
+        "e2e": {"value": n * pts * NT / t_grad / 1e6, "unit": METRIC,
+                "h2d_bytes_per_step": (start.nbytes + n * 0) / NT, "d2h_bytes_per_step": grad_sum.nbytes / NT / n,
+                "path": "cgfdm_set_medium + cgfdm_gradient (host observed data in, host gradient out)"},
+        "gpu_launches": int(n * NT * (6 + 6 + 9)),
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 # ------------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -342,6 +448,8 @@ def main():
 
     if args.workload.startswith("batch"):
         return bench_batch(args, world, rank, local_rank)
+    if args.workload.startswith("adjoint"):
+        return bench_adjoint(args, world, rank, local_rank)
 
     dist = None
     if world > 1:

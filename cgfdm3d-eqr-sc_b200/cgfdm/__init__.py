@@ -77,6 +77,7 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
     L.cgfdm_set_wavefield.argtypes = [vp, fp, ctypes.c_longlong]
     L.cgfdm_set_medium.argtypes = [vp, fp, ctypes.c_longlong]
     L.cgfdm_adjoint_apply.argtypes = [vp, ctypes.c_int, fp, ctypes.c_longlong]
+    L.cgfdm_gradient_profile.argtypes = [vp, fp]
     L.cgfdm_gradient.argtypes = [vp, fp, ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(ctypes.c_double), fp,
                                  ctypes.c_longlong]
     L.cgfdm_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
@@ -202,6 +203,13 @@ class Session:
         self._check(self.L.cgfdm_gradient(self._h, _fptr(obs), obs.size, int(checkpoint_every), ctypes.byref(J),
                                           _fptr(grad), grad.size))
         return J.value, grad
+
+    def gradient_profile(self):
+        """Device ms of the last gradient's phases: forward with checkpoints,
+        segment re-runs storing the stage RHS, adjoint steps."""
+        ms = np.zeros(3, np.float32)
+        self._check(self.L.cgfdm_gradient_profile(self._h, _fptr(ms)))
+        return tuple(float(x) for x in ms)
 
     def close(self) -> None:
         if self._h:

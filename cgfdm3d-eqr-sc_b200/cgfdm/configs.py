@@ -312,3 +312,55 @@ def batch_shots(root: str, n: int = 32, steps: int = 1500, seed: int = 5, sizes=
         cases.write_case(c, d)
         dirs.append(d)
     return dirs
+
+
+def adjoint_layers(NX: int, NY: int, NZ: int, DH: float, anomaly: bool, radius: float = 2000.0,
+                   dvs: float = 0.08) -> np.ndarray:
+    """Medium of the adjoint workload, [nzp][nyp][nxp][3] (Vs, Vp, rho):
+    four layers over a half-space under a flat surface (Vp 4500 -> 7000 m/s,
+    Vs = Vp / 1.73, Gardner density), and, with ``anomaly``, a ball of
+    radius ``radius`` (2 km) of Vs + ``dvs`` (8 %) centred at 40 % of the
+    model depth."""
+    nxp, nyp, nzp = NX + 2 * HALO, NY + 2 * HALO, NZ + 2 * HALO
+    depth = (NZ - 1 - (np.arange(nzp) - HALO)) * DH          # metres below the surface
+    tops = np.array([0.0, 0.15, 0.3, 0.5, 0.7]) * NZ * DH
+    vps = np.array([4500.0, 5200.0, 5900.0, 6500.0, 7000.0])
+    li = np.clip(np.searchsorted(tops, depth, side="right") - 1, 0, len(tops) - 1)
+    vp = np.broadcast_to(vps[li][:, None, None], (nzp, nyp, nxp)).astype(np.float64)
+    vs = vp / 1.73
+    rho = 310.0 * vp ** 0.25
+    if anomaly:
+        kk, jj, ii = np.meshgrid(np.arange(nzp), np.arange(nyp), np.arange(nxp), indexing="ij")
+        zc = (NZ - 1) - 0.4 * NZ + HALO
+        r = np.sqrt((ii - (nxp - 1) / 2) ** 2 + (jj - (nyp - 1) / 2) ** 2 + (kk - zc) ** 2) * DH
+        vs = vs * np.where(r < radius, 1.0 + dvs, 1.0)
+    return np.stack([vs, vp, rho], -1).astype(np.float32)
+
+
+def adjoint_shots(root: str, steps: int = 2000, NX: int = 192, NY: int = 192, NZ: int = 128, DH: float = 100.0,
+                  nPML: int = 12, n_shots: int = 4, n_side: int = 8, courant: float = 0.8, seed: int = 9) -> dict:
+    """The adjoint workload: ``n_shots`` run directories root/shot_<i> over
+    one model (the starting medium, no anomaly, as medium.bin; the true
+    medium with the Vs ball beside it as medium_true.bin), each with one 2 Hz
+    Ricker point source at a seeded position at 1/4 of the model depth and
+    the same n_side x n_side surface stations (64).  Returns the shot
+    directories, DT and the two media."""
+    rng = np.random.default_rng(seed)
+    start = adjoint_layers(NX, NY, NZ, DH, False)
+    true = adjoint_layers(NX, NY, NZ, DH, True)
+    vp_max = float(true[..., 1].max())
+    DT = cases.cfl_dt(DH, vp_max, courant)
+    stations = surface_stations(NX, NY, NZ, nPML, n_side)
+    dirs = []
+    for s in range(n_shots):
+        d = os.path.join(root, f"shot_{s}")
+        os.makedirs(d, exist_ok=True)
+        X = int(rng.integers(nPML + 16, NX - nPML - 16))
+        Y = int(rng.integers(nPML + 16, NY - nPML - 16))
+        c = cases.Case(NX=NX, NY=NY, NZ=NZ, DH=DH, DT=DT, steps=steps, nPML=nPML, stations=stations,
+                       ricker_point=(X, Y, int(NZ * 0.75), 2.0),
+                       extra={"mediumFile": "medium.bin", "useMedium": 1})
+        cases.write_case(c, d)
+        start.tofile(os.path.join(d, "medium.bin"))
+        dirs.append(d)
+    return {"dirs": dirs, "DT": DT, "start": start, "true": true}

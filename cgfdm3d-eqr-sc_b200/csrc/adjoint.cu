@@ -34,6 +34,21 @@
 #include "kernels.cuh"
 #include "surface_matrix.cuh"
 
+#ifndef ADJ_TY
+#define ADJ_TY 4            // block rows (the block is 32 x ADJ_TY points of one plane)
+#endif
+// optional minimum resident blocks per SM (a register cap) of each pass
+#ifdef ADJ_MINB_PRE
+#define ADJ_BOUNDS_PRE __launch_bounds__(32 * ADJ_TY, ADJ_MINB_PRE)
+#else
+#define ADJ_BOUNDS_PRE __launch_bounds__(32 * ADJ_TY)
+#endif
+#ifdef ADJ_MINB_GATHER
+#define ADJ_BOUNDS_GATHER __launch_bounds__(32 * ADJ_TY, ADJ_MINB_GATHER)
+#else
+#define ADJ_BOUNDS_GATHER __launch_bounds__(32 * ADJ_TY)
+#endif
+
 namespace cgfdm {
 
 // dir_rhs^T: the 9-vector adjoint of the nine scaled derivatives along one
@@ -76,7 +91,7 @@ __device__ __forceinline__ bool in_pml_cell(const AdjStageArgs &a, int i, int j,
 // --------------------------------------------------------------- pass 1
 // Point-wise: Phi_d(p) for the three directions, the surface channels and
 // the RK4 adjoint of the PML auxiliaries.
-__global__ void __launch_bounds__(128) k_adj_pre(const __grid_constant__ AdjStageArgs a)
+__global__ void ADJ_BOUNDS_PRE k_adj_pre(const __grid_constant__ AdjStageArgs a)
 {
     const DevGrid g = a.g;
     const int i = CGFDM_HALO + blockIdx.x * blockDim.x + threadIdx.x;
@@ -102,6 +117,7 @@ __global__ void __launch_bounds__(128) k_adj_pre(const __grid_constant__ AdjStag
 
     // per direction: the adjoint of R_d(p) times the scaled derivatives
     float nu[3][9], extra[3][3];
+#pragma unroll
     for (int d = 0; d < 3; d++) {
         for (int f = 0; f < 9; f++) nu[d][f] = (DT * sd[d]) * mu_s[f];
         // free surface: velocity rows are handled at the tap points, and the
@@ -118,7 +134,9 @@ __global__ void __launch_bounds__(128) k_adj_pre(const __grid_constant__ AdjStag
         for (int f = 3; f < 9; f++) w_top[f] = DT * mu_s[f];
         float wz[3];
         dir_stress_t(mt[2][0], mt[2][1], mt[2][2], w_top, mu, lam, wz);
+#pragma unroll
         for (int d = 0; d < 2; d++)
+#pragma unroll
             for (int c = 0; c < 3; c++) {
                 const float *r = a.rdz + (long long)(d * 9) * P + s;
                 float v = 0.0f;
@@ -132,6 +150,7 @@ __global__ void __launch_bounds__(128) k_adj_pre(const __grid_constant__ AdjStag
         const int n = a.nPML;
         const bool sel[5] = {i < CGFDM_HALO + n, j < CGFDM_HALO + n, k < CGFDM_HALO + n, i >= _nx - n, j >= _ny - n};
         const int i0p = i - CGFDM_HALO, j0p = j - CGFDM_HALO, k0p = k - CGFDM_HALO;
+#pragma unroll
         for (int fc = 0; fc < 5; fc++) {
             if (!sel[fc]) continue;
             const int dir = fc == 0 || fc == 3 ? 0 : fc == 1 || fc == 4 ? 1 : 2;
@@ -149,9 +168,15 @@ __global__ void __launch_bounds__(128) k_adj_pre(const __grid_constant__ AdjStag
             const float *dd = dir == 0 ? a.pml_d_x : dir == 1 ? a.pml_d_y : a.pml_d_z;
             const int ix = dir == 0 ? i : dir == 1 ? j : k;
             const float dval = dd[ix], beta = be[ix], alpha_d = dval + al[ix];
-            float muA[9];
-            for (int f = 0; f < 9; f++)
-                muA[f] = a.irk == 3 ? RK_BETA4 * Pf.A[f * Pf.count + pos] : Pf.B[f * Pf.count + pos];
+            // the face's lambda', mu and running sum, all loaded before any store
+            float fa[9], muA[9], ft[9];
+#pragma unroll
+            for (int f = 0; f < 9; f++) {
+                const long long e = f * Pf.count + pos;
+                fa[f] = a.irk != 0 ? Pf.A[e] : 0.0f;
+                muA[f] = a.irk == 3 ? RK_BETA4 * fa[f] : Pf.B[e];
+                ft[f] = a.irk != 3 ? Pf.T[e] : 0.0f;
+            }
             for (int f = 0; f < 9; f++) nu[dir][f] += (DT * dval) * muA[f];
             if (top && dir < 2) {
                 // src/pml_freeSurface.cpp:90-125: the auxiliary's stress rows
@@ -167,26 +192,19 @@ __global__ void __launch_bounds__(128) k_adj_pre(const __grid_constant__ AdjStag
                 }
             }
             // RK4 adjoint of the auxiliary (src/pml_rk.cpp:18-73)
+            const float rb = a.irk == 3 ? RK_BETA3 : a.irk == 2 ? RK_BETA2 : RK_BETA1;
+            const float ra = a.irk == 3 ? 1.0f : a.irk == 2 ? RK_ALPHA3 : RK_ALPHA2;
+#pragma unroll
             for (int f = 0; f < 9; f++) {
                 const float nuA = -DT * (alpha_d * muA[f] + beta * mu_s[f]);
                 const long long e = f * Pf.count + pos;
-                if (a.irk == 3) {
-                    const float lp = Pf.A[e];
-                    Pf.B[e] = RK_BETA3 * lp + nuA;
-                    Pf.T[e] = lp + nuA;
-                } else if (a.irk == 2) {
-                    Pf.B[e] = RK_BETA2 * Pf.A[e] + RK_ALPHA3 * nuA;
-                    Pf.T[e] = Pf.T[e] + nuA;
-                } else if (a.irk == 1) {
-                    Pf.B[e] = RK_BETA1 * Pf.A[e] + RK_ALPHA2 * nuA;
-                    Pf.T[e] = Pf.T[e] + nuA;
-                } else {
-                    Pf.T[e] = Pf.T[e] + nuA;
-                }
+                if (a.irk != 0) Pf.B[e] = rb * fa[f] + ra * nuA;
+                Pf.T[e] = (a.irk == 3 ? fa[f] : ft[f]) + nuA;
             }
         }
     }
 
+#pragma unroll
     for (int d = 0; d < 3; d++) {
         float phi[9];
         dir_rhs_t(mt[d][0], mt[d][1], mt[d][2], nu[d], mu, lam, buo, phi);
@@ -227,7 +245,7 @@ __device__ __forceinline__ float tap_sum(const float *__restrict__ f, long long 
     return s;
 }
 
-__global__ void __launch_bounds__(128) k_adj_gather(const __grid_constant__ AdjStageArgs a)
+__global__ void ADJ_BOUNDS_GATHER k_adj_gather(const __grid_constant__ AdjStageArgs a)
 {
     const DevGrid g = a.g;
     const int i = CGFDM_HALO + blockIdx.x * blockDim.x + threadIdx.x;
@@ -303,34 +321,31 @@ __global__ void __launch_bounds__(128) k_adj_gather(const __grid_constant__ AdjS
         }
     }
 
-    // RK4 adjoint (src/wave_rk.cpp:17-104 transposed)
-    float mus[9];
-    if (a.irk == 3) {
-        for (int f = 0; f < 9; f++) {
-            const float lp = a.Lp[f * F + q];
-            mus[f] = RK_BETA4 * lp;
-            a.M[f * F + q] = RK_BETA3 * lp + nu[f];
-            a.Lam[f * F + q] = lp + nu[f];
-        }
-    } else if (a.irk == 2 || a.irk == 1) {
-        const float beta = a.irk == 2 ? RK_BETA2 : RK_BETA1;
-        const float alpha = a.irk == 2 ? RK_ALPHA3 : RK_ALPHA2;
-        for (int f = 0; f < 9; f++) {
-            mus[f] = a.M[f * F + q];
-            a.M[f * F + q] = beta * a.Lp[f * F + q] + alpha * nu[f];
-            a.Lam[f * F + q] = a.Lam[f * F + q] + nu[f];
-        }
-    } else {
-        for (int f = 0; f < 9; f++) {
-            mus[f] = a.M[f * F + q];
-            a.Lam[f * F + q] = a.Lam[f * F + q] + nu[f];
-        }
+    // RK4 adjoint (src/wave_rk.cpp:17-104 transposed).  Every operand is
+    // loaded before the first store, so the loads issue together.
+    const int irk = a.irk;
+    const bool grad = a.h && !in_pml_cell(a, i, j, k, _nx, _ny);
+    float mus[9], lp[9], lm[9], h[9], g3[3], mu = 0.0f, lam = 0.0f, buo = 1.0f;
+#pragma unroll
+    for (int f = 0; f < 9; f++) {
+        lp[f] = irk != 0 ? a.Lp[f * F + q] : 0.0f;
+        mus[f] = irk == 3 ? RK_BETA4 * lp[f] : a.M[f * F + q];
+        lm[f] = irk != 3 ? a.Lam[f * F + q] : 0.0f;
+        h[f] = grad ? a.h[f * F + q] : 0.0f;
+    }
+    if (grad) {
+        for (int c = 0; c < 3; c++) g3[c] = a.grad[c * F + q];
+        mu = a.cjm[C_MU * F + q], lam = a.cjm[C_LAMBDA * F + q], buo = a.cjm[C_BUOY * F + q];
+    }
+    const float beta = irk == 3 ? RK_BETA3 : irk == 2 ? RK_BETA2 : RK_BETA1;
+    const float alpha = irk == 3 ? 1.0f : irk == 2 ? RK_ALPHA3 : RK_ALPHA2;
+#pragma unroll
+    for (int f = 0; f < 9; f++) {
+        if (irk != 0) a.M[f * F + q] = beta * lp[f] + alpha * nu[f];
+        a.Lam[f * F + q] = (irk == 3 ? lp[f] : lm[f]) + nu[f];
     }
 
-    if (!a.h || in_pml_cell(a, i, j, k, _nx, _ny)) return;
-    float h[9];
-    for (int f = 0; f < 9; f++) h[f] = a.h[f * F + q];
-    const float mu = a.cjm[C_MU * F + q], lam = a.cjm[C_LAMBDA * F + q], buo = a.cjm[C_BUOY * F + q];
+    if (!grad) return;
     const float gb = ((mus[0] * h[0] + mus[1] * h[1]) + mus[2] * h[2]) / buo;
     const float ddiv = ((h[3] + h[4]) + h[5]) / (3.0f * lam + 2.0f * mu);
     float gl = ((mus[3] + mus[4]) + mus[5]) * ddiv;
@@ -356,14 +371,14 @@ __global__ void __launch_bounds__(128) k_adj_gather(const __grid_constant__ AdjS
             else gl += acc;
         }
     }
-    a.grad[0 * F + q] += gm;
-    a.grad[1 * F + q] += gl;
-    a.grad[2 * F + q] += gb;
+    a.grad[0 * F + q] = g3[0] + gm;
+    a.grad[1 * F + q] = g3[1] + gl;
+    a.grad[2 * F + q] = g3[2] + gb;
 }
 
 cudaError_t launch_adj_stage(const AdjStageArgs &a, cudaStream_t st)
 {
-    dim3 b(32, 4), gr((a.g.nx + 31) / 32, (a.g.ny + 3) / 4, a.g.nz);
+    dim3 b(32, ADJ_TY), gr((a.g.nx + 31) / 32, (a.g.ny + ADJ_TY - 1) / ADJ_TY, a.g.nz);
     k_adj_pre<<<gr, b, 0, st>>>(a);
     CUDA_TRY(cudaGetLastError());
     k_adj_gather<<<gr, b, 0, st>>>(a);

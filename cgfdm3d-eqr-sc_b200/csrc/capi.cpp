@@ -181,6 +181,13 @@ int cgfdm_gradient(cgfdm_session *s, const float *observed, long long obs_count,
     return s->s.gradient(observed, checkpoint_every, misfit, grad);
 }
 
+int cgfdm_gradient_profile(const cgfdm_session *s, float *ms3)
+{
+    if (!s || !ms3) return CGFDM_E_ARG;
+    for (int c = 0; c < 3; c++) ms3[c] = s->s.grad_ms[c];
+    return CGFDM_OK;
+}
+
 int cgfdm_batch_create(cgfdm_session *const *sessions, int n, cgfdm_batch **out)
 {
     if (!sessions || n <= 0 || !out) {

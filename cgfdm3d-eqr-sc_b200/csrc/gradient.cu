@@ -324,13 +324,61 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
     CU(sc.get((void **)&d_med, sizeof(float) * npad * 3));
     CU(sc.get((void **)&d_grad, sizeof(float) * (size_t)m.g.nx * m.g.ny * m.g.nz * 3));
 
-    // 1. forward with checkpoints
+    cudaEvent_t ev[2];
+    CU(cudaEventCreate(&ev[0]));
+    CU(cudaEventCreate(&ev[1]));
+    struct EvFree {
+        cudaEvent_t *e;
+        ~EvFree() { cudaEventDestroy(e[0]), cudaEventDestroy(e[1]); }
+    } evfree{ev};
+    float ms_re = 0.0f, ms_adj = 0.0f;
+    auto lap = [&](float *acc) -> int {
+        CU(cudaEventRecord(ev[1], stream));
+        CU(cudaEventSynchronize(ev[1]));
+        float ms = 0.0f;
+        CU(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+        *acc += ms;
+        CU(cudaEventRecord(ev[0], stream));
+        return ST_OK;
+    };
+
+    // steps n0 .. n1-1 from the current state, storing each stage's RHS
+    auto run_storing = [&](int n0, int n1) -> int {
+        for (int n = n0; n < n1; n++) {
+            if (int st = launch_sources_on(stream)) return st;
+            int FB[3];
+            fb_signs(n, FB);
+            for (int irk = 0; irk < 4; irk++) {
+                CgStageDesc d = desc_host_[irk];
+                d.a.pgv = nullptr;
+                d.a.dis = nullptr;
+                d.a.hstore = hstore + (size_t)F * 9 * ((n - n0) * 4 + irk);
+                d.a.vdstore = vdstore + (size_t)g.plane * 6 * ((n - n0) * 4 + irk);
+                const int sgn = (irk & 1) ? -1 : 1;
+                CU(launch_cg_stage(FB[0] * sgn, FB[1] * sgn, FB[2] * sgn, d, work_dev_, grid_ctas_, stream));
+            }
+            if (int st = launch_stations_on(stream)) return st;
+            kernel_launches += 6;
+        }
+        return ST_OK;
+    };
+
+    // 1. forward with checkpoints; the last segment stores its stage RHS
+    //    on the way, so it needs no second run
+    grad_ms[0] = grad_ms[1] = grad_ms[2] = 0.0f;
+    CU(cudaEventRecord(ev[0], stream));
     for (int s = 0; s < nseg; s++) {
         if (int st = save_state(ckpt + sb * s)) return st;
-        if (int st = run_plain(std::min(K, NT - it))) return st;
+        const int n = std::min(K, NT - it);
+        if (s + 1 < nseg) {
+            if (int st = run_plain(n)) return st;
+        } else {
+            if (int st = run_storing(it, it + n)) return st;
+            it += n;
+        }
     }
     if (int st = save_state(final_state)) return st;
-    CU(cudaStreamSynchronize(stream));
+    if (int st = lap(&grad_ms[0])) return st;
     if (int st = check_device_error()) return st;
 
     // residuals and misfit
@@ -351,6 +399,7 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
     if (misfit) *misfit = J;
 
     // 2. backward, segment by segment
+    CU(cudaEventRecord(ev[0], stream));
     CU(cudaMemsetAsync(adj_.Lp, 0, sizeof(float) * F * 9, stream));
     CU(cudaMemsetAsync(adj_.Lam, 0, sizeof(float) * F * 9, stream));
     CU(cudaMemsetAsync(adj_.grad, 0, sizeof(float) * F * 3, stream));
@@ -361,24 +410,12 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
         }
     for (int s = nseg - 1; s >= 0; s--) {
         const int n0 = s * K, n1 = std::min(NT, n0 + K);
-        if (int st = load_state(ckpt + sb * s)) return st;
-        CU(cudaMemcpyAsync(it_dev_, &n0, sizeof(int), cudaMemcpyHostToDevice, stream));
-        // forward again, storing each stage's RHS
-        for (int n = n0; n < n1; n++) {
-            if (int st = launch_sources_on(stream)) return st;
-            int FB[3];
-            fb_signs(n, FB);
-            for (int irk = 0; irk < 4; irk++) {
-                CgStageDesc d = desc_host_[irk];
-                d.a.pgv = nullptr;
-                d.a.dis = nullptr;
-                d.a.hstore = hstore + (size_t)F * 9 * ((n - n0) * 4 + irk);
-                d.a.vdstore = vdstore + (size_t)g.plane * 6 * ((n - n0) * 4 + irk);
-                const int sgn = (irk & 1) ? -1 : 1;
-                CU(launch_cg_stage(FB[0] * sgn, FB[1] * sgn, FB[2] * sgn, d, work_dev_, grid_ctas_, stream));
-            }
-            if (int st = launch_stations_on(stream)) return st;
-            kernel_launches += 6;
+        if (s + 1 < nseg) {
+            // forward again from the segment's checkpoint, storing each stage's RHS
+            if (int st = load_state(ckpt + sb * s)) return st;
+            CU(cudaMemcpyAsync(it_dev_, &n0, sizeof(int), cudaMemcpyHostToDevice, stream));
+            if (int st = run_storing(n0, n1)) return st;
+            if (int st = lap(&ms_re)) return st;
         }
         // and back through it
         for (int n = n1 - 1; n >= n0; n--) {
@@ -391,7 +428,10 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
             if (int st = adj_step(n, h4, vd4)) return st;
             kernel_launches += 1;
         }
+        if (int st = lap(&ms_adj)) return st;
     }
+    grad_ms[1] = ms_re;
+    grad_ms[2] = ms_adj;
 
     // 3. chain rule and output; the session returns to its final state
     CU(cudaMemcpyAsync(d_med, m.medium.data(), sizeof(float) * npad * 3, cudaMemcpyHostToDevice, stream));

@@ -43,6 +43,7 @@ public:
     int adjoint_apply(int nsteps, float *host_aos);  // transpose of the last nsteps steps, in place
     int gradient(const float *obs, int ckpt_every, double *misfit, float *grad);
     int set_medium(const float *host_medium);       // [_nz_][_ny_][_nx_][3] (Vs, Vp, rho); back to step 0
+    float grad_ms[3] = {0, 0, 0};                   // last gradient: forward, re-runs, adjoint steps (device ms)
 
     Model m;
     DevGrid g;

@@ -158,6 +158,10 @@ int cgfdm_set_medium(cgfdm_session *s, const float *medium, long long count);
 int cgfdm_gradient(cgfdm_session *s, const float *observed, long long obs_count, int checkpoint_every,
                    double *misfit, float *grad, long long grad_count);
 int cgfdm_adjoint_apply(cgfdm_session *s, int nsteps, float *state, long long count);
+/* Device time of the phases of the last cgfdm_gradient in ms: ms3[0] the
+ * forward run with checkpoints, ms3[1] the segment re-runs that store the
+ * stage right-hand sides, ms3[2] the adjoint steps. */
+int cgfdm_gradient_profile(const cgfdm_session *s, float *ms3);
 
 /* Batches: several CGFDM sessions -- independent shots or media of uneven
  * grid sizes -- advanced together, every RK stage of all of them in one

@@ -150,3 +150,27 @@ def test_gradient_against_fp64_finite_differences(tmp_path):
               f"(max abs err / max abs {worst:.2e})")
     for p, e, g, f in rows:
         assert e <= 1e-3, (p, e, list(zip(cells, g, f)))
+
+
+@pytest.mark.gpu
+def test_autograd_function_matches_session_gradient(tmp_path):
+    import torch
+
+    from cgfdm.autograd import misfit
+
+    c = _grad_case(steps=40)
+    d = cases.write_case(c, str(tmp_path / "run"))
+    med = _medium(c, 11, False)
+    med.tofile(os.path.join(d, "medium.bin"))
+    rng = np.random.default_rng(2)
+    with Session(d) as s:
+        obs = (rng.standard_normal((s.info.n_stations, s.info.NT, 3)) * 1e-9).astype(np.float32)
+        inner = med[3:-3, 3:-3, 3:-3]
+        vs, vp, rho = (torch.tensor(inner[..., c].copy(), requires_grad=True) for c in range(3))
+        J = misfit(vp, vs, rho, s, torch.from_numpy(obs), 10)
+        (2.0 * J).backward()
+        s.set_medium(med)
+        J0, g0 = s.gradient(obs, 10)
+    assert float(J) == J0
+    for t, g in zip((vp, vs, rho), g0):
+        np.testing.assert_array_equal(t.grad.numpy(), 2.0 * g)
