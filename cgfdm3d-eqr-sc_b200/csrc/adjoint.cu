@@ -37,7 +37,14 @@
 #ifndef ADJ_TY
 #define ADJ_TY 4            // block rows (the block is 32 x ADJ_TY points of one plane)
 #endif
-// optional minimum resident blocks per SM (a register cap) of each pass
+// minimum resident blocks per SM (a register cap) of each pass: 5 and 5
+// measured 3 % faster than the uncapped 4 and 5
+#ifndef ADJ_MINB_PRE
+#define ADJ_MINB_PRE 5
+#endif
+#ifndef ADJ_MINB_GATHER
+#define ADJ_MINB_GATHER 5
+#endif
 #ifdef ADJ_MINB_PRE
 #define ADJ_BOUNDS_PRE __launch_bounds__(32 * ADJ_TY, ADJ_MINB_PRE)
 #else
@@ -382,6 +389,397 @@ cudaError_t launch_adj_stage(const AdjStageArgs &a, cudaStream_t st)
     k_adj_pre<<<gr, b, 0, st>>>(a);
     CUDA_TRY(cudaGetLastError());
     k_adj_gather<<<gr, b, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------- fused stage
+// One kernel per RK stage.  A block of 32 x ADJF_TY columns walks a chunk
+// of planes upward.  Each thread keeps Phi_z of its own column for the last
+// five planes (private shared-memory slots); for every output plane the
+// block fills Phi_x over its rows with a 3-point halo in x and Phi_y over
+// its columns with a 3-point halo in y in shared memory (with the surface
+// layers' velocity-row channels), and every thread gathers its transposed
+// differences.  Phi never goes to HBM.  Blocks read mu_s (and the faces'
+// mu_s) at their neighbours' points while those write mu_{s-1}, so the
+// output goes to a second buffer (M2, faceB2) that the host swaps in.
+#ifndef ADJF_TY
+#define ADJF_TY 4
+#endif
+#define ADJF_BX (32 + 6)
+#define ADJF_BY (ADJF_TY + 6)
+#define ADJF_NT (32 * ADJF_TY)
+#define ADJF_SMEM_FLOATS (12 * ADJF_TY * ADJF_BX + 12 * ADJF_BY * 32 + 5 * 9 * ADJF_NT + 15 * ADJF_NT)
+
+__device__ __forceinline__ void load_mu_s(const AdjStageArgs &a, long long q, long long F, float m[9])
+{
+#pragma unroll
+    for (int f = 0; f < 9; f++) m[f] = a.irk == 3 ? RK_BETA4 * a.Lp[f * F + q] : a.M[f * F + q];
+}
+
+// index of point (i, j, k) in face fc's slab (the forward's layout)
+__device__ __forceinline__ long long face_pos(const DevGrid &g, int fc, int n, int i, int j, int k)
+{
+    const int i0p = i - CGFDM_HALO, j0p = j - CGFDM_HALO, k0p = k - CGFDM_HALO;
+    if (fc == 0 || fc == 3)
+        return (long long)(i0p - (fc == 3 ? g.nx - n : 0)) + (long long)j0p * n + (long long)k0p * n * g.ny;
+    if (fc == 1 || fc == 4)
+        return (long long)i0p + (long long)(j0p - (fc == 4 ? g.ny - n : 0)) * g.nx + (long long)k0p * g.nx * n;
+    return (long long)i0p + (long long)j0p * g.nx + (long long)k0p * g.nx * g.ny;
+}
+
+// Phi_d at interior point (i, j, k), as k_adj_pre forms it; with X given,
+// also the surface layers' velocity-row channel of direction d
+// (DT buo / J mu_V, times the stretch s_d for d < 2).
+__device__ void phi_point(const AdjStageArgs &a, int d, int i, int j, int k, float phi[9], float *X)
+{
+    const DevGrid &g = a.g;
+    const int _nx = g.nxp - CGFDM_HALO, _ny = g.nyp - CGFDM_HALO, _nz = g.nzp - CGFDM_HALO;
+    const long long F = g.fstride, q = g.at(i, j, k), P = g.plane;
+    const float DT = a.DT;
+    float m[9];
+    load_mu_s(a, q, F, m);
+    const float m0 = a.cjm[(3 * d + 0) * F + q], m1 = a.cjm[(3 * d + 1) * F + q], m2 = a.cjm[(3 * d + 2) * F + q];
+    const float mu = a.cjm[C_MU * F + q], lam = a.cjm[C_LAMBDA * F + q], buo = a.cjm[C_BUOY * F + q];
+    const int ix = d == 0 ? i : d == 1 ? j : k;
+    const float sd = (d == 0 ? a.pml_beta_x : d == 1 ? a.pml_beta_y : a.pml_beta_z)[ix];
+    const bool fs = a.fs_on && k >= _nz - 3, top = a.fs_on && k == _nz - 1;
+    float nu[9];
+#pragma unroll
+    for (int f = 0; f < 9; f++) nu[f] = (DT * sd) * m[f];
+    if (fs) {
+        nu[0] = nu[1] = nu[2] = 0.0f;
+        if (d == 2)
+            for (int f = 3; f < 9; f++) nu[f] = 0.0f;
+    }
+    float extra[3] = {0.0f, 0.0f, 0.0f};
+    const long long s = g.at2(i, j);
+    if (top && d < 2) {
+        float w[9], wz[3];
+        for (int f = 3; f < 9; f++) w[f] = DT * m[f];
+        dir_stress_t(a.cjm[C_ZT_X * F + q], a.cjm[C_ZT_Y * F + q], a.cjm[C_ZT_Z * F + q], w, mu, lam, wz);
+        const float *r = a.rdz + (long long)(d * 9) * P + s;
+        for (int c = 0; c < 3; c++) {
+            float v = 0.0f;
+            for (int rr = 0; rr < 3; rr++) v += r[(rr * 3 + c) * P] * wz[rr];
+            extra[c] += sd * v;
+        }
+    }
+    if (a.pml_on) {
+        const int n = a.nPML;
+        int fc = -1;
+        if (d == 0) fc = i < CGFDM_HALO + n ? 0 : (i >= _nx - n ? 3 : -1);
+        else if (d == 1) fc = j < CGFDM_HALO + n ? 1 : (j >= _ny - n ? 4 : -1);
+        else fc = k < CGFDM_HALO + n ? 2 : -1;
+        if (fc >= 0) {
+            const PmlFace &Pf = a.face[fc];
+            const long long pos = face_pos(g, fc, n, i, j, k);
+            const float dval = (d == 0 ? a.pml_d_x : d == 1 ? a.pml_d_y : a.pml_d_z)[ix];
+            float muA[9];
+#pragma unroll
+            for (int f = 0; f < 9; f++)
+                muA[f] = a.irk == 3 ? RK_BETA4 * Pf.A[f * Pf.count + pos] : Pf.B[f * Pf.count + pos];
+#pragma unroll
+            for (int f = 0; f < 9; f++) nu[f] += (DT * dval) * muA[f];
+            if (top && d < 2) {
+                float w[9], wz[3];
+                for (int f = 3; f < 9; f++) w[f] = DT * muA[f];
+                dir_stress_t(a.cjm[C_ZT_X * F + q], a.cjm[C_ZT_Y * F + q], a.cjm[C_ZT_Z * F + q], w, mu, lam, wz);
+                const float *r = a.rdz + (long long)(d * 9) * P + s;
+                for (int c = 0; c < 3; c++) {
+                    float v = 0.0f;
+                    for (int rr = 0; rr < 3; rr++) v += r[(rr * 3 + c) * P] * wz[rr];
+                    extra[c] += dval * v;
+                }
+            }
+        }
+    }
+    dir_rhs_t(m0, m1, m2, nu, mu, lam, buo, phi);
+    for (int c = 0; c < 3; c++) phi[c] += extra[c];
+    if (X) {
+        if (fs) {
+            const float bj = buo * (1.0f / a.cjm[C_JAC * F + q]);
+            for (int c = 0; c < 3; c++) {
+                const float chi = DT * bj * m[c];
+                X[c] = d < 2 ? sd * chi : chi;
+            }
+        } else {
+            X[0] = X[1] = X[2] = 0.0f;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(ADJF_NT) k_adj_fused(const __grid_constant__ AdjStageArgs a)
+{
+    extern __shared__ __align__(16) float adj_smem[];
+    float(*sx)[ADJF_TY][ADJF_BX] = reinterpret_cast<float(*)[ADJF_TY][ADJF_BX]>(adj_smem);
+    float(*sy)[ADJF_BY][32] = reinterpret_cast<float(*)[ADJF_BY][32]>(adj_smem + 12 * ADJF_TY * ADJF_BX);
+    float(*zr)[9][ADJF_NT] =
+        reinterpret_cast<float(*)[9][ADJF_NT]>(adj_smem + 12 * ADJF_TY * ADJF_BX + 12 * ADJF_BY * 32);
+    float(*fz)[ADJF_NT] = reinterpret_cast<float(*)[ADJF_NT]>(adj_smem + 12 * ADJF_TY * ADJF_BX +
+                                                             12 * ADJF_BY * 32 + 5 * 9 * ADJF_NT);
+    const DevGrid g = a.g;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const int i0 = CGFDM_HALO + blockIdx.x * 32, j0 = CGFDM_HALO + blockIdx.y * ADJF_TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const int _nx = g.nxp - CGFDM_HALO, _ny = g.nyp - CGFDM_HALO, _nz = g.nzp - CGFDM_HALO;
+    const bool active = i < _nx && j < _ny;
+    const int kb = CGFDM_HALO + blockIdx.z * a.kchunk, ke = min(kb + a.kchunk, _nz);
+    const long long F = g.fstride, P = g.plane;
+    const float rDH = a.rDH, DT = a.DT;
+    const int FB1 = a.FB1, FB2 = a.FB2, FB3 = a.FB3;
+    const int lag = FB3 > 0 ? 1 : 3, lo = FB3 > 0 ? 3 : 1;
+    const long long s = active ? g.at2(i, j) : 0;
+
+    // the own column's surface channels: X_z of the three surface layers
+    // and w_z of the two below the surface (k_adj_pre's SF channels 6-11)
+    const bool near_top = a.fs_on && ke > _nz - 7;
+    if (near_top && active) {
+        for (int L = 0; L < 3; L++) {
+            const int k = _nz - 1 - L;
+            const long long q = g.at(i, j, k);
+            float m[9];
+            load_mu_s(a, q, F, m);
+            const float buo = a.cjm[C_BUOY * F + q];
+            const float bj = buo * (1.0f / a.cjm[C_JAC * F + q]);
+            for (int c = 0; c < 3; c++) fz[L * 3 + c][tid] = DT * bj * m[c];
+            if (L > 0) {
+                float w[9], wz[3];
+                for (int f = 3; f < 9; f++) w[f] = DT * m[f];
+                dir_stress_t(a.cjm[C_ZT_X * F + q], a.cjm[C_ZT_Y * F + q], a.cjm[C_ZT_Z * F + q], w,
+                             a.cjm[C_MU * F + q], a.cjm[C_LAMBDA * F + q], wz);
+                for (int c = 0; c < 3; c++) fz[9 + (L - 1) * 3 + c][tid] = wz[c];
+            }
+        }
+    }
+
+    const int kfirst = kb - lo;
+    auto slot = [&](int kk) { return (kk - kfirst) % 5; };
+    for (int kin = kfirst; kin < ke + lag; kin++) {
+        if (active) {
+            float ph[9];
+            if (kin >= CGFDM_HALO && kin < _nz) {
+                phi_point(a, 2, i, j, kin, ph, nullptr);
+            } else {
+#pragma unroll
+                for (int f = 0; f < 9; f++) ph[f] = 0.0f;
+            }
+            const int sl = slot(kin);
+#pragma unroll
+            for (int f = 0; f < 9; f++) zr[sl][f][tid] = ph[f];
+        }
+        const int kout = kin - lag;
+        if (kout < kb) continue;
+        const bool fsl = a.fs_on && kout >= _nz - 3;
+        __syncthreads();   // the previous plane's readers of sx, sy are done
+        for (int e = tid; e < ADJF_TY * ADJF_BX; e += ADJF_NT) {
+            const int r = e / ADJF_BX, c = e - r * ADJF_BX;
+            const int pi = i0 - 3 + c, pj = j0 + r;
+            float ph[9], X[3] = {0.0f, 0.0f, 0.0f};
+            if (pi >= CGFDM_HALO && pi < _nx && pj < _ny) {
+                phi_point(a, 0, pi, pj, kout, ph, fsl ? X : nullptr);
+            } else {
+#pragma unroll
+                for (int f = 0; f < 9; f++) ph[f] = 0.0f;
+            }
+#pragma unroll
+            for (int f = 0; f < 9; f++) sx[f][r][c] = ph[f];
+            for (int f = 0; f < 3; f++) sx[9 + f][r][c] = X[f];
+        }
+        for (int e = tid; e < ADJF_BY * 32; e += ADJF_NT) {
+            const int r = e / 32, c = e - r * 32;
+            const int pi = i0 + c, pj = j0 - 3 + r;
+            float ph[9], X[3] = {0.0f, 0.0f, 0.0f};
+            if (pi < _nx && pj >= CGFDM_HALO && pj < _ny) {
+                phi_point(a, 1, pi, pj, kout, ph, fsl ? X : nullptr);
+            } else {
+#pragma unroll
+                for (int f = 0; f < 9; f++) ph[f] = 0.0f;
+            }
+#pragma unroll
+            for (int f = 0; f < 9; f++) sy[f][r][c] = ph[f];
+            for (int f = 0; f < 3; f++) sy[9 + f][r][c] = X[f];
+        }
+        __syncthreads();
+        if (!active) continue;
+
+        // transposed differences: x and y from the planes in shared
+        // memory, z from the column's ring
+        const int cx = tx + 3, ry = ty + 3;
+        const int sp1 = slot(kout + FB3), s0 = slot(kout), sm1 = slot(kout - FB3), sm2 = slot(kout - 2 * FB3),
+                  sm3 = slot(kout - 3 * FB3);
+        float nu[9];
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+            float ax = CG_AF_1 * sx[f][ty][cx + FB1] + CG_AF0 * sx[f][ty][cx];
+            ax = ax + CG_AF1 * sx[f][ty][cx - FB1];
+            ax = ax + CG_AF2 * sx[f][ty][cx - 2 * FB1];
+            ax = ax + CG_AF3 * sx[f][ty][cx - 3 * FB1];
+            float ay = CG_AF_1 * sy[f][ry + FB2][tx] + CG_AF0 * sy[f][ry][tx];
+            ay = ay + CG_AF1 * sy[f][ry - FB2][tx];
+            ay = ay + CG_AF2 * sy[f][ry - 2 * FB2][tx];
+            ay = ay + CG_AF3 * sy[f][ry - 3 * FB2][tx];
+            float az = CG_AF_1 * zr[sp1][f][tid] + CG_AF0 * zr[s0][f][tid];
+            az = az + CG_AF1 * zr[sm1][f][tid];
+            az = az + CG_AF2 * zr[sm2][f][tid];
+            az = az + CG_AF3 * zr[sm3][f][tid];
+            nu[f] = (((float)FB1 * ax) * rDH + ((float)FB2 * ay) * rDH) + ((float)FB3 * az) * rDH;
+        }
+        const long long q = g.at(i, j, kout);
+
+        if (a.fs_on && kout >= _nz - 6) {
+            float px[3] = {0, 0, 0}, py[3] = {0, 0, 0}, pz[3] = {0, 0, 0};
+            if (fsl) {
+                for (int c = 0; c < 3; c++) {
+                    float ax = CG_AF_1 * sx[9 + c][ty][cx + FB1] + CG_AF0 * sx[9 + c][ty][cx];
+                    ax = ax + CG_AF1 * sx[9 + c][ty][cx - FB1];
+                    ax = ax + CG_AF2 * sx[9 + c][ty][cx - 2 * FB1];
+                    ax = ax + CG_AF3 * sx[9 + c][ty][cx - 3 * FB1];
+                    float ay = CG_AF_1 * sy[9 + c][ry + FB2][tx] + CG_AF0 * sy[9 + c][ry][tx];
+                    ay = ay + CG_AF1 * sy[9 + c][ry - FB2][tx];
+                    ay = ay + CG_AF2 * sy[9 + c][ry - 2 * FB2][tx];
+                    ay = ay + CG_AF3 * sy[9 + c][ry - 3 * FB2][tx];
+                    px[c] = ((float)FB1 * ax) * rDH;
+                    py[c] = ((float)FB2 * ay) * rDH;
+                }
+            }
+            const float af[5] = {CG_AF_1, CG_AF0, CG_AF1, CG_AF2, CG_AF3};
+            for (int L = 0; L < 3; L++) {
+                const int kp = _nz - 1 - L, ks_rel = L + 3;
+                for (int m = 0; m < 5; m++) {
+                    const int l = 3 + (m - 1) * FB3;
+                    int src = l;
+                    float sign = 1.0f;
+                    if (l > ks_rel) src = 2 * ks_rel - l, sign = -1.0f;
+                    if (src == ks_rel || kp + src - 3 != kout) continue;
+                    const float w = sign * ((float)FB3 * af[m]) * rDH;
+                    for (int c = 0; c < 3; c++) pz[c] += w * fz[L * 3 + c][tid];
+                }
+            }
+            const float jac = a.cjm[C_JAC * F + q];
+            const float *ps[3] = {px, py, pz};
+            for (int d = 0; d < 3; d++) {
+                const float m0 = a.cjm[(3 * d) * F + q], m1 = a.cjm[(3 * d + 1) * F + q],
+                            m2 = a.cjm[(3 * d + 2) * F + q];
+                const float *p = ps[d];
+                nu[3] += jac * (m0 * p[0]);
+                nu[4] += jac * (m1 * p[1]);
+                nu[5] += jac * (m2 * p[2]);
+                nu[6] += jac * (m1 * p[0] + m0 * p[1]);
+                nu[7] += jac * (m2 * p[0] + m0 * p[2]);
+                nu[8] += jac * (m2 * p[1] + m1 * p[2]);
+            }
+            const float c1 = (float)FB3 * rDH;
+            const int kp = _nz - 2;
+            if (kout == kp + FB3)
+                for (int c = 0; c < 3; c++) nu[c] += c1 * fz[9 + c][tid];
+            if (kout == kp)
+                for (int c = 0; c < 3; c++) nu[c] -= c1 * fz[9 + c][tid];
+            const int kp2 = _nz - 3;
+            const float cf[3] = {CG_CF1, CG_CF2, CG_CF3};
+            for (int n = 0; n < 3; n++)
+                if (kout == kp2 + n * FB3)
+                    for (int c = 0; c < 3; c++) nu[c] += (c1 * cf[n]) * fz[12 + c][tid];
+        }
+
+        // point-wise: RK4 adjoint of the wavefield and the auxiliaries, gradient
+        const int irk = a.irk;
+        const bool grad = a.h && !in_pml_cell(a, i, j, kout, _nx, _ny);
+        float mus[9], lp[9], lm[9], h[9], g3[3] = {0.0f, 0.0f, 0.0f}, mu = 0.0f, lam = 0.0f, buo = 1.0f;
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+            lp[f] = irk != 0 ? a.Lp[f * F + q] : 0.0f;
+            mus[f] = irk == 3 ? RK_BETA4 * lp[f] : a.M[f * F + q];
+            lm[f] = irk != 3 ? a.Lam[f * F + q] : 0.0f;
+            h[f] = grad ? a.h[f * F + q] : 0.0f;
+        }
+        if (grad) {
+            for (int c = 0; c < 3; c++) g3[c] = a.grad[c * F + q];
+            mu = a.cjm[C_MU * F + q], lam = a.cjm[C_LAMBDA * F + q], buo = a.cjm[C_BUOY * F + q];
+        }
+        const float beta = irk == 3 ? RK_BETA3 : irk == 2 ? RK_BETA2 : RK_BETA1;
+        const float alpha = irk == 3 ? 1.0f : irk == 2 ? RK_ALPHA3 : RK_ALPHA2;
+#pragma unroll
+        for (int f = 0; f < 9; f++) {
+            if (irk != 0) a.M2[f * F + q] = beta * lp[f] + alpha * nu[f];
+            a.Lam[f * F + q] = (irk == 3 ? lp[f] : lm[f]) + nu[f];
+        }
+        if (a.pml_on) {
+            const int n = a.nPML;
+            const bool sel[5] = {i < CGFDM_HALO + n, j < CGFDM_HALO + n, kout < CGFDM_HALO + n, i >= _nx - n,
+                                 j >= _ny - n};
+#pragma unroll
+            for (int fc = 0; fc < 5; fc++) {
+                if (!sel[fc]) continue;
+                const int dir = fc == 0 || fc == 3 ? 0 : fc == 1 || fc == 4 ? 1 : 2;
+                const PmlFace &Pf = a.face[fc];
+                const long long pos = face_pos(g, fc, n, i, j, kout);
+                const int ix = dir == 0 ? i : dir == 1 ? j : kout;
+                const float *al = dir == 0 ? a.pml_alpha_x : dir == 1 ? a.pml_alpha_y : a.pml_alpha_z;
+                const float *be = dir == 0 ? a.pml_beta_x : dir == 1 ? a.pml_beta_y : a.pml_beta_z;
+                const float *dd = dir == 0 ? a.pml_d_x : dir == 1 ? a.pml_d_y : a.pml_d_z;
+                const float dval = dd[ix], pb = be[ix], alpha_d = dval + al[ix];
+                float fa[9], muA[9], ft[9];
+#pragma unroll
+                for (int f = 0; f < 9; f++) {
+                    const long long e = f * Pf.count + pos;
+                    fa[f] = irk != 0 ? Pf.A[e] : 0.0f;
+                    muA[f] = irk == 3 ? RK_BETA4 * fa[f] : Pf.B[e];
+                    ft[f] = irk != 3 ? Pf.T[e] : 0.0f;
+                }
+                const float rb = irk == 3 ? RK_BETA3 : irk == 2 ? RK_BETA2 : RK_BETA1;
+                const float ra = irk == 3 ? 1.0f : irk == 2 ? RK_ALPHA3 : RK_ALPHA2;
+                float *B2 = a.faceB2[fc];
+#pragma unroll
+                for (int f = 0; f < 9; f++) {
+                    const float nuA = -DT * (alpha_d * muA[f] + pb * mus[f]);
+                    const long long e = f * Pf.count + pos;
+                    if (irk != 0) B2[e] = rb * fa[f] + ra * nuA;
+                    Pf.T[e] = (irk == 3 ? fa[f] : ft[f]) + nuA;
+                }
+            }
+        }
+        if (!grad) continue;
+        const float gb = ((mus[0] * h[0] + mus[1] * h[1]) + mus[2] * h[2]) / buo;
+        const float ddiv = ((h[3] + h[4]) + h[5]) / (3.0f * lam + 2.0f * mu);
+        float gl = ((mus[3] + mus[4]) + mus[5]) * ddiv;
+        float th = 0.0f;
+        for (int f = 3; f < 9; f++) th += mus[f] * h[f];
+        float gm = (th - lam * gl) / mu;
+        if (a.fs_on && kout == _nz - 1 && a.vd && a.drdz) {
+            float w[9], wz[3];
+            for (int f = 3; f < 9; f++) w[f] = DT * mus[f];
+            dir_stress_t(a.cjm[C_ZT_X * F + q], a.cjm[C_ZT_Y * F + q], a.cjm[C_ZT_Z * F + q], w, mu, lam, wz);
+            float vd[6];
+            for (int c = 0; c < 6; c++) vd[c] = a.vd[c * P + s];
+            for (int par = 0; par < 2; par++) {
+                const float *dx = a.drdz + (long long)(par * 18) * P + s;
+                const float *dy = a.drdz + (long long)(par * 18 + 9) * P + s;
+                float acc = 0.0f;
+                for (int r = 0; r < 3; r++) {
+                    float dv = 0.0f;
+                    for (int c = 0; c < 3; c++) dv += dx[(r * 3 + c) * P] * vd[c] + dy[(r * 3 + c) * P] * vd[3 + c];
+                    acc += wz[r] * dv;
+                }
+                if (par == 0) gm += acc;
+                else gl += acc;
+            }
+        }
+        a.grad[0 * F + q] = g3[0] + gm;
+        a.grad[1 * F + q] = g3[1] + gl;
+        a.grad[2 * F + q] = g3[2] + gb;
+    }
+}
+
+cudaError_t launch_adj_stage_fused(const AdjStageArgs &a, cudaStream_t st)
+{
+    static bool attr = false;
+    const size_t smem = sizeof(float) * ADJF_SMEM_FLOATS;
+    if (!attr) {
+        CUDA_TRY(cudaFuncSetAttribute(k_adj_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
+    }
+    dim3 b(32, ADJF_TY), gr((a.g.nx + 31) / 32, (a.g.ny + ADJF_TY - 1) / ADJF_TY, a.nchunk);
+    k_adj_fused<<<gr, b, smem, st>>>(a);
     return cudaGetLastError();
 }
 

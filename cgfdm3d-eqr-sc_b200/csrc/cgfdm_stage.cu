@@ -513,7 +513,8 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
             }
         }
 
-        if (a.hstore)
+        // the adjoint's gradient reads h outside the PML layers only
+        if (a.hstore && !(inx1 || iny1 || inz1 || inx2 || iny2))
 #pragma unroll
             for (int f = 0; f < 9; f++) a.hstore[f * F + q] = h[f];
 

@@ -21,6 +21,10 @@
 #include "session.hpp"
 #include "session_util.hpp"
 
+#ifndef ADJF_KCHUNK
+#define ADJF_KCHUNK 28   // planes per block of the fused adjoint kernel
+#endif
+
 namespace cgfdm {
 
 __global__ void k_zero_halo(float *W, int nf, DevGrid g)
@@ -161,8 +165,12 @@ int Session::adj_prepare()
     ALLOC(adj_.Lp, float, F * 9);
     ALLOC(adj_.M, float, F * 9);
     ALLOC(adj_.Lam, float, F * 9);
-    ALLOC(adj_.Phi, float, F * 27);
-    ALLOC(adj_.SF, float, g.plane * 36);
+    if (m.p.adj_two_pass) {
+        ALLOC(adj_.Phi, float, F * 27);
+        ALLOC(adj_.SF, float, g.plane * 36);
+    } else {
+        ALLOC(adj_.M2, float, F * 9);
+    }
     ALLOC(adj_.grad, float, F * 3);
     ALLOC(adj_.drdz, float, g.plane * 36);
     for (int fc = 0; fc < 5; fc++) {
@@ -171,6 +179,7 @@ int Session::adj_prepare()
         ALLOC(adj_.face[fc].A, float, face_[fc].count * 9);
         ALLOC(adj_.face[fc].B, float, face_[fc].count * 9);
         ALLOC(adj_.face[fc].T, float, face_[fc].count * 9);
+        if (!m.p.adj_two_pass) ALLOC(adj_.B2[fc], float, face_[fc].count * 9);
     }
     return ST_OK;
 }
@@ -190,7 +199,10 @@ void Session::adj_args(AdjStageArgs &a, int irk, const int FB[3]) const
     a.Lam = adj_.Lam;
     a.Phi = adj_.Phi;
     a.SF = adj_.SF;
-    for (int fc = 0; fc < 5; fc++) a.face[fc] = adj_.face[fc];
+    for (int fc = 0; fc < 5; fc++) a.face[fc] = adj_.face[fc], a.faceB2[fc] = adj_.B2[fc];
+    a.M2 = adj_.M2;
+    a.kchunk = std::min(m.g.nz, ADJF_KCHUNK);
+    a.nchunk = (m.g.nz + a.kchunk - 1) / a.kchunk;
     a.grad = adj_.grad;
     a.irk = irk;
     const int sgn = (irk & 1) ? -1 : 1;
@@ -219,9 +231,16 @@ int Session::adj_step(int n, float *const *h4, float *const *vd4)
         a.h = h4 ? h4[irk] : nullptr;
         a.vd = vd4 ? vd4[irk] : nullptr;
         if (!a.h) a.grad = nullptr;
-        CU(launch_adj_stage(a, stream));
+        if (m.p.adj_two_pass) {
+            CU(launch_adj_stage(a, stream));
+        } else {
+            CU(launch_adj_stage_fused(a, stream));
+            // mu_{s-1} was written beside mu_s
+            std::swap(adj_.M, adj_.M2);
+            for (int fc = 0; fc < 5; fc++) std::swap(adj_.face[fc].B, adj_.B2[fc]);
+        }
     }
-    kernel_launches += 8;
+    kernel_launches += m.p.adj_two_pass ? 8 : 4;
     adj_swap();
     return ST_OK;
 }
@@ -303,21 +322,30 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
     Scratch sc;
     char *ckpt = nullptr, *final_state = nullptr;
     float *hstore = nullptr, *vdstore = nullptr, *res = nullptr, *d_med = nullptr, *d_grad = nullptr;
-    const size_t hbytes = sizeof(float) * (size_t)F * 9 * 4 * K, vdbytes = sizeof(float) * (size_t)g.plane * 6 * 4 * K;
+    // stage stores of one segment; the last R segments are stored during the
+    // first forward run (as many as device memory holds), the others are
+    // re-run from their checkpoints into slot 0
+    const size_t hseg = sizeof(float) * (size_t)F * 9 * 4 * K, vseg = sizeof(float) * (size_t)g.plane * 6 * 4 * K;
+    int R = 1;
     {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
-        const size_t need = sb * (nseg + 1) + hbytes + vdbytes;
-        if (need + (256u << 20) > fr) {
-            err = "the gradient needs " + std::to_string(need >> 20) + " MiB of device memory for checkpoints and " +
-                  "stage stores at this checkpoint interval; " + std::to_string(fr >> 20) + " MiB are free";
+        const size_t reserve = (size_t)768 << 20;
+        const size_t other = sb * (nseg + 1) + sizeof(float) * ((size_t)nst * NT * 3 + (size_t)m.g.npad() * 3 +
+                                                                 (size_t)m.g.nx * m.g.ny * m.g.nz * 3);
+        if (other + hseg + vseg + reserve > fr) {
+            err = "the gradient needs " + std::to_string((other + hseg + vseg) >> 20) + " MiB of device memory for " +
+                  "checkpoints and stage stores at this checkpoint interval; " + std::to_string(fr >> 20) +
+                  " MiB are free";
             return ST_ALLOC;
         }
+        R = (int)std::min<size_t>((size_t)nseg, (fr - other - reserve) / (hseg + vseg));
     }
     CU(sc.get((void **)&ckpt, sb * nseg));
     CU(sc.get((void **)&final_state, sb));
-    CU(sc.get((void **)&hstore, hbytes));
-    CU(sc.get((void **)&vdstore, vdbytes));
+    CU(sc.get((void **)&hstore, hseg * R));
+    CU(sc.get((void **)&vdstore, vseg * R));
+    auto slot_of = [&](int s) { return s >= nseg - R ? s - (nseg - R) : 0; };
     const long long nres = (long long)nst * NT * 3;
     if (nres) CU(sc.get((void **)&res, sizeof(float) * nres));
     const long long npad = m.g.npad();
@@ -343,7 +371,11 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
     };
 
     // steps n0 .. n1-1 from the current state, storing each stage's RHS
-    auto run_storing = [&](int n0, int n1) -> int {
+    auto hptr = [&](int slot, int t, int irk) { return hstore + (size_t)F * 9 * (((size_t)slot * K + t) * 4 + irk); };
+    auto vdptr = [&](int slot, int t, int irk) {
+        return vdstore + (size_t)g.plane * 6 * (((size_t)slot * K + t) * 4 + irk);
+    };
+    auto run_storing = [&](int n0, int n1, int slot) -> int {
         for (int n = n0; n < n1; n++) {
             if (int st = launch_sources_on(stream)) return st;
             int FB[3];
@@ -352,8 +384,8 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
                 CgStageDesc d = desc_host_[irk];
                 d.a.pgv = nullptr;
                 d.a.dis = nullptr;
-                d.a.hstore = hstore + (size_t)F * 9 * ((n - n0) * 4 + irk);
-                d.a.vdstore = vdstore + (size_t)g.plane * 6 * ((n - n0) * 4 + irk);
+                d.a.hstore = hptr(slot, n - n0, irk);
+                d.a.vdstore = vdptr(slot, n - n0, irk);
                 const int sgn = (irk & 1) ? -1 : 1;
                 CU(launch_cg_stage(FB[0] * sgn, FB[1] * sgn, FB[2] * sgn, d, work_dev_, grid_ctas_, stream));
             }
@@ -363,17 +395,17 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
         return ST_OK;
     };
 
-    // 1. forward with checkpoints; the last segment stores its stage RHS
-    //    on the way, so it needs no second run
+    // 1. forward with checkpoints; the last R segments store their stage
+    //    RHS on the way, so they need no second run
     grad_ms[0] = grad_ms[1] = grad_ms[2] = 0.0f;
     CU(cudaEventRecord(ev[0], stream));
     for (int s = 0; s < nseg; s++) {
         if (int st = save_state(ckpt + sb * s)) return st;
         const int n = std::min(K, NT - it);
-        if (s + 1 < nseg) {
+        if (s < nseg - R) {
             if (int st = run_plain(n)) return st;
         } else {
-            if (int st = run_storing(it, it + n)) return st;
+            if (int st = run_storing(it, it + n, slot_of(s))) return st;
             it += n;
         }
     }
@@ -410,11 +442,11 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
         }
     for (int s = nseg - 1; s >= 0; s--) {
         const int n0 = s * K, n1 = std::min(NT, n0 + K);
-        if (s + 1 < nseg) {
+        if (s < nseg - R) {
             // forward again from the segment's checkpoint, storing each stage's RHS
             if (int st = load_state(ckpt + sb * s)) return st;
             CU(cudaMemcpyAsync(it_dev_, &n0, sizeof(int), cudaMemcpyHostToDevice, stream));
-            if (int st = run_storing(n0, n1)) return st;
+            if (int st = run_storing(n0, n1, 0)) return st;
             if (int st = lap(&ms_re)) return st;
         }
         // and back through it
@@ -422,8 +454,8 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
             CU(launch_adj_residual(adj_.Lp, g, st_idx_, nst, NT, n, res, stream));
             float *h4[4], *vd4[4];
             for (int irk = 0; irk < 4; irk++) {
-                h4[irk] = hstore + (size_t)F * 9 * ((n - n0) * 4 + irk);
-                vd4[irk] = vdstore + (size_t)g.plane * 6 * ((n - n0) * 4 + irk);
+                h4[irk] = hptr(slot_of(s), n - n0, irk);
+                vd4[irk] = vdptr(slot_of(s), n - n0, irk);
             }
             if (int st = adj_step(n, h4, vd4)) return st;
             kernel_launches += 1;

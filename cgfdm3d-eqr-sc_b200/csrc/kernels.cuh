@@ -134,12 +134,16 @@ struct AdjStageArgs {
     const float *h;      // stored RHS h_s of the forward stage (9 fields), or null: no gradient
     const float *vd;     // stored surface xi/eta velocity derivatives (6 x plane) of the stage
     float *grad;         // 3 fields: d J / d (mu, lambda, buoyancy), accumulated
+    float *M2;           // fused kernel: receives mu_{s-1} (M is read at neighbours meanwhile)
+    float *faceB2[5];    // fused kernel: the faces' mu_{s-1}
+    int kchunk, nchunk;  // fused kernel: z planes per block, blocks along z
     int irk;
     int FB1, FB2, FB3;
     int nPML, pml_on, fs_on;
     float rDH, DT;
 };
-cudaError_t launch_adj_stage(const AdjStageArgs &a, cudaStream_t st);
+cudaError_t launch_adj_stage(const AdjStageArgs &a, cudaStream_t st);        // two passes through Phi in HBM
+cudaError_t launch_adj_stage_fused(const AdjStageArgs &a, cudaStream_t st);  // one pass, Phi in shared memory
 // Adds the seismogram residual of sample n, res[station][n][3], to the
 // velocity of lambda (the misfit is 1/2 sum (v - d)^2).
 cudaError_t launch_adj_residual(float *Lp, DevGrid g, const int *st_idx, int nst, int NT, int n, const float *res,

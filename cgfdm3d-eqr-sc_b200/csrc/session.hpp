@@ -106,6 +106,7 @@ private:
     // auxiliaries' adjoints per face, the gradient and d rdz / d (mu, lambda)
     struct Adjoint {
         float *Lp = nullptr, *M = nullptr, *Lam = nullptr, *Phi = nullptr, *SF = nullptr;
+        float *M2 = nullptr, *B2[5] = {};   // the fused kernel's second mu buffers
         PmlFace face[5] = {};
         float *grad = nullptr, *drdz = nullptr;
     } adj_;

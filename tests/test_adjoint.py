@@ -15,6 +15,7 @@ oracle/fd_gradient.py) on the reference's own model of the same run.
 """
 
 import dataclasses
+import json
 import os
 import shutil
 
@@ -47,13 +48,14 @@ def _source_free(hill: bool, steps: int) -> cases.Case:
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kernel", ["fused", "two-pass"])
 @pytest.mark.parametrize("flavor", ["fast", "exact"])
 @pytest.mark.parametrize("hill", [False, True], ids=["flat", "hill"])
-def test_dot_product(tmp_path, hill, flavor):
+def test_dot_product(tmp_path, hill, flavor, kernel):
     n = 12
     d = cases.write_case(_source_free(hill, n), str(tmp_path / "run"))
     rng = np.random.default_rng(3 + hill)
-    with Session(d, flavor=flavor) as s:
+    with Session(d, options=json.dumps({"adjointKernel": kernel}), flavor=flavor) as s:
         i = s.info
         shape = (i.nzp, i.nyp, i.nxp, 9)
         zr = 2670.0 * 6000.0   # impedance: balances velocity and stress entries
@@ -130,6 +132,14 @@ def test_gradient_against_fp64_finite_differences(tmp_path):
         s.set_medium(start_med)
         J1, grad1 = s.gradient(observed, checkpoint_every=s.info.NT)
     assert J1 == J and np.array_equal(grad1, grad)
+    # the fused kernel (Phi in shared memory) agrees with the default two passes
+    with Session(d, options=json.dumps({"adjointKernel": "fused"})) as s2:
+        s2.set_medium(start_med)
+        J2, grad2 = s2.gradient(observed, checkpoint_every=25)
+    assert J2 == J
+    print(f"fused vs two-pass gradient: rel L2 {pu.rel_l2(grad, grad2):.2e}")
+    assert pu.rel_l2(grad, grad2) > 0.0   # a different summation order: not the same kernel
+    assert pu.rel_l2(grad, grad2) <= 1e-5
     assert np.abs(grad[:, :NPML]).max() == 0 and np.abs(grad[:, :, :, -NPML:]).max() == 0
     # the reference's model of the starting medium, and FP64 differences
     ref_dir = str(tmp_path / "ref")
@@ -169,8 +179,9 @@ def test_autograd_function_matches_session_gradient(tmp_path):
         vs, vp, rho = (torch.tensor(inner[..., c].copy(), requires_grad=True) for c in range(3))
         J = misfit(vp, vs, rho, s, torch.from_numpy(obs), 10)
         (2.0 * J).backward()
+        J = J.item()
         s.set_medium(med)
         J0, g0 = s.gradient(obs, 10)
-    assert float(J) == J0
+    assert J == J0
     for t, g in zip((vp, vs, rho), g0):
         np.testing.assert_array_equal(t.grad.numpy(), 2.0 * g)
