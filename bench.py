@@ -308,11 +308,12 @@ ADJ_BYTES_PER_POINT_STAGE = 4 * (9 + 9 + 9 + 12 + 18 + 9 + 6)
 
 
 def bench_adjoint(args, world, rank, local_rank):
-    """``--workload adjoint[_STEPS]``: the misfit gradient with respect to
+    """``--workload adjoint[_STEPS[_NXxNYxNZ]]``: the misfit gradient with respect to
     Vp, Vs and rho (cgfdm_gradient) on the 192 x 192 x 128 layered model
     with a 2 km, +8 % Vs ball in the true medium (cgfdm.configs.adjoint_shots):
     four shots (2 Hz Ricker point sources), 64 surface stations, NT = 2000
-    steps each (or STEPS), checkpoints every 100 steps.  The observed data
+    steps each (or STEPS; with a grid size, one shot of that size),
+    checkpoints every --checkpoint-every steps (100).  The observed data
     are the true medium's seismograms; the gradient is taken at the starting
     medium (no ball) and summed over the shots.  Reports gradient throughput
     (shots x points x NT / seconds) and the adjoint/forward cost: wall time
@@ -323,26 +324,30 @@ def bench_adjoint(args, world, rank, local_rank):
     import torch
     from cgfdm import Session, configs
 
-    NT = int(args.workload.split("_")[1]) if "_" in args.workload else 2000
-    root = os.path.join(WORK, f"adjoint_{NT}")
+    parts = args.workload.split("_")
+    NT = int(parts[1]) if len(parts) > 1 else 2000
+    NX, NY, NZ = (int(v) for v in parts[2].split("x")) if len(parts) > 2 else (192, 192, 128)
+    DH = 100.0
+    n_shots = 4 if len(parts) <= 2 else 1
+    root = os.path.join(WORK, f"adjoint_{NT}_{NX}x{NY}x{NZ}_{n_shots}")
     marker = os.path.join(root, ".done")
     if not os.path.exists(marker):
         if os.path.exists(root):
             shutil.rmtree(root)
-        configs.adjoint_shots(root, steps=NT)
+        configs.adjoint_shots(root, steps=NT, NX=NX, NY=NY, NZ=NZ, n_shots=n_shots)
         open(marker, "w").close()
     dirs = sorted(os.path.join(root, d) for d in os.listdir(root) if d.startswith("shot_"))
-    NX, NY, NZ, DH = 192, 192, 128, 100.0
     true = configs.adjoint_layers(NX, NY, NZ, DH, True)
     start = configs.adjoint_layers(NX, NY, NZ, DH, False)
-    K = 100
+    K = args.checkpoint_every
+    opts = json.dumps({"adjointStoreSegments": args.store_segments}) if args.store_segments else None
     t_fwd = t_grad = 0.0
     phases = np.zeros(3)
     grad_sum = None
     J_sum = 0.0
     with ClockSampler(local_rank) as clk:
         for d in dirs:
-            s = Session(d, device=local_rank)
+            s = Session(d, options=opts, device=local_rank)
             info = s.info
             s.set_medium(true)
             s.run(info.NT)
@@ -382,9 +387,9 @@ def bench_adjoint(args, world, rank, local_rank):
         "metric": METRIC, "value": n * pts * NT / t_grad / 1e6, "unit": METRIC, "n_gpus": 1, "steps": NT,
         "warmup": 0, "ms_per_step": t_grad * 1e3 / steps_adj, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "scheme": "CGFDM",
-        "config": {"workload": "adjoint: CGFDM misfit gradient w.r.t. Vp, Vs, rho, 192x192x128, DH=100 m, 4 layers "
-                               "+ half-space, true model with a 2 km-radius +8% Vs ball, 4 shots (2 Hz Ricker "
-                               "point sources), 64 surface stations, checkpoint every 100 steps, FP32",
+        "config": {"workload": f"adjoint: CGFDM misfit gradient w.r.t. Vp, Vs, rho, {NX}x{NY}x{NZ}, DH=100 m, "
+                               f"4 layers + half-space, true model with a 2 km-radius +8% Vs ball, {n} shot(s) "
+                               f"(2 Hz Ricker point sources), 64 surface stations, checkpoint every {K} steps, FP32",
                    "points": pts, "shots": n, "NT": NT, "checkpoint_every": K,
                    "l2": "inputs larger than L2 (%.1f GB resident per session)" % dev_gb,
                    "parallelism": "replicas x1"},
@@ -418,6 +423,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="terrain_fault")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--checkpoint-every", type=int, default=100, help="adjoint workload: checkpoint interval")
+    ap.add_argument("--store-segments", type=int, default=0,
+                    help="adjoint workload: cap on segments stored during the first forward (0: memory decides)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -88,11 +88,15 @@ __device__ __forceinline__ void dir_stress_t(float m0, float m1, float m2, const
     out[2] = lam * m2 * W + m2mu * m2 * w[5] + mu * (m0 * w[7] + m1 * w[8]);
 }
 
-__device__ __forceinline__ bool in_pml_cell(const AdjStageArgs &a, int i, int j, int k, int _nx, int _ny)
+// index of point (i, j, k) in face fc's slab (the forward's layout)
+__device__ __forceinline__ long long face_pos(const DevGrid &g, int fc, int n, int i, int j, int k)
 {
-    const int n = a.nPML;
-    return a.pml_on && (i < CGFDM_HALO + n || i >= _nx - n || j < CGFDM_HALO + n || j >= _ny - n ||
-                        k < CGFDM_HALO + n);
+    const int i0p = i - CGFDM_HALO, j0p = j - CGFDM_HALO, k0p = k - CGFDM_HALO;
+    if (fc == 0 || fc == 3)
+        return (long long)(i0p - (fc == 3 ? g.nx - n : 0)) + (long long)j0p * n + (long long)k0p * n * g.ny;
+    if (fc == 1 || fc == 4)
+        return (long long)i0p + (long long)(j0p - (fc == 4 ? g.ny - n : 0)) * g.nx + (long long)k0p * g.nx * n;
+    return (long long)i0p + (long long)j0p * g.nx + (long long)k0p * g.nx * g.ny;
 }
 
 // --------------------------------------------------------------- pass 1
@@ -331,14 +335,15 @@ __global__ void ADJ_BOUNDS_GATHER k_adj_gather(const __grid_constant__ AdjStageA
     // RK4 adjoint (src/wave_rk.cpp:17-104 transposed).  Every operand is
     // loaded before the first store, so the loads issue together.
     const int irk = a.irk;
-    const bool grad = a.h && !in_pml_cell(a, i, j, k, _nx, _ny);
+    const bool grad = a.h && a.hbox.contains(i, j, k);
+    const long long hq = grad ? a.hbox.at(i, j, k) : 0;
     float mus[9], lp[9], lm[9], h[9], g3[3], mu = 0.0f, lam = 0.0f, buo = 1.0f;
 #pragma unroll
     for (int f = 0; f < 9; f++) {
         lp[f] = irk != 0 ? a.Lp[f * F + q] : 0.0f;
         mus[f] = irk == 3 ? RK_BETA4 * lp[f] : a.M[f * F + q];
         lm[f] = irk != 3 ? a.Lam[f * F + q] : 0.0f;
-        h[f] = grad ? a.h[f * F + q] : 0.0f;
+        h[f] = grad ? a.h[f * a.hbox.fstride + hq] : 0.0f;
     }
     if (grad) {
         for (int c = 0; c < 3; c++) g3[c] = a.grad[c * F + q];
@@ -403,7 +408,7 @@ cudaError_t launch_adj_stage(const AdjStageArgs &a, cudaStream_t st)
 // mu_s) at their neighbours' points while those write mu_{s-1}, so the
 // output goes to a second buffer (M2, faceB2) that the host swaps in.
 #ifndef ADJF_TY
-#define ADJF_TY 4
+#define ADJF_TY 8
 #endif
 #define ADJF_BX (32 + 6)
 #define ADJF_BY (ADJF_TY + 6)
@@ -414,17 +419,6 @@ __device__ __forceinline__ void load_mu_s(const AdjStageArgs &a, long long q, lo
 {
 #pragma unroll
     for (int f = 0; f < 9; f++) m[f] = a.irk == 3 ? RK_BETA4 * a.Lp[f * F + q] : a.M[f * F + q];
-}
-
-// index of point (i, j, k) in face fc's slab (the forward's layout)
-__device__ __forceinline__ long long face_pos(const DevGrid &g, int fc, int n, int i, int j, int k)
-{
-    const int i0p = i - CGFDM_HALO, j0p = j - CGFDM_HALO, k0p = k - CGFDM_HALO;
-    if (fc == 0 || fc == 3)
-        return (long long)(i0p - (fc == 3 ? g.nx - n : 0)) + (long long)j0p * n + (long long)k0p * n * g.ny;
-    if (fc == 1 || fc == 4)
-        return (long long)i0p + (long long)(j0p - (fc == 4 ? g.ny - n : 0)) * g.nx + (long long)k0p * g.nx * n;
-    return (long long)i0p + (long long)j0p * g.nx + (long long)k0p * g.nx * g.ny;
 }
 
 // Phi_d at interior point (i, j, k), as k_adj_pre forms it; with X given,
@@ -683,14 +677,15 @@ __global__ void __launch_bounds__(ADJF_NT) k_adj_fused(const __grid_constant__ A
 
         // point-wise: RK4 adjoint of the wavefield and the auxiliaries, gradient
         const int irk = a.irk;
-        const bool grad = a.h && !in_pml_cell(a, i, j, kout, _nx, _ny);
+        const bool grad = a.h && a.hbox.contains(i, j, kout);
+        const long long hq = grad ? a.hbox.at(i, j, kout) : 0;
         float mus[9], lp[9], lm[9], h[9], g3[3] = {0.0f, 0.0f, 0.0f}, mu = 0.0f, lam = 0.0f, buo = 1.0f;
 #pragma unroll
         for (int f = 0; f < 9; f++) {
             lp[f] = irk != 0 ? a.Lp[f * F + q] : 0.0f;
             mus[f] = irk == 3 ? RK_BETA4 * lp[f] : a.M[f * F + q];
             lm[f] = irk != 3 ? a.Lam[f * F + q] : 0.0f;
-            h[f] = grad ? a.h[f * F + q] : 0.0f;
+            h[f] = grad ? a.h[f * a.hbox.fstride + hq] : 0.0f;
         }
         if (grad) {
             for (int c = 0; c < 3; c++) g3[c] = a.grad[c * F + q];

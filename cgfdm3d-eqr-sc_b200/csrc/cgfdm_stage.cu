@@ -514,9 +514,11 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         }
 
         // the adjoint's gradient reads h outside the PML layers only
-        if (a.hstore && !(inx1 || iny1 || inz1 || inx2 || iny2))
+        if (a.hstore && a.hbox.contains(i, j, k)) {
+            const long long hq = a.hbox.at(i, j, k);
 #pragma unroll
-            for (int f = 0; f < 9; f++) a.hstore[f * F + q] = h[f];
+            for (int f = 0; f < 9; f++) a.hstore[f * a.hbox.fstride + hq] = h[f];
+        }
 
         // ---- RK4 update of the wavefield (src/wave_rk.cpp:17-104)
         float wout[9];

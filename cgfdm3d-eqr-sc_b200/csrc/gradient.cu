@@ -17,12 +17,14 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "session.hpp"
 #include "session_util.hpp"
 
 #ifndef ADJF_KCHUNK
-#define ADJF_KCHUNK 28   // planes per block of the fused adjoint kernel
+#define ADJF_KCHUNK 16   // planes per block of the fused adjoint kernel (16 x 8-row tiles measured fastest)
 #endif
 
 namespace cgfdm {
@@ -165,7 +167,7 @@ int Session::adj_prepare()
     ALLOC(adj_.Lp, float, F * 9);
     ALLOC(adj_.M, float, F * 9);
     ALLOC(adj_.Lam, float, F * 9);
-    if (m.p.adj_two_pass) {
+    if (!m.p.adj_fused) {
         ALLOC(adj_.Phi, float, F * 27);
         ALLOC(adj_.SF, float, g.plane * 36);
     } else {
@@ -179,15 +181,26 @@ int Session::adj_prepare()
         ALLOC(adj_.face[fc].A, float, face_[fc].count * 9);
         ALLOC(adj_.face[fc].B, float, face_[fc].count * 9);
         ALLOC(adj_.face[fc].T, float, face_[fc].count * 9);
-        if (!m.p.adj_two_pass) ALLOC(adj_.B2[fc], float, face_[fc].count * 9);
+        if (m.p.adj_fused) ALLOC(adj_.B2[fc], float, face_[fc].count * 9);
     }
     return ST_OK;
+}
+
+HBox Session::hbox() const
+{
+    const int n = m.p.pml ? m.g.nPML : 0;
+    HBox b;
+    b.x0 = CGFDM_HALO + n, b.y0 = CGFDM_HALO + n, b.z0 = CGFDM_HALO + n;
+    b.nx = m.g.nx - 2 * n, b.ny = m.g.ny - 2 * n, b.nz = m.g.nz - n;   // no PML under the free surface
+    b.fstride = ((long long)b.nx * b.ny * b.nz + 63) / 64 * 64;
+    return b;
 }
 
 void Session::adj_args(AdjStageArgs &a, int irk, const int FB[3]) const
 {
     std::memset(&a, 0, sizeof a);
     a.g = g;
+    a.hbox = hbox();
     a.cjm = cjm_;
     a.rdz = rdz_;
     a.drdz = adj_.drdz;
@@ -231,7 +244,7 @@ int Session::adj_step(int n, float *const *h4, float *const *vd4)
         a.h = h4 ? h4[irk] : nullptr;
         a.vd = vd4 ? vd4[irk] : nullptr;
         if (!a.h) a.grad = nullptr;
-        if (m.p.adj_two_pass) {
+        if (!m.p.adj_fused) {
             CU(launch_adj_stage(a, stream));
         } else {
             CU(launch_adj_stage_fused(a, stream));
@@ -240,7 +253,7 @@ int Session::adj_step(int n, float *const *h4, float *const *vd4)
             for (int fc = 0; fc < 5; fc++) std::swap(adj_.face[fc].B, adj_.B2[fc]);
         }
     }
-    kernel_launches += m.p.adj_two_pass ? 8 : 4;
+    kernel_launches += m.p.adj_fused ? 4 : 8;
     adj_swap();
     return ST_OK;
 }
@@ -277,21 +290,61 @@ int Session::adjoint_apply(int nsteps, float *host)
 }
 
 // RAII for the gradient's scratch allocations
+// Scratch of the gradient (checkpoints, stage stores, residuals): one
+// device block per device, kept while a session exists on that device and
+// reused by the next gradient call of any of them, so a run of gradient
+// calls maps its tens of GB once.  Gradient calls on one device take turns.
 namespace {
-struct Scratch {
-    std::vector<void *> p;
-    ~Scratch()
+struct Arena {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int sessions = 0;
+    std::mutex mu;
+};
+std::mutex g_arenas_mu;
+std::map<int, Arena> g_arenas;
+
+Arena &arena_of(int device)
+{
+    std::lock_guard<std::mutex> lk(g_arenas_mu);
+    return g_arenas[device];
+}
+
+// carves aligned sub-buffers out of the arena
+struct Carve {
+    char *base;
+    size_t off = 0;
+    template <typename T>
+    T *take(size_t bytes)
     {
-        for (void *x : p) cudaFree(x);
-    }
-    cudaError_t get(void **out, size_t bytes)
-    {
-        cudaError_t e = cudaMalloc(out, bytes);
-        if (e == cudaSuccess) p.push_back(*out);
-        return e;
+        T *r = reinterpret_cast<T *>(base + off);
+        off += (bytes + 255) / 256 * 256;
+        return r;
     }
 };
 }  // namespace
+
+void arena_session_add(int device)
+{
+    Arena &A = arena_of(device);
+    std::lock_guard<std::mutex> lk(A.mu);
+    A.sessions++;
+}
+
+void arena_session_remove(int device)
+{
+    Arena &A = arena_of(device);
+    std::lock_guard<std::mutex> lk(A.mu);
+    if (--A.sessions == 0 && A.p) {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(device);
+        cudaFree(A.p);
+        cudaSetDevice(cur);
+        A.p = nullptr;
+        A.bytes = 0;
+    }
+}
 
 int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
 {
@@ -319,38 +372,54 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
     const long long F = g.fstride;
     const size_t sb = state_bytes();
 
-    Scratch sc;
+    Arena &arena = arena_of(device);
+    std::lock_guard<std::mutex> arena_lock(arena.mu);
     char *ckpt = nullptr, *final_state = nullptr;
     float *hstore = nullptr, *vdstore = nullptr, *res = nullptr, *d_med = nullptr, *d_grad = nullptr;
     // stage stores of one segment; the last R segments are stored during the
     // first forward run (as many as device memory holds), the others are
     // re-run from their checkpoints into slot 0
-    const size_t hseg = sizeof(float) * (size_t)F * 9 * 4 * K, vseg = sizeof(float) * (size_t)g.plane * 6 * 4 * K;
+    const HBox hb = hbox();
+    const size_t hseg = sizeof(float) * (size_t)hb.fstride * 9 * 4 * K;
+    const size_t vseg = sizeof(float) * (size_t)g.plane * 6 * 4 * K;
+    const long long nres = (long long)nst * NT * 3;
+    const long long npad = m.g.npad();
+    auto round256 = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t other = round256(sb * nseg) + round256(sb) + round256(sizeof(float) * nres) +
+                         round256(sizeof(float) * npad * 3) +
+                         round256(sizeof(float) * (size_t)m.g.nx * m.g.ny * m.g.nz * 3);
     int R = 1;
     {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
+        fr += arena.bytes;   // the arena's block is available to this call
         const size_t reserve = (size_t)768 << 20;
-        const size_t other = sb * (nseg + 1) + sizeof(float) * ((size_t)nst * NT * 3 + (size_t)m.g.npad() * 3 +
-                                                                 (size_t)m.g.nx * m.g.ny * m.g.nz * 3);
-        if (other + hseg + vseg + reserve > fr) {
+        if (other + round256(hseg) + round256(vseg) + reserve > fr) {
             err = "the gradient needs " + std::to_string((other + hseg + vseg) >> 20) + " MiB of device memory for " +
                   "checkpoints and stage stores at this checkpoint interval; " + std::to_string(fr >> 20) +
                   " MiB are free";
             return ST_ALLOC;
         }
-        R = (int)std::min<size_t>((size_t)nseg, (fr - other - reserve) / (hseg + vseg));
+        R = (int)std::min<size_t>((size_t)nseg, (fr - other - reserve) / (round256(hseg) + round256(vseg)));
+        if (m.p.adj_store_max > 0) R = std::min(R, m.p.adj_store_max);
     }
-    CU(sc.get((void **)&ckpt, sb * nseg));
-    CU(sc.get((void **)&final_state, sb));
-    CU(sc.get((void **)&hstore, hseg * R));
-    CU(sc.get((void **)&vdstore, vseg * R));
+    const size_t need = other + R * (round256(hseg) + round256(vseg));
+    if (arena.bytes < need) {
+        if (arena.p) CU(cudaFree(arena.p));
+        arena.p = nullptr;
+        arena.bytes = 0;
+        CU(cudaMalloc(&arena.p, need));
+        arena.bytes = need;
+    }
+    Carve cv{static_cast<char *>(arena.p)};
+    ckpt = cv.take<char>(sb * nseg);
+    final_state = cv.take<char>(sb);
+    hstore = cv.take<float>(hseg * R);   // R whole segments: round256(hseg) == hseg for 256-byte multiples
+    vdstore = cv.take<float>(vseg * R);
+    if (nres) res = cv.take<float>(sizeof(float) * nres);
+    d_med = cv.take<float>(sizeof(float) * npad * 3);
+    d_grad = cv.take<float>(sizeof(float) * (size_t)m.g.nx * m.g.ny * m.g.nz * 3);
     auto slot_of = [&](int s) { return s >= nseg - R ? s - (nseg - R) : 0; };
-    const long long nres = (long long)nst * NT * 3;
-    if (nres) CU(sc.get((void **)&res, sizeof(float) * nres));
-    const long long npad = m.g.npad();
-    CU(sc.get((void **)&d_med, sizeof(float) * npad * 3));
-    CU(sc.get((void **)&d_grad, sizeof(float) * (size_t)m.g.nx * m.g.ny * m.g.nz * 3));
 
     cudaEvent_t ev[2];
     CU(cudaEventCreate(&ev[0]));
@@ -371,7 +440,9 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
     };
 
     // steps n0 .. n1-1 from the current state, storing each stage's RHS
-    auto hptr = [&](int slot, int t, int irk) { return hstore + (size_t)F * 9 * (((size_t)slot * K + t) * 4 + irk); };
+    auto hptr = [&](int slot, int t, int irk) {
+        return hstore + (size_t)hb.fstride * 9 * (((size_t)slot * K + t) * 4 + irk);
+    };
     auto vdptr = [&](int slot, int t, int irk) {
         return vdstore + (size_t)g.plane * 6 * (((size_t)slot * K + t) * 4 + irk);
     };
@@ -385,6 +456,7 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
                 d.a.pgv = nullptr;
                 d.a.dis = nullptr;
                 d.a.hstore = hptr(slot, n - n0, irk);
+                d.a.hbox = hb;
                 d.a.vdstore = vdptr(slot, n - n0, irk);
                 const int sgn = (irk & 1) ? -1 : 1;
                 CU(launch_cg_stage(FB[0] * sgn, FB[1] * sgn, FB[2] * sgn, d, work_dev_, grid_ctas_, stream));

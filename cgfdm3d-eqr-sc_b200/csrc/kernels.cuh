@@ -23,9 +23,26 @@ struct PmlFace {
     int n0, n1;          // slab extent along its two fastest axes (see pml_pos)
 };
 
+// The points outside the PML layers, where the adjoint takes a gradient:
+// i in [x0, x0 + nx), j in [y0, y0 + ny), k in [z0, z0 + nz) (padded-grid
+// indices), stored field by field as [k][j][i] with `fstride` floats a field.
+struct HBox {
+    int x0, y0, z0, nx, ny, nz;
+    long long fstride;
+    __host__ __device__ __forceinline__ bool contains(int i, int j, int k) const
+    {
+        return i >= x0 && i < x0 + nx && j >= y0 && j < y0 + ny && k >= z0 && k < z0 + nz;
+    }
+    __host__ __device__ __forceinline__ long long at(int i, int j, int k) const
+    {
+        return ((long long)(k - z0) * ny + (j - y0)) * nx + (i - x0);
+    }
+};
+
 // --------------------------------------------------------- CGFDM stage
 struct CgStageArgs {
     DevGrid g;
+    HBox hbox;           // layout of hstore
     const float *Win;    // stencil input of this stage
     const float *Wm;     // values at the start of the step (RK "m")
     float *T;            // RK accumulator
@@ -38,7 +55,7 @@ struct CgStageArgs {
     PmlFace face[5];     // x1 y1 z1 x2 y2 (order of src/pml_deriv.cpp:633-646)
     float *pgv;          // [ny][nx][2] running max, stage 3 only
     float *dis;          // displacement, 3 fields in the W layout, stage 3 only
-    float *hstore;       // or null: receives this stage's RHS h (9 fields, W layout) for the adjoint
+    float *hstore;       // or null: receives this stage's RHS h for the adjoint (9 fields, HBox layout)
     float *vdstore;      // or null: receives the surface layer's xi/eta velocity derivatives (6 x plane)
     int *err;            // device error word: bit 0 = a bounded wait gave up
     int ntiles_x, ntiles_y, nchunk;  // work items: tiles x tiles x z-chunks
@@ -120,6 +137,7 @@ cudaError_t launch_sc_sjac(const float *cjm, DevGrid g, float DT, float rDH, flo
 // for the wavefield and, point-wise, for the PML auxiliaries.
 struct AdjStageArgs {
     DevGrid g;
+    HBox hbox;           // layout of h
     const float *cjm, *rdz;
     const float *drdz;   // d rdz / d mu (18 fields) then d rdz / d lambda (18), [36][plane], or null
     const float *pml_alpha_x, *pml_beta_x, *pml_d_x;
@@ -131,7 +149,7 @@ struct AdjStageArgs {
     float *Phi;          // 27 fields: per direction, the adjoint of its one-sided differences
     float *SF;           // surface layers L = 0..2 (k = _nz-1-L): 12 channels each, [3][12][plane]
     PmlFace face[5];     // adjoint auxiliaries per face: A = lambda', B = mu, T = running sum
-    const float *h;      // stored RHS h_s of the forward stage (9 fields), or null: no gradient
+    const float *h;      // stored RHS h_s of the forward stage (9 fields, HBox layout), or null: no gradient
     const float *vd;     // stored surface xi/eta velocity derivatives (6 x plane) of the stage
     float *grad;         // 3 fields: d J / d (mu, lambda, buoyancy), accumulated
     float *M2;           // fused kernel: receives mu_{s-1} (M is read at neighbours meanwhile)

@@ -655,7 +655,8 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
         if ((it = o.get("SOLVE_DISPLACEMENT"))) m.p.solve_displacement = it->as_int();
         if ((it = o.get("metricPrecision")) && it->kind == JsonValue::String) m.p.metric_fp64 = it->str == "fp64";
         if ((it = o.get("storage")) && it->kind == JsonValue::String) m.p.storage = it->str;
-        if ((it = o.get("adjointKernel")) && it->kind == JsonValue::String) m.p.adj_two_pass = it->str != "fused";
+        if ((it = o.get("adjointKernel")) && it->kind == JsonValue::String) m.p.adj_fused = it->str == "fused";
+        if ((it = o.get("adjointStoreSegments"))) m.p.adj_store_max = it->as_int();
         if ((it = o.get("OUT")) && it->kind == JsonValue::String) m.p.OUT = it->str;
     }
     Params &p = m.p;

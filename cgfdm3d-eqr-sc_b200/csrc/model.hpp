@@ -67,7 +67,8 @@ struct Params {
     int exp_decay = 0;               // exponential sponge (SCFDM default build)
     int solve_displacement = 0;      // SOLVE_DISPLACEMENT
     int metric_fp64 = 0;             // "metricPrecision": "fp64" -> metrics computed in FP64
-    int adj_two_pass = 1;            // options "adjointKernel": "two-pass" (default) | "fused"
+    int adj_fused = 0;               // options "adjointKernel": "two-pass" (default) | "fused"
+    int adj_store_max = 0;           // options "adjointStoreSegments": cap on segments kept from the forward (0: memory decides)
     std::string storage = "fp32";    // "storage": "fp32" | "fp16" | "bf16"
     // extension inputs (raw arrays the reference has no reader for)
     std::string terrainFile;         // float32 [_ny_][_nx_] surface height (m)

@@ -82,6 +82,7 @@ __global__ void k_hrange(const float *__restrict__ coord, int nxp, int nyp, int 
 // ----------------------------------------------------------------- util
 Session::~Session()
 {
+    if (counted_) arena_session_remove(device);
     if (graph8_) cudaGraphExecDestroy(graph8_);
     if (graph8_src_) cudaGraphDestroy(graph8_src_);
     for (auto &e : ev_)
@@ -132,6 +133,8 @@ int Session::create(const std::string &dir, const std::string &options, int dev)
         return ST_OPTIONS;
     }
     CU(cudaSetDevice(dev));
+    arena_session_add(dev);
+    counted_ = true;
     CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     for (auto &e : ev_) CU(cudaEventCreate(&e));
     return setup_device();

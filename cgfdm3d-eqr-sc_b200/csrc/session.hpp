@@ -15,6 +15,9 @@ namespace cgfdm {
 // FB signs of the first RK stage of a step (src/propagate.cpp:158-168);
 // each later stage flips all three.
 void fb_signs(int step, int fb[3]);
+// gradient scratch kept per device while sessions live there (csrc/gradient.cu)
+void arena_session_add(int device);
+void arena_session_remove(int device);
 
 struct DevBuf {
     void *p = nullptr;
@@ -51,6 +54,7 @@ public:
     std::string run_dir;
     int device = 0;
     int it = 0;  // steps completed
+    bool counted_ = false;  // registered with the device's gradient scratch
     int nst = 0;
     cudaStream_t stream = nullptr;
     long long graph_launches = 0, kernel_launches = 0;
@@ -111,6 +115,7 @@ private:
         float *grad = nullptr, *drdz = nullptr;
     } adj_;
     int adj_prepare();
+    HBox hbox() const;                                          // points outside the PML layers
     void adj_args(AdjStageArgs &a, int irk, const int FB[3]) const;
     int adj_step(int n, float *const *h4, float *const *vd4);  // lambda_{n+1} -> lambda_n
     void adj_swap();

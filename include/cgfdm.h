@@ -145,8 +145,14 @@ int cgfdm_set_medium(cgfdm_session *s, const float *medium, long long count);
  * steps in device memory, then per segment, last first, re-runs it storing
  * each RK stage's right-hand side and steps the transposed operator back
  * through it.  Device memory: (NT / checkpoint_every + 1) states plus
- * 36 * checkpoint_every wavefield-sized fields; CGFDM_E_ALLOC names the
- * amount when it is not free.  The session ends at step NT with the forward
+ * 36 * checkpoint_every wavefield-sized fields per stored segment;
+ * CGFDM_E_ALLOC names the amount when one segment does not fit.  The last
+ * segments are stored during the first forward run, as many as the free
+ * device memory holds (the options key "adjointStoreSegments" caps that
+ * number), and need no second run.  This scratch stays allocated on the
+ * device after the call, for the next cgfdm_gradient of any session on that
+ * device, until the device's last session is destroyed; gradient calls on
+ * one device run one at a time.  The session ends at step NT with the forward
  * run's state and station traces.
  *
  * cgfdm_adjoint_apply: applies the transpose of the last `nsteps` steps the

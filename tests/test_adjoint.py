@@ -48,7 +48,7 @@ def _source_free(hill: bool, steps: int) -> cases.Case:
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kernel", ["fused", "two-pass"])
+@pytest.mark.parametrize("kernel", ["two-pass", "fused"])
 @pytest.mark.parametrize("flavor", ["fast", "exact"])
 @pytest.mark.parametrize("hill", [False, True], ids=["flat", "hill"])
 def test_dot_product(tmp_path, hill, flavor, kernel):
@@ -138,8 +138,7 @@ def test_gradient_against_fp64_finite_differences(tmp_path):
         J2, grad2 = s2.gradient(observed, checkpoint_every=25)
     assert J2 == J
     print(f"fused vs two-pass gradient: rel L2 {pu.rel_l2(grad, grad2):.2e}")
-    assert pu.rel_l2(grad, grad2) > 0.0   # a different summation order: not the same kernel
-    assert pu.rel_l2(grad, grad2) <= 1e-5
+    assert 0.0 < pu.rel_l2(grad, grad2) <= 1e-5   # another summation order, the same gradient
     assert np.abs(grad[:, :NPML]).max() == 0 and np.abs(grad[:, :, :, -NPML:]).max() == 0
     # the reference's model of the starting medium, and FP64 differences
     ref_dir = str(tmp_path / "ref")
