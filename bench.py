@@ -73,6 +73,18 @@ def traffic_ratio():
     return None
 
 
+def adj_traffic_per_point_stage():
+    """DRAM bytes per point and stage of the adjoint kernels, from the
+    committed ncu summary (profiles/adj_stage_traffic.txt), or None."""
+    path = os.path.join(ROOT, "profiles", "adj_stage_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_point_stage:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
 def make_workload(name, steps, directory):
     from cgfdm import cases, configs
 
@@ -400,7 +412,9 @@ def bench_adjoint(args, world, rank, local_rank):
         "misfit": J_sum,
         "grad_vs_ball_over_outside": float(np.abs(gvs[inside]).mean() / max(np.abs(gvs[~inside]).mean(), 1e-300)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / hbm_peak, "peak_kind": peak_kind,
+                     "traffic": (adj_traffic_per_point_stage() or 0) * 4 * pts or None,
+                     "traffic_source": "ncu bytes per point and stage on adjoint_24_144x144x112 x points x 4 stages",
                      "kernel": "k_adj_pre + k_adj_gather (one adjoint step = 4 stages x 2 launches)",
                      "algo_bytes_per_step": algo, "mean_step_ms": adj_ms_step},
         "e2e": {"value": n * pts * NT / t_grad / 1e6, "unit": METRIC,
