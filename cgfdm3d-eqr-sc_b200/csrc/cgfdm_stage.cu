@@ -35,6 +35,21 @@
 #include "device.cuh"
 #include "kernels.cuh"
 
+// L2 promotion of the plane-ring (halo) and point-operand tensor maps, and
+// which point operands are prefetched into L2 ahead of their loads.
+#ifndef CG_PROMO_HALO
+#define CG_PROMO_HALO CU_TENSOR_MAP_L2_PROMOTION_L2_256B
+#endif
+#ifndef CG_PROMO_POINT
+#define CG_PROMO_POINT CU_TENSOR_MAP_L2_PROMOTION_L2_256B
+#endif
+#ifndef CG_PREFETCH_C
+#define CG_PREFETCH_C 1
+#endif
+#ifndef CG_PREFETCH_MT
+#define CG_PREFETCH_MT 1
+#endif
+
 namespace cgfdm {
 
 // 32 x 4 tiles, three CTAs per SM (12 warps, 168 registers): 5 % faster on
@@ -301,9 +316,9 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     const int ke = min(kb + a.kchunk, _nz);
     if (kb >= ke) continue;
     const int kf = kb - za;                 // first plane this item loads
-    const int tx0 = g.xoff + i0 - 4;        // halo box origin column: a multiple of 32
+    const int tx0 = g.xoff + i0 - 4;        // halo box origin column: a multiple of 4 (16 bytes)
     const int ty0 = j0 - hyL;
-    const int px0 = g.xoff + i0;            // point box origin column: 4 mod 32
+    const int px0 = g.xoff + i0;            // point box origin column: a multiple of 4
 
     // plane kk of this item is fill number seq0 + (kk - kf) of the CTA
     auto slot_of = [&](int kk) { return (int)((seq0 + (unsigned)(kk - kf)) % NSLOT); };
@@ -317,9 +332,9 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     };
     // point operands of plane kk into L2 ahead of their plain loads
     auto prefetch_points = [&](int kk) {
-        tma_prefetch_4d(tmC, px0, j0, kk, 0);
-        if (a.irk == 1 || a.irk == 2) tma_prefetch_4d(tmM, px0, j0, kk, 0);
-        if (a.irk != 0) tma_prefetch_4d(tmT, px0, j0, kk, 0);
+        if (CG_PREFETCH_C) tma_prefetch_4d(tmC, px0, j0, kk, 0);
+        if (CG_PREFETCH_MT && (a.irk == 1 || a.irk == 2)) tma_prefetch_4d(tmM, px0, j0, kk, 0);
+        if (CG_PREFETCH_MT && a.irk != 0) tma_prefetch_4d(tmT, px0, j0, kk, 0);
     };
 
     const int klast = ke - za + 3;          // last plane of the last window
@@ -649,7 +664,7 @@ cudaError_t make_field_tmap(void *out, const float *base, const DevGrid &g, int 
     cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = encode(reinterpret_cast<CUtensorMap *>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, (void *)base, dims,
                         strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                        halo_box ? CG_PROMO_HALO : CG_PROMO_POINT, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 

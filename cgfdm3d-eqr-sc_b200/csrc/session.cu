@@ -143,7 +143,7 @@ int Session::create(const std::string &dir, const std::string &options, int dev)
 int Session::setup_device()
 {
     const Grid &G = m.g;
-    g = make_devgrid(G.nx, G.ny, G.nz);
+    g = make_devgrid(G.nx, G.ny, G.nz, m.p.scheme == SCHEME_CGFDM ? 29 : 1);
     const long long F = g.fstride;
     const long long npad = G.npad();
     const bool cg = m.p.scheme == SCHEME_CGFDM;
