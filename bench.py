@@ -254,7 +254,7 @@ def bench_batch(args, world, rank, local_rank):
     from cgfdm import Batch, Session, configs
 
     n = int(args.workload[len("batch"):] or 32)
-    total = args.warmup + 2 * args.steps + 8  # batched steps, then the same number per shot alone
+    total = args.warmup + 2 * args.steps + 24  # batched steps, then the same number per shot alone
     root = os.path.join(WORK, f"{args.workload}_{total}")
     marker = os.path.join(root, ".done")
     if not os.path.exists(marker):
@@ -268,6 +268,10 @@ def bench_batch(args, world, rank, local_rank):
     algo = sum(s.info.algo_bytes_per_step for s in sessions)
     b = Batch(sessions)
     b.run(args.warmup)
+    # the default decomposition, then the autotuner's choice (timed below)
+    ms_default = b.run_timed(8)
+    tuned = b.autotune(3)
+    b.run(1)
     torch.cuda.synchronize(local_rank)
     with ClockSampler(local_rank) as clk:
         ms = b.run_timed(args.steps)
@@ -301,6 +305,8 @@ def bench_batch(args, world, rank, local_rank):
                                "stage launch per RK stage for all shots, 8-step CUDA graphs",
                    "points": pts, "shots": n,
                    "alone_Mpts_step_s": pts * args.steps / (alone_ms * 1e-3) / 1e6,
+                   "autotuned": {"kchunk": tuned[0], "ctas": tuned[1], "trial_ms_per_step": tuned[2],
+                                 "default_ms_per_step": ms_default / 8},
                    "l2": "inputs larger than L2", "parallelism": "batch x1"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "peak_kind": peak_kind, "traffic": None,

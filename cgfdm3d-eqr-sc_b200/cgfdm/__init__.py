@@ -78,6 +78,11 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
     L.cgfdm_set_medium.argtypes = [vp, fp, ctypes.c_longlong]
     L.cgfdm_adjoint_apply.argtypes = [vp, ctypes.c_int, fp, ctypes.c_longlong]
     L.cgfdm_gradient_profile.argtypes = [vp, fp]
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.cgfdm_autotune.argtypes = [vp, ctypes.c_int, ip, ip, ctypes.POINTER(ctypes.c_float)]
+    L.cgfdm_set_tiling.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.cgfdm_get_tiling.argtypes = [vp, ip, ip]
+    L.cgfdm_batch_autotune.argtypes = [vp, ctypes.c_int, ip, ip, ctypes.POINTER(ctypes.c_float)]
     L.cgfdm_gradient.argtypes = [vp, fp, ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(ctypes.c_double), fp,
                                  ctypes.c_longlong]
     L.cgfdm_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
@@ -204,6 +209,22 @@ class Session:
                                           _fptr(grad), grad.size))
         return J.value, grad
 
+    def autotune(self, trial_steps: int = 4):
+        """Times candidate work decompositions of the stage kernel and keeps
+        the fastest (cgfdm_autotune); returns (kchunk, ctas, ms_per_step)."""
+        kc, ct, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        self._check(self.L.cgfdm_autotune(self._h, int(trial_steps), ctypes.byref(kc), ctypes.byref(ct),
+                                          ctypes.byref(ms)))
+        return kc.value, ct.value, ms.value
+
+    def set_tiling(self, kchunk: int, ctas: int) -> None:
+        self._check(self.L.cgfdm_set_tiling(self._h, int(kchunk), int(ctas)))
+
+    def tiling(self):
+        kc, ct = ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.cgfdm_get_tiling(self._h, ctypes.byref(kc), ctypes.byref(ct)))
+        return kc.value, ct.value
+
     def gradient_profile(self):
         """Device ms of the last gradient's phases: forward with checkpoints,
         segment re-runs storing the stage RHS, adjoint steps."""
@@ -254,6 +275,14 @@ class Batch:
         ms = ctypes.c_float()
         self._check(self.L.cgfdm_batch_run_timed(self._h, int(nsteps), ctypes.byref(ms)))
         return ms.value
+
+    def autotune(self, trial_steps: int = 4):
+        """Tunes the batched launch's work decomposition (cgfdm_batch_autotune);
+        returns (kchunk, ctas, ms_per_step)."""
+        kc, ct, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        self._check(self.L.cgfdm_batch_autotune(self._h, int(trial_steps), ctypes.byref(kc), ctypes.byref(ct),
+                                                ctypes.byref(ms)))
+        return kc.value, ct.value, ms.value
 
     def close(self) -> None:
         if self._h:

@@ -76,24 +76,41 @@ int Batch::create(const std::vector<Session *> &sessions)
     BCU(cudaEventCreate(&ev_[0]));
     BCU(cudaEventCreate(&ev_[1]));
     const int n = (int)s.size();
+    for (int irk = 0; irk < 4; irk++) BCU(cudaMalloc(&desc_[irk], sizeof(CgStageDesc) * n));
+    BCU(cudaMalloc(&items_, sizeof(int) * (n + 1)));
+    BCU(cudaMalloc(&work_, sizeof(int) * 2));
+    BCU(cudaMemset(work_, 0, sizeof(int) * 2));
+    points = 0;
+    for (Session *x : s) points += (double)x->m.g.nx * x->m.g.ny * x->m.g.nz;
+    return build_tables();
+}
+
+// The sessions' stage descriptors and work-item prefix in device memory,
+// and the persistent CTA count of the batched launch.
+int Batch::build_tables()
+{
+    const int n = (int)s.size();
     std::vector<int> items(n + 1, 0);
     for (int i = 0; i < n; i++) items[i + 1] = items[i] + s[i]->stage_items();
     std::vector<CgStageDesc> d(n);
     for (int irk = 0; irk < 4; irk++) {
         for (int i = 0; i < n; i++) s[i]->stage_desc(irk, d[i]);
-        BCU(cudaMalloc(&desc_[irk], sizeof(CgStageDesc) * n));
         BCU(cudaMemcpy(desc_[irk], d.data(), sizeof(CgStageDesc) * n, cudaMemcpyHostToDevice));
     }
-    BCU(cudaMalloc(&items_, sizeof(int) * (n + 1)));
     BCU(cudaMemcpy(items_, items.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
-    BCU(cudaMalloc(&work_, sizeof(int) * 2));
-    BCU(cudaMemset(work_, 0, sizeof(int) * 2));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    grid_ctas_ = std::min(sms * cg_stage_ctas_per_sm(), items[n]);
-    points = 0;
-    for (Session *x : s) points += (double)x->m.g.nx * x->m.g.ny * x->m.g.nz;
+    const int full = sms * cg_stage_ctas_per_sm();
+    grid_ctas_ = std::min(want_ctas_ > 0 ? std::min(want_ctas_, full) : full, items[n]);
     return ST_OK;
+}
+
+void Batch::drop_graph()
+{
+    if (graph8_) cudaGraphExecDestroy(graph8_);
+    if (graph8_src_) cudaGraphDestroy(graph8_src_);
+    graph8_ = nullptr;
+    graph8_src_ = nullptr;
 }
 
 int Batch::remaining() const

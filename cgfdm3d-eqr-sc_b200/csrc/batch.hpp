@@ -16,6 +16,10 @@ public:
     int create(const std::vector<Session *> &sessions);
     int run(int nsteps, float *ms = nullptr);   // ms: device time of the steps, if given
     int remaining() const;                      // steps left to the shortest session's NT
+    // autotuner of the batched launch (csrc/autotune.cu): z planes per work
+    // item (every session) and persistent CTAs
+    int set_tiling(int kchunk, int ctas);
+    int autotune(int trial_steps, int *kchunk, int *ctas, float *ms_per_step);
 
     std::vector<Session *> s;
     int device = 0;
@@ -27,6 +31,9 @@ public:
 
 private:
     int launch_step(int step);
+    int build_tables();                         // descriptor table, item prefix, CTA count
+    void drop_graph();
+    int want_ctas_ = 0;                         // requested persistent CTAs (0: all resident)
     CgStageDesc *desc_[4] = {};
     int *items_ = nullptr;
     int *work_ = nullptr;

@@ -181,6 +181,32 @@ int cgfdm_gradient(cgfdm_session *s, const float *observed, long long obs_count,
     return s->s.gradient(observed, checkpoint_every, misfit, grad);
 }
 
+int cgfdm_autotune(cgfdm_session *s, int trial_steps, int *kchunk, int *ctas, float *ms_per_step)
+{
+    if (!s || trial_steps < 1) return CGFDM_E_ARG;
+    return s->s.autotune(trial_steps, kchunk, ctas, ms_per_step);
+}
+
+int cgfdm_set_tiling(cgfdm_session *s, int kchunk, int ctas)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.set_tiling(kchunk, ctas);
+}
+
+int cgfdm_get_tiling(const cgfdm_session *s, int *kchunk, int *ctas)
+{
+    if (!s) return CGFDM_E_ARG;
+    if (kchunk) *kchunk = s->s.kchunk();
+    if (ctas) *ctas = s->s.ctas();
+    return CGFDM_OK;
+}
+
+int cgfdm_batch_autotune(cgfdm_batch *b, int trial_steps, int *kchunk, int *ctas, float *ms_per_step)
+{
+    if (!b || trial_steps < 1) return CGFDM_E_ARG;
+    return b->b.autotune(trial_steps, kchunk, ctas, ms_per_step);
+}
+
 int cgfdm_gradient_profile(const cgfdm_session *s, float *ms3)
 {
     if (!s || !ms3) return CGFDM_E_ARG;

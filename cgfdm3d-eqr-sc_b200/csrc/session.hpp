@@ -47,6 +47,19 @@ public:
     int gradient(const float *obs, int ckpt_every, double *misfit, float *grad);
     int set_medium(const float *host_medium);       // [_nz_][_ny_][_nx_][3] (Vs, Vp, rho); back to step 0
     float grad_ms[3] = {0, 0, 0};                   // last gradient: forward, re-runs, adjoint steps (device ms)
+    // work decomposition of the CGFDM stage kernel (csrc/autotune.cu): z
+    // planes per work item and persistent CTAs; autotune times candidates
+    // on trial steps and keeps the fastest, the state restored after each
+    int set_tiling(int kchunk, int ctas);
+    int autotune(int trial_steps, int *kchunk, int *ctas, float *ms_per_step);
+    int kchunk() const { return kchunk_; }
+    int ctas() const { return grid_ctas_; }
+    // device copy of the state a trial step changes (wavefield, PML
+    // auxiliaries, PGV, displacement); the step counter goes back to `it`
+    size_t tune_bytes() const;
+    int tune_save(char *dev);
+    int tune_load(const char *dev);
+    int time_steps(int nsteps, float *ms);          // direct launches from `it`, `it` unchanged
 
     Model m;
     DevGrid g;

@@ -169,6 +169,22 @@ int cgfdm_adjoint_apply(cgfdm_session *s, int nsteps, float *state, long long co
  * stage right-hand sides, ms3[2] the adjoint steps. */
 int cgfdm_gradient_profile(const cgfdm_session *s, float *ms3);
 
+/* Autotuner of the CGFDM stage launch (no counterpart in src/).  The stage
+ * kernel's persistent CTAs take work items of 32 x 4 columns by `kchunk`
+ * planes; cgfdm_autotune times candidate pencil lengths and CTA counts on
+ * `trial_steps` steps each (from a device copy of the state, which is put
+ * back: tuning does not advance the run), keeps the fastest and returns it
+ * with its device time per step.  Results are bit-identical for every
+ * tiling.  cgfdm_set_tiling / cgfdm_get_tiling set and read it directly
+ * (ctas is clamped to the resident maximum and the work items).
+ * cgfdm_batch_autotune does the same for a batch's shared launch, trying
+ * one pencil length for all its sessions against their own default ones
+ * (*kchunk = 0 when those are kept).  A candidate replaces the current
+ * decomposition only when faster by more than 1 %. */
+int cgfdm_autotune(cgfdm_session *s, int trial_steps, int *kchunk, int *ctas, float *ms_per_step);
+int cgfdm_set_tiling(cgfdm_session *s, int kchunk, int ctas);
+int cgfdm_get_tiling(const cgfdm_session *s, int *kchunk, int *ctas);
+
 /* Batches: several CGFDM sessions -- independent shots or media of uneven
  * grid sizes -- advanced together, every RK stage of all of them in one
  * persistent launch of the fused stage kernel, eight steps per replay of a
@@ -184,6 +200,7 @@ int cgfdm_batch_run(cgfdm_batch *b, int nsteps);
 /* As cgfdm_batch_run, returning the device time of the steps in ms. */
 int cgfdm_batch_run_timed(cgfdm_batch *b, int nsteps, float *ms);
 int cgfdm_batch_destroy(cgfdm_batch *b);
+int cgfdm_batch_autotune(cgfdm_batch *b, int trial_steps, int *kchunk, int *ctas, float *ms_per_step);
 /* Last failure of b, or of the last failed cgfdm_batch_create in this
  * thread when b is NULL. */
 const char *cgfdm_batch_last_error(const cgfdm_batch *b);
