@@ -325,6 +325,26 @@ def bench_batch(args, world, rank, local_rank):
 ADJ_BYTES_PER_POINT_STAGE = 4 * (9 + 9 + 9 + 12 + 18 + 9 + 6)
 
 
+def shots_of_rank(items, world, rank):
+    """The shots a rank computes: every world-th one from its rank on
+    (independent units; no exchange while they run)."""
+    return list(items)[rank::world]
+
+
+def sum_over_ranks(array, dist, device):
+    """Sum of a gradient volume over all ranks (the array itself without a
+    process group): the multi-shot gradient's one collective, an all-reduce
+    of the three gradient volumes after every rank has finished its shots."""
+    import numpy as np
+    import torch
+
+    if not dist:
+        return array
+    t = torch.from_numpy(np.ascontiguousarray(array, np.float32)).to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.cpu().numpy()
+
+
 def bench_adjoint(args, world, rank, local_rank):
     """``--workload adjoint[_STEPS[_NXxNYxNZ]]``: the misfit gradient with respect to
     Vp, Vs and rho (cgfdm_gradient) on the 192 x 192 x 128 layered model
@@ -336,8 +356,10 @@ def bench_adjoint(args, world, rank, local_rank):
     medium (no ball) and summed over the shots.  Reports gradient throughput
     (shots x points x NT / seconds) and the adjoint/forward cost: wall time
     of the gradient over that of a forward run of the same shot (both from
-    step 0, medium set, traces read back).  One GPU; --steps/--warmup do
-    not apply (a shot is one unit)."""
+    step 0, medium set, traces read back).  With N ranks (torchrun) every
+    rank takes every N-th shot; the gradient volumes are then summed with one
+    all-reduce (NCCL) and times are the slowest rank's.  --steps/--warmup
+    do not apply (a shot is one unit)."""
     import numpy as np
     import torch
     from cgfdm import Session, configs
@@ -347,14 +369,23 @@ def bench_adjoint(args, world, rank, local_rank):
     NX, NY, NZ = (int(v) for v in parts[2].split("x")) if len(parts) > 2 else (192, 192, 128)
     DH = 100.0
     n_shots = 4 if len(parts) <= 2 else 1
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=900))
     root = os.path.join(WORK, f"adjoint_{NT}_{NX}x{NY}x{NZ}_{n_shots}")
     marker = os.path.join(root, ".done")
-    if not os.path.exists(marker):
+    if rank == 0 and not os.path.exists(marker):
         if os.path.exists(root):
             shutil.rmtree(root)
         configs.adjoint_shots(root, steps=NT, NX=NX, NY=NY, NZ=NZ, n_shots=n_shots)
         open(marker, "w").close()
-    dirs = sorted(os.path.join(root, d) for d in os.listdir(root) if d.startswith("shot_"))
+    if dist:
+        dist.barrier()
+    all_dirs = sorted(os.path.join(root, d) for d in os.listdir(root) if d.startswith("shot_"))
+    dirs = shots_of_rank(all_dirs, world, rank)
     true = configs.adjoint_layers(NX, NY, NZ, DH, True)
     start = configs.adjoint_layers(NX, NY, NZ, DH, False)
     K = args.checkpoint_every
@@ -363,6 +394,7 @@ def bench_adjoint(args, world, rank, local_rank):
     phases = np.zeros(3)
     grad_sum = None
     J_sum = 0.0
+    dev_gb = 0.0
     with ClockSampler(local_rank) as clk:
         for d in dirs:
             s = Session(d, options=opts, device=local_rank)
@@ -387,12 +419,21 @@ def bench_adjoint(args, world, rank, local_rank):
             phases += np.array(s.gradient_profile())
             J_sum += J
             grad_sum = g if grad_sum is None else grad_sum + g
-            pts = info.nx * info.ny * info.nz
             dev_gb = info.device_bytes / 1e9
             s.close()
-    n = len(dirs)
-    steps_adj = n * NT
+    # one collective: the gradient volumes summed over the ranks' shots;
+    # times are the slowest rank's
+    dev = f"cuda:{local_rank}"
+    if dist:
+        dist.barrier()
+    grad_sum = sum_over_ranks(grad_sum if grad_sum is not None else np.zeros((3, NZ, NY, NX), np.float32), dist, dev)
+    J_sum = float(sum_over_ranks(np.array([J_sum], np.float32), dist, dev)[0])
+    t_fwd = max_over_ranks(t_fwd, dist, dev)
+    t_grad = max_over_ranks(t_grad, dist, dev)
+    n = len(all_dirs)
+    steps_adj = max(1, len(dirs)) * NT
     adj_ms_step = phases[2] / steps_adj
+    pts = NX * NY * NZ
     algo = ADJ_BYTES_PER_POINT_STAGE * 4 * pts
     achieved = algo / (adj_ms_step * 1e-3) / 1e9
     hbm_peak, peak_kind = peaks()
@@ -402,7 +443,7 @@ def bench_adjoint(args, world, rank, local_rank):
     inside = np.sqrt((ii - (NX - 1) / 2) ** 2 + (jj - (NY - 1) / 2) ** 2 + (kk - zc) ** 2) * DH < 2000.0
     gvs = grad_sum[1]
     line = {
-        "metric": METRIC, "value": n * pts * NT / t_grad / 1e6, "unit": METRIC, "n_gpus": 1, "steps": NT,
+        "metric": METRIC, "value": n * pts * NT / t_grad / 1e6, "unit": METRIC, "n_gpus": world, "steps": NT,
         "warmup": 0, "ms_per_step": t_grad * 1e3 / steps_adj, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "scheme": "CGFDM",
         "config": {"workload": f"adjoint: CGFDM misfit gradient w.r.t. Vp, Vs, rho, {NX}x{NY}x{NZ}, DH=100 m, "
@@ -410,7 +451,7 @@ def bench_adjoint(args, world, rank, local_rank):
                                f"(2 Hz Ricker point sources), 64 surface stations, checkpoint every {K} steps, FP32",
                    "points": pts, "shots": n, "NT": NT, "checkpoint_every": K,
                    "l2": "inputs larger than L2 (%.1f GB resident per session)" % dev_gb,
-                   "parallelism": "replicas x1"},
+                   "parallelism": f"shots over {world} rank(s), gradient volumes all-reduced"},
         "adjoint_over_forward": t_grad / t_fwd,
         "forward_s": t_fwd, "gradient_s": t_grad,
         "phases_ms": {"forward_with_checkpoints": phases[0], "segment_reruns_storing_rhs": phases[1],
@@ -431,6 +472,9 @@ def bench_adjoint(args, world, rank, local_rank):
     }
     if rank == 0:
         print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
