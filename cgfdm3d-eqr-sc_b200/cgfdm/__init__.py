@@ -39,6 +39,7 @@ class Info(ctypes.Structure):
         ("kernel_launches", ctypes.c_longlong),
         ("algo_bytes_per_step", ctypes.c_double),
         ("stage_kernels_per_step", ctypes.c_int),
+        ("pgv_fields", ctypes.c_int),
     ]
 
 
@@ -172,7 +173,7 @@ class Session:
 
     def pgv(self) -> np.ndarray:
         i = self.info
-        out = np.zeros((i.ny, i.nx, 2), np.float32)
+        out = np.zeros((i.ny, i.nx, i.pgv_fields), np.float32)
         self._check(self.L.cgfdm_get_pgv(self._h, _fptr(out), out.size))
         return out
 

@@ -64,6 +64,7 @@ size_t Session::tune_bytes() const
 {
     size_t b = state_bytes() + sizeof(float) * (size_t)m.g.nx * m.g.ny * 2;
     if (dis_) b += sizeof(float) * (size_t)g.fstride * 3;
+    if (pga_) b += sizeof(float) * (size_t)m.g.nx * m.g.ny * 2;
     return b;
 }
 
@@ -75,6 +76,8 @@ int Session::tune_save(char *dev)
     CU(cudaMemcpyAsync(dev + off, pgv_, pb, cudaMemcpyDeviceToDevice, stream));
     off += pb;
     if (dis_) CU(cudaMemcpyAsync(dev + off, dis_, sizeof(float) * g.fstride * 3, cudaMemcpyDeviceToDevice, stream));
+    if (dis_) off += sizeof(float) * g.fstride * 3;
+    if (pga_) CU(cudaMemcpyAsync(dev + off, pga_, pb, cudaMemcpyDeviceToDevice, stream));
     return ST_OK;
 }
 
@@ -86,6 +89,8 @@ int Session::tune_load(const char *dev)
     CU(cudaMemcpyAsync(pgv_, dev + off, pb, cudaMemcpyDeviceToDevice, stream));
     off += pb;
     if (dis_) CU(cudaMemcpyAsync(dis_, dev + off, sizeof(float) * g.fstride * 3, cudaMemcpyDeviceToDevice, stream));
+    if (dis_) off += sizeof(float) * g.fstride * 3;
+    if (pga_) CU(cudaMemcpyAsync(pga_, dev + off, pb, cudaMemcpyDeviceToDevice, stream));
     CU(cudaMemcpyAsync(it_dev_, &it, sizeof(int), cudaMemcpyHostToDevice, stream));
     return ST_OK;
 }

@@ -130,6 +130,8 @@ int Batch::launch_step(int step)
         FB1 = -FB1, FB2 = -FB2, FB3 = -FB3;
     }
     for (Session *x : s)
+        if (int st = x->launch_pga_on(stream)) return st;
+    for (Session *x : s)
         if (int st = x->launch_stations_on(stream)) return st;
     return ST_OK;
 }

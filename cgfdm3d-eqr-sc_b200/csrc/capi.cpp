@@ -85,6 +85,7 @@ int cgfdm_info_get(const cgfdm_session *s, cgfdm_info *o)
     o->kernel_launches = S.kernel_launches;
     o->algo_bytes_per_step = S.algo_bytes_per_step();
     o->stage_kernels_per_step = S.m.p.scheme == 0 ? 4 : 3;
+    o->pgv_fields = S.pgv_fields();
     return CGFDM_OK;
 }
 
@@ -122,7 +123,7 @@ int cgfdm_get_cjm(const cgfdm_session *s, float *out, long long count, int *nfie
 int cgfdm_get_pgv(const cgfdm_session *s, float *out, long long count)
 {
     if (!s || !out) return CGFDM_E_ARG;
-    if (count < (long long)s->s.m.g.nx * s->s.m.g.ny * 2) return CGFDM_E_ARG;
+    if (count < (long long)s->s.m.g.nx * s->s.m.g.ny * s->s.pgv_fields()) return CGFDM_E_ARG;
     return s->s.get_pgv(out);
 }
 

@@ -143,6 +143,7 @@ int Session::set_medium(const float *host)
             CU(cudaMemsetAsync(face_[fc].T, 0, b, stream));
         }
     CU(cudaMemsetAsync(pgv_, 0, sizeof(float) * m.g.nx * m.g.ny * 2, stream));
+    if (pga_) CU(cudaMemsetAsync(pga_, 0, sizeof(float) * m.g.nx * m.g.ny * 2, stream));
     if (dis_) CU(cudaMemsetAsync(dis_, 0, sizeof(float) * g.fstride * 3, stream));
     if (st_out_) CU(cudaMemsetAsync(st_out_, 0, sizeof(float) * nst * std::max(m.NT, 1) * 9, stream));
     CU(cudaMemsetAsync(it_dev_, 0, sizeof(int), stream));

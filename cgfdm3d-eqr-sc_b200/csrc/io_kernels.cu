@@ -203,6 +203,45 @@ __global__ void k_from_aos(const float *__restrict__ in, int nf, DevGrid g, floa
     for (int f = 0; f < nf; f++) W[f * g.fstride + q] = in[n * nf + f];
 }
 
+// Peak ground acceleration as the reference's SOLVE_PGA build computes it
+// (src/PGV.cpp:140-171 with src/propagate.cpp:26-58,188-192): after every
+// step with it % 10 == 0, A = (V - V_pre) / (10 DT) for the surface
+// velocity V, maxima of |(Ax, Ay)| and |A| kept.  The reference's V_pre copy
+// (stroage_W_pre_gpu) moves W_pre[n] = W[n] for the first _nx_ _ny_ _nz_
+// floats of the nine-field array only, which never reaches a surface
+// point's velocity (at 9 * index + c), so V_pre reads zero there: the value
+// is |V| / (10 DT) at every tenth step, kept here bit for bit.
+__global__ void k_pga(const float *__restrict__ W, const float *__restrict__ cjm, DevGrid g, const int *it_dev,
+                      float DT, int scheme, float *pga)
+{
+    if (*it_dev % 10 != 0) return;
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x, jj = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ii >= g.nx || jj >= g.ny) return;
+    const long long F = g.fstride;
+    const long long q = g.at(ii + CGFDM_HALO, jj + CGFDM_HALO, g.nzp - CGFDM_HALO - 1);
+    float V[3];
+    for (int c = 0; c < 3; c++) {
+        V[c] = W[c * F + q];
+        if (scheme == 1) V[c] = __fmul_rn(V[c], __fmul_rn(cjm[C_BUOY * F + q], 1.0f));
+    }
+    const float d10 = __fmul_rn(10.0f, DT);
+    float A[3];
+    for (int c = 0; c < 3; c++) A[c] = __fdiv_rn(__fsub_rn(V[c], 0.0f), d10);
+    const float h2 = __fadd_rn(__fmul_rn(A[0], A[0]), __fmul_rn(A[1], A[1]));
+    const float Ah = __fsqrt_rn(h2), Am = __fsqrt_rn(__fadd_rn(h2, __fmul_rn(A[2], A[2])));
+    float *p = pga + ((long long)jj * g.nx + ii) * 2;
+    if (p[0] < Ah) p[0] = Ah;
+    if (p[1] < Am) p[1] = Am;
+}
+
+cudaError_t launch_pga(const float *W, const float *cjm, DevGrid g, const int *it_dev, float DT, int scheme,
+                       float *pga, cudaStream_t st)
+{
+    dim3 b(32, 8), gr((g.nx + 31) / 32, (g.ny + 7) / 8);
+    k_pga<<<gr, b, 0, st>>>(W, cjm, g, it_dev, DT, scheme, pga);
+    return cudaGetLastError();
+}
+
 // One plane of one field for the snapshot files (pack_iodata_x/y/z,
 // src/data_io.cpp:96-250): axis 0 is the plane i = idx laid out [nz][ny],
 // axis 1 the plane j = idx as [nz][nx], axis 2 the plane k = idx as [ny][nx].

@@ -198,6 +198,10 @@ cudaError_t launch_point(float *W, float *Wb, float *Wc, const float *cjm, DevGr
 // Records 9 components per station at step *it_dev, then advances *it_dev.
 cudaError_t launch_stations(const float *W, const float *cjm, DevGrid g, const int *st_idx, int nst, int NT,
                             float *out, int *it_dev, int scheme, cudaStream_t st);
+// Peak ground acceleration [ny][nx][2] (PGAh, PGA) after a step whose index
+// *it_dev is a multiple of 10 (the reference's SOLVE_PGA).
+cudaError_t launch_pga(const float *W, const float *cjm, DevGrid g, const int *it_dev, float DT, int scheme,
+                       float *pga, cudaStream_t st);
 // One slice of field `comp` of W for the snapshot files: axis 0/1/2 = the
 // plane i/j/k = idx, in the reference's [nz][ny] / [nz][nx] / [ny][nx]
 // order; SCFDM (scheme 1, cjm given) converts momentum to velocity.

@@ -111,6 +111,7 @@ int read_params(const std::string &path, Params &p, std::string &err)
     GETI("PML", pml);
     GETI("EXP_DECAY", exp_decay);
     GETI("SOLVE_DISPLACEMENT", solve_displacement);
+    GETI("SOLVE_PGA", solve_pga);
     if ((it = root.get("metricPrecision")) && it->kind == JsonValue::String) p.metric_fp64 = it->str == "fp64";
     GETS("storage", storage);
     GETS("terrainFile", terrainFile);
@@ -653,6 +654,7 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
         if ((it = o.get("PML"))) m.p.pml = it->as_int();
         if ((it = o.get("EXP_DECAY"))) m.p.exp_decay = it->as_int();
         if ((it = o.get("SOLVE_DISPLACEMENT"))) m.p.solve_displacement = it->as_int();
+        if ((it = o.get("SOLVE_PGA"))) m.p.solve_pga = it->as_int();
         if ((it = o.get("metricPrecision")) && it->kind == JsonValue::String) m.p.metric_fp64 = it->str == "fp64";
         if ((it = o.get("storage")) && it->kind == JsonValue::String) m.p.storage = it->str;
         if ((it = o.get("adjointKernel")) && it->kind == JsonValue::String) m.p.adj_fused = it->str == "fused";

@@ -66,6 +66,7 @@ struct Params {
     int pml = 1;                     // PML on 5 faces (CGFDM default build)
     int exp_decay = 0;               // exponential sponge (SCFDM default build)
     int solve_displacement = 0;      // SOLVE_DISPLACEMENT
+    int solve_pga = 0;               // SOLVE_PGA: peak ground acceleration beside PGV
     int metric_fp64 = 0;             // "metricPrecision": "fp64" -> metrics computed in FP64
     int adj_fused = 0;               // options "adjointKernel": "two-pass" (default) | "fused"
     int adj_store_max = 0;           // options "adjointStoreSegments": cap on segments kept from the forward (0: memory decides)

@@ -251,6 +251,7 @@ int Session::setup_device()
 
     // PGV, displacement, stations, step counter
     ALLOC(pgv_, float, (long long)G.nx * G.ny * 2);
+    if (m.p.solve_pga) ALLOC(pga_, float, (long long)G.nx * G.ny * 2);
     if (m.p.solve_displacement) ALLOC(dis_, float, F * 3);
     nst = (int)m.stations.size() / 3;
     if (nst > 0) {
@@ -437,6 +438,7 @@ int Session::launch_step(int step, bool timed_stages)
         CU(launch_sc_surface(A, cjm_, g, decay_, SC_DECAY_LAYERS, pgv_, dis_, DT, stream));
         kernel_launches += 10;
     }
+    if (int st = launch_pga_on(stream)) return st;
     if (int st = launch_stations_on(stream)) return st;
     kernel_launches += 1 + (fault_.npts > 0) + (point_.kind != 0 && point_.inside);
     return ST_OK;
@@ -448,6 +450,15 @@ int Session::launch_sources_on(cudaStream_t st)
     const float DT = (float)m.p.DT;
     CU(launch_point(W_[0], W_[1], W_[2], cjm_, g, point_, it_dev_, DT, m.g.DH, m.p.scheme, st));
     CU(launch_sources(W_[0], cjm_, g, fault_, point_, it_dev_, DT, m.g.DH, m.p.scheme, st));
+    return ST_OK;
+}
+
+// Peak ground acceleration of the step just completed (SOLVE_PGA).
+int Session::launch_pga_on(cudaStream_t st)
+{
+    if (!pga_) return ST_OK;
+    CU(launch_pga(W_[0], cjm_, g, it_dev_, (float)m.p.DT, m.p.scheme, pga_, st));
+    kernel_launches += 1;
     return ST_OK;
 }
 
@@ -639,10 +650,23 @@ int Session::get_stations(float *host) const
 
 int Session::get_pgv(float *host) const
 {
-    cudaError_t e = cudaMemcpyAsync(host, pgv_, sizeof(float) * (size_t)m.g.nx * m.g.ny * 2, cudaMemcpyDeviceToHost,
-                                    stream);
+    const size_t n = (size_t)m.g.nx * m.g.ny;
+    if (!pga_) {
+        cudaError_t e = cudaMemcpyAsync(host, pgv_, sizeof(float) * n * 2, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        return e == cudaSuccess ? ST_OK : ST_CUDA;
+    }
+    // the reference's PGVSIZE = 4 record: PGVh, PGV, PGAh, PGA (src/PGV.cpp:140-171)
+    std::vector<float> v(n * 2), a(n * 2);
+    cudaError_t e = cudaMemcpyAsync(v.data(), pgv_, sizeof(float) * n * 2, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(a.data(), pga_, sizeof(float) * n * 2, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    return e == cudaSuccess ? ST_OK : ST_CUDA;
+    if (e != cudaSuccess) return ST_CUDA;
+    for (size_t p = 0; p < n; p++) {
+        host[p * 4 + 0] = v[p * 2], host[p * 4 + 1] = v[p * 2 + 1];
+        host[p * 4 + 2] = a[p * 2], host[p * 4 + 3] = a[p * 2 + 1];
+    }
+    return ST_OK;
 }
 
 // Output files of one rank in the reference's formats: station traces
@@ -772,7 +796,7 @@ int Session::write_outputs() const
         std::fclose(fp);
     }
     {
-        std::vector<float> p((size_t)m.g.nx * m.g.ny * 2);
+        std::vector<float> p((size_t)m.g.nx * m.g.ny * pgv_fields());
         int st = get_pgv(p.data());
         if (st) return st;
         std::string path = out + "/PGV_Z_mpi_0_0_0.bin";
@@ -803,6 +827,7 @@ void Session::ckpt_parts(std::vector<std::pair<void *, size_t>> &parts) const
     if (m.p.scheme == SCHEME_CGFDM && m.p.pml)
         for (int fc = 0; fc < 5; fc++) parts.push_back({face_[fc].A, sizeof(float) * face_[fc].count * 9});
     parts.push_back({pgv_, sizeof(float) * (size_t)m.g.nx * m.g.ny * 2});
+    if (pga_) parts.push_back({pga_, sizeof(float) * (size_t)m.g.nx * m.g.ny * 2});
     if (dis_) parts.push_back({dis_, sizeof(float) * F * 3});
     if (nst > 0) parts.push_back({st_out_, sizeof(float) * (size_t)nst * std::max(m.NT, 1) * 9});
 }

@@ -35,7 +35,8 @@ public:
     int get_wavefield(float *host_aos) const;       // [_nz_][_ny_][_nx_][9]
     int get_cjm(float *host_aos, int *nfield) const;  // [_nz_][_ny_][_nx_][nfield]
     int get_stations(float *host) const;            // [nst][NT][9]
-    int get_pgv(float *host) const;                 // [ny][nx][2]
+    int get_pgv(float *host) const;                 // [ny][nx][pgv_fields()]
+    int pgv_fields() const { return pga_ ? 4 : 2; } // PGVh, PGV (+ PGAh, PGA)
     int write_outputs() const;
     int sync() const;
     size_t checkpoint_bytes() const;
@@ -87,7 +88,7 @@ private:
     float *cjm_ = nullptr, *rdz_ = nullptr;
     float *pml_[9] = {};
     PmlFace face_[5] = {};
-    float *pgv_ = nullptr, *dis_ = nullptr;
+    float *pgv_ = nullptr, *dis_ = nullptr, *pga_ = nullptr;
     int *st_idx_ = nullptr;
     float *st_out_ = nullptr;
     int *it_dev_ = nullptr;
@@ -114,6 +115,7 @@ public:
     int stage_items() const;
     int launch_sources_on(cudaStream_t st);
     int launch_stations_on(cudaStream_t st);
+    int launch_pga_on(cudaStream_t st);
     int check_errors() { return check_device_error(); }
     bool snapshots_on() const;
 

@@ -55,6 +55,7 @@ typedef struct cgfdm_info {
     long long kernel_launches; /* kernels of this library launched so far */
     double algo_bytes_per_step; /* bytes a step must move at minimum (see cgfdm_profile_stages) */
     int stage_kernels_per_step; /* fused stage launches per step (4 for RK4, 3 for TVD-RK3) */
+    int pgv_fields;      /* floats per point of the PGV record: 2, or 4 with SOLVE_PGA */
 } cgfdm_info;
 
 /* Builds the model of a run directory on GPU `device`: reads params.json
@@ -63,7 +64,7 @@ typedef struct cgfdm_info {
  * Replaces src/run.cpp:28-116 up to the call of propagate().
  * `options_json` (may be NULL) overrides run-time switches with the
  * reference's flag names: {"scheme": "CGFDM"|"SCFDM", "PML": 0|1,
- * "EXP_DECAY": 0|1, "SOLVE_DISPLACEMENT": 0|1, "metricPrecision":
+ * "EXP_DECAY": 0|1, "SOLVE_DISPLACEMENT": 0|1, "SOLVE_PGA": 0|1, "metricPrecision":
  * "fp32"|"fp64", "OUT": "..."}. */
 int cgfdm_create(const char *run_dir, const char *options_json, int device, cgfdm_session **out);
 
@@ -98,7 +99,10 @@ int cgfdm_get_wavefield(const cgfdm_session *s, float *out, long long count);
  * with nfield 13 (CGFDM) or 19 (SCFDM); with out == NULL only *nfield is set. */
 int cgfdm_get_cjm(const cgfdm_session *s, float *out, long long count, int *nfield);
 
-/* Peak ground velocity at the surface, [ny][nx][2] (PGVh, PGV) (src/PGV.cpp:61-175). */
+/* Peak ground velocity at the surface, [ny][nx][2] (PGVh, PGV) (src/PGV.cpp:61-175);
+ * with SOLVE_PGA [ny][nx][4] (PGVh, PGV, PGAh, PGA), the peak acceleration as the
+ * reference's SOLVE_PGA build evaluates it (|V| / (10 DT) at every tenth step:
+ * its previous-velocity copy never reaches the surface points). */
 int cgfdm_get_pgv(const cgfdm_session *s, float *out, long long count);
 
 /* Writes OUT/station_mpi_0_0_0.bin and OUT/PGV_Z_mpi_0_0_0.bin in the

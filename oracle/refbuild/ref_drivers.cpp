@@ -41,6 +41,7 @@ void compare_pgv(float *pgv, FLOAT *W, int nx, int ny, int nz, float DT, int it
 
 /* The reference's kernel takes (pgv, W, nx, ny, nz, DT, it [, CJM]); DT and
  * it only matter under SOLVE_PGA (src/PGV.cpp:61-175). */
+#ifndef SOLVE_PGA
 void compare_pgv(float *pgv, FLOAT *W, int nx, int ny, int nz)
 {
     compare_pgv(pgv, W, nx, ny, nz, 0.0f, 0
@@ -50,6 +51,40 @@ void compare_pgv(float *pgv, FLOAT *W, int nx, int ny, int nz)
 #endif
     );
 }
+#else
+/* Under SOLVE_PGA the kernel also takes W_pre; the shipped CPU branch of
+ * comparePGV (src/PGV.cpp:187-229) passes five arguments, so the driver
+ * below replaces it (the build renames the shipped one). */
+void compare_pgv(float *pgv, FLOAT *W, int nx, int ny, int nz, float DT, int it
+#ifdef SCFDM
+                 , FLOAT *CJM
+#endif
+                 , FLOAT *W_pre);
+void compare_pgv(float *pgv, FLOAT *W, int nx, int ny, int nz) { (void)pgv, (void)W, (void)nx, (void)ny, (void)nz; }
+
+void comparePGV(GRID grid, MPI_COORDINATE thisMPICoord, FLOAT *W, float *pgv, float DT, int it
+#ifdef SCFDM
+                , FLOAT *CJM
+#endif
+                , FLOAT *W_pre)
+{
+    (void)thisMPICoord;
+    compare_pgv(pgv, W, grid.nx, grid.ny, grid.nz, DT, it
+#ifdef SCFDM
+                , CJM
+#endif
+                , W_pre);
+}
+
+/* src/propagate.cpp:26-58 (cut from the build): one GPU thread per point
+ * index copies W_pre[index] = W[index] over _nx_ * _ny_ * _nz_ indices --
+ * the first ninth of the nine-field array -- on the CPU the same loop. */
+void storage_W_pre(GRID grid, WAVE wave)
+{
+    const long long n = (long long)grid._nx_ * grid._ny_ * grid._nz_;
+    for (long long index = 0; index < n; index++) wave.W_pre[index] = wave.W[index];
+}
+#endif
 
 /* ---------------------------------------------------------- point sources */
 void load_smooth_source_ricker(SOURCE S, FLOAT *h_W, int _nx_, int _ny_, int _nz_,

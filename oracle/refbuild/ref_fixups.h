@@ -23,6 +23,12 @@ static inline int cudaDeviceSynchronize(void) { return 0; }
 /* PGV.cpp:224 calls compare_pgv with five arguments on the CPU path. */
 void compare_pgv(float *pgv, FLOAT *W, int nx, int ny, int nz);
 
+#ifdef SOLVE_PGA
+/* defined in the SOLVE_PGA block that the build cuts from propagate.cpp
+ * (GPU-only code); ref_drivers.cpp has the CPU copy. */
+void storage_W_pre(GRID grid, WAVE wave);
+#endif
+
 /* singleSource.cpp:210,355 call an undefined CPU helper. */
 void load_smooth_source(SOURCE S, FLOAT *h_W, int _nx_, int _ny_, int _nz_,
                         FLOAT *CJM, int it, int irk, float DT, float DH, int nGauss, float rickerfc);

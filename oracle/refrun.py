@@ -24,16 +24,17 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
 
-def ref_binary(scheme: str = "CGFDM", displacement: bool = False) -> str:
+def ref_binary(scheme: str = "CGFDM", displacement: bool = False, pga: bool = False) -> str:
     """The build of one scheme; ``displacement`` picks the one compiled with
     SOLVE_DISPLACEMENT (src/propagate.cpp:101-104, 264-266, 305-307), which
-    also writes FreeSurfUx/Uy/Uz with the free-surface snapshots."""
+    also writes FreeSurfUx/Uy/Uz with the free-surface snapshots; ``pga``
+    the one compiled with SOLVE_PGA (a four-field PGV file, src/PGV.cpp:61-175)."""
     name = "cgfdm_ref" if scheme.upper() == "CGFDM" else "scfdm_ref"
-    return os.path.join(REF_DIR, name + ("_dis" if displacement else ""))
+    return os.path.join(REF_DIR, name + ("_dis" if displacement else "") + ("_pga" if pga else ""))
 
 
-def available(scheme: str = "CGFDM", displacement: bool = False) -> bool:
-    return os.access(ref_binary(scheme, displacement), os.X_OK)
+def available(scheme: str = "CGFDM", displacement: bool = False, pga: bool = False) -> bool:
+    return os.access(ref_binary(scheme, displacement, pga), os.X_OK)
 
 
 def _params(run_dir: str) -> dict:
@@ -43,13 +44,13 @@ def _params(run_dir: str) -> dict:
 
 
 def run(run_dir: str, scheme: str = "CGFDM", timeout: float = 3600.0, log: Optional[str] = None,
-        displacement: bool = False) -> float:
+        displacement: bool = False, pga: bool = False) -> float:
     """Runs the reference binary in run_dir; returns wall seconds."""
     out = os.path.join(run_dir, _params(run_dir).get("out", "./output"))
     os.makedirs(out, exist_ok=True)
     t0 = time.perf_counter()
     with open(log or os.path.join(run_dir, "ref.log"), "w") as lf:
-        subprocess.run([ref_binary(scheme, displacement)], cwd=run_dir, stdout=lf, stderr=subprocess.STDOUT, check=True,
+        subprocess.run([ref_binary(scheme, displacement, pga)], cwd=run_dir, stdout=lf, stderr=subprocess.STDOUT, check=True,
                        timeout=timeout)
     return time.perf_counter() - t0
 
@@ -87,7 +88,8 @@ def read_outputs(run_dir: str, scheme: str = "CGFDM") -> Dict[str, np.ndarray]:
         res["CJM"] = np.fromfile(cp, np.float32).reshape(nzp, nyp, nxp, nf)
     pg = os.path.join(out, "PGV_Z_mpi_0_0_0.bin")
     if os.path.exists(pg):
-        res["PGV"] = np.fromfile(pg, np.float32).reshape(NY, NX, 2)
+        raw = np.fromfile(pg, np.float32)
+        res["PGV"] = raw.reshape(NY, NX, raw.size // (NY * NX))   # 2 fields, 4 with SOLVE_PGA
     return res
 
 
