@@ -66,6 +66,8 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
     L.cgfdm_info_get.argtypes = [vp, ctypes.POINTER(Info)]
     L.cgfdm_profile_stages.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     fp = ctypes.POINTER(ctypes.c_float)
+    L.cgfdm_model_medium.argtypes = [ctypes.c_char_p, ctypes.c_char_p, fp, ctypes.c_longlong,
+                                     ctypes.POINTER(ctypes.c_int)]
     L.cgfdm_get_stations.argtypes = [vp, fp, ctypes.c_longlong]
     L.cgfdm_get_wavefield.argtypes = [vp, fp, ctypes.c_longlong]
     L.cgfdm_get_cjm.argtypes = [vp, fp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)]
@@ -101,6 +103,22 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
 
 def _fptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def model_medium(run_dir: str, options: Optional[str] = None, flavor: str = "fast") -> np.ndarray:
+    """The medium a run directory describes, [nzp][nyp][nxp][3] (Vs, Vp, rho),
+    built on the host without a GPU (cgfdm_model_medium)."""
+    L = load(flavor)
+    dims = (ctypes.c_int * 3)()
+    o = options.encode() if options else None
+    rc = L.cgfdm_model_medium(run_dir.encode(), o, None, 0, dims)
+    if rc:
+        raise CgfdmError(rc, L.cgfdm_last_error(None).decode())
+    out = np.zeros((dims[0], dims[1], dims[2], 3), np.float32)
+    rc = L.cgfdm_model_medium(run_dir.encode(), o, _fptr(out), out.size, dims)
+    if rc:
+        raise CgfdmError(rc, L.cgfdm_last_error(None).decode())
+    return out
 
 
 class Session:

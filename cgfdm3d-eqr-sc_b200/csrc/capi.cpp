@@ -51,6 +51,29 @@ int cgfdm_create(const char *run_dir, const char *options_json, int device, cgfd
     return CGFDM_OK;
 }
 
+int cgfdm_model_medium(const char *run_dir, const char *options_json, float *out, long long count, int *dims)
+{
+    if (!run_dir) {
+        g_create_error = "run_dir must not be NULL";
+        return CGFDM_E_ARG;
+    }
+    cgfdm::Model m;
+    std::string err;
+    int st = cgfdm::build_model(run_dir, options_json ? options_json : "", m, err);
+    if (st) {
+        g_create_error = err;
+        return st;
+    }
+    if (dims) dims[0] = m.g._nz_, dims[1] = m.g._ny_, dims[2] = m.g._nx_;
+    if (!out) return CGFDM_OK;
+    if (count < (long long)m.medium.size()) {
+        g_create_error = "output array too small for the medium";
+        return CGFDM_E_ARG;
+    }
+    std::memcpy(out, m.medium.data(), sizeof(float) * m.medium.size());
+    return CGFDM_OK;
+}
+
 int cgfdm_run(cgfdm_session *s, int nsteps)
 {
     if (!s) return CGFDM_E_ARG;

@@ -563,7 +563,9 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         for (int f = 0; f < 9; f++) a.Wout[f * F + q] = wout[f];
 
         if (a.irk == 3) {
-            if (a.dis)
+            // displacement: only the surface layer is ever read (the FreeSurfU
+            // files, src/data_io.cpp:619-633), so only it is integrated
+            if (a.dis && k == _nz - 1)
                 for (int c = 0; c < 3; c++) a.dis[c * F + q] = a.dis[c * F + q] + wout[c] * DT;
             if (a.pgv && k == _nz - 1) {
                 long long pp = (long long)(i - CGFDM_HALO) + (long long)(j - CGFDM_HALO) * g.nx;

@@ -361,10 +361,6 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
         err = "the gradient takes point sources (a finite-fault table is scaled by mu)";
         return ST_OPTIONS;
     }
-    if (m.p.solve_displacement || snapshots_on()) {
-        err = "the gradient runs without displacement and snapshot output";
-        return ST_OPTIONS;
-    }
     if (int st = adj_prepare()) return st;
     CU(launch_surface_derivs(cjm_, g, adj_.drdz, stream));  // of the current medium
     const int NT = m.NT;
@@ -447,21 +443,27 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
     auto vdptr = [&](int slot, int t, int irk) {
         return vdstore + (size_t)g.plane * 6 * (((size_t)slot * K + t) * 4 + irk);
     };
-    auto run_storing = [&](int n0, int n1, int slot) -> int {
+    // (first: the forward run itself, which keeps PGV, PGA and displacement;
+    // a re-run must not add its displacement a second time)
+    auto run_storing = [&](int n0, int n1, int slot, bool first) -> int {
         for (int n = n0; n < n1; n++) {
             if (int st = launch_sources_on(stream)) return st;
             int FB[3];
             fb_signs(n, FB);
             for (int irk = 0; irk < 4; irk++) {
                 CgStageDesc d = desc_host_[irk];
-                d.a.pgv = nullptr;
-                d.a.dis = nullptr;
+                if (!first) {
+                    d.a.pgv = nullptr;
+                    d.a.dis = nullptr;
+                }
                 d.a.hstore = hptr(slot, n - n0, irk);
                 d.a.hbox = hb;
                 d.a.vdstore = vdptr(slot, n - n0, irk);
                 const int sgn = (irk & 1) ? -1 : 1;
                 CU(launch_cg_stage(FB[0] * sgn, FB[1] * sgn, FB[2] * sgn, d, work_dev_, grid_ctas_, stream));
             }
+            if (first)
+                if (int st = launch_pga_on(stream)) return st;
             if (int st = launch_stations_on(stream)) return st;
             kernel_launches += 6;
         }
@@ -478,7 +480,7 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
         if (s < nseg - R) {
             if (int st = run_plain(n)) return st;
         } else {
-            if (int st = run_storing(it, it + n, slot_of(s))) return st;
+            if (int st = run_storing(it, it + n, slot_of(s), true)) return st;
             it += n;
         }
     }
@@ -519,7 +521,7 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
             // forward again from the segment's checkpoint, storing each stage's RHS
             if (int st = load_state(ckpt + sb * s)) return st;
             CU(cudaMemcpyAsync(it_dev_, &n0, sizeof(int), cudaMemcpyHostToDevice, stream));
-            if (int st = run_storing(n0, n1, 0)) return st;
+            if (int st = run_storing(n0, n1, 0, false)) return st;
             if (int st = lap(&ms_re)) return st;
         }
         // and back through it

@@ -86,6 +86,17 @@ int read_params(const std::string &path, Params &p, std::string &err)
     GETF("rickerfc", rickerfc);
     GETI("ShenModel", ShenModel);
     GETI("Crust_1Model", Crust_1Model);
+    GETF("MLonStart", MLonStart);
+    GETF("MLatStart", MLatStart);
+    GETF("MLonEnd", MLonEnd);
+    GETF("MLatEnd", MLatEnd);
+    GETF("MLonStep", MLonStep);
+    GETF("MLatStep", MLatStep);
+    GETF("CrustLonStep", CrustLonStep);
+    GETF("CrustLatStep", CrustLatStep);
+    GETF("MVeticalStep", MVeticalStep);
+    GETS("MediumDir", MediumDir);
+    GETS("CrustDir", CrustDir);
     GETS("OUT", OUT);
     GETF("Depth(km)", Depth);
     GETI("sourceX", sourceX);
@@ -105,9 +116,11 @@ int read_params(const std::string &path, Params &p, std::string &err)
             return ST_OPTIONS;
         }
     }
-    // defaults of the two reference builds (Makefile_CGFDM / Makefile_SCFDM)
+    // defaults of the two reference builds (Makefile_CGFDM / Makefile_SCFDM:
+    // PML or EXP_DECAY by scheme, SOLVE_DISPLACEMENT on in both)
     p.pml = p.scheme == SCHEME_CGFDM ? 1 : 0;
     p.exp_decay = p.scheme == SCHEME_SCFDM ? 1 : 0;
+    p.solve_displacement = 1;
     GETI("PML", pml);
     GETI("EXP_DECAY", exp_decay);
     GETI("SOLVE_DISPLACEMENT", solve_displacement);
@@ -213,8 +226,172 @@ static int terrain_file(Model &m, const std::string &path, std::string &err)
 }
 
 // ----------------------------------------------------------------- medium
-// Homogeneous default (src/medium.cpp:115-140), then the 1-D layered model
-// (src/medium.cpp:143-267, LayeredStructureTerrain on as in Makefile_CGFDM).
+// Longitude and latitude (degrees) of every column of the padded grid: the
+// inverse azimuthal-equidistant projection about the centre of the x, y of
+// its top interior point (src/terrain.cpp:450-536, cart2LonLat), after the
+// check that the model corners with a 2-point margin lie inside the data's
+// range (calculateCutLonLat, :120-157; MPI_Abort 1001 there).
+static int column_lonlat(const Model &m, float lonMin, float lonMax, float latMin, float latMax,
+                         std::vector<double> &lon, std::vector<double> &lat, std::string &err)
+{
+    const Grid &g = m.g;
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%lf", (double)(float)m.p.centerLongitude);
+    const double lon0 = std::atof(buf) * (3.14159265358979323846 / 180.0);
+    std::snprintf(buf, sizeof buf, "%lf", (double)(float)m.p.centerLatitude);
+    const double lat0 = std::atof(buf) * (3.14159265358979323846 / 180.0);
+    const double r2d = 180.0 / (double)REF_PI;
+    const int NX_ = m.p.NX + 2 * HALO, NY_ = m.p.NY + 2 * HALO;
+    const int ox = g.originalX + HALO, oy = g.originalY + HALO;
+    const double corner[4][2] = {{(double)(-(ox + 2) * g.DH), (double)(-(oy + 2) * g.DH)},
+                                 {(double)(-(ox + 2) * g.DH), (double)(((NY_ - oy) + 2) * g.DH)},
+                                 {(double)(((NX_ - ox) + 2) * g.DH), (double)(-(oy + 2) * g.DH)},
+                                 {(double)(((NX_ - ox) + 2) * g.DH), (double)(((NY_ - oy) + 2) * g.DH)}};
+    for (int c = 0; c < 4; c++) {
+        double la, ph;
+        cgfdm_aeqd_inv(lon0, lat0, corner[c][0], corner[c][1], &la, &ph);
+        const float lo = (float)(la * r2d), at = (float)(ph * r2d);
+        if (lo > lonMax || lo < lonMin || at > latMax || at < latMin) {
+            err = "the longitude or latitude range of the model extends beyond the medium data's range";
+            return 1001;
+        }
+    }
+    lon.assign((size_t)g._nx_ * g._ny_, 0.0);
+    lat.assign((size_t)g._nx_ * g._ny_, 0.0);
+    const int k = g._nz - 1;
+    for (int j = 0; j < g._ny_; j++)
+        for (int i = 0; i < g._nx_; i++) {
+            const long long id = g.idx(i, j, k) * 3;
+            double la, ph;
+            cgfdm_aeqd_inv(lon0, lat0, (double)m.coord[id + 0], (double)m.coord[id + 1], &la, &ph);
+            lon[(size_t)i + (size_t)j * g._nx_] = la * r2d;
+            lat[(size_t)i + (size_t)j * g._nx_] = ph * r2d;
+        }
+    return ST_OK;
+}
+
+// Two-point Lagrange (bilinear) interpolation in double, the evaluation
+// order of src/terrain.cpp:563-600: z = {A, C, B, D} for the corners
+// (x1, y1), (x1, y2), (x2, y1), (x2, y2).
+static double interp2d(const double x[2], const double y[2], const double z[4], double x_, double y_)
+{
+    double Lx[2], Ly[2];
+    Lx[0] = 1.0 * (x_ - x[1]) / (x[0] - x[1]);
+    Lx[1] = 1.0 * (x_ - x[0]) / (x[1] - x[0]);
+    Ly[0] = 1.0 * (y_ - y[1]) / (y[0] - y[1]);
+    Ly[1] = 1.0 * (y_ - y[0]) / (y[1] - y[0]);
+    double Li = 0.0;
+    for (int jj = 0; jj < 2; jj++)
+        for (int ii = 0; ii < 2; ii++) Li = Li + Lx[ii] * Ly[jj] * z[ii * 2 + jj];
+    return Li;
+}
+
+// Weisen Shen's Vs model (src/dealMedium.cpp:49-360): one text file per
+// node "<MediumDir>/<lon %.1f>_<lat %.1f>.mod" on MLonStart..MLonEnd x
+// MLatStart..MLatEnd by MLonStep x MLatStep, NLayer = int((Depth + 30 km) /
+// MVeticalStep) lines "depth vs error" (km/s).  Per layer, Vs is
+// interpolated to each column's longitude and latitude; the first layer
+// takes the second's values (DealWithFirstLayer, on in the reference's
+// builds); a point takes layer K = int(-(z - top)) / MVeticalStep below the
+// model top DZ (NZ - 1) - Depth (StructureTerrain), Vp and rho from Vs by
+// the relations of src/dealMedium.cpp:186-189.
+static int shen_medium(Model &m, const std::string &run_dir, std::string &err)
+{
+    const Params &p = m.p;
+    const Grid &g = m.g;
+    const float LonStart = p.MLonStart, LatStart = p.MLatStart, LonStep = p.MLonStep, LatStep = p.MLatStep;
+    if (!(LonStep > 0.0f) || !(LatStep > 0.0f) || !(p.MVeticalStep > 0.0f)) {
+        err = "ShenModel needs positive MLonStep, MLatStep and MVeticalStep";
+        return ST_OPTIONS;
+    }
+    const int nLon = int((p.MLonEnd - LonStart) / LonStep + 0.5 + 1);
+    const int nLat = int((p.MLatEnd - LatStart) / LatStep + 0.5 + 1);
+    const float Depth = (float)(p.Depth * 1e3 + 3e4);
+    const int NLayer = int(Depth / p.MVeticalStep);
+    if (nLon < 2 || nLat < 2 || NLayer < 2) {
+        err = "ShenModel grid too small";
+        return ST_OPTIONS;
+    }
+    std::vector<float> VModel((size_t)nLon * nLat * NLayer);
+    const std::string dir = join(run_dir, p.MediumDir);
+    for (int j = 0; j < nLat; j++)
+        for (int i = 0; i < nLon; i++) {
+            char name[64];
+            std::snprintf(name, sizeof name, "%.1f_%.1f.mod", (double)(LonStart + i * LonStep),
+                          (double)(LatStart + j * LatStep));
+            const std::string path = dir + "/" + name;
+            FILE *f = std::fopen(path.c_str(), "r");
+            if (!f) {
+                err = "cannot open Shen model file " + path;
+                return ST_IO;
+            }
+            for (int K = 0; K < NLayer; K++) {
+                double dep, vs, e;
+                if (std::fscanf(f, "%lf %lf %lf", &dep, &vs, &e) != 3) {
+                    std::fclose(f);
+                    err = "Shen model file too short: " + path;
+                    return ST_IO;
+                }
+                VModel[(size_t)K + ((size_t)i + (size_t)j * nLon) * NLayer] = (float)(vs * 1e3);
+            }
+            std::fclose(f);
+        }
+    std::vector<double> lon, lat;
+    if (int st = column_lonlat(m, LonStart, p.MLonEnd, LatStart, p.MLatEnd, lon, lat, err)) return st;
+
+    const size_t plane = (size_t)g._nx_ * g._ny_;
+    std::vector<float> Vs(plane * NLayer);
+    for (int K = 0; K < NLayer; K++)
+        for (int j = 0; j < g._ny_; j++)
+            for (int i = 0; i < g._nx_; i++) {
+                const size_t c = (size_t)i + (size_t)j * g._nx_;
+                const double x_ = lon[c], y_ = lat[c];
+                const int I = int((x_ - (double)LonStart) / LonStep);
+                const int J = int((y_ - (double)LatStart) / LatStep);
+                if (I < 0 || J < 0 || I + 1 >= nLon || J + 1 >= nLat) {
+                    err = "a grid column falls outside the Shen model's nodes";
+                    return 1001;
+                }
+                const double x1 = (float)(I * LonStep) + (double)LonStart;
+                const double y1 = (float)(J * LatStep) + (double)LatStart;
+                const double x[2] = {x1, x1 + LonStep}, y[2] = {y1, y1 + LatStep};
+                auto at = [&](int a, int b) { return (double)VModel[(size_t)K + ((size_t)a + (size_t)b * nLon) * NLayer]; };
+                const double z[4] = {at(I, J), at(I, J + 1), at(I + 1, J), at(I + 1, J + 1)};
+                Vs[(size_t)K * plane + c] = (float)interp2d(x, y, z, x_, y_);
+            }
+    for (size_t c = 0; c < plane; c++) Vs[c] = Vs[plane + c];   // DealWithFirstLayer
+
+    const int NZ = p.NZ;
+    const double DepthM = p.Depth * 1e3;
+    for (int k = 0; k < g._nz_; k++)
+        for (int j = 0; j < g._ny_; j++)
+            for (int i = 0; i < g._nx_; i++) {
+                const long long id = g.idx(i, j, k);
+                const double DZ = (double)(m.coord[g.idx(i, j, 4) * 3 + 2] - m.coord[g.idx(i, j, 3) * 3 + 2]);
+                const double top = DZ * double(NZ - 1) - std::fabs(DepthM);
+                int K = (int)((float)int(-((double)m.coord[id * 3 + 2] - top)) / p.MVeticalStep);
+                if (K <= 0) K = 0;
+                if (K >= NLayer) {
+                    err = "a grid point lies below the Shen model's deepest layer";
+                    return ST_OPTIONS;
+                }
+                const float VS = (float)(Vs[(size_t)K * plane + (size_t)i + (size_t)j * g._nx_] * 1e-3);
+                const float VP = (float)(0.9409 + 2.0947 * VS - 0.8206 * std::pow((double)VS, 2.0) +
+                                         0.2683 * std::pow((double)VS, 3.0) - 0.0251 * std::pow((double)VS, 4.0));
+                const float RHO = (float)(1.6612 * VP - 0.4721 * std::pow((double)VP, 2.0) +
+                                          0.0671 * std::pow((double)VP, 3.0) - 0.0043 * std::pow((double)VP, 4.0) +
+                                          0.000106 * std::pow((double)VP, 5.0));
+                float *md = &m.medium[id * 3];
+                md[0] = (float)(VS * 1e3);
+                md[1] = (float)(VP * 1e3);
+                md[2] = (float)(RHO * 1e3);
+            }
+    return ST_OK;
+}
+
+// Homogeneous default (src/medium.cpp:115-140), then the media the switches
+// select in the reference's order (src/medium.cpp:251-295): CRUST1.0, Shen,
+// the 1-D layered model (LayeredStructureTerrain on as in Makefile_CGFDM).
 static int build_medium(Model &m, const std::string &run_dir, std::string &err)
 {
     const Grid &g = m.g;
@@ -225,10 +402,12 @@ static int build_medium(Model &m, const std::string &run_dir, std::string &err)
         m.medium[n * 3 + 2] = 2700.0f;
     }
     if (!m.p.useMedium) return ST_OK;
-    if (m.p.ShenModel || m.p.Crust_1Model) {
-        err = "ShenModel/Crust_1Model media need PROJ and external model files; not supported";
+    if (m.p.Crust_1Model) {
+        err = "Crust_1Model media are not supported; use ShenModel, LayeredModel or a mediumFile";
         return ST_OPTIONS;
     }
+    if (m.p.ShenModel)
+        if (int st = shen_medium(m, run_dir, err)) return st;
     if (!m.p.LayeredModel) return ST_OK;
     std::string path = join(run_dir, m.p.LayeredFileName);
     std::ifstream f(path, std::ios::binary);

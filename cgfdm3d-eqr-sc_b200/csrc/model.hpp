@@ -55,6 +55,9 @@ struct Params {
     int useSingleSource_double_couple = 0;
     float strike = 0, dip = 0, rake = 0, Mw = 0, duration = 0;
     int ShenModel = 0, Crust_1Model = 0, LayeredModel = 0;
+    float MLonStart = 0, MLatStart = 0, MLonEnd = 0, MLatEnd = 0, MLonStep = 0, MLatStep = 0;
+    float MVeticalStep = 0, CrustLonStep = 0, CrustLatStep = 0;
+    std::string MediumDir, CrustDir;
     std::string LayeredFileName;
     std::string OUT;
     float Depth = 0;

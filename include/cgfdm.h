@@ -68,6 +68,15 @@ typedef struct cgfdm_info {
  * "fp32"|"fp64", "OUT": "..."}. */
 int cgfdm_create(const char *run_dir, const char *options_json, int device, cgfdm_session **out);
 
+/* Host-only: builds the model of a run directory as cgfdm_create does --
+ * parameters, grid, coordinates and the medium from the switches that
+ * select it (homogeneous, CRUST1.0, Shen, layered, mediumFile;
+ * src/medium.cpp:251-295) -- without touching a GPU, and copies the medium
+ * [nzp][nyp][nxp][3] (Vs, Vp, rho) into `out` (NULL: only the dimensions
+ * nzp, nyp, nxp go to dims).  Errors as cgfdm_create, message from
+ * cgfdm_last_error(NULL). */
+int cgfdm_model_medium(const char *run_dir, const char *options_json, float *out, long long count, int *dims);
+
 /* Advances up to `nsteps` time steps (clamped to NT).  One step is the body
  * of the time loop, src/propagate.cpp:186-321: source term into W, the RK
  * stages with derivative, free surface and PML, station recording and PGV. */
@@ -144,7 +153,8 @@ int cgfdm_set_medium(cgfdm_session *s, const float *medium, long long count);
  * components 0..2), d = observed [n_stations][NT][3], with respect to Vp,
  * Vs and rho at every interior grid point: grad [3][nz][ny][nx] (Vp, Vs,
  * rho; zero inside the PML layers), *misfit = J.  The session must stand at
- * step 0 (new, or after cgfdm_set_medium) and have point sources only; it
+ * step 0 (new, or after cgfdm_set_medium) and have point sources only (it
+ * writes no snapshot files; PGV and displacement follow the forward run); it
  * runs the whole forward once keeping the state every `checkpoint_every`
  * steps in device memory, then per segment, last first, re-runs it storing
  * each RK stage's right-hand side and steps the transposed operator back

@@ -1,0 +1,95 @@
+"""Real-data medium inputs against the reference's CPU build: Weisen Shen's
+Vs model (ShenModel, src/dealMedium.cpp:49-360) read from per-node ".mod"
+text files, interpolated to the grid's longitudes and latitudes (inverse
+azimuthal-equidistant projection about the centre), layered by depth below
+the model top, Vp and rho from Vs.  The packed medium (mu, lambda,
+buoyancy of every padded point) must equal the reference's bit for bit.
+
+The node files are synthetic: seeded Vs profiles of the published format
+(depth, Vs, error per line, km and km/s) on a 0.1-degree grid around the
+model, whose 12 x 10 km extent spans several nodes."""
+
+import os
+
+import numpy as np
+import pytest
+
+import parity_util as pu
+import refrun
+from cgfdm import Session, cases
+
+
+def write_shen_nodes(directory, lon0, lon1, lat0, lat1, step, nlayer, dz_km, seed=4):
+    rng = np.random.default_rng(seed)
+    os.makedirs(directory, exist_ok=True)
+    nlon = int(round((lon1 - lon0) / step)) + 1
+    nlat = int(round((lat1 - lat0) / step)) + 1
+    for j in range(nlat):
+        for i in range(nlon):
+            lon = np.float32(np.float32(lon0) + np.float32(i) * np.float32(step))
+            lat = np.float32(np.float32(lat0) + np.float32(j) * np.float32(step))
+            base = rng.uniform(2.2, 3.0)
+            grad = rng.uniform(0.03, 0.06)
+            with open(os.path.join(directory, f"{float(lon):.1f}_{float(lat):.1f}.mod"), "w") as f:
+                for k in range(nlayer):
+                    dep = k * dz_km
+                    vs = min(4.6, base + grad * dep + 0.05 * np.sin(0.7 * k + i - j))
+                    f.write(f"{dep:.3f} {vs:.4f} {0.01:.3f}\n")
+
+
+def _case(steps=6):
+    c = pu.small_halfspace(steps=steps, NX=60, NY=50, NZ=40, DH=200.0, vp=8500.0)
+    c.fault = []
+    c.double_couple = dict(X=30, Y=25, Z=30, strike=30.0, dip=60.0, rake=90.0, Mw=4.0, duration=0.3)
+    c.stations = [(20, 20, c.NZ - 1), (40, 30, c.NZ - 1)]
+    c.layers = ()
+    c.extra = dict(c.extra, useMedium=1, LayeredModel=0, ShenModel=1, MLonStart=99.8, MLonEnd=100.2,
+                   MLatStart=29.8, MLatEnd=30.2, MLonStep=0.1, MLatStep=0.1, MVeticalStep=500.0,
+                   MediumDir="./MediumDir")
+    return c
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scheme", ["CGFDM", "SCFDM"])
+def test_shen_medium_matches_reference(tmp_path, scheme):
+    if not refrun.available(scheme):
+        pytest.skip("reference CPU build not present")
+    c = _case()
+    d = cases.write_case(c, str(tmp_path / "run"), scheme=scheme)
+    depth_km = c.DH * c.NZ * 1e-3
+    nlayer = int((depth_km * 1e3 + 3e4) / 500.0)
+    write_shen_nodes(os.path.join(d, "MediumDir"), 99.8, 100.2, 29.8, 30.2, 0.1, nlayer, 0.5)
+    refrun.run(d, scheme)
+    ref = refrun.read_outputs(d, scheme)["CJM"]
+    with Session(d, flavor="exact") as s:
+        mine = s.cjm()
+    med = slice(10, 13)   # mu, lambda, buoyancy
+    assert np.unique(ref[..., 10]).size > 20, "the medium must vary"
+    np.testing.assert_array_equal(mine[..., med], ref[..., med])
+
+
+def _cjm_medium(med):
+    """mu, lambda, buoyancy from (Vs, Vp, rho) with the float32 operations of
+    the reference's CJM fill (src/CJM.cpp:52-77)."""
+    vs, vp, rho = (med[..., c].astype(np.float32) for c in range(3))
+    mu = rho * (vs * vs)
+    lam = rho * (vp * vp - (np.float32(2) * vs) * vs)
+    return np.stack([mu, lam, np.float32(1) / rho], -1)
+
+
+def test_shen_medium_host_matches_reference(tmp_path):
+    """The same comparison on the CPU: the library builds the medium on the
+    host (cgfdm_model_medium), the reference's CPU build packs it into CJM."""
+    from cgfdm import model_medium
+
+    if not refrun.available("CGFDM"):
+        pytest.skip("reference CPU build not present")
+    c = _case(steps=2)
+    d = cases.write_case(c, str(tmp_path / "run"))
+    nlayer = int((c.DH * c.NZ + 3e4) / 500.0)
+    write_shen_nodes(os.path.join(d, "MediumDir"), 99.8, 100.2, 29.8, 30.2, 0.1, nlayer, 0.5)
+    med = model_medium(d)
+    refrun.run(d, "CGFDM")
+    ref = refrun.read_outputs(d)["CJM"][..., 10:13]
+    assert np.unique(med[..., 0]).size > 20
+    np.testing.assert_array_equal(_cjm_medium(med), ref)
