@@ -389,6 +389,108 @@ static int shen_medium(Model &m, const std::string &run_dir, std::string &err)
     return ST_OK;
 }
 
+// CRUST1.0 (src/crustMedium.cpp:67-370): the text files crust1.vs, .vp,
+// .rho, .bnds of CrustDir, 64800 one-degree cells (from 179.5 W, 89.5 N,
+// longitude fastest) x 9 layers each (km/s, g/cm^3, km), read cell by cell;
+// every layer's values are interpolated to each column's longitude and
+// latitude on the CrustLonStep x CrustLatStep grid; a point takes the layer
+// whose boundaries (m) bracket its height, skipping layers less than 1 km
+// thick below the boundary it falls under (BoundaryDifference).
+static int crust_medium(Model &m, const std::string &run_dir, std::string &err)
+{
+    const Params &p = m.p;
+    const Grid &g = m.g;
+    const int nLon = 360, nLat = 180, nLayer = 9, nLL = nLon * nLat;
+    const std::string dir = join(run_dir, p.CrustDir);
+    const char *names[4] = {"crust1.vs", "crust1.vp", "crust1.rho", "crust1.bnds"};
+    std::vector<float> file[4];
+    FILE *fp[4] = {};
+    for (int f = 0; f < 4; f++) {
+        const std::string path = dir + "/" + names[f];
+        fp[f] = std::fopen(path.c_str(), "r");
+        if (!fp[f]) {
+            for (int q = 0; q < f; q++) std::fclose(fp[q]);
+            err = "cannot open CRUST1.0 file " + path;
+            return ST_IO;
+        }
+        file[f].assign((size_t)nLL * nLayer, 0.0f);
+    }
+    bool ok = true;
+    for (int i = 0; i < nLL && ok; i++)
+        for (int n = 0; n < nLayer && ok; n++)
+            for (int f = 0; f < 4 && ok; f++) ok = std::fscanf(fp[f], "%f", &file[f][(size_t)i + (size_t)n * nLL]) == 1;
+    for (int f = 0; f < 4; f++) std::fclose(fp[f]);
+    if (!ok) {
+        err = "CRUST1.0 files too short in " + dir;
+        return ST_IO;
+    }
+    if (!(p.CrustLonStep > 0.0f) || !(p.CrustLatStep > 0.0f)) {
+        err = "Crust_1Model needs positive CrustLonStep and CrustLatStep";
+        return ST_OPTIONS;
+    }
+    std::vector<double> lon, lat;
+    if (int st = column_lonlat(m, -180.0f, 180.0f, -90.0f, 90.0f, lon, lat, err)) return st;
+
+    const size_t plane = (size_t)g._nx_ * g._ny_;
+    std::vector<float> interp[4];
+    for (int f = 0; f < 4; f++) interp[f].assign(plane * nLayer, 0.0f);
+    const float LonStart = -179.5f, LatStart = 89.5f, LonStep = p.CrustLonStep, LatStep = p.CrustLatStep;
+    for (int K = 0; K < nLayer; K++)
+        for (int j = 0; j < g._ny_; j++)
+            for (int i = 0; i < g._nx_; i++) {
+                const size_t c = (size_t)i + (size_t)j * g._nx_;
+                const double x_ = lon[c], y_ = lat[c];
+                const int I = int((x_ - LonStart) / LonStep);
+                const int J = int((LatStart - y_) / LatStep) + 1;
+                if (I < 0 || I + 1 >= nLon || J < 1 || J >= nLat) {
+                    err = "a grid column falls outside the CRUST1.0 cells";
+                    return 1001;
+                }
+                const double x1 = I * LonStep + LonStart, y1 = LatStart - J * LatStep;
+                const double x[2] = {x1, x1 + LonStep}, y[2] = {y1, y1 + LatStep};
+                auto at = [&](int f, int a, int b) {
+                    return (double)file[f][(size_t)a + (size_t)b * nLon + (size_t)K * nLL];
+                };
+                for (int f = 0; f < 4; f++) {
+                    const double z[4] = {at(f, I, J), at(f, I, J - 1), at(f, I + 1, J), at(f, I + 1, J - 1)};
+                    interp[f][(size_t)K * plane + c] = (float)interp2d(x, y, z, x_, y_);
+                }
+            }
+    std::vector<float> &bnds = interp[3];
+    for (size_t e = 0; e < bnds.size(); e++) bnds[e] = (float)(bnds[e] * 1e3);
+
+    const float BoundaryDifference = 1000.0f;
+    float vs = 0.0f, vp = 0.0f, rho = 0.0f;
+    for (int k = 0; k < g._nz_; k++)
+        for (int j = 0; j < g._ny_; j++)
+            for (int i = 0; i < g._nx_; i++) {
+                const long long id = g.idx(i, j, k);
+                const size_t c = (size_t)i + (size_t)j * g._nx_;
+                const float coordZ = m.coord[id * 3 + 2];
+                auto B = [&](int l) { return bnds[(size_t)l * plane + c]; };
+                // the layer above the first boundary at least 1 km below boundary `from`
+                auto take_below = [&](int from) {
+                    int l = from;
+                    while (l < nLayer && std::fabs(B(from) - B(l)) < BoundaryDifference) l++;
+                    const size_t q = (size_t)(l - 1) * plane + c;
+                    vs = interp[0][q], vp = interp[1][q], rho = interp[2][q];
+                };
+                if (coordZ > B(0)) take_below(0);
+                if (coordZ <= B(nLayer - 1)) {
+                    const size_t q = (size_t)(nLayer - 1) * plane + c;
+                    vs = interp[0][q], vp = interp[1][q], rho = interp[2][q];
+                }
+                if (coordZ <= B(0) && coordZ > B(nLayer - 1))
+                    for (int mm = 0; mm < nLayer - 1; mm++)
+                        if (coordZ <= B(mm) && coordZ > B(mm + 1)) take_below(mm);
+                float *md = &m.medium[id * 3];
+                md[0] = (float)(vs * 1e3);
+                md[1] = (float)(vp * 1e3);
+                md[2] = (float)(rho * 1e3);
+            }
+    return ST_OK;
+}
+
 // Homogeneous default (src/medium.cpp:115-140), then the media the switches
 // select in the reference's order (src/medium.cpp:251-295): CRUST1.0, Shen,
 // the 1-D layered model (LayeredStructureTerrain on as in Makefile_CGFDM).
@@ -402,10 +504,8 @@ static int build_medium(Model &m, const std::string &run_dir, std::string &err)
         m.medium[n * 3 + 2] = 2700.0f;
     }
     if (!m.p.useMedium) return ST_OK;
-    if (m.p.Crust_1Model) {
-        err = "Crust_1Model media are not supported; use ShenModel, LayeredModel or a mediumFile";
-        return ST_OPTIONS;
-    }
+    if (m.p.Crust_1Model)
+        if (int st = crust_medium(m, run_dir, err)) return st;
     if (m.p.ShenModel)
         if (int st = shen_medium(m, run_dir, err)) return st;
     if (!m.p.LayeredModel) return ST_OK;

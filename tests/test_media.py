@@ -93,3 +93,52 @@ def test_shen_medium_host_matches_reference(tmp_path):
     ref = refrun.read_outputs(d)["CJM"][..., 10:13]
     assert np.unique(med[..., 0]).size > 20
     np.testing.assert_array_equal(_cjm_medium(med), ref)
+
+
+def write_crust1(directory, seed=6):
+    """Synthetic CRUST1.0 files (crust1.vs/.vp/.rho/.bnds): 64800 one-degree
+    cells from 179.5 W, 89.5 N, longitude fastest, 9 layers per cell (water,
+    ice, three sediment, three crust layers, mantle), smooth in space."""
+    rng = np.random.default_rng(seed)
+    os.makedirs(directory, exist_ok=True)
+    lon = -179.5 + np.arange(360)
+    lat = 89.5 - np.arange(180)
+    LO, LA = np.meshgrid(np.radians(lon), np.radians(lat))
+    f = lambda a, b: np.sin(a * LO + rng.uniform(0, 6)) * np.cos(b * LA + rng.uniform(0, 6))
+    topo = 0.4 + 0.3 * f(7, 5)
+    thick = [np.zeros_like(topo), np.zeros_like(topo), 0.4 + 0.3 * f(11, 9) ** 2, 0.9 + 0.6 * f(5, 13) ** 2,
+             1.5 + 0.8 * f(9, 3) ** 2, 11 + 3 * f(3, 4), 10 + 2 * f(4, 6), 12 + 2 * f(6, 2)]
+    bnds = [topo]
+    for t in thick:
+        bnds.append(bnds[-1] - t)
+    vs0 = [0.0, 1.9, 1.0, 1.7, 2.4, 3.5, 3.7, 3.9, 4.5]
+    vp0 = [1.5, 3.8, 2.5, 3.4, 4.4, 6.0, 6.4, 6.9, 8.1]
+    rho0 = [1.02, 0.92, 2.0, 2.3, 2.5, 2.7, 2.85, 3.0, 3.35]
+    vs = [v + 0.1 * f(3 + n, 2 + n) * (v > 0) for n, v in enumerate(vs0)]
+    vp = [v + 0.15 * f(2 + n, 3 + n) for n, v in enumerate(vp0)]
+    rho = [v + 0.05 * f(4 + n, 5 + n) for n, v in enumerate(rho0)]
+    for name, arr in (("vs", vs), ("vp", vp), ("rho", rho), ("bnds", bnds)):
+        a = np.stack([x.reshape(-1) for x in arr], axis=1)   # [cell][layer]
+        np.savetxt(os.path.join(directory, f"crust1.{name}"), a, fmt="%.4f")
+
+
+def _crust_case(steps=2):
+    c = _case(steps)
+    c.extra = dict(c.extra, ShenModel=0, Crust_1Model=1, CrustLonStep=1.0, CrustLatStep=1.0, CrustDir="./crust")
+    return c
+
+
+def test_crust1_medium_host_matches_reference(tmp_path):
+    """CRUST1.0 (Crust_1Model, src/crustMedium.cpp:67-370), on the CPU."""
+    from cgfdm import model_medium
+
+    if not refrun.available("CGFDM"):
+        pytest.skip("reference CPU build not present")
+    c = _crust_case()
+    d = cases.write_case(c, str(tmp_path / "run"))
+    write_crust1(os.path.join(d, "crust"))
+    med = model_medium(d)
+    refrun.run(d, "CGFDM")
+    ref = refrun.read_outputs(d)["CJM"][..., 10:13]
+    assert np.unique(med[..., 0]).size > 20
+    np.testing.assert_array_equal(_cjm_medium(med), ref)
