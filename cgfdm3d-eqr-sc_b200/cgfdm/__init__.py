@@ -68,6 +68,8 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
     fp = ctypes.POINTER(ctypes.c_float)
     L.cgfdm_model_medium.argtypes = [ctypes.c_char_p, ctypes.c_char_p, fp, ctypes.c_longlong,
                                      ctypes.POINTER(ctypes.c_int)]
+    L.cgfdm_model_coord.argtypes = [ctypes.c_char_p, ctypes.c_char_p, fp, ctypes.c_longlong, fp,
+                                    ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)]
     L.cgfdm_get_stations.argtypes = [vp, fp, ctypes.c_longlong]
     L.cgfdm_get_wavefield.argtypes = [vp, fp, ctypes.c_longlong]
     L.cgfdm_get_cjm.argtypes = [vp, fp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)]
@@ -119,6 +121,24 @@ def model_medium(run_dir: str, options: Optional[str] = None, flavor: str = "fas
     if rc:
         raise CgfdmError(rc, L.cgfdm_last_error(None).decode())
     return out
+
+
+def model_coord(run_dir: str, options: Optional[str] = None, flavor: str = "fast"):
+    """The surface height [nyp][nxp] and the coordinates [nzp][nyp][nxp][3]
+    (x, y, z) a run directory describes, built on the host without a GPU
+    (cgfdm_model_coord)."""
+    L = load(flavor)
+    dims = (ctypes.c_int * 3)()
+    o = options.encode() if options else None
+    rc = L.cgfdm_model_coord(run_dir.encode(), o, None, 0, None, 0, dims)
+    if rc:
+        raise CgfdmError(rc, L.cgfdm_last_error(None).decode())
+    terrain = np.zeros((dims[1], dims[2]), np.float32)
+    coord = np.zeros((dims[0], dims[1], dims[2], 3), np.float32)
+    rc = L.cgfdm_model_coord(run_dir.encode(), o, _fptr(terrain), terrain.size, _fptr(coord), coord.size, dims)
+    if rc:
+        raise CgfdmError(rc, L.cgfdm_last_error(None).decode())
+    return terrain, coord
 
 
 class Session:

@@ -74,6 +74,30 @@ int cgfdm_model_medium(const char *run_dir, const char *options_json, float *out
     return CGFDM_OK;
 }
 
+int cgfdm_model_coord(const char *run_dir, const char *options_json, float *terrain, long long terrain_count,
+                      float *coord, long long coord_count, int *dims)
+{
+    if (!run_dir) {
+        g_create_error = "run_dir must not be NULL";
+        return CGFDM_E_ARG;
+    }
+    cgfdm::Model m;
+    std::string err;
+    int st = cgfdm::build_model(run_dir, options_json ? options_json : "", m, err);
+    if (st) {
+        g_create_error = err;
+        return st;
+    }
+    if (dims) dims[0] = m.g._nz_, dims[1] = m.g._ny_, dims[2] = m.g._nx_;
+    if ((terrain && terrain_count < (long long)m.terrain.size()) || (coord && coord_count < (long long)m.coord.size())) {
+        g_create_error = "output array too small";
+        return CGFDM_E_ARG;
+    }
+    if (terrain) std::memcpy(terrain, m.terrain.data(), sizeof(float) * m.terrain.size());
+    if (coord) std::memcpy(coord, m.coord.data(), sizeof(float) * m.coord.size());
+    return CGFDM_OK;
+}
+
 int cgfdm_run(cgfdm_session *s, int nsteps)
 {
     if (!s) return CGFDM_E_ARG;

@@ -96,6 +96,12 @@ int read_params(const std::string &path, Params &p, std::string &err)
     GETF("CrustLatStep", CrustLatStep);
     GETF("MVeticalStep", MVeticalStep);
     GETS("MediumDir", MediumDir);
+    GETI("SRTM90", SRTM90);
+    GETS("TerrainDir", TerrainDir);
+    GETI("lonStart", lonStart);
+    GETI("latStart", latStart);
+    GETI("blockX", blockX);
+    GETI("blockY", blockY);
     GETS("CrustDir", CrustDir);
     GETS("OUT", OUT);
     GETF("Depth(km)", Depth);
@@ -225,6 +231,202 @@ static int terrain_file(Model &m, const std::string &path, std::string &err)
     return ST_OK;
 }
 
+// ---------------------------------------------------------- SRTM terrain
+// Two-point Lagrange (bilinear) interpolation in double, the evaluation
+// order of src/terrain.cpp:563-600: z = {A, C, B, D} for the corners
+// (x1, y1), (x1, y2), (x2, y1), (x2, y2).
+static double interp2d(const double x[2], const double y[2], const double z[4], double x_, double y_)
+{
+    double Lx[2], Ly[2];
+    Lx[0] = 1.0 * (x_ - x[1]) / (x[0] - x[1]);
+    Lx[1] = 1.0 * (x_ - x[0]) / (x[1] - x[0]);
+    Ly[0] = 1.0 * (y_ - y[1]) / (y[0] - y[1]);
+    Ly[1] = 1.0 * (y_ - y[0]) / (y[1] - y[0]);
+    double Li = 0.0;
+    for (int jj = 0; jj < 2; jj++)
+        for (int ii = 0; ii < 2; ii++) Li = Li + Lx[ii] * Ly[jj] * z[ii * 2 + jj];
+    return Li;
+}
+
+// The projection centre as the reference hands it to PROJ: a float printed
+// with "%lf" (src/terrain.cpp:325-331, 490-505), in radians.
+static void proj_centre(const Params &p, double *lon0, double *lat0)
+{
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%lf", (double)(float)p.centerLongitude);
+    *lon0 = std::atof(buf) * (3.14159265358979323846 / 180.0);
+    std::snprintf(buf, sizeof buf, "%lf", (double)(float)p.centerLatitude);
+    *lat0 = std::atof(buf) * (3.14159265358979323846 / 180.0);
+}
+
+// 11-point Gaussian of the terrain smoothing (Terrain_Smooth, on in the
+// reference's builds): GAUSS_FUN(n - 5, 2.5, 0) of src/macro.h:37.
+static void smooth_weights(double Dg[11])
+{
+    const double ra = 5 * 0.5;
+    for (int n = 0; n < 11; n++) {
+        const double t = ((n - 5) - 0.0) / ra;
+        Dg[n] = std::exp(-(t * t)) / (ra * 1.772453850905516);
+    }
+}
+
+static int column_lonlat(const Model &m, float lonMin, float lonMax, float latMin, float latMax,
+                         std::vector<double> &lon, std::vector<double> &lat, std::string &err);
+
+// SRTM90 surface (src/terrain.cpp:206-290, 307-447, 602-770): 5 x 5 degree
+// tiles "<TerrainDir>/srtm_<lat>N<lon>E.bin" of 6000 x 6000 float heights
+// (blockX x blockY of them from lonStart, latStart), joined with one shared
+// row and column; around the model, points whose central-difference
+// gradient exceeds 100 m take the mean of their four neighbours, then an
+// 11 x 11 Gaussian smooths the map; each column's height is interpolated
+// at its longitude and latitude (on a grid widened by 5 points) and smoothed
+// again with the same Gaussian.  The reference's third corner value is
+// taken at (I + 1, J + 1) as well as the fourth; kept.
+static int srtm_terrain(Model &m, const std::string &run_dir, std::string &err)
+{
+    const Params &p = m.p;
+    const Grid &g = m.g;
+    const int PPB = 6000, DPB = 5;
+    if (p.blockX < 1 || p.blockY < 1) {
+        err = "SRTM90 needs blockX, blockY >= 1";
+        return ST_OPTIONS;
+    }
+    const int TX = (PPB - 1) * p.blockX + 1, TY = (PPB - 1) * p.blockY + 1;
+    std::vector<float> total((size_t)TX * TY, 0.0f), tile((size_t)PPB * PPB);
+    const std::string dir = join(run_dir, p.TerrainDir);
+    for (int jb = 0; jb < p.blockY; jb++)
+        for (int ib = 0; ib < p.blockX; ib++) {
+            const int lat = p.latStart + jb * DPB, lon = p.lonStart + ib * DPB;
+            char name[96];
+            std::snprintf(name, sizeof name, "srtm_%dN%dE.bin", lat, lon);
+            const std::string path = dir + "/" + name;
+            FILE *f = std::fopen(path.c_str(), "rb");
+            if (!f) {
+                err = "There is no such file " + path;
+                return ST_IO;
+            }
+            const size_t got = std::fread(tile.data(), sizeof(float), tile.size(), f);
+            std::fclose(f);
+            if (got != tile.size()) {
+                err = "SRTM tile too short: " + path;
+                return ST_IO;
+            }
+            for (int jj = 0; jj < PPB - 1; jj++)
+                for (int ii = 0; ii < PPB - 1; ii++)
+                    total[(size_t)(ib * (PPB - 1) + ii) + (size_t)(jb * (PPB - 1) + jj) * TX] =
+                        tile[(size_t)ii + (size_t)jj * PPB];
+        }
+
+    double lon0, lat0;
+    proj_centre(p, &lon0, &lat0);
+    const double r2d = 180.0 / (double)REF_PI;
+    const float DH = g.DH;
+    const double lonStart = p.lonStart, latStart = p.latStart;
+    const double dLon = double(DPB * p.blockX) / double(TX), dLat = double(DPB * p.blockY) / double(TY);
+    double Dg[11];
+    smooth_weights(Dg);
+
+    // despiking and smoothing of the tiles around the model (callibrateTotalTerrain)
+    {
+        const double xs[2] = {(double)((0 - HALO) * DH - g.originalX * DH), (double)((g._nx_ - HALO) * DH - g.originalX * DH)};
+        const double ys[2] = {(double)((0 - HALO) * DH - g.originalY * DH), (double)((g._ny_ - HALO) * DH - g.originalY * DH)};
+        float maxLon = -1000.0f, maxLat = -1000.0f, minLon = 1000.0f, minLat = 1000.0f;
+        const double cx[4] = {xs[0], xs[0], xs[1], xs[1]}, cy[4] = {ys[0], ys[1], ys[0], ys[1]};
+        for (int c = 0; c < 4; c++) {
+            double la, ph;
+            cgfdm_aeqd_inv(lon0, lat0, cx[c], cy[c], &la, &ph);
+            const double Lon = la * r2d, Lat = ph * r2d;
+            if (maxLon <= Lon) maxLon = (float)Lon;
+            if (maxLat <= Lat) maxLat = (float)Lat;
+            if (minLon >= Lon) minLon = (float)Lon;
+            if (minLat >= Lat) minLat = (float)Lat;
+        }
+        const int I0 = int((minLon - lonStart) / dLon) - 10, J0 = int((minLat - latStart) / dLat) - 10;
+        const int I1 = int((maxLon - lonStart) / dLon) + 10, J1 = int((maxLat - latStart) / dLat) + 10;
+        if (I0 - 5 < 0 || J0 - 5 < 0 || I1 + 5 > TX || J1 + 5 > TY) {
+            err = "the model lies too close to the edge of the SRTM tiles";
+            return 1001;
+        }
+        std::vector<float> next(total);
+        for (int j = J0; j < J1; j++)
+            for (int i = I0; i < I1; i++) {
+                const float a = total[(size_t)(i + 1) + (size_t)j * TX], b = total[(size_t)(i - 1) + (size_t)j * TX];
+                const float c = total[(size_t)i + (size_t)(j + 1) * TX], d = total[(size_t)i + (size_t)(j - 1) * TX];
+                const float gx = a - b, gy = c - d;
+                const float grad = std::sqrt(gx * gx + gy * gy);
+                if (grad > 100.0) next[(size_t)i + (size_t)j * TX] = (float)((a + b + c + d) * 0.25);
+            }
+        total = next;
+        for (int j = J0; j < J1; j++)
+            for (int i = I0; i < I1; i++) {
+                double sum = 0.0;
+                for (int jj = j - 5; jj < j + 6; jj++)
+                    for (int ii = i - 5; ii < i + 6; ii++) {
+                        const double amp = Dg[ii + 5 - i] * Dg[jj + 5 - j] / 0.996768;
+                        sum += amp * total[(size_t)ii + (size_t)jj * TX];
+                    }
+                next[(size_t)i + (size_t)j * TX] = (float)sum;
+            }
+        total.swap(next);
+    }
+
+    // the model with its 2-point margin inside the tiles, and the columns'
+    // longitude and latitude for the projection output (projTrans)
+    {
+        const float lonMax = (float)(p.lonStart + p.blockX * DPB), latMax = (float)(p.latStart + p.blockY * DPB);
+        if (int st = column_lonlat(m, (float)p.lonStart, lonMax, (float)p.latStart, latMax, m.lon, m.lat, err))
+            return st;
+    }
+
+    // the columns' heights (terrainInterp), on a grid widened by 5 points
+    const int ng = 5, enx = g._nx_ + 2 * ng, eny = g._ny_ + 2 * ng;
+    std::vector<float> ex((size_t)enx * eny);
+    for (int j = -ng; j < g._ny_ + ng; j++)
+        for (int i = -ng; i < g._nx_ + ng; i++) {
+            const double px = (double)((i - HALO) * DH - g.originalX * DH);
+            const double py = (double)((j - HALO) * DH - g.originalY * DH);
+            double la, ph;
+            cgfdm_aeqd_inv(lon0, lat0, px, py, &la, &ph);
+            const double x_ = la * r2d, y_ = ph * r2d;
+            const int I = int((x_ - lonStart) / dLon), J = int((y_ - latStart) / dLat);
+            if (I < 0 || J < 0 || I + 1 >= TX || J + 1 >= TY) {
+                err = "the model extends beyond the SRTM tiles";
+                return 1001;
+            }
+            const double x1 = I * dLon + lonStart, y1 = J * dLat + latStart;
+            const double x[2] = {x1, x1 + dLon}, y[2] = {y1, y1 + dLat};
+            auto T = [&](int a, int b) { return (double)total[(size_t)a + (size_t)b * TX]; };
+            const double z[4] = {T(I, J), T(I + 1, J + 1), T(I + 1, J), T(I + 1, J + 1)};
+            ex[(size_t)(i + ng) + (size_t)(j + ng) * enx] = (float)interp2d(x, y, z, x_, y_);
+        }
+    for (int j = ng; j < g._ny_ + ng; j++)
+        for (int i = ng; i < g._nx_ + ng; i++) {
+            double sum = 0.0;
+            for (int jj = j - ng; jj < j + ng + 1; jj++)
+                for (int ii = i - ng; ii < i + ng + 1; ii++) {
+                    const double amp = Dg[ii + ng - i] * Dg[jj + ng - j] / 0.996768;
+                    sum += amp * ex[(size_t)ii + (size_t)jj * enx];
+                }
+            m.terrain[(size_t)(i - ng) + (size_t)(j - ng) * g._nx_] = (float)sum;
+        }
+    return ST_OK;
+}
+
+// z of every point below a surface of the reference's useTerrain path
+// (src/terrain.cpp:834-858), in double: -|Depth| + K (h + |Depth|) / (NZ - 1).
+static void terrain_z_double(Model &m)
+{
+    const Grid &g = m.g;
+    const double Depth = m.p.Depth * 1e3;
+    for (int k = 0; k < g._nz_; k++)
+        for (int j = 0; j < g._ny_; j++)
+            for (int i = 0; i < g._nx_; i++) {
+                const int K = k - HALO;
+                const double DZ = double(m.terrain[(size_t)i + (size_t)j * g._nx_] + std::fabs(Depth)) / double(g.NZ - 1);
+                m.coord[g.idx(i, j, k) * 3 + 2] = (float)(-std::fabs(Depth) + DZ * K);
+            }
+}
+
 // ----------------------------------------------------------------- medium
 // Longitude and latitude (degrees) of every column of the padded grid: the
 // inverse azimuthal-equidistant projection about the centre of the x, y of
@@ -235,11 +437,8 @@ static int column_lonlat(const Model &m, float lonMin, float lonMax, float latMi
                          std::vector<double> &lon, std::vector<double> &lat, std::string &err)
 {
     const Grid &g = m.g;
-    char buf[64];
-    std::snprintf(buf, sizeof buf, "%lf", (double)(float)m.p.centerLongitude);
-    const double lon0 = std::atof(buf) * (3.14159265358979323846 / 180.0);
-    std::snprintf(buf, sizeof buf, "%lf", (double)(float)m.p.centerLatitude);
-    const double lat0 = std::atof(buf) * (3.14159265358979323846 / 180.0);
+    double lon0, lat0;
+    proj_centre(m.p, &lon0, &lat0);
     const double r2d = 180.0 / (double)REF_PI;
     const int NX_ = m.p.NX + 2 * HALO, NY_ = m.p.NY + 2 * HALO;
     const int ox = g.originalX + HALO, oy = g.originalY + HALO;
@@ -268,22 +467,6 @@ static int column_lonlat(const Model &m, float lonMin, float lonMax, float latMi
             lat[(size_t)i + (size_t)j * g._nx_] = ph * r2d;
         }
     return ST_OK;
-}
-
-// Two-point Lagrange (bilinear) interpolation in double, the evaluation
-// order of src/terrain.cpp:563-600: z = {A, C, B, D} for the corners
-// (x1, y1), (x1, y2), (x2, y1), (x2, y2).
-static double interp2d(const double x[2], const double y[2], const double z[4], double x_, double y_)
-{
-    double Lx[2], Ly[2];
-    Lx[0] = 1.0 * (x_ - x[1]) / (x[0] - x[1]);
-    Lx[1] = 1.0 * (x_ - x[0]) / (x[1] - x[0]);
-    Ly[0] = 1.0 * (y_ - y[1]) / (y[0] - y[1]);
-    Ly[1] = 1.0 * (y_ - y[0]) / (y[1] - y[0]);
-    double Li = 0.0;
-    for (int jj = 0; jj < 2; jj++)
-        for (int ii = 0; ii < 2; ii++) Li = Li + Lx[ii] * Ly[jj] * z[ii * 2 + jj];
-    return Li;
 }
 
 // Weisen Shen's Vs model (src/dealMedium.cpp:49-360): one text file per
@@ -958,10 +1141,6 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
         err = "no source set";
         return ST_OPTIONS;
     }
-    if (p.useTerrain && p.terrainFile.empty()) {
-        err = "useTerrain (SRTM90 + PROJ) is not supported; give a raw height map as terrainFile";
-        return ST_OPTIONS;
-    }
     if (p.gauss_hill && !p.terrainFile.empty()) {
         err = "gauss_hill and terrainFile are exclusive";
         return ST_OPTIONS;
@@ -989,6 +1168,11 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
     if (p.gauss_hill) gauss_hill(m);
     else if (!p.terrainFile.empty()) {
         if ((st = terrain_file(m, join(run_dir, p.terrainFile), err))) return st;
+    }
+    if (p.useTerrain) {   // src/coord.cpp:325-328
+        if (p.SRTM90 == 1)
+            if ((st = srtm_terrain(m, run_dir, err))) return st;
+        terrain_z_double(m);
     }
     if ((st = build_medium(m, run_dir, err))) return st;
     if (!p.mediumFile.empty())

@@ -58,6 +58,8 @@ struct Params {
     float MLonStart = 0, MLatStart = 0, MLonEnd = 0, MLatEnd = 0, MLonStep = 0, MLatStep = 0;
     float MVeticalStep = 0, CrustLonStep = 0, CrustLatStep = 0;
     std::string MediumDir, CrustDir;
+    int SRTM90 = 0, lonStart = 0, latStart = 0, blockX = 1, blockY = 1;
+    std::string TerrainDir;
     std::string LayeredFileName;
     std::string OUT;
     float Depth = 0;
@@ -124,6 +126,7 @@ struct Model {
     int NT = 0;
     std::vector<float> coord;        // [_nz_][_ny_][_nx_][3] (AoS, reference layout)
     std::vector<float> terrain;      // [_ny_][_nx_]
+    std::vector<double> lon, lat;    // [_ny_][_nx_] column longitude, latitude (SRTM90 runs)
     std::vector<float> medium;       // [_nz_][_ny_][_nx_][3] Vs Vp rho
     float H_min = 0, H_max = 0, Vs_min = 0, Vs_max = 0, Vp_min = 0, Vp_max = 0, rho_min = 0, rho_max = 0;
     float dtmax = 0;

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <sys/stat.h>
 
 namespace cgfdm {
 
@@ -671,11 +672,15 @@ int Session::get_pgv(float *host) const
 
 // Output files of one rank in the reference's formats: station traces
 // (src/station.cpp:422-443) and peak ground velocity (src/PGV.cpp:177-185).
+// The directory is created when missing, as the reference creates OUT at
+// start-up (src/create_dir.cpp).
 std::string Session::out_dir() const
 {
     std::string out = m.p.OUT;
     if (out.empty()) out = "./output";
     if (out[0] != '/') out = run_dir + "/" + out;
+    for (size_t p = 1; p <= out.size(); p++)
+        if (p == out.size() || out[p] == '/') mkdir(out.substr(0, p).c_str(), 0755);
     return out;
 }
 
@@ -777,12 +782,38 @@ static int write_model_slices(const Model &m, const std::string &out)
     return ST_OK;
 }
 
+// The "projection data" of an SRTM90 run (src/terrain.cpp:49-118): longitude,
+// latitude and surface height of the interior columns, y outer, as float.
+static int write_projection(const Model &m, const std::string &out)
+{
+    if (!(m.p.useTerrain && m.p.SRTM90 == 1) || m.lon.empty()) return ST_OK;
+    const Grid &G = m.g;
+    std::vector<float> lon, lat, h;
+    for (int j = HALO; j < G._ny; j++)
+        for (int i = HALO; i < G._nx; i++) {
+            const size_t c = (size_t)i + (size_t)j * G._nx_;
+            lon.push_back((float)m.lon[c]);
+            lat.push_back((float)m.lat[c]);
+            h.push_back(m.terrain[c]);
+        }
+    const std::pair<const char *, const std::vector<float> *> files[3] = {{"lon", &lon}, {"lat", &lat}, {"terrain", &h}};
+    for (auto &f : files) {
+        std::string path = out + "/" + f.first + "_mpi_0_0_0.bin";
+        FILE *fp = std::fopen(path.c_str(), "wb");
+        if (!fp) return ST_IO;
+        std::fwrite(f.second->data(), sizeof(float), f.second->size(), fp);
+        std::fclose(fp);
+    }
+    return ST_OK;
+}
+
 int Session::write_outputs() const
 {
     const std::string out = out_dir();
     {
         int st = write_model_slices(m, out);
         if (st) return st;
+        if ((st = write_projection(m, out))) return st;
     }
     if (nst > 0) {
         std::vector<float> w((size_t)nst * m.NT * 9);

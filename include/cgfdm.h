@@ -77,6 +77,14 @@ int cgfdm_create(const char *run_dir, const char *options_json, int device, cgfd
  * cgfdm_last_error(NULL). */
 int cgfdm_model_medium(const char *run_dir, const char *options_json, float *out, long long count, int *dims);
 
+/* Host-only, as cgfdm_model_medium: the surface height of every column,
+ * [nyp][nxp] (gauss_hill, terrainFile or, with useTerrain and SRTM90, the
+ * SRTM tiles of src/terrain.cpp:206-770), into `terrain`, and the grid's
+ * coordinates [nzp][nyp][nxp][3] (x, y, z) into `coord` (either may be
+ * NULL; counts in floats); dims as cgfdm_model_medium. */
+int cgfdm_model_coord(const char *run_dir, const char *options_json, float *terrain, long long terrain_count,
+                      float *coord, long long coord_count, int *dims);
+
 /* Advances up to `nsteps` time steps (clamped to NT).  One step is the body
  * of the time loop, src/propagate.cpp:186-321: source term into W, the RK
  * stages with derivative, free surface and PML, station recording and PGV. */

@@ -252,6 +252,8 @@ static bool oracle_read_raw(const std::string &path, float *dst, size_t n)
     return true;
 }
 
+static void oracle_dump(const char *name, const void *data, size_t bytes);
+
 void oracle_hook_constructCoord(MPI_Comm comm_cart, MPI_COORD thisMPICoord, GRID grid, PARAMS params, float *coord,
                                 float *cpu_coord, float *terrain, float *cpu_terrain)
 {
@@ -262,6 +264,10 @@ void oracle_hook_constructCoord(MPI_Comm comm_cart, MPI_COORD thisMPICoord, GRID
         construct_terrain_coord(cpu_coord, cpu_terrain, grid._nx_, grid._ny_, grid._nz_, grid.frontNZ, grid.NZ,
                                 params.Depth * 1000);
     }
+    /* the padded coordinates [_nz_][_ny_][_nx_][3] and surface [_ny_][_nx_] */
+    g_oracle_params = params;
+    oracle_dump("oracle_coord.bin", cpu_coord, sizeof(float) * 3 * (size_t)grid._nx_ * grid._ny_ * grid._nz_);
+    oracle_dump("oracle_terrain.bin", cpu_terrain, sizeof(float) * (size_t)grid._nx_ * grid._ny_);
 }
 
 void oracle_hook_constructMedium(MPI_COORD thisMPICoord, PARAMS params, GRID grid, float *cpu_coord,

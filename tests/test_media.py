@@ -142,3 +142,101 @@ def test_crust1_medium_host_matches_reference(tmp_path):
     ref = refrun.read_outputs(d)["CJM"][..., 10:13]
     assert np.unique(med[..., 0]).size > 20
     np.testing.assert_array_equal(_cjm_medium(med), ref)
+
+
+# ------------------------------------------------------------ SRTM terrain
+def write_srtm_tile(directory, lat, lon, seed=8):
+    """One synthetic SRTM90 tile "srtm_<lat>N<lon>E.bin": 6000 x 6000
+    float32 heights (m), longitude fastest, rows from the tile's southern
+    edge, 5/6000 degree apart; smooth hills plus scattered single-point
+    spikes around the tile's centre, which the despiking replaces."""
+    rng = np.random.default_rng(seed)
+    os.makedirs(directory, exist_ok=True)
+    n = 6000
+    x = (np.arange(n, dtype=np.float32) * np.float32(5.0 / n))
+    sx = np.sin(x * np.float32(2 * np.pi / 0.37)).astype(np.float32)
+    cy = np.cos(x * np.float32(2 * np.pi / 0.29)).astype(np.float32)
+    h = np.float32(1200) + np.float32(600) * cy[:, None] * sx[None, :]
+    h += np.float32(150) * np.sin(x * np.float32(2 * np.pi / 0.05)).astype(np.float32)[None, :]
+    ii = rng.integers(2850, 3150, 3000)
+    jj = rng.integers(2850, 3150, 3000)
+    h[jj, ii] += rng.choice([-400.0, 400.0], 3000).astype(np.float32)
+    h.astype(np.float32).tofile(os.path.join(directory, f"srtm_{lat}N{lon}E.bin"))
+
+
+def _terrain_case(kind):
+    c = pu.small_halfspace(steps=2, NX=60, NY=50, NZ=40, DH=200.0, vp=8500.0)
+    c.fault = []
+    c.double_couple = dict(X=30, Y=25, Z=30, strike=30.0, dip=60.0, rake=90.0, Mw=4.0, duration=0.3)
+    c.stations = [(20, 20, c.NZ - 1), (40, 30, c.NZ - 1)]
+    c.layers = ()
+    c.center_lon, c.center_lat = 102.5, 32.5
+    c.extra = dict(c.extra, useTerrain=1, SRTM90=int(kind == "srtm"), TerrainDir="./terrain",
+                   lonStart=100, latStart=30, blockX=1, blockY=1)
+    if kind == "gauss":
+        c.gauss_hill = 1
+    return c
+
+
+@pytest.mark.parametrize("kind", ["flat", "gauss", "srtm"])
+def test_terrain_host_matches_reference(tmp_path, kind):
+    """useTerrain (src/coord.cpp:325-328, src/terrain.cpp:772-858) on the
+    CPU: the SRTM90 surface (tiles read, despiked and smoothed around the
+    model, interpolated to every column and smoothed again) and the
+    terrain-following z of every point, against the reference's CPU build,
+    bit for bit; "flat" and "gauss" apply only the z mapping."""
+    from cgfdm import model_coord
+
+    if not refrun.available("CGFDM"):
+        pytest.skip("reference CPU build not present")
+    c = _terrain_case(kind)
+    d = cases.write_case(c, str(tmp_path / "run"))
+    if kind == "srtm":
+        write_srtm_tile(os.path.join(d, "terrain"), 30, 100)
+    terrain, coord = model_coord(d)
+    refrun.run(d, "CGFDM")
+    out = os.path.join(d, "output")
+    ref_coord = np.fromfile(os.path.join(out, "oracle_coord.bin"), np.float32).reshape(coord.shape)
+    ref_terrain = np.fromfile(os.path.join(out, "oracle_terrain.bin"), np.float32).reshape(terrain.shape)
+    np.testing.assert_array_equal(coord, ref_coord)
+    np.testing.assert_array_equal(terrain, ref_terrain)
+    if kind == "srtm":
+        assert np.unique(terrain).size > 1000 and terrain.max() - terrain.min() > 100.0
+        written = np.fromfile(os.path.join(out, "terrain_mpi_0_0_0.bin"), np.float32)
+        np.testing.assert_array_equal(written.reshape(c.NY, c.NX), terrain[3:-3, 3:-3])
+
+
+def test_srtm_outside_tiles_is_an_error(tmp_path):
+    """A model whose corners leave the tiles fails as the reference aborts
+    (error 1001, src/terrain.cpp:512-519)."""
+    from cgfdm import CgfdmError, model_coord
+
+    c = _terrain_case("srtm")
+    c.center_lon = 100.02
+    d = cases.write_case(c, str(tmp_path / "run"))
+    write_srtm_tile(os.path.join(d, "terrain"), 30, 100)
+    with pytest.raises(CgfdmError):
+        model_coord(d)
+
+
+@pytest.mark.gpu
+def test_srtm_terrain_metrics_match_reference(tmp_path):
+    """The SRTM90 surface through the whole setup on the GPU: the packed
+    metric and medium (CJM) of the exact build against the reference's."""
+    if not refrun.available("CGFDM"):
+        pytest.skip("reference CPU build not present")
+    c = _terrain_case("srtm")
+    d = cases.write_case(c, str(tmp_path / "run"))
+    write_srtm_tile(os.path.join(d, "terrain"), 30, 100)
+    refrun.run(d, "CGFDM")
+    ref = refrun.read_outputs(d)["CJM"]
+    ref_out = os.path.join(d, "output")
+    mine_out = os.path.join(d, "mine")
+    with Session(d, options='{"OUT": "%s"}' % mine_out, flavor="exact") as s:
+        mine = s.cjm()
+        s.write_outputs()
+    np.testing.assert_array_equal(mine, ref)
+    for name in ("lon", "lat", "terrain"):   # the projection data files
+        f = f"{name}_mpi_0_0_0.bin"
+        a = np.fromfile(os.path.join(mine_out, f), np.float32)
+        np.testing.assert_array_equal(a, np.fromfile(os.path.join(ref_out, f), np.float32), err_msg=f)
