@@ -74,6 +74,7 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
     L.cgfdm_get_wavefield.argtypes = [vp, fp, ctypes.c_longlong]
     L.cgfdm_get_cjm.argtypes = [vp, fp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int)]
     L.cgfdm_get_pgv.argtypes = [vp, fp, ctypes.c_longlong]
+    L.cgfdm_get_array.argtypes = [vp, ctypes.c_char_p, vp, ctypes.POINTER(ctypes.c_longlong)]
     L.cgfdm_write_outputs.argtypes = [vp]
     L.cgfdm_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.cgfdm_checkpoint.argtypes = [vp, vp, ctypes.c_longlong]
@@ -213,6 +214,19 @@ class Session:
         i = self.info
         out = np.zeros((i.ny, i.nx, i.pgv_fields), np.float32)
         self._check(self.L.cgfdm_get_pgv(self._h, _fptr(out), out.size))
+        return out
+
+    _ARRAY_DTYPES = {"srcIndex": np.int64, "stationXYZ": np.int32}
+
+    def array(self, name: str) -> np.ndarray:
+        """A model array in the reference's layout (cgfdm_get_array): rDZ_DX,
+        rDZ_DY, pml_{alpha,beta,d}_{x,y,z}, srcIndex, momentRate, stationXYZ."""
+        n = ctypes.c_longlong(0)
+        self._check(self.L.cgfdm_get_array(self._h, name.encode(), None, ctypes.byref(n)))
+        dt = np.dtype(self._ARRAY_DTYPES.get(name, np.float32))
+        out = np.zeros(n.value // dt.itemsize, dt)
+        self._check(self.L.cgfdm_get_array(self._h, name.encode(), out.ctypes.data_as(ctypes.c_void_p),
+                                           ctypes.byref(n)))
         return out
 
     def write_outputs(self) -> None:

@@ -174,6 +174,12 @@ int cgfdm_get_pgv(const cgfdm_session *s, float *out, long long count)
     return s->s.get_pgv(out);
 }
 
+int cgfdm_get_array(cgfdm_session *s, const char *name, void *out, long long *bytes)
+{
+    if (!s || !name || !bytes) return CGFDM_E_ARG;
+    return s->s.get_array(name, out, bytes);
+}
+
 int cgfdm_write_outputs(const cgfdm_session *s)
 {
     if (!s) return CGFDM_E_ARG;

@@ -32,6 +32,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include "cg_ops.cuh"
 #include "device.cuh"
 #include "kernels.cuh"
 
@@ -119,52 +120,6 @@ __device__ __forceinline__ void tma_prefetch_4d(const void *tmap, int x, int y, 
                      (unsigned long long)tmap),
                  "r"(x), "r"(y), "r"(z), "r"(f)
                  : "memory");
-}
-
-// ------------------------------------------------------------- operators
-// Contribution of one grid direction to the RHS, given the metric row
-// (xi, eta or zeta gradient) and the nine scaled derivatives along it
-// (src/wave_deriv.cpp:244-272; the same form in pml_deriv and
-// pml_free_surface).  out: Vx Vy Vz Txx Tyy Tzz Txy Txz Tyz.
-__device__ __forceinline__ void dir_rhs(float m0, float m1, float m2, const float d[9], float mu, float lam,
-                                        float buo, float out[9])
-{
-    out[0] = ((m0 * d[3] + m1 * d[6]) + m2 * d[7]) * buo;
-    out[1] = ((m0 * d[6] + m1 * d[4]) + m2 * d[8]) * buo;
-    out[2] = ((m0 * d[7] + m1 * d[8]) + m2 * d[5]) * buo;
-    float dv = (m0 * d[0] + m1 * d[1]) + m2 * d[2];
-    float m2mu = 2.0f * mu;
-    out[3] = dv * lam + m2mu * (m0 * d[0]);
-    out[4] = dv * lam + m2mu * (m1 * d[1]);
-    out[5] = dv * lam + m2mu * (m2 * d[2]);
-    out[6] = (m1 * d[0] + m0 * d[1]) * mu;
-    out[7] = (m2 * d[0] + m0 * d[2]) * mu;
-    out[8] = (m2 * d[1] + m1 * d[2]) * mu;
-}
-
-// stress part only (components 3..8) from velocity derivatives v[0..2]
-__device__ __forceinline__ void dir_stress(float m0, float m1, float m2, const float v[3], float mu, float lam,
-                                           float out[9])
-{
-    float dv = (m0 * v[0] + m1 * v[1]) + m2 * v[2];
-    float m2mu = 2.0f * mu;
-    out[3] = dv * lam + m2mu * (m0 * v[0]);
-    out[4] = dv * lam + m2mu * (m1 * v[1]);
-    out[5] = dv * lam + m2mu * (m2 * v[2]);
-    out[6] = (m1 * v[0] + m0 * v[1]) * mu;
-    out[7] = (m2 * v[0] + m0 * v[2]) * mu;
-    out[8] = (m2 * v[1] + m1 * v[2]) * mu;
-}
-
-// One-sided 5-point operator of the L macro (src/axis.h:287):
-// FB * (af_1 w[-FB] + af0 w[0] + af1 w[FB] + af2 w[2FB] + af3 w[3FB]) * rDH
-__device__ __forceinline__ float lop(float wm, float w0, float w1, float w2, float w3, int FB, float rDH)
-{
-    float s = CG_AF_1 * wm + CG_AF0 * w0;
-    s = s + CG_AF1 * w1;
-    s = s + CG_AF2 * w2;
-    s = s + CG_AF3 * w3;
-    return ((float)FB * s) * rDH;
 }
 
 // Stencil taps in the ring: zp[m] points at this thread's cell of plane

@@ -36,6 +36,9 @@ public:
     int get_cjm(float *host_aos, int *nfield) const;  // [_nz_][_ny_][_nx_][nfield]
     int get_stations(float *host) const;            // [nst][NT][9]
     int get_pgv(float *host) const;                 // [ny][nx][pgv_fields()]
+    // model arrays in the reference's layouts, by name (csrc/shims.cu);
+    // out NULL: the size in *bytes
+    int get_array(const char *name, void *out, long long *bytes);
     int pgv_fields() const { return pga_ ? 4 : 2; } // PGVh, PGV (+ PGAh, PGA)
     int write_outputs() const;
     int sync() const;

@@ -85,6 +85,17 @@ int cgfdm_model_medium(const char *run_dir, const char *options_json, float *out
 int cgfdm_model_coord(const char *run_dir, const char *options_json, float *terrain, long long terrain_count,
                       float *coord, long long coord_count, int *dims);
 
+/* The session's model arrays in the reference's device layouts, for a
+ * caller that drives the per-function entry points of cgfdm_shims.h:
+ * "rDZ_DX", "rDZ_DY" (float [_ny_][_nx_][9]); "pml_alpha_x", "pml_beta_x",
+ * "pml_d_x" and the same for y, z (float [_nx_], [_ny_], [_nz_]);
+ * "srcIndex" (int64 [npts], padded-grid point index of each finite-fault
+ * cell) and "momentRate" (float [nt][npts][6], before calculateMomentRate);
+ * "stationXYZ" (int32 [n][3], padded indices).  Host copies: `out` NULL
+ * writes the size in bytes to *bytes; otherwise *bytes is the capacity of
+ * `out` on entry and the size on return. */
+int cgfdm_get_array(cgfdm_session *s, const char *name, void *out, long long *bytes);
+
 /* Advances up to `nsteps` time steps (clamped to NT).  One step is the body
  * of the time loop, src/propagate.cpp:186-321: source term into W, the RK
  * stages with derivative, free surface and PML, station recording and PGV. */
