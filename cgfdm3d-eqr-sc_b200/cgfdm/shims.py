@@ -1,7 +1,9 @@
 """ctypes binding of the per-function entry points (include/cgfdm_shims.h):
 the reference's step drivers -- waveDeriv, freeSurfaceDeriv, pmlDeriv,
 pmlFreeSurfaceDeriv, waveRk, pmlRk, calculateMomentRate, addMomenteRate,
-storageStation, comparePGV, SolveDisplacement, storage_W_pre -- on device
+storageStation, comparePGV, SolveDisplacement, storage_W_pre and, for
+ME-AWENO, waveDeriv_alternative_flux_FD, waveRk_tvd, charfreeSurfaceDeriv,
+expDecayLayers -- on device
 arrays in the reference's layouts, here torch CUDA tensors.  Argument names
 and meanings are the reference's (src/propagate.cpp:186-309); the grid is
 passed as the padded sizes (_nx_, _ny_, _nz_).  Errors raise CgfdmError
@@ -25,12 +27,16 @@ _SIGS = {
     "cgfdm_pmlFreeSurfaceDeriv": [_i, _i, _i, _i, _f, _p, _p, _pp, _p, _p, _p, _p, _ip, _i, _i, _f, _p],
     "cgfdm_waveRk": [_i, _i, _i, _i, _p, _p, _p, _p, _p],
     "cgfdm_pmlRk": [_i, _i, _i, _i, _i, _pp, _ip, _i, _p],
-    "cgfdm_calculateMomentRate": [_ll, _ll, _p, _p, _p, _f, _p],
+    "cgfdm_calculateMomentRate": [_ll, _ll, _p, _p, _p, _f, _i, _p],
     "cgfdm_addMomenteRate": [_ll, _i, _f, _p, _p, _p, _p, _i, _i, _f, _i, _p, _p],
     "cgfdm_storageStation": [_i, _i, _i, _i, _i, _p, _p, _p, _i, _i, _p, _p],
     "cgfdm_comparePGV": [_i, _i, _i, _p, _p, _f, _i, _i, _p, _p, _p],
     "cgfdm_SolveDisplacement": [_i, _i, _i, _p, _p, _i, _p, _f, _p],
     "cgfdm_storage_W_pre": [_i, _i, _i, _p, _p, _p],
+    "cgfdm_waveDeriv_alternative_flux_FD": [_i, _i, _i, _f, _p, _p, _p, _p, _f, _f, _p],
+    "cgfdm_waveRk_tvd": [_i, _i, _i, _i, _p, _p, _p, _p],
+    "cgfdm_charfreeSurfaceDeriv": [_i, _i, _i, _p, _p, _p],
+    "cgfdm_expDecayLayers": [_i, _i, _i, _p, _i, _p],
 }
 
 
@@ -84,8 +90,9 @@ class Shims:
         self._call("cgfdm_pmlRk", nx, ny, nz, nPML, irk, _ptrs(aux), (ctypes.c_int * 6)(*border),
                    int(free_surface), stream)
 
-    def calculateMomentRate(self, npts, nt, CJM, momentRate, srcIndex, DH, stream=None):
-        self._call("cgfdm_calculateMomentRate", npts, nt, _ptr(CJM), _ptr(momentRate), _ptr(srcIndex), DH, stream)
+    def calculateMomentRate(self, npts, nt, CJM, momentRate, srcIndex, DH, scheme=0, stream=None):
+        self._call("cgfdm_calculateMomentRate", npts, nt, _ptr(CJM), _ptr(momentRate), _ptr(srcIndex), DH, scheme,
+                   stream)
 
     def addMomenteRate(self, npts, nt, dt, W, srcIndex, momentRate, momentRateSlice, it, irk, DT, scheme=0,
                        CJM=None, stream=None):
@@ -105,6 +112,19 @@ class Shims:
 
     def storage_W_pre(self, g, W_pre, W, stream=None):
         self._call("cgfdm_storage_W_pre", *g, _ptr(W_pre), _ptr(W), stream)
+
+    def waveDeriv_alternative_flux_FD(self, g, h_W, W, Riemann_flux, CJM, alpha, DT, stream=None):
+        self._call("cgfdm_waveDeriv_alternative_flux_FD", *g, g.rDH, _ptr(h_W), _ptr(W), _ptr(Riemann_flux),
+                   _ptr(CJM), alpha, DT, stream)
+
+    def waveRk_tvd(self, g, irk, h_W, W, m_W, stream=None):
+        self._call("cgfdm_waveRk_tvd", *g, irk, _ptr(h_W), _ptr(W), _ptr(m_W), stream)
+
+    def charfreeSurfaceDeriv(self, g, W, CJM, stream=None):
+        self._call("cgfdm_charfreeSurfaceDeriv", *g, _ptr(W), _ptr(CJM), stream)
+
+    def expDecayLayers(self, g, W, free_surface=True, stream=None):
+        self._call("cgfdm_expDecayLayers", *g, _ptr(W), int(free_surface), stream)
 
 
 class Grid(tuple):

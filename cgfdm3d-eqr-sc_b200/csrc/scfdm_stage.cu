@@ -42,6 +42,7 @@
 // the flux-difference corrections into one six-tap filter.
 #include "device.cuh"
 #include "kernels.cuh"
+#include "sc_ops.cuh"
 
 namespace cgfdm {
 
@@ -50,30 +51,7 @@ namespace {
 constexpr int SC_THREADS = 256;
 
 // ------------------------------------------------------------ WENO5-JS
-#ifdef CGFDM_EXACT
-// The reference's WENO5_JS term by term (src/alternative_flux_FD.cpp:42-59):
-// float polynomials, double (beta + 1e-6)^2 and the division by it.
-__device__ __forceinline__ float weno5_ref(float u1, float u2, float u3, float u4, float u5)
-{
-    float b1 = 10.0f * u3 * u3 - 31.0f * u3 * u4 + 25.0f * u4 * u4 + 11.0f * u3 * u5 - 19.0f * u4 * u5 +
-               4.0f * u5 * u5;
-    float b2 = 4.0f * u2 * u2 - 13.0f * u2 * u3 + 13.0f * u3 * u3 + 5.0f * u2 * u4 - 13.0f * u3 * u4 +
-               4.0f * u4 * u4;
-    float b3 = 4.0f * u1 * u1 - 19.0f * u1 * u2 + 25.0f * u2 * u2 + 11.0f * u1 * u3 - 31.0f * u2 * u3 +
-               10.0f * u3 * u3;
-    b1 = 0.3333333333f * b1;
-    b2 = 0.3333333333f * b2;
-    b3 = 0.3333333333f * b3;
-    double e1 = __dadd_rn((double)b1, 1e-6), e2 = __dadd_rn((double)b2, 1e-6), e3 = __dadd_rn((double)b3, 1e-6);
-    b1 = __double2float_rn(__ddiv_rn(0.3125, __dmul_rn(e1, e1)));
-    b2 = __double2float_rn(__ddiv_rn(0.625, __dmul_rn(e2, e2)));
-    b3 = __double2float_rn(__ddiv_rn(0.0625, __dmul_rn(e3, e3)));
-    float tw = __fdiv_rn(1.0f, b1 + b2 + b3);
-    return (b1 * tw) * (0.375f * u3 + 0.75f * u4 - 0.125f * u5) +
-           (b2 * tw) * (-0.125f * u2 + 0.75f * u3 + 0.375f * u4) +
-           (b3 * tw) * (0.375f * u1 - 1.25f * u2 + 1.875f * u3);
-}
-#else
+#ifndef CGFDM_EXACT
 __device__ __forceinline__ float rcp_approx(float x)
 {
     float r;
@@ -119,32 +97,12 @@ __device__ __forceinline__ void weno_pair(float a, float b, float c, float d, fl
 #endif
 }
 
-// Physical flux along the metric row (n0, n1, n2) of the state u
-// (src/alternative_flux_FD.cpp:146-154; the same form is hu at 1259-1268).
-__device__ __forceinline__ void point_flux(float n0, float n1, float n2, float lam, float mu, float buo,
-                                           const float u[9], float f[9])
-{
-    f[0] = -(n0 * (lam * u[4] + lam * u[5] + u[3] * (lam + 2.0f * mu)) + mu * n1 * u[8] + mu * n2 * u[7]);
-    f[1] = -(n1 * (lam * u[3] + lam * u[5] + u[4] * (lam + 2.0f * mu)) + mu * n0 * u[8] + mu * n2 * u[6]);
-    f[2] = -(n2 * (lam * u[3] + lam * u[4] + u[5] * (lam + 2.0f * mu)) + mu * n0 * u[7] + mu * n1 * u[6]);
-    f[3] = -((n0 * u[0]) * buo);
-    f[4] = -((n1 * u[1]) * buo);
-    f[5] = -((n2 * u[2]) * buo);
-    f[6] = -((n1 * u[2]) * buo + (n2 * u[1]) * buo);
-    f[7] = -((n0 * u[2]) * buo + (n2 * u[0]) * buo);
-    f[8] = -((n0 * u[1]) * buo + (n1 * u[0]) * buo);
-}
-
 // Lax-Friedrichs flux of a face from its left (uL) and right (uR) states.
 __device__ __forceinline__ void lf_flux(float n0, float n1, float n2, float lam, float mu, float buo, float alpha,
                                         const float uL[9], const float uR[9], float F[9])
 {
 #ifdef CGFDM_EXACT
-    float fL[9], fR[9];
-    point_flux(n0, n1, n2, lam, mu, buo, uL, fL);
-    point_flux(n0, n1, n2, lam, mu, buo, uR, fR);
-#pragma unroll
-    for (int v = 0; v < 9; v++) F[v] = 0.5f * (fR[v] + fL[v] - alpha * (uR[v] - uL[v]));
+    lf_flux_ref(n0, n1, n2, lam, mu, buo, alpha, uL, uR, F);
 #else
     // the flux is linear in the state: f(uL) + f(uR) = f(uL + uR)
     float s[9], fs[9];
@@ -236,12 +194,7 @@ __device__ __noinline__ void surface_diff(const ScDirArgs &a, long long q, long 
 __device__ __forceinline__ float interior_diff(const float f[6], float coef)
 {
 #ifdef CGFDM_EXACT
-    const float c24 = 1.0f / 24, c7 = 7.0f / 5760;
-    const float A = f[3] - c24 * ((1.0f / 12) * ((((-f[1] + 16.0f * f[2]) - 30.0f * f[3]) + 16.0f * f[4]) - f[5])) +
-                    c7 * ((((f[1] - 4.0f * f[2]) + 6.0f * f[3]) - 4.0f * f[4]) + f[5]);
-    const float B = f[2] - c24 * ((1.0f / 12) * ((((-f[0] + 16.0f * f[1]) - 30.0f * f[2]) + 16.0f * f[3]) - f[4])) +
-                    c7 * ((((f[0] - 4.0f * f[1]) + 6.0f * f[2]) - 4.0f * f[3]) + f[4]);
-    return coef * (-(A - B));
+    return interior_diff_ref(f, coef);
 #else
     // corrected face flux Fh = c2 F-2 + c1 F-1 + c0 F0 + c1 F+1 + c2 F+2 with
     // c0 = 6402/5760, c1 = -348/5760, c2 = 27/5760; val = -coef (Fh[p] - Fh[p-1])
@@ -451,80 +404,13 @@ __global__ void k_sc_surface(float *W, const float *__restrict__ cjm, DevGrid g,
     const long long F = g.fstride;
     const long long q = g.at(i, j, _nz - 1);
     const float mu = cjm[C_MU * F + q], lam = cjm[C_LAMBDA * F + q], buo = cjm[C_BUOY * F + q];
-    const float rho = 1.0f / buo;
-    const float vs = sqrtf(mu * buo), vp = sqrtf((lam + 2.0f * mu) * buo);
-
-    // orthonormalised surface normal and the two tangent directions
-    const double jac = cjm[C_JAC * F + q];
-    double n[3] = {cjm[C_ZT_X * F + q] / jac, cjm[C_ZT_Y * F + q] / jac, cjm[C_ZT_Z * F + q] / jac};
-    double s[3] = {cjm[C_X_XI * F + q], cjm[C_Y_XI * F + q], cjm[C_Z_XI * F + q]};
-    double t[3] = {cjm[C_X_ET * F + q], cjm[C_Y_ET * F + q], cjm[C_Z_ET * F + q]};
-    auto normalise = [](double *x) {
-        double r = 1.0 / sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
-        x[0] *= r, x[1] *= r, x[2] *= r;
-    };
-    normalise(n), normalise(s), normalise(t);
-    auto cross = [](const double *x, const double *y, double *o) {
-        o[0] = x[1] * y[2] - x[2] * y[1];
-        o[1] = x[2] * y[0] - x[0] * y[2];
-        o[2] = x[0] * y[1] - x[1] * y[0];
-    };
-    // rows of B^-1: (s x t, t x n, n x s) / det
-    double R[3][3];
-    cross(s, t, R[0]), cross(t, n, R[1]), cross(n, s, R[2]);
-    const double det = n[0] * R[0][0] + n[1] * R[0][1] + n[2] * R[0][2];
-    for (int r = 0; r < 3; r++)
-        for (int c = 0; c < 3; c++) R[r][c] /= det;
-
-    // conservative -> physical: stress from strain, velocity from momentum
-    double u[9];
+    float u[9], o[9];
     for (int v = 0; v < 9; v++) u[v] = W[v * F + q];
-    const double L = lam, M = mu, Bu = buo;
-    const double tr = u[3] + u[4] + u[5];
-    double S[3][3];
-    S[0][0] = L * tr + 2.0 * M * u[3];
-    S[1][1] = L * tr + 2.0 * M * u[4];
-    S[2][2] = L * tr + 2.0 * M * u[5];
-    S[0][1] = S[1][0] = M * u[8];
-    S[0][2] = S[2][0] = M * u[7];
-    S[1][2] = S[2][1] = M * u[6];
-    const double vel[3] = {u[0] * Bu, u[1] * Bu, u[2] * Bu};
-
-    // into the (n, s, t) basis
-    double RS[3][3], T[3][3], vb[3];
-    for (int r = 0; r < 3; r++)
-        for (int c = 0; c < 3; c++) RS[r][c] = R[r][0] * S[0][c] + R[r][1] * S[1][c] + R[r][2] * S[2][c];
-    for (int r = 0; r < 3; r++)
-        for (int c = 0; c < 3; c++) T[r][c] = RS[r][0] * R[c][0] + RS[r][1] * R[c][1] + RS[r][2] * R[c][2];
-    for (int r = 0; r < 3; r++) vb[r] = R[r][0] * vel[0] + R[r][1] * vel[1] + R[r][2] * vel[2];
-
-    // characteristic free-surface condition (src/freeSurface.cpp:142-150)
-    const double rho_d = rho, vs_d = vs, vp_d = vp;
-    const double ratio = L / (L + 2.0 * M);
-    T[1][1] -= T[0][0] * ratio;
-    T[2][2] -= T[0][0] * ratio;
-    vb[1] -= T[0][1] / (vs_d * rho_d);
-    vb[2] -= T[0][2] / (vs_d * rho_d);
-    vb[0] -= T[0][0] / (vp_d * rho_d);
-    T[0][0] = 0.0, T[0][1] = T[1][0] = 0.0, T[0][2] = T[2][0] = 0.0;
-
-    // back: sigma = B T B^T, v = B v'
-    const double Bm[3][3] = {{n[0], s[0], t[0]}, {n[1], s[1], t[1]}, {n[2], s[2], t[2]}};
-    double BT[3][3], Sg[3][3], v2[3];
-    for (int r = 0; r < 3; r++)
-        for (int c = 0; c < 3; c++) BT[r][c] = Bm[r][0] * T[0][c] + Bm[r][1] * T[1][c] + Bm[r][2] * T[2][c];
-    for (int r = 0; r < 3; r++)
-        for (int c = 0; c < 3; c++) Sg[r][c] = BT[r][0] * Bm[c][0] + BT[r][1] * Bm[c][1] + BT[r][2] * Bm[c][2];
-    for (int r = 0; r < 3; r++) v2[r] = Bm[r][0] * vb[0] + Bm[r][1] * vb[1] + Bm[r][2] * vb[2];
-
-    // physical -> conservative: momentum, and strain by the isotropic compliance
-    const double comp = 1.0 / (2.0 * M * (3.0 * L + 2.0 * M));
-    const double strace = Sg[0][0] + Sg[1][1] + Sg[2][2];
-    double o[9];
-    o[0] = v2[0] * rho_d, o[1] = v2[1] * rho_d, o[2] = v2[2] * rho_d;
-    for (int d = 0; d < 3; d++) o[3 + d] = (2.0 * (L + M) * Sg[d][d] - L * (strace - Sg[d][d])) * comp;
-    o[6] = Sg[1][2] / M, o[7] = Sg[0][2] / M, o[8] = Sg[0][1] / M;
-    for (int v = 0; v < 9; v++) W[v * F + q] = (float)o[v];
+    const float nrm[3] = {cjm[C_ZT_X * F + q], cjm[C_ZT_Y * F + q], cjm[C_ZT_Z * F + q]};
+    const float tan1[3] = {cjm[C_X_XI * F + q], cjm[C_Y_XI * F + q], cjm[C_Z_XI * F + q]};
+    const float tan2[3] = {cjm[C_X_ET * F + q], cjm[C_Y_ET * F + q], cjm[C_Z_ET * F + q]};
+    char_surface_point(u, mu, lam, buo, cjm[C_JAC * F + q], nrm, tan1, tan2, o);
+    for (int v = 0; v < 9; v++) W[v * F + q] = o[v];
 
     // cubic extrapolation into the three halo layers above
     // (src/freeSurface.cpp:180-190: extrap3 = 4 k1 - 6 k2 + 4 k3 - k4)

@@ -15,12 +15,14 @@
 #include "../../include/cgfdm.h"
 #include "../../include/cgfdm_shims.h"
 
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "cg_ops.cuh"
 #include "device.cuh"
+#include "sc_ops.cuh"
 #include "kernels.cuh"
 #include "session.hpp"
 
@@ -237,14 +239,14 @@ __global__ void k_rk(float *__restrict__ h_W, float *__restrict__ W, float *__re
 }
 
 // ------------------------------------------------- src/addMoment.cpp:25-223
-__global__ void k_calc_moment_rate(long long npts, long long nt, const float *__restrict__ CJM, float *rate,
-                                   const long long *__restrict__ idx, float DH)
+__global__ void k_calc_moment_rate(long long npts, long long nt, const float *__restrict__ CJM, int nfield,
+                                   float *rate, const long long *__restrict__ idx, float DH)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long t = (long long)blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= npts || t >= nt) return;
     const long long q = idx[i];
-    const float jac = CJM[q * 13 + C_JAC], mu = CJM[q * 13 + C_MU];
+    const float jac = CJM[q * nfield + C_JAC], mu = CJM[q * nfield + C_MU];
     float V = jac * DH * DH * DH;
     V = (float)(1.0 / (double)V);
     V = V * 1.0f;   // * Cv (= 1)
@@ -374,6 +376,156 @@ __global__ void k_copy_prefix(float *__restrict__ dst, const float *__restrict__
 {
     const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (x < n) dst[x] = src[x];
+}
+
+// ====================================================== ME-AWENO (SCFDM)
+// CJM has 19 fields per point here (src/macro.h:56-60).
+#define SC_NF 19
+
+// --------------------------------- src/alternative_flux_FD.cpp:61-399 (LF)
+// Lax-Friedrichs flux of the face between the points q and q + step, stored
+// at q; along DIR the faces from index HALO - 1, across it the interior.
+__global__ void k_sc_flux(float *__restrict__ RF, const float *__restrict__ W, const float *__restrict__ CJM, Aos a,
+                          int dir, float alpha)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + HALO_ - (dir == 0);
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + HALO_ - (dir == 1);
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + HALO_ - (dir == 2);
+    if (i >= a.nx_ - HALO_ || j >= a.ny_ - HALO_ || k >= a.nz_ - HALO_) return;
+    const long long q = a.at(i, j, k);
+    const long long s = dir == 0 ? 1 : dir == 1 ? (long long)a.nx_ : (long long)a.nx_ * a.ny_;
+    const float *c = CJM + q * SC_NF;
+    float uL[9], uR[9], F[9];
+    for (int v = 0; v < 9; v++) {
+        const float w_2 = W[(q - 2 * s) * 9 + v], w_1 = W[(q - s) * 9 + v], w0 = W[q * 9 + v];
+        const float w1 = W[(q + s) * 9 + v], w2 = W[(q + 2 * s) * 9 + v], w3 = W[(q + 3 * s) * 9 + v];
+        uL[v] = weno5_ref(w_2, w_1, w0, w1, w2);
+        uR[v] = weno5_ref(w3, w2, w1, w0, w_1);
+    }
+    lf_flux_ref(c[3 * dir + 0], c[3 * dir + 1], c[3 * dir + 2], c[C_LAMBDA], c[C_MU], c[C_BUOY], alpha, uL, uR, F);
+    for (int v = 0; v < 9; v++) RF[q * 9 + v] = F[v];
+}
+
+// ---------------------------------- src/alternative_flux_FD.cpp:1215-1435
+// Flux difference of the interior points along DIR: h_W = (x) or += (y, z)
+// DT rDH / J times the corrected difference; in the top three layers the
+// corrections come from point fluxes (the surface variant).
+__global__ void k_sc_du(float *__restrict__ h_W, const float *__restrict__ RF, const float *__restrict__ W,
+                        const float *__restrict__ CJM, Aos a, int dir, float rDH, float DT)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + HALO_;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + HALO_;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + HALO_;
+    const int _nz = a.nz_ - HALO_;
+    if (i >= a.nx_ - HALO_ || j >= a.ny_ - HALO_ || k >= _nz) return;
+    const long long q = a.at(i, j, k);
+    const long long s = dir == 0 ? 1 : dir == 1 ? (long long)a.nx_ : (long long)a.nx_ * a.ny_;
+    const float jac = (float)(1.0 / (double)CJM[q * SC_NF + C_JAC]);
+    const float coef = DT * rDH * jac;
+    float val[9];
+    if (k >= _nz - 3) {
+        float hu[7][9];
+        for (int n = 0; n < 7; n++) {
+            const long long qn = q + (n - 3) * s;
+            const float *c = CJM + qn * SC_NF;
+            point_flux(c[3 * dir + 0], c[3 * dir + 1], c[3 * dir + 2], c[C_LAMBDA], c[C_MU], c[C_BUOY], W + qn * 9,
+                       hu[n]);
+        }
+        auto o2 = [&](int b, int v) {   // -5 u1 + 39 u2 - 34 u3 - 34 u4 + 39 u5 - 5 u6
+            return ((((-5.0f * hu[b][v] + 39.0f * hu[b + 1][v]) - 34.0f * hu[b + 2][v]) - 34.0f * hu[b + 3][v]) +
+                    39.0f * hu[b + 4][v]) -
+                   5.0f * hu[b + 5][v];
+        };
+        auto o4 = [&](int b, int v) {   // u1 - 3 u2 + 2 u3 + 2 u4 - 3 u5 + u6
+            return ((((hu[b][v] - 3.0f * hu[b + 1][v]) + 2.0f * hu[b + 2][v]) + 2.0f * hu[b + 3][v]) -
+                    3.0f * hu[b + 4][v]) +
+                   hu[b + 5][v];
+        };
+        const float c24 = 1.0f / 24, c7 = 7.0f / 5760;
+        for (int v = 0; v < 9; v++) {
+            const float A = RF[q * 9 + v] - c24 * ((1.0f / 48) * o2(1, v)) + c7 * ((1.0f / 2) * o4(1, v));
+            const float B = RF[(q - s) * 9 + v] - c24 * ((1.0f / 48) * o2(0, v)) + c7 * ((1.0f / 2) * o4(0, v));
+            val[v] = coef * (-(A - B));
+        }
+    } else {
+        for (int v = 0; v < 9; v++) {
+            float f[6];
+            for (int m = 0; m < 6; m++) f[m] = RF[(q + (m - 3) * s) * 9 + v];
+            val[v] = interior_diff_ref(f, coef);
+        }
+    }
+    for (int v = 0; v < 9; v++) h_W[q * 9 + v] = dir == 0 ? val[v] : h_W[q * 9 + v] + val[v];
+}
+
+// ------------------------------------------------ src/wave_rk_tvd.cpp:17-78
+__global__ void k_tvd(const float *__restrict__ h_W, float *__restrict__ W, float *__restrict__ m_W, long long n,
+                      int irk)
+{
+    const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= n) return;
+    const float h = h_W[x], w = W[x];
+    if (irk == 0) {
+        m_W[x] = w;
+        W[x] = w + h;
+    } else if (irk == 1) {
+        const double m = m_W[x];
+        W[x] = __double2float_rn(
+            __dadd_rn(__dadd_rn(__dmul_rn(0.75, m), __dmul_rn(0.25, (double)w)), __dmul_rn(0.25, (double)h)));
+    } else {
+        const double m = m_W[x];
+        W[x] = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(1.0 / 3.0, m), __dmul_rn(2.0 / 3.0, (double)w)),
+                                           __dmul_rn(2.0 / 3.0, (double)h)));
+    }
+}
+
+// ------------------------------------------------ src/freeSurface.cpp:40-194
+__global__ void k_char_free_surface(float *__restrict__ W, const float *__restrict__ CJM, Aos a)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + HALO_;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + HALO_;
+    const int _nz = a.nz_ - HALO_;
+    if (i >= a.nx_ - HALO_ || j >= a.ny_ - HALO_) return;
+    const long long q = a.at(i, j, _nz - 1);
+    const float *c = CJM + q * SC_NF;
+    float u[9], o[9];
+    for (int v = 0; v < 9; v++) u[v] = W[q * 9 + v];
+    const float nrm[3] = {c[C_ZT_X], c[C_ZT_Y], c[C_ZT_Z]};
+    const float t1[3] = {c[C_X_XI], c[C_Y_XI], c[C_Z_XI]}, t2[3] = {c[C_X_ET], c[C_Y_ET], c[C_Z_ET]};
+    char_surface_point(u, c[C_MU], c[C_LAMBDA], c[C_BUOY], c[C_JAC], nrm, t1, t2, o);
+    for (int v = 0; v < 9; v++) W[q * 9 + v] = o[v];
+    // cubic extrapolation into the halo above: 4 k1 - 6 k2 + 4 k3 - k4
+    const long long P = (long long)a.nx_ * a.ny_;
+    for (int v = 0; v < 9; v++)
+        for (int h = 1; h <= HALO_; h++) {
+            const float *b = W + (q + (h - 1) * P) * 9 + v;
+            W[(q + h * P) * 9 + v] = 4.0f * b[0] - 6.0f * b[-P * 9] + 4.0f * b[-2 * P * 9] - b[-3 * P * 9];
+        }
+}
+
+// --------------------------------------------- src/exp_decay_absorb.cpp:19-106
+struct DecayTable {
+    float G[21];
+};
+
+__global__ void k_exp_decay(float *__restrict__ W, Aos a, DecayTable t, int nl, int free_surface)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + HALO_;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + HALO_;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + HALO_;
+    if (i >= a.nx_ - HALO_ || j >= a.ny_ - HALO_ || k >= a.nz_ - HALO_) return;
+    const int X = i - HALO_, Y = j - HALO_, Z = k - HALO_;
+    const int nx = a.nx_ - 2 * HALO_, ny = a.ny_ - 2 * HALO_, nz = a.nz_ - 2 * HALO_;
+    float *w = W + a.at(i, j, k) * 9;
+    float G[6];
+    int ng = 0;
+    if (X <= nl) G[ng++] = t.G[nl - X];
+    if (X >= nx - nl) G[ng++] = t.G[nl - (nx - X)];
+    if (Y <= nl) G[ng++] = t.G[nl - Y];
+    if (Y >= ny - nl) G[ng++] = t.G[nl - (ny - Y)];
+    if (Z <= nl) G[ng++] = t.G[nl - Z];
+    if (!free_surface && Z >= nz - nl) G[ng++] = t.G[nl - (nz - Z)];
+    for (int g = 0; g < ng; g++)
+        for (int v = 0; v < 9; v++) w[v] = w[v] * G[g];
 }
 
 // ------------------------------------------------------------ model arrays
@@ -567,13 +719,14 @@ int cgfdm_pmlRk(int nx, int ny, int nz, int nPML, int irk, float *const *aux, co
 }
 
 int cgfdm_calculateMomentRate(long long npts, long long nt, const float *CJM, float *momentRate,
-                              const long long *srcIndex, float DH, void *stream)
+                              const long long *srcIndex, float DH, int scheme, void *stream)
 {
     if (npts == 0) return ST_OK;
     if (npts < 0 || nt < 1 || !CJM || !momentRate || !srcIndex)
         return fail("cgfdm_calculateMomentRate: bad argument", ST_ARG);
     const dim3 t(16, 16, 1), b(blocks_for(npts, 16), blocks_for(nt, 16), 1);
-    k_calc_moment_rate<<<b, t, 0, (cudaStream_t)stream>>>(npts, nt, CJM, momentRate, srcIndex, DH);
+    k_calc_moment_rate<<<b, t, 0, (cudaStream_t)stream>>>(npts, nt, CJM, scheme == SCHEME_SCFDM ? SC_NF : 13,
+                                                          momentRate, srcIndex, DH);
     return launched("cgfdm_calculateMomentRate");
 }
 
@@ -631,6 +784,64 @@ int cgfdm_SolveDisplacement(int _nx_, int _ny_, int _nz_, const float *W, float 
     k_solve_displacement<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(W, Dis, CJM, 19, n, DT,
                                                                                scheme == SCHEME_SCFDM);
     return launched("cgfdm_SolveDisplacement");
+}
+
+int cgfdm_waveDeriv_alternative_flux_FD(int _nx_, int _ny_, int _nz_, float rDH, float *h_W, const float *W,
+                                        float *Riemann_flux, const float *CJM, float alpha, float DT, void *stream)
+{
+    if (!h_W || !W || !Riemann_flux || !CJM || !grid_ok(_nx_, _ny_, _nz_) || _nz_ < 4 * HALO_)
+        return fail("cgfdm_waveDeriv_alternative_flux_FD: bad argument", ST_ARG);
+    const Aos a{_nx_, _ny_, _nz_};
+    const dim3 t(32, 4, 4);
+    const int n[3] = {_nx_ - 2 * HALO_, _ny_ - 2 * HALO_, _nz_ - 2 * HALO_};
+    // x flux, x difference, y flux, y difference, z flux, z difference
+    // (src/alternative_flux_FD.cpp:1477-1537), one flux buffer
+    for (int dir = 0; dir < 3; dir++) {
+        const dim3 bf(blocks_for(n[0] + (dir == 0), 32), blocks_for(n[1] + (dir == 1), 4),
+                      blocks_for(n[2] + (dir == 2), 4));
+        k_sc_flux<<<bf, t, 0, (cudaStream_t)stream>>>(Riemann_flux, W, CJM, a, dir, alpha);
+        if (int st = launched("cgfdm_waveDeriv_alternative_flux_FD")) return st;
+        const dim3 bd(blocks_for(n[0], 32), blocks_for(n[1], 4), blocks_for(n[2], 4));
+        k_sc_du<<<bd, t, 0, (cudaStream_t)stream>>>(h_W, Riemann_flux, W, CJM, a, dir, rDH, DT);
+        if (int st = launched("cgfdm_waveDeriv_alternative_flux_FD")) return st;
+    }
+    return ST_OK;
+}
+
+int cgfdm_waveRk_tvd(int _nx_, int _ny_, int _nz_, int irk, const float *h_W, float *W, float *m_W, void *stream)
+{
+    if (!h_W || !W || !m_W || irk < 0 || irk > 2 || _nx_ < 1 || _ny_ < 1 || _nz_ < 1)
+        return fail("cgfdm_waveRk_tvd: bad argument", ST_ARG);
+    const long long n = (long long)_nx_ * _ny_ * _nz_ * 9;
+    k_tvd<<<blocks_for(n, 1024), 1024, 0, (cudaStream_t)stream>>>(h_W, W, m_W, n, irk);
+    return launched("cgfdm_waveRk_tvd");
+}
+
+int cgfdm_charfreeSurfaceDeriv(int _nx_, int _ny_, int _nz_, float *W, const float *CJM, void *stream)
+{
+    if (!W || !CJM || !grid_ok(_nx_, _ny_, _nz_) || _nz_ < 4 * HALO_)
+        return fail("cgfdm_charfreeSurfaceDeriv: bad argument", ST_ARG);
+    const dim3 t(32, 4, 1), b(blocks_for(_nx_ - 2 * HALO_, 32), blocks_for(_ny_ - 2 * HALO_, 4), 1);
+    k_char_free_surface<<<b, t, 0, (cudaStream_t)stream>>>(W, CJM, Aos{_nx_, _ny_, _nz_});
+    return launched("cgfdm_charfreeSurfaceDeriv");
+}
+
+int cgfdm_expDecayLayers(int _nx_, int _ny_, int _nz_, float *W, int free_surface, void *stream)
+{
+    if (!W || !grid_ok(_nx_, _ny_, _nz_)) return fail("cgfdm_expDecayLayers: bad argument", ST_ARG);
+    // 20 layers, alpha 0.015 (src/exp_decay_absorb.cpp:110-111); G[p] =
+    // exp(-(alpha p)^2) in float, as the reference's kernel evaluates it
+    DecayTable tab;
+    const int nl = 20;
+    const float alpha = (float)0.015;
+    for (int p = 0; p <= nl; p++) {
+        const float x = alpha * (float)p;
+        tab.G[p] = std::exp(-x * x);
+    }
+    const dim3 t(32, 4, 1);
+    const dim3 b(blocks_for(_nx_ - 2 * HALO_, 32), blocks_for(_ny_ - 2 * HALO_, 4), _nz_ - 2 * HALO_);
+    k_exp_decay<<<b, t, 0, (cudaStream_t)stream>>>(W, Aos{_nx_, _ny_, _nz_}, tab, nl, free_surface);
+    return launched("cgfdm_expDecayLayers");
 }
 
 int cgfdm_storage_W_pre(int _nx_, int _ny_, int _nz_, float *W_pre, const float *W, void *stream)

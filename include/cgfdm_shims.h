@@ -70,7 +70,7 @@ int cgfdm_pmlRk(int nx, int ny, int nz, int nPML, int irk, float *const *aux, co
  * table momentRate [nt][npts][6] by mu / (J DH^3) at each cell srcIndex
  * (int64 padded-grid point index). */
 int cgfdm_calculateMomentRate(long long npts, long long nt, const float *CJM, float *momentRate,
-                              const long long *srcIndex, float DH, void *stream);
+                              const long long *srcIndex, float DH, int scheme, void *stream);
 
 /* addMomenteRate (src/addMoment.cpp:262-377, NO_SOURCE_SMOOTH as the
  * reference defines it): interpolates the table at the stage time of (it,
@@ -96,6 +96,31 @@ int cgfdm_comparePGV(int nx, int ny, int nz, const float *W, float *pgv, float D
  * whole padded grid, Dis [_nz_][_ny_][_nx_][3]. */
 int cgfdm_SolveDisplacement(int _nx_, int _ny_, int _nz_, const float *W, float *Dis, int scheme, const float *CJM,
                             float DT, void *stream);
+
+/* ---- ME-AWENO (SCFDM build: CJM with 19 fields, conserved variables) ---- */
+
+/* waveDeriv_alternative_flux_FD (src/alternative_flux_FD.cpp:1437-1566, LF
+ * flux): per direction x, y, z the WENO5-JS Lax-Friedrichs face fluxes into
+ * Riemann_flux (zero-initialised by the caller, [_nz_][_ny_][_nx_][9], faces
+ * never written stay zero) and their corrected difference into h_W (x
+ * assigns, y and z add).  alpha: the Lax-Friedrichs speed, the reference's
+ * vp_max_for_SCFDM. */
+int cgfdm_waveDeriv_alternative_flux_FD(int _nx_, int _ny_, int _nz_, float rDH, float *h_W, const float *W,
+                                        float *Riemann_flux, const float *CJM, float alpha, float DT, void *stream);
+
+/* waveRk_tvd (src/wave_rk_tvd.cpp:80-97): TVD-RK3 stage irk (0..2). */
+int cgfdm_waveRk_tvd(int _nx_, int _ny_, int _nz_, int irk, const float *h_W, float *W, float *m_W, void *stream);
+
+/* charfreeSurfaceDeriv (src/freeSurface.cpp:196-239): the characteristic
+ * free-surface condition on the surface layer and the cubic extrapolation
+ * into the halo above it.  The condition is evaluated in double through the
+ * inverse surface basis (agreeing with the reference's float formulas to
+ * about 2e-7 relative). */
+int cgfdm_charfreeSurfaceDeriv(int _nx_, int _ny_, int _nz_, float *W, const float *CJM, void *stream);
+
+/* expDecayLayers (src/exp_decay_absorb.cpp:108-145): 20-layer exponential
+ * sponge on x1 x2 y1 y2 z1 (and z2 unless free_surface). */
+int cgfdm_expDecayLayers(int _nx_, int _ny_, int _nz_, float *W, int free_surface, void *stream);
 
 /* storage_W_pre (src/propagate.cpp:26-58): copies the first _nx_ _ny_ _nz_
  * floats of W into W_pre, as the reference's kernel does. */

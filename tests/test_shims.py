@@ -91,12 +91,77 @@ def test_reference_loop_on_entry_points_matches_session(tmp_path):
     c.gauss_hill = 1
     d = cases.write_case(c, str(tmp_path / "run"))
     with Session(d, flavor="exact") as s:
+        assert s.info.scheme == 0
         W, st, pgv = propagate(Shims("exact"), s, torch, s.info.NT, c.nPML, float(np.float32(c.fault_dt)))
         assert s.info.n_fault_cells > 1 and s.info.n_stations > 0
         s.run(s.info.NT)
         np.testing.assert_array_equal(W, s.wavefield())
         np.testing.assert_array_equal(st, s.stations())
         np.testing.assert_array_equal(pgv, s.pgv()[..., :2])
+    assert np.abs(W).max() > 0
+
+
+def propagate_scfdm(sh, s, torch, nsteps, fault_dt):
+    """The reference's ME-AWENO loop (src/propagate.cpp:186-296 with SCFDM,
+    LF, EXP_DECAY, FREE_SURFACE) over the entry points."""
+    from cgfdm.shims import Grid
+
+    info = s.info
+    nx, ny, nz, NT = info.nx, info.ny, info.nz, info.NT
+    DT, DH = info.DT, info.DH
+    g = Grid(info.nxp, info.nyp, info.nzp, float(np.float32(1.0 / np.float64(np.float32(DH)))))
+    dev = torch.device("cuda:0")
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    npad = info.nxp * info.nyp * info.nzp
+    h_W, W, RF, m_W = (torch.zeros(npad * 9, dtype=torch.float32, device=dev) for _ in range(4))
+    CJM = T(s.cjm())
+    idx = T(s.array("srcIndex"))
+    npts = idx.numel()
+    rate = T(s.array("momentRate"))
+    nt_src = rate.numel() // max(npts * 6, 1)
+    slice_ = torch.zeros(max(npts, 1) * 6, dtype=torch.float32, device=dev)
+    XYZ = T(s.array("stationXYZ"))
+    nst = XYZ.numel() // 3
+    wave = torch.zeros(nst * NT * 9, dtype=torch.float32, device=dev)
+    pgv = torch.zeros(nx * ny * 2, dtype=torch.float32, device=dev)
+    Dis = torch.zeros(npad * 3, dtype=torch.float32, device=dev)
+
+    sh.calculateMomentRate(npts, nt_src, CJM, rate, idx, DH, scheme=1)
+    for it in range(nsteps):
+        sh.addMomenteRate(npts, nt_src, fault_dt, W, idx, rate, slice_, it, 0, DT, scheme=1, CJM=CJM)
+        for irk in range(3):
+            sh.waveDeriv_alternative_flux_FD(g, h_W, W, RF, CJM, info.Vp_max, DT)
+            sh.waveRk_tvd(g, irk, h_W, W, m_W)
+        sh.charfreeSurfaceDeriv(g, W, CJM)
+        sh.expDecayLayers(g, W, True)
+        sh.SolveDisplacement(g, W, Dis, DT, scheme=1, CJM=CJM)
+        sh.storageStation(g, NT, nst, XYZ, wave, W, it, scheme=1, CJM=CJM)
+        sh.comparePGV(nx, ny, nz, W, pgv, DT, it, scheme=1, CJM=CJM)
+    torch.cuda.synchronize()
+    return (W.cpu().numpy().reshape(info.nzp, info.nyp, info.nxp, 9),
+            wave.cpu().numpy().reshape(nst, NT, 9), pgv.cpu().numpy().reshape(ny, nx, 2))
+
+
+@pytest.mark.gpu
+def test_reference_scfdm_loop_on_entry_points_matches_session(tmp_path):
+    """The same for ME-AWENO: WENO5-JS Lax-Friedrichs fluxes and their
+    corrected differences, TVD-RK3, the characteristic free surface and the
+    sponge, against the session's exact build (which evaluates the
+    characteristic condition with the same restatement)."""
+    import torch
+
+    from cgfdm.shims import Shims
+
+    c = pu.multi_fault(steps=20, courant=0.45)
+    c.gauss_hill = 1
+    d = cases.write_case(c, str(tmp_path / "run"), scheme="SCFDM")
+    with Session(d, flavor="exact") as s:
+        assert s.info.scheme == 1
+        W, st, pgv = propagate_scfdm(Shims("exact"), s, torch, s.info.NT, float(np.float32(c.fault_dt)))
+        s.run(s.info.NT)
+        np.testing.assert_array_equal(st, s.stations())
+        np.testing.assert_array_equal(pgv, s.pgv()[..., :2])
+        np.testing.assert_array_equal(W, s.wavefield())
     assert np.abs(W).max() > 0
 
 
