@@ -33,6 +33,9 @@ _SIGS = {
     "cgfdm_comparePGV": [_i, _i, _i, _p, _p, _f, _i, _i, _p, _p, _p],
     "cgfdm_SolveDisplacement": [_i, _i, _i, _p, _p, _i, _p, _f, _p],
     "cgfdm_storage_W_pre": [_i, _i, _i, _p, _p, _p],
+    "cgfdm_loadPointSource_ricker": [_i, _i, _i, _i, _i, _i, _p, _p, _i, _i, _f, _f, _f, _i, _p],
+    "cgfdm_loadPointSource_double_couple": [_i, _i, _i, _i, _i, _i, _p, _p, _i, _i, _f, _f, _f, _f, _f, _f, _f,
+                                            _i, _p],
     "cgfdm_waveDeriv_alternative_flux_FD": [_i, _i, _i, _f, _p, _p, _p, _p, _f, _f, _p],
     "cgfdm_waveRk_tvd": [_i, _i, _i, _i, _p, _p, _p, _p],
     "cgfdm_charfreeSurfaceDeriv": [_i, _i, _i, _p, _p, _p],
@@ -98,6 +101,15 @@ class Shims:
                        CJM=None, stream=None):
         self._call("cgfdm_addMomenteRate", npts, nt, dt, _ptr(W), _ptr(srcIndex), _ptr(momentRate),
                    _ptr(momentRateSlice), it, irk, DT, scheme, _ptr(CJM), stream)
+
+    def loadPointSource_ricker(self, g, S, W, CJM, it, irk, DT, DH, rickerfc, scheme=0, stream=None):
+        self._call("cgfdm_loadPointSource_ricker", *g, *S, _ptr(W), _ptr(CJM), it, irk, DT, DH, rickerfc, scheme,
+                   stream)
+
+    def loadPointSource_double_couple(self, g, S, W, CJM, it, irk, DT, DH, strike, dip, rake, Mw, duration,
+                                      scheme=0, stream=None):
+        self._call("cgfdm_loadPointSource_double_couple", *g, *S, _ptr(W), _ptr(CJM), it, irk, DT, DH, strike, dip,
+                   rake, Mw, duration, scheme, stream)
 
     def storageStation(self, g, NT, stationNum, XYZ, wave, W, it, scheme=0, CJM=None, stream=None):
         self._call("cgfdm_storageStation", *g, NT, stationNum, _ptr(XYZ), _ptr(wave), _ptr(W), it, scheme,

@@ -821,7 +821,7 @@ static void build_pml(Model &m)
 // ---------------------------------------------------------- point sources
 // Gaussian spatial weights of the 7x7x7 smoothed point source
 // (src/singleSource.cpp:134-143, GAUSS_FUN of src/macro.h:37).
-static std::vector<float> gauss_weights(int nGauss)
+std::vector<float> point_gauss_weights(int nGauss)
 {
     std::vector<float> amp;
     float ra = (float)(nGauss * 0.5);
@@ -840,10 +840,17 @@ static std::vector<float> gauss_weights(int nGauss)
     return amp;
 }
 
-// Stage-0 source time t = (it + 0.0f) * DT (src/singleSource.cpp:47-59).
-static float ricker_value(float rickerfc, int it, float DT)
+// Source time of stage irk of step it (src/singleSource.cpp:47-59).
+static float stage_time(int it, int irk, float DT)
 {
-    float t = (it + 0.0f) * DT;
+    if (irk == 0) return (it + 0.0f) * DT;
+    if (irk == 3) return (it + 1.0f) * DT;
+    return (it + 0.5f) * DT;
+}
+
+float point_ricker(float rickerfc, int it, int irk, float DT)
+{
+    float t = stage_time(it, irk, DT);
     float tdelay = 1.0f / rickerfc;
     float r = REF_PI * rickerfc * (t - tdelay);
     float rr = r * r;
@@ -853,9 +860,9 @@ static float ricker_value(float rickerfc, int it, float DT)
     return s;
 }
 
-static float gauss_stf(float duration, int it, float DT)
+float point_gauss_stf(float duration, int it, int irk, float DT)
 {
-    float t = (it + 0.0f) * DT;
+    float t = stage_time(it, irk, DT);
     float tdelay = duration / 2 + 1;
     return expf(-(t - tdelay) * (t - tdelay) / (duration * duration)) / (sqrtf(REF_PI) * duration);
 }
@@ -889,20 +896,25 @@ static void build_point_source(Model &m)
     // src/singleSource.cpp:25-40 (locateSource), single rank
     ps.X = m.p.sourceX + HALO, ps.Y = m.p.sourceY + HALO, ps.Z = m.p.sourceZ + HALO;
     ps.inside = ps.X >= HALO && ps.X < g._nx && ps.Y >= HALO && ps.Y < g._ny && ps.Z >= HALO && ps.Z < g._nz;
-    ps.amp = gauss_weights(3);
+    ps.amp = point_gauss_weights(3);
     float DT = (float)m.p.DT;
     ps.stf.resize(m.NT);
     if (ps.kind == 1) {
-        for (int it = 0; it < m.NT; it++) ps.stf[it] = ricker_value(m.p.rickerfc, it, DT);
+        for (int it = 0; it < m.NT; it++) ps.stf[it] = point_ricker(m.p.rickerfc, it, 0, DT);
     } else {
-        for (int it = 0; it < m.NT; it++) ps.stf[it] = gauss_stf(m.p.duration, it, DT);
-        float s = (float)(m.p.strike * REF_DEG2RAD), d = (float)(m.p.dip * REF_DEG2RAD);
-        float r = (float)(m.p.rake * REF_DEG2RAD);
-        MT t = moment_tensor(s, d, r);
-        ps.mom[0] = t.M22, ps.mom[1] = t.M11, ps.mom[2] = t.M33;
-        ps.mom[3] = t.M12, ps.mom[4] = -t.M23, ps.mom[5] = -t.M13;
-        ps.m0 = (float)(1.5 * powf(10, m.p.Mw + 6));
+        for (int it = 0; it < m.NT; it++) ps.stf[it] = point_gauss_stf(m.p.duration, it, 0, DT);
+        point_moment(m.p.strike, m.p.dip, m.p.rake, m.p.Mw, ps.mom, &ps.m0);
     }
+}
+
+void point_moment(float strike, float dip, float rake, float Mw, float mom[6], float *m0)
+{
+    float s = (float)(strike * REF_DEG2RAD), d = (float)(dip * REF_DEG2RAD);
+    float r = (float)(rake * REF_DEG2RAD);
+    MT t = moment_tensor(s, d, r);
+    mom[0] = t.M22, mom[1] = t.M11, mom[2] = t.M33;
+    mom[3] = t.M12, mom[4] = -t.M23, mom[5] = -t.M13;
+    *m0 = (float)(1.5 * powf(10, Mw + 6));
 }
 
 // ----------------------------------------------------- finite-fault source

@@ -141,6 +141,15 @@ struct Model {
     std::vector<int> stations_global;// [n][3] global indices as read
 };
 
+// Single point sources (src/singleSource.cpp:42-99, 111-330): the 7 x 7 x 7
+// Gaussian weights [dk][dj][di], the Ricker and Gaussian source-time values
+// at the stage time of (it, irk), and the moment-tensor components (Mxx,
+// Myy, Mzz, Mxy, Mxz, Myz) with m0 of a double couple (degrees).
+std::vector<float> point_gauss_weights(int nGauss);
+float point_ricker(float rickerfc, int it, int irk, float DT);
+float point_gauss_stf(float duration, int it, int irk, float DT);
+void point_moment(float strike, float dip, float rake, float Mw, float mom[6], float *m0);
+
 // Whole setup from a run directory: params, grid, coordinates, medium, CFL,
 // PML profiles, sources and stations.  Metrics are computed on the GPU
 // (metrics.cu) from coord and medium.

@@ -378,6 +378,54 @@ __global__ void k_copy_prefix(float *__restrict__ dst, const float *__restrict__
     if (x < n) dst[x] = src[x];
 }
 
+// --------------------------------------------- src/singleSource.cpp:111-330
+// One 7 x 7 x 7 Gaussian-smoothed point source at the padded point (X, Y,
+// Z): kind 1 explosive Ricker (value on the normal stresses), kind 2 double
+// couple (moment-rate tensor on the six stresses); SCFDM converts to
+// strain rates with the medium of each point.
+struct PointArgs {
+    float amp[343];
+    float mom[6];
+    float s, m0;
+    int X, Y, Z, kind;
+};
+
+__global__ void k_point_source(float *__restrict__ W, const float *__restrict__ CJM, int nfield, Aos a,
+                               const PointArgs p, float DT, float DH, int scfdm)
+{
+    const int t = threadIdx.x;
+    if (t >= 343) return;
+    const int i = p.X + t % 7 - 3, j = p.Y + (t / 7) % 7 - 3, k = p.Z + t / 49 - 3;
+    const long long q = a.at(i, j, k);
+    const float jacb = CJM[a.at(p.X, p.Y, p.Z) * nfield + C_JAC];
+    const float vol = jacb * (DH * DH * DH);
+    float *w = W + q * 9;
+    if (p.kind == 1) {
+        float value = -1.0f * p.s * p.amp[t] / vol;
+        value = (float)((double)value * (1.0 * (double)DT));   // value *= Cs * DT
+        if (scfdm) value = value / (3 * CJM[q * nfield + C_LAMBDA] + 2 * CJM[q * nfield + C_MU]);
+        for (int c = 0; c < 3; c++) w[3 + c] = w[3 + c] + value;
+        return;
+    }
+    float rate = -1.0f * p.s * p.amp[t] / vol * p.m0;
+    rate = (float)((double)rate * (1.0 * (double)DT));
+    float mr[6];
+    for (int c = 0; c < 6; c++) mr[c] = p.mom[c] * rate;
+    if (scfdm) {
+        const float mu = CJM[q * nfield + C_MU], lam = CJM[q * nfield + C_LAMBDA];
+        const float den = 2 * (mu * mu) + 3 * lam * mu;
+        float e[6];
+        e[0] = (mr[0] * (lam + mu)) / den - (lam * mr[1]) / (2 * den) - (lam * mr[2]) / (2 * den);
+        e[1] = (mr[1] * (lam + mu)) / den - (lam * mr[0]) / (2 * den) - (lam * mr[2]) / (2 * den);
+        e[2] = (mr[2] * (lam + mu)) / den - (lam * mr[0]) / (2 * den) - (lam * mr[1]) / (2 * den);
+        e[3] = mr[5] / mu;
+        e[4] = mr[4] / mu;
+        e[5] = mr[3] / mu;
+        for (int c = 0; c < 6; c++) mr[c] = e[c];
+    }
+    for (int c = 0; c < 6; c++) w[3 + c] = w[3 + c] - mr[c];
+}
+
 // ====================================================== ME-AWENO (SCFDM)
 // CJM has 19 fields per point here (src/macro.h:56-60).
 #define SC_NF 19
@@ -784,6 +832,45 @@ int cgfdm_SolveDisplacement(int _nx_, int _ny_, int _nz_, const float *W, float 
     k_solve_displacement<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(W, Dis, CJM, 19, n, DT,
                                                                                scheme == SCHEME_SCFDM);
     return launched("cgfdm_SolveDisplacement");
+}
+
+static int point_source(const char *what, int _nx_, int _ny_, int _nz_, int X, int Y, int Z, float *W,
+                        const float *CJM, PointArgs &p, float DT, float DH, int scheme, void *stream)
+{
+    if (!W || !CJM || !grid_ok(_nx_, _ny_, _nz_)) return fail(std::string(what) + ": bad argument", ST_ARG);
+    // the reference launches only for a source inside the interior
+    if (!(X >= HALO_ && X < _nx_ - HALO_ && Y >= HALO_ && Y < _ny_ - HALO_ && Z >= HALO_ && Z < _nz_ - HALO_))
+        return ST_OK;
+    p.X = X, p.Y = Y, p.Z = Z;
+    const std::vector<float> amp = point_gauss_weights(3);
+    for (int t = 0; t < 343; t++) p.amp[t] = amp[t];
+    k_point_source<<<1, 352, 0, (cudaStream_t)stream>>>(W, CJM, scheme == SCHEME_SCFDM ? SC_NF : 13,
+                                                        Aos{_nx_, _ny_, _nz_}, p, DT, DH, scheme == SCHEME_SCFDM);
+    return launched(what);
+}
+
+int cgfdm_loadPointSource_ricker(int _nx_, int _ny_, int _nz_, int X, int Y, int Z, float *W, const float *CJM,
+                                 int it, int irk, float DT, float DH, float rickerfc, int scheme, void *stream)
+{
+    if (irk < 0 || irk > 3) return fail("cgfdm_loadPointSource_ricker: bad argument", ST_ARG);
+    PointArgs p{};
+    p.kind = 1;
+    p.s = point_ricker(rickerfc, it, irk, DT);
+    return point_source("cgfdm_loadPointSource_ricker", _nx_, _ny_, _nz_, X, Y, Z, W, CJM, p, DT, DH, scheme,
+                        stream);
+}
+
+int cgfdm_loadPointSource_double_couple(int _nx_, int _ny_, int _nz_, int X, int Y, int Z, float *W,
+                                        const float *CJM, int it, int irk, float DT, float DH, float strike,
+                                        float dip, float rake, float Mw, float duration, int scheme, void *stream)
+{
+    if (irk < 0 || irk > 3) return fail("cgfdm_loadPointSource_double_couple: bad argument", ST_ARG);
+    PointArgs p{};
+    p.kind = 2;
+    p.s = point_gauss_stf(duration, it, irk, DT);
+    point_moment(strike, dip, rake, Mw, p.mom, &p.m0);
+    return point_source("cgfdm_loadPointSource_double_couple", _nx_, _ny_, _nz_, X, Y, Z, W, CJM, p, DT, DH,
+                        scheme, stream);
 }
 
 int cgfdm_waveDeriv_alternative_flux_FD(int _nx_, int _ny_, int _nz_, float rDH, float *h_W, const float *W,

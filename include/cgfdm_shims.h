@@ -81,6 +81,19 @@ int cgfdm_addMomenteRate(long long npts, int nt, float dt, float *W, const long 
                          const float *momentRate, float *momentRateSlice, int it, int irk, float DT, int scheme,
                          const float *CJM, void *stream);
 
+/* loadPointSource_ricker, loadPointSource_double_couple (src/singleSource.cpp:
+ * 175-214, 331-359): a 7 x 7 x 7 Gaussian-smoothed point source at the
+ * padded point (X, Y, Z) (struct SOURCE), added to the stresses of W at the
+ * stage time of (it, irk); nothing when the point is outside the interior.
+ * The weights and source-time values are evaluated on the host in the
+ * reference's float/double mix (Ricker M0 = 1e9, double couple m0 = 1.5
+ * 10^(Mw + 6)); angles in degrees. */
+int cgfdm_loadPointSource_ricker(int _nx_, int _ny_, int _nz_, int X, int Y, int Z, float *W, const float *CJM,
+                                 int it, int irk, float DT, float DH, float rickerfc, int scheme, void *stream);
+int cgfdm_loadPointSource_double_couple(int _nx_, int _ny_, int _nz_, int X, int Y, int Z, float *W,
+                                        const float *CJM, int it, int irk, float DT, float DH, float strike,
+                                        float dip, float rake, float Mw, float duration, int scheme, void *stream);
+
 /* storageStation (src/station.cpp:382-411): the nine components at each
  * station XYZ [n][3] (padded indices) into wave [n][NT][9] at step it. */
 int cgfdm_storageStation(int _nx_, int _ny_, int _nz_, int NT, int stationNum, const int *XYZ, float *wave,

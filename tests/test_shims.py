@@ -7,7 +7,9 @@ patched propagate.cpp would call them.  Against the session's fused path
 (itself bit-exact against the reference's CPU build): the final wavefield,
 the station traces and the PGV must agree bit for bit in the exact build,
 on a curvilinear grid (Gaussian hill) with PML on five faces, the traction
-free surface and a finite fault of several cells.
+free surface and each source kind (finite fault of several cells, Ricker
+and double-couple point sources); for ME-AWENO the same with the
+characteristic free surface and the sponge.
 
 CPU-only checks: every entry point the header declares is exported, and
 argument errors come back as CGFDM_E_ARG without touching a GPU."""
@@ -27,9 +29,23 @@ FB_TABLE = [(-1, -1, -1), (1, 1, -1), (1, 1, 1), (-1, -1, 1), (-1, 1, -1), (1, -
 HEADER = os.path.join(os.path.dirname(__file__), "..", "include", "cgfdm_shims.h")
 
 
-def propagate(sh, s, torch, nsteps, nPML, fault_dt):
+def _add_point(sh, g, c, W, CJM, it, DT, DH, scheme):
+    """The single point source of case c at stage 0 of step it, as
+    src/propagate.cpp:195-198 calls it."""
+    f32 = lambda x: float(np.float32(x))
+    if c.ricker_point is not None:
+        X, Y, Z, fc = c.ricker_point
+        sh.loadPointSource_ricker(g, (X + 3, Y + 3, Z + 3), W, CJM, it, 0, DT, DH, f32(fc), scheme)
+    if c.double_couple is not None:
+        d = c.double_couple
+        sh.loadPointSource_double_couple(g, (d["X"] + 3, d["Y"] + 3, d["Z"] + 3), W, CJM, it, 0, DT, DH,
+                                         f32(d["strike"]), f32(d["dip"]), f32(d["rake"]), f32(d["Mw"]),
+                                         f32(d["duration"]), scheme)
+
+
+def propagate(sh, s, torch, nsteps, nPML, fault_dt, c=None):
     """The reference's loop over the entry points, for a CGFDM session with
-    PML, free surface, a finite fault and stations."""
+    PML, free surface, a finite fault or point source, and stations."""
     from cgfdm.shims import Grid
 
     info = s.info
@@ -64,6 +80,8 @@ def propagate(sh, s, torch, nsteps, nPML, fault_dt):
     sh.calculateMomentRate(npts, nt_src, CJM, rate, idx, DH)
     for it in range(nsteps):
         FB = list(FB_TABLE[it % 8])
+        if c is not None:
+            _add_point(sh, g, c, W, CJM, it, DT, DH, 0)
         sh.addMomenteRate(npts, nt_src, fault_dt, W, idx, rate, slice_, it, 0, DT)
         for irk in range(4):
             sh.waveDeriv(g, h_W, W, CJM, beta, FB, DT)
@@ -81,19 +99,26 @@ def propagate(sh, s, torch, nsteps, nPML, fault_dt):
             wave.cpu().numpy().reshape(nst, NT, 9), pgv.cpu().numpy().reshape(ny, nx, 2))
 
 
+def _source_case(kind, steps, **kw):
+    c = {"fault": pu.multi_fault, "ricker": pu.ricker_point, "double_couple": pu.double_couple}[kind](
+        steps=steps, courant=0.45, **kw)
+    c.gauss_hill = 1
+    return c
+
+
 @pytest.mark.gpu
-def test_reference_loop_on_entry_points_matches_session(tmp_path):
+@pytest.mark.parametrize("kind", ["fault", "ricker", "double_couple"])
+def test_reference_loop_on_entry_points_matches_session(tmp_path, kind):
     import torch
 
     from cgfdm.shims import Shims
 
-    c = pu.multi_fault(steps=24, courant=0.45)
-    c.gauss_hill = 1
+    c = _source_case(kind, 24)
     d = cases.write_case(c, str(tmp_path / "run"))
     with Session(d, flavor="exact") as s:
         assert s.info.scheme == 0
-        W, st, pgv = propagate(Shims("exact"), s, torch, s.info.NT, c.nPML, float(np.float32(c.fault_dt)))
-        assert s.info.n_fault_cells > 1 and s.info.n_stations > 0
+        W, st, pgv = propagate(Shims("exact"), s, torch, s.info.NT, c.nPML, float(np.float32(c.fault_dt)), c)
+        assert (s.info.n_fault_cells > 1) == (kind == "fault") and s.info.n_stations > 0
         s.run(s.info.NT)
         np.testing.assert_array_equal(W, s.wavefield())
         np.testing.assert_array_equal(st, s.stations())
@@ -101,7 +126,7 @@ def test_reference_loop_on_entry_points_matches_session(tmp_path):
     assert np.abs(W).max() > 0
 
 
-def propagate_scfdm(sh, s, torch, nsteps, fault_dt):
+def propagate_scfdm(sh, s, torch, nsteps, fault_dt, c=None):
     """The reference's ME-AWENO loop (src/propagate.cpp:186-296 with SCFDM,
     LF, EXP_DECAY, FREE_SURFACE) over the entry points."""
     from cgfdm.shims import Grid
@@ -128,6 +153,8 @@ def propagate_scfdm(sh, s, torch, nsteps, fault_dt):
 
     sh.calculateMomentRate(npts, nt_src, CJM, rate, idx, DH, scheme=1)
     for it in range(nsteps):
+        if c is not None:
+            _add_point(sh, g, c, W, CJM, it, DT, DH, 1)
         sh.addMomenteRate(npts, nt_src, fault_dt, W, idx, rate, slice_, it, 0, DT, scheme=1, CJM=CJM)
         for irk in range(3):
             sh.waveDeriv_alternative_flux_FD(g, h_W, W, RF, CJM, info.Vp_max, DT)
@@ -143,7 +170,8 @@ def propagate_scfdm(sh, s, torch, nsteps, fault_dt):
 
 
 @pytest.mark.gpu
-def test_reference_scfdm_loop_on_entry_points_matches_session(tmp_path):
+@pytest.mark.parametrize("kind", ["fault", "double_couple"])
+def test_reference_scfdm_loop_on_entry_points_matches_session(tmp_path, kind):
     """The same for ME-AWENO: WENO5-JS Lax-Friedrichs fluxes and their
     corrected differences, TVD-RK3, the characteristic free surface and the
     sponge, against the session's exact build (which evaluates the
@@ -152,12 +180,11 @@ def test_reference_scfdm_loop_on_entry_points_matches_session(tmp_path):
 
     from cgfdm.shims import Shims
 
-    c = pu.multi_fault(steps=20, courant=0.45)
-    c.gauss_hill = 1
+    c = _source_case(kind, 20)
     d = cases.write_case(c, str(tmp_path / "run"), scheme="SCFDM")
     with Session(d, flavor="exact") as s:
         assert s.info.scheme == 1
-        W, st, pgv = propagate_scfdm(Shims("exact"), s, torch, s.info.NT, float(np.float32(c.fault_dt)))
+        W, st, pgv = propagate_scfdm(Shims("exact"), s, torch, s.info.NT, float(np.float32(c.fault_dt)), c)
         s.run(s.info.NT)
         np.testing.assert_array_equal(st, s.stations())
         np.testing.assert_array_equal(pgv, s.pgv()[..., :2])
