@@ -51,6 +51,72 @@ int cgfdm_create(const char *run_dir, const char *options_json, int device, cgfd
     return CGFDM_OK;
 }
 
+int cgfdm_create_part(const char *run_dir, const char *options_json, const int *parts, const int *coord, int device,
+                      cgfdm_session **out)
+{
+    if (!run_dir || !out || !parts || !coord) {
+        g_create_error = "run_dir, parts, coord and out must not be NULL";
+        return CGFDM_E_ARG;
+    }
+    *out = nullptr;
+    cgfdm_session *h = new (std::nothrow) cgfdm_session;
+    if (!h) {
+        g_create_error = "out of host memory";
+        return CGFDM_E_ALLOC;
+    }
+    int st = h->s.create_part(run_dir, options_json ? options_json : "", parts, coord, device);
+    if (st) {
+        g_create_error = h->s.err;
+        delete h;
+        return st;
+    }
+    *out = h;
+    return CGFDM_OK;
+}
+
+int cgfdm_part_info(const cgfdm_session *s, int *lo, int *n, int *top)
+{
+    if (!s) return CGFDM_E_ARG;
+    const cgfdm::Model &m = s->s.m;
+    if (lo) lo[0] = m.part_lo[0], lo[1] = m.part_lo[1], lo[2] = m.part_lo[2];
+    if (n) n[0] = m.g.nx, n[1] = m.g.ny, n[2] = m.g.nz;
+    if (top) *top = m.fs_top ? 1 : 0;
+    return CGFDM_OK;
+}
+
+int cgfdm_part_station_ids(const cgfdm_session *s, int *ids, int count)
+{
+    if (!s || (!ids && count)) return CGFDM_E_ARG;
+    const std::vector<int> &v = s->s.m.station_ids;
+    if (count < (int)v.size()) return CGFDM_E_ARG;
+    for (size_t i = 0; i < v.size(); i++) ids[i] = v[i];
+    return CGFDM_OK;
+}
+
+int cgfdm_part_advance(cgfdm_session *s, int *phase)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.part_advance(phase);
+}
+
+long long cgfdm_halo_count(const cgfdm_session *s, int face, int which)
+{
+    if (!s) return -1;
+    return s->s.halo_count(face, which);
+}
+
+int cgfdm_halo_pack(cgfdm_session *s, int face, int which, float *d_buf)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.halo_copy(face, which, d_buf, true);
+}
+
+int cgfdm_halo_unpack(cgfdm_session *s, int face, int which, const float *d_buf)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.halo_copy(face, which, const_cast<float *>(d_buf), false);
+}
+
 int cgfdm_model_medium(const char *run_dir, const char *options_json, float *out, long long count, int *dims)
 {
     if (!run_dir) {

@@ -307,8 +307,9 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     }
 
     const float bx = active ? a.pml_beta_x[i] : 1.0f, by = active ? a.pml_beta_y[j] : 1.0f;
-    const bool inx1 = a.pml_on && i < CGFDM_HALO + nPML, inx2 = a.pml_on && i >= _nx - nPML;
-    const bool iny1 = a.pml_on && j < CGFDM_HALO + nPML, iny2 = a.pml_on && j >= _ny - nPML;
+    // pml_on: one bit per absorbing face, x1 y1 z1 x2 y2 (bits 0..4)
+    const bool inx1 = (a.pml_on & 1) && i < CGFDM_HALO + nPML, inx2 = (a.pml_on & 8) && i >= _nx - nPML;
+    const bool iny1 = (a.pml_on & 2) && j < CGFDM_HALO + nPML, iny2 = (a.pml_on & 16) && j >= _ny - nPML;
 
     for (int k = kb; k < ke; k++) {
         __syncthreads();                    // every thread is done with plane k - za - 1's slot
@@ -420,7 +421,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         }
 
         // ---- PML auxiliaries, faces in the reference's launch order x1 y1 z1 x2 y2
-        const bool inz1 = a.pml_on && k < CGFDM_HALO + nPML;
+        const bool inz1 = (a.pml_on & 4) && k < CGFDM_HALO + nPML;
         if (inx1 || iny1 || inz1 || inx2 || iny2) {
             const int i0p = i - CGFDM_HALO, j0p = j - CGFDM_HALO, k0p = k - CGFDM_HALO;
             const int nx = g.nx, ny = g.ny;

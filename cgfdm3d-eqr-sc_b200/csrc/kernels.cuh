@@ -61,7 +61,9 @@ struct CgStageArgs {
     int ntiles_x, ntiles_y, nchunk;  // work items: tiles x tiles x z-chunks
     int irk;
     int FB1, FB2, FB3;
-    int nPML, pml_on, fs_on;
+    int nPML;
+    int pml_on;          // absorbing faces, one bit each: x1 y1 z1 x2 y2 (bits 0..4)
+    int fs_on;           // the traction free surface in the top three layers
     int kchunk;
     float rDH, DT;
 };

@@ -139,6 +139,15 @@ struct Model {
     PointSource point;
     std::vector<int> stations;       // [n][3] padded indices
     std::vector<int> stations_global;// [n][3] global indices as read
+    // a sub-domain of a decomposed grid (partition.cpp): interior offset of
+    // this part in the global interior, decomposition and this part's place
+    // in it, whether it holds the free surface, and the global number of
+    // each of its stations
+    int part_lo[3] = {0, 0, 0};
+    int parts[3] = {1, 1, 1};
+    int part_coord[3] = {0, 0, 0};
+    bool fs_top = true;
+    std::vector<int> station_ids;
 };
 
 // Single point sources (src/singleSource.cpp:42-99, 111-330): the 7 x 7 x 7
@@ -149,6 +158,15 @@ std::vector<float> point_gauss_weights(int nGauss);
 float point_ricker(float rickerfc, int it, int irk, float DT);
 float point_gauss_stf(float duration, int it, int irk, float DT);
 void point_moment(float strike, float dip, float rake, float Mw, float mom[6], float *m0);
+
+// One part of a PX x PY x PZ decomposition of the global model G (the
+// reference's MPI layout, src/init_grid.cpp): interior sizes split as evenly
+// as possible, the padded arrays sliced with their 3-cell halos, PML on the
+// faces at the global boundary only, the free surface in the top layer of
+// parts, sources and stations of the part's interior.  CGFDM only.
+int slice_model(const Model &G, const int parts[3], const int coord[3], Model &m, std::string &err);
+// interior offset and size of part c of n along an axis of N points
+void part_extent(int N, int n, int c, int *lo, int *len);
 
 // Whole setup from a run directory: params, grid, coordinates, medium, CFL,
 // PML profiles, sources and stations.  Metrics are computed on the GPU

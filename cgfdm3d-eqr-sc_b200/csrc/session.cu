@@ -233,6 +233,7 @@ int Session::setup_device()
         const long long cnt[5] = {nP * G.ny * G.nz, nP * G.nx * G.nz, nP * G.nx * G.ny, nP * G.ny * G.nz,
                                   nP * G.nx * G.nz};
         for (int fc = 0; fc < 5; fc++) {
+            if (!(pml_faces() & (1 << fc))) continue;   // a part away from that boundary
             face_[fc].count = cnt[fc];
             ALLOC(face_[fc].A, float, cnt[fc] * 9);
             ALLOC(face_[fc].B, float, cnt[fc] * 9);
@@ -362,8 +363,8 @@ void Session::stage_desc(int irk, CgStageDesc &d) const
     a.dis = irk == 3 ? dis_ : nullptr;
     a.irk = irk;
     a.nPML = m.g.nPML;
-    a.pml_on = m.p.pml;
-    a.fs_on = 1;
+    a.pml_on = pml_faces();
+    a.fs_on = m.fs_top ? 1 : 0;
     a.kchunk = kchunk_;
     a.rDH = m.g.rDH;
     a.DT = (float)m.p.DT;
@@ -376,6 +377,14 @@ void Session::stage_desc(int irk, CgStageDesc &d) const
 }
 
 int Session::stage_items() const { return ntx_ * nty_ * nchunk_; }
+
+// Absorbing faces as stage-kernel bits x1 y1 z1 x2 y2 (PML off: none).
+int Session::pml_faces() const
+{
+    if (!m.p.pml) return 0;
+    return (m.border[0] ? 1 : 0) | (m.border[2] ? 2 : 0) | (m.border[4] ? 4 : 0) | (m.border[1] ? 8 : 0) |
+           (m.border[3] ? 16 : 0);
+}
 
 int Session::build_stage_descs()
 {
@@ -525,6 +534,10 @@ int Session::run(int nsteps)
     if (nsteps < 0) {
         err = "negative step count";
         return ST_ARG;
+    }
+    if (is_part_) {
+        err = "a part of a decomposed grid steps with part_advance and halo exchanges";
+        return ST_STATE;
     }
     int n = std::min(nsteps, m.NT - it);
     if (!snapshots_on()) {

@@ -29,6 +29,13 @@ public:
     ~Session();
     int create(const std::string &run_dir, const std::string &options, int device);
     int run(int nsteps);
+    // a part of a decomposed grid (csrc/partition.cpp, csrc/halo.cu): the
+    // step in five phases with a halo exchange after each of the first four
+    int create_part(const std::string &run_dir, const std::string &options, const int parts[3], const int coord[3],
+                    int device);
+    int part_advance(int *phase_done);
+    long long halo_count(int face, int which) const;      // floats; which 0 wavefield, 1 metric (13 fields)
+    int halo_copy(int face, int which, float *dev, bool pack);
     int run_timed(int nsteps, float *ms, float *stage_ms);
     int profile_stages(int nsteps, float *mean_stage_ms);
     double algo_bytes_per_step() const;
@@ -71,6 +78,8 @@ public:
     std::string run_dir;
     int device = 0;
     int it = 0;  // steps completed
+    bool is_part_ = false;  // a part of a decomposition: stepped by part_advance
+    int phase_ = 0, cur_ = 0;
     bool counted_ = false;  // registered with the device's gradient scratch
     int nst = 0;
     cudaStream_t stream = nullptr;
@@ -116,6 +125,7 @@ public:
     // the stage descriptor of RK stage irk, and the stage's work items (batches use these)
     void stage_desc(int irk, CgStageDesc &d) const;
     int stage_items() const;
+    int pml_faces() const;
     int launch_sources_on(cudaStream_t st);
     int launch_stations_on(cudaStream_t st);
     int launch_pga_on(cudaStream_t st);

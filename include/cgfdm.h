@@ -68,6 +68,35 @@ typedef struct cgfdm_info {
  * "fp32"|"fp64", "OUT": "..."}. */
 int cgfdm_create(const char *run_dir, const char *options_json, int device, cgfdm_session **out);
 
+/* ---- Domain decomposition (the reference's MPI layout, src/init_grid.cpp) ----
+ * A grid too large for one GPU runs as parts[0] x parts[1] x parts[2]
+ * sub-domains, one session per part (one per GPU and process, or several on
+ * one GPU).  cgfdm_create_part builds part `coord` (0 <= coord[a] <
+ * parts[a]) of the run directory's model: interior sizes split as evenly as
+ * possible, the model's padded arrays sliced with 3-cell halos, PML only on
+ * the faces at the global boundary, the free surface only in the top parts,
+ * the finite-fault cells and stations of the part's interior (a point
+ * source's 7x7x7 cube must lie inside one part).  CGFDM only.
+ *
+ * Stepping: cgfdm_part_advance runs the next of the five phases of a step
+ * (0: the source; 1..4: RK stage 0..3, the stations after the last) and
+ * returns the phase it ran.  After phases 0..3 every part refreshes its
+ * halos: per axis x, y, z in turn, cgfdm_halo_pack(face) the faces it
+ * shares with a neighbour into a device buffer of cgfdm_halo_count floats,
+ * send each to the neighbour on that side, and cgfdm_halo_unpack(face) what
+ * arrives from the neighbour on side `face`.  Faces: 0 x-low, 1 x-high,
+ * 2 y-low, 3 y-high, 4 z-low, 5 z-high; which: 0 the wavefield the phase
+ * wrote, 1 the 13 metric and medium fields (exchanged once after create).
+ * Pack and unpack finish before they return.  cgfdm_run refuses parts. */
+int cgfdm_create_part(const char *run_dir, const char *options_json, const int *parts, const int *coord, int device,
+                      cgfdm_session **out);
+int cgfdm_part_info(const cgfdm_session *s, int *lo, int *n, int *top);
+int cgfdm_part_station_ids(const cgfdm_session *s, int *ids, int count);
+int cgfdm_part_advance(cgfdm_session *s, int *phase);
+long long cgfdm_halo_count(const cgfdm_session *s, int face, int which);
+int cgfdm_halo_pack(cgfdm_session *s, int face, int which, float *d_buf);
+int cgfdm_halo_unpack(cgfdm_session *s, int face, int which, const float *d_buf);
+
 /* Host-only: builds the model of a run directory as cgfdm_create does --
  * parameters, grid, coordinates and the medium from the switches that
  * select it (homogeneous, CRUST1.0, Shen, layered, mediumFile;

@@ -1,0 +1,160 @@
+"""Domain decomposition (cgfdm_create_part, cgfdm.domain): a grid split into
+parts, one session each, the halos at internal faces refreshed after every
+phase of a step, as the reference's MPI ranks exchange them
+(src/MPI_send_recv_FLOAT.cpp).
+
+GPU: every part on one device (halos moved by device copies) must reproduce
+the single-domain run bit for bit -- interior wavefield, station traces in
+the run's order, surface PGV -- for several decompositions of a curvilinear
+grid with PML on five faces, the free surface and a finite fault whose cells
+fall in several parts.
+
+CPU: the decomposition's arithmetic, and the exchange orchestration between
+two gloo ranks with array-backed parts: each rank's halos must equal its
+neighbour's interior layers afterwards."""
+
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import parity_util as pu
+from cgfdm import Session, cases, domain
+
+
+def test_plan_covers_grid_once():
+    shape, parts = (34, 30, 26), (3, 2, 2)
+    cover = np.zeros(shape[::-1], int)
+    P = domain.plan(shape, parts)
+    assert len(P) == 12 and sum(p["top"] for p in P) == 6
+    for p in P:
+        (x, y, z), (nx, ny, nz) = p["lo"], p["n"]
+        cover[z:z + nz, y:y + ny, x:x + nx] += 1
+        assert domain.rank_of(parts, p["coord"]) == p["rank"]
+        for f, q in p["neighbours"].items():
+            if q is not None:
+                assert domain.neighbour(parts, q, f ^ 1) == p["coord"]
+    assert (cover == 1).all()
+    assert [domain.extent(10, 3, c) for c in range(3)] == [(0, 4), (4, 3), (7, 3)]
+
+
+class ArrayPart:
+    """A part backed by a padded numpy array [nz+6][ny+6][nx+6][nf] whose
+    interior holds the global index of each point; pack/unpack as the
+    library's kernels do (three layers next to / beyond the face, the other
+    axes over their padded extent)."""
+
+    def __init__(self, shape, parts, coord, nf=2):
+        lo, n = zip(*(domain.extent(shape[a], parts[a], coord[a]) for a in range(3)))
+        self.lo, self.n, self.nf = lo, n, nf
+        self.a = np.full((n[2] + 6, n[1] + 6, n[0] + 6, nf), -1.0, np.float32)
+        z, y, x = np.meshgrid(*(np.arange(lo[a], lo[a] + n[a]) for a in (2, 1, 0)), indexing="ij")
+        g = (z * shape[1] + y) * shape[0] + x
+        for f in range(nf):
+            self.a[3:-3, 3:-3, 3:-3, f] = g + 1000000 * f
+
+    def _box(self, face, send):
+        axis, hi = divmod(face, 2)
+        n = self.n[axis]
+        start = (n if hi else 3) if send else (n + 3 if hi else 0)
+        sl = [slice(None)] * 3
+        sl[2 - axis] = slice(start, start + 3)   # array axes are z, y, x
+        return tuple(sl)
+
+    def halo_count(self, face, which):
+        return int(self.a[self._box(face, True)].size)
+
+    def new_buffer(self, n):
+        return torch.zeros(n, dtype=torch.float32)
+
+    def pack(self, face, which, buf):
+        buf.copy_(torch.from_numpy(np.ascontiguousarray(self.a[self._box(face, True)]).reshape(-1)))
+
+    def unpack(self, face, which, buf):
+        box = self._box(face, False)
+        self.a[box] = buf.numpy().reshape(self.a[box].shape)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, shape, parts, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        coord = domain.coord_of(parts, rank)
+        p = ArrayPart(shape, parts, coord)
+        domain.exchange(p, coord, parts, 0, domain.torch_transport(None, parts, coord))
+        np.save(os.path.join(out, f"part{rank}.npy"), p.a)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("parts", [(2, 1, 1), (1, 1, 2)])
+def test_exchange_between_gloo_ranks(tmp_path, parts):
+    shape = (14, 9, 12)
+    world = parts[0] * parts[1] * parts[2]
+    mp.spawn(_worker, args=(world, _free_port(), shape, parts, str(tmp_path)), nprocs=world, join=True)
+    for r in range(world):
+        c = domain.coord_of(parts, r)
+        a = np.load(tmp_path / f"part{r}.npy")
+        ref = ArrayPart(shape, parts, c)
+        # every halo layer on an internal face now holds the neighbour's points
+        for f in range(6):
+            if domain.neighbour(parts, c, f) is None:
+                continue
+            axis, hi = divmod(f, 2)
+            lo, n = ref.lo[axis], ref.n[axis]
+            idx = np.arange(lo + n, lo + n + 3) if hi else np.arange(lo - 3, lo)
+            box = ref._box(f, False)
+            sub = [slice(3, -3)] * 3
+            sub[2 - axis] = slice(None)
+            got = a[box][tuple(sub)][..., 0]
+            zz, yy, xx = [np.arange(ref.lo[b], ref.lo[b] + ref.n[b]) for b in (2, 1, 0)]
+            axes = [zz, yy, xx]
+            axes[2 - axis] = idx
+            Z, Y, X = np.meshgrid(*axes, indexing="ij")
+            np.testing.assert_array_equal(got, (Z * shape[1] + Y) * shape[0] + X)
+
+
+def _case():
+    c = pu.multi_fault(steps=24, courant=0.45)
+    c.gauss_hill = 1
+    return c
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("parts", [(2, 1, 2), (1, 2, 1), (2, 2, 2)])
+def test_decomposed_run_matches_single_domain(tmp_path, parts):
+    c = _case()
+    d = cases.write_case(c, str(tmp_path / "run"))
+    with Session(d) as s:
+        s.run(s.info.NT)
+        ref = (s.wavefield()[3:-3, 3:-3, 3:-3], s.stations(), s.pgv()[..., :2])
+        assert s.info.n_fault_cells > 1
+    got = domain.run_local(d, parts)
+    for a, b in zip(got, ref):
+        np.testing.assert_array_equal(a, b)
+    assert np.abs(got[0]).max() > 0
+
+
+@pytest.mark.gpu
+def test_part_refuses_plain_run(tmp_path):
+    from cgfdm import CgfdmError
+
+    d = cases.write_case(_case(), str(tmp_path / "run"))
+    p = domain.Part(d, (2, 1, 1), (0, 0, 0))
+    try:
+        with pytest.raises(CgfdmError):
+            p.run(1)
+    finally:
+        p.close()
