@@ -104,6 +104,7 @@ class Part(Session):
         L.cgfdm_part_info.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 3
         L.cgfdm_part_station_ids.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.cgfdm_part_advance.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        L.cgfdm_part_link.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         L.cgfdm_halo_count.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.cgfdm_halo_count.restype = ctypes.c_longlong
         L.cgfdm_halo_pack.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
@@ -127,6 +128,10 @@ class Part(Session):
         ph = ctypes.c_int()
         self._check(self.L.cgfdm_part_advance(self._h, ctypes.byref(ph)))
         return ph.value
+
+    def link(self, face: int, nbr: "Part") -> None:
+        """Stages store the layers next to `face` into nbr's halo directly."""
+        self._check(self.L.cgfdm_part_link(self._h, face, nbr._h))
 
     def halo_count(self, face: int, which: int) -> int:
         return int(self.L.cgfdm_halo_count(self._h, face, which))
@@ -176,10 +181,12 @@ def _assemble(ps: Dict, shape, nst_total: int, NT: int):
 
 
 def run_local(run_dir: str, parts: Sequence[int], nsteps: Optional[int] = None, options: Optional[str] = None,
-              device: int = 0, flavor: str = "fast"):
+              device: int = 0, flavor: str = "fast", fused: bool = False):
     """Every part on one GPU; returns the interior wavefield [nz][ny][nx][9],
     the station traces [n][NT][9] in the run's station order and the PGV
-    [ny][nx][2], assembled from the parts."""
+    [ny][nx][2], assembled from the parts.  fused: the stages store their
+    boundary layers into the neighbours' halos (cgfdm_part_link), leaving
+    one explicit exchange per step, after the source."""
     parts = tuple(parts)
     ps = {}
     try:
@@ -187,6 +194,12 @@ def run_local(run_dir: str, parts: Sequence[int], nsteps: Optional[int] = None, 
             c = coord_of(parts, r)
             ps[c] = Part(run_dir, parts, c, options, device, flavor)
         _exchange_all_local(ps, parts, 1)           # metric and medium halos
+        if fused:
+            for c, p in ps.items():
+                for f in range(FACES):
+                    q = neighbour(parts, c, f)
+                    if q is not None:
+                        p.link(f, ps[q])
         any_part = next(iter(ps.values()))
         NT = any_part.info.NT
         steps = NT if nsteps is None else min(nsteps, NT)
@@ -194,7 +207,7 @@ def run_local(run_dir: str, parts: Sequence[int], nsteps: Optional[int] = None, 
             for phase in range(5):
                 for p in ps.values():
                     assert p.advance() == phase
-                if phase < 4:
+                if phase == 0 or (phase < 4 and not fused):
                     _exchange_all_local(ps, parts, 0)
         shape = tuple(max(p.lo[a] + p.n[a] for p in ps.values()) for a in range(3))
         nst_total = 1 + max([max(p.station_ids) for p in ps.values() if p.station_ids], default=-1)

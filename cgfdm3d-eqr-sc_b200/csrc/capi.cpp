@@ -99,6 +99,12 @@ int cgfdm_part_advance(cgfdm_session *s, int *phase)
     return s->s.part_advance(phase);
 }
 
+int cgfdm_part_link(cgfdm_session *s, int face, const cgfdm_session *nbr)
+{
+    if (!s || !nbr) return CGFDM_E_ARG;
+    return s->s.link_halo(face, nbr->s);
+}
+
 long long cgfdm_halo_count(const cgfdm_session *s, int face, int which)
 {
     if (!s) return -1;

@@ -206,7 +206,7 @@ __device__ __forceinline__ void ljt_z(const float *__restrict__ W, const float *
 // and tensor maps in parameter space).  BATCH = true: the work items of
 // nsess sessions, their descriptors in global memory; a CTA copies the
 // arguments of the session its current item belongs to into shared memory.
-template <int FB1, int FB2, int FB3, bool BATCH>
+template <int FB1, int FB2, int FB3, bool BATCH, bool HOUT>
 __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     k_cg_stage(const __grid_constant__ CgStageDesc d1, const CgStageDesc *__restrict__ descs,
                const int *__restrict__ item_start, int nsess, int *work)
@@ -517,6 +517,24 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         }
 #pragma unroll
         for (int f = 0; f < 9; f++) a.Wout[f * F + q] = wout[f];
+        if (HOUT) {
+            // a part of a decomposed grid: the interior layers next to a face
+            // shared with a neighbour go straight into the neighbour's halo
+#pragma unroll 1
+            for (int fc = 0; fc < 6; fc++) {
+                const HaloOut &h = a.ho[fc];
+                if (!h.base) continue;
+                const int axis = fc >> 1;
+                const int c = axis == 0 ? i : axis == 1 ? j : k;
+                const int n = axis == 0 ? g.nx : axis == 1 ? g.ny : g.nz;
+                if ((fc & 1) ? c < n : c >= 2 * CGFDM_HALO) continue;
+                const long long d = (long long)(k + (axis == 2 ? h.shift : 0)) * h.plane +
+                                    (long long)(j + (axis == 1 ? h.shift : 0)) * h.pitch + h.xoff +
+                                    (i + (axis == 0 ? h.shift : 0));
+#pragma unroll
+                for (int f = 0; f < 9; f++) h.base[f * h.fstride + d] = wout[f];
+            }
+        }
 
         if (a.irk == 3) {
             // displacement: only the surface layer is ever read (the FreeSurfU
@@ -561,48 +579,50 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
 int cg_stage_ctas_per_sm() { return CG_CTAS_PER_SM; }
 int cg_stage_tile_y() { return TY; }
 
-template <int FB1, int FB2, int FB3, bool BATCH>
+template <int FB1, int FB2, int FB3, bool BATCH, bool HOUT>
 static cudaError_t launch_t(const CgStageDesc &d1, const CgStageDesc *descs, const int *item_start, int nsess,
                             int *work, int ctas, cudaStream_t st)
 {
     static bool attr = false;
     if (!attr) {
-        CUDA_TRY(cudaFuncSetAttribute(k_cg_stage<FB1, FB2, FB3, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)cg_stage_smem_bytes()));
+        CUDA_TRY(cudaFuncSetAttribute(k_cg_stage<FB1, FB2, FB3, BATCH, HOUT>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cg_stage_smem_bytes()));
         attr = true;
     }
-    k_cg_stage<FB1, FB2, FB3, BATCH>
+    k_cg_stage<FB1, FB2, FB3, BATCH, HOUT>
         <<<ctas, dim3(TX, TY, 1), cg_stage_smem_bytes(), st>>>(d1, descs, item_start, nsess, work);
     return cudaGetLastError();
 }
 
-template <bool BATCH>
+template <bool BATCH, bool HOUT>
 static cudaError_t launch_b(int FB1, int FB2, int FB3, const CgStageDesc &d1, const CgStageDesc *descs,
                             const int *item_start, int nsess, int *work, int ctas, cudaStream_t st)
 {
     const int key = (FB1 > 0) * 4 + (FB2 > 0) * 2 + (FB3 > 0);
     switch (key) {
-    case 0: return launch_t<-1, -1, -1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
-    case 1: return launch_t<-1, -1, 1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
-    case 2: return launch_t<-1, 1, -1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
-    case 3: return launch_t<-1, 1, 1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
-    case 4: return launch_t<1, -1, -1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
-    case 5: return launch_t<1, -1, 1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
-    case 6: return launch_t<1, 1, -1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
-    default: return launch_t<1, 1, 1, BATCH>(d1, descs, item_start, nsess, work, ctas, st);
+    case 0: return launch_t<-1, -1, -1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
+    case 1: return launch_t<-1, -1, 1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
+    case 2: return launch_t<-1, 1, -1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
+    case 3: return launch_t<-1, 1, 1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
+    case 4: return launch_t<1, -1, -1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
+    case 5: return launch_t<1, -1, 1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
+    case 6: return launch_t<1, 1, -1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
+    default: return launch_t<1, 1, 1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
     }
 }
 
-cudaError_t launch_cg_stage(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int ctas, cudaStream_t st)
+cudaError_t launch_cg_stage(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int ctas, cudaStream_t st,
+                            bool halo_out)
 {
-    return launch_b<false>(FB1, FB2, FB3, d, nullptr, nullptr, 1, work, ctas, st);
+    if (halo_out) return launch_b<false, true>(FB1, FB2, FB3, d, nullptr, nullptr, 1, work, ctas, st);
+    return launch_b<false, false>(FB1, FB2, FB3, d, nullptr, nullptr, 1, work, ctas, st);
 }
 
 cudaError_t launch_cg_stage_batch(int FB1, int FB2, int FB3, const CgStageDesc *descs, const int *item_start,
                                   int nsess, int *work, int ctas, cudaStream_t st)
 {
     static const CgStageDesc unused{};
-    return launch_b<true>(FB1, FB2, FB3, unused, descs, item_start, nsess, work, ctas, st);
+    return launch_b<true, false>(FB1, FB2, FB3, unused, descs, item_start, nsess, work, ctas, st);
 }
 
 cudaError_t make_field_tmap(void *out, const float *base, const DevGrid &g, int nf, bool halo_box)

@@ -84,6 +84,36 @@ int Session::halo_copy(int face, int which, float *dev, bool pack)
     return ST_OK;
 }
 
+int Session::link_halo(int face, const Session &nbr)
+{
+    if (face < 0 || face > 5 || nbr.m.p.scheme != SCHEME_CGFDM || m.p.scheme != SCHEME_CGFDM) {
+        err = "bad face or scheme for a halo link";
+        return ST_ARG;
+    }
+    const int axis = face / 2;
+    const int n_self = axis == 0 ? g.nx : axis == 1 ? g.ny : g.nz;
+    const int n_nbr = axis == 0 ? nbr.g.nx : axis == 1 ? nbr.g.ny : nbr.g.nz;
+    // the other two axes must match (a tensor-product decomposition)
+    const int os[2] = {axis == 0 ? g.nyp : g.nxp, axis == 2 ? g.nyp : g.nzp};
+    const int on[2] = {axis == 0 ? nbr.g.nyp : nbr.g.nxp, axis == 2 ? nbr.g.nyp : nbr.g.nzp};
+    if (os[0] != on[0] || os[1] != on[1]) {
+        err = "the neighbour's grid does not match on the shared face";
+        return ST_ARG;
+    }
+    static const int wout[4] = {1, 2, 1, 0};   // output buffer of RK stage irk
+    for (int irk = 0; irk < 4; irk++) {
+        HaloOut &h = ho_[irk][face];
+        h.base = nbr.W_[wout[irk]];
+        h.plane = nbr.g.plane, h.fstride = nbr.g.fstride;
+        h.pitch = nbr.g.pitch, h.xoff = nbr.g.xoff;
+        // high face: interior n_self..n_self+2 -> neighbour halo 0..2;
+        // low face: interior 3..5 -> neighbour halo n_nbr+3..n_nbr+5
+        h.shift = (face & 1) ? -n_self : n_nbr;
+    }
+    halo_out_ = true;
+    return build_stage_descs();
+}
+
 int Session::create_part(const std::string &dir, const std::string &options, const int parts[3],
                          const int coord[3], int dev)
 {
@@ -125,7 +155,8 @@ int Session::part_advance(int *phase_done)
         int fb[3];
         fb_signs(it, fb);
         const int sgn = (irk & 1) ? -1 : 1;
-        CU(launch_cg_stage(fb[0] * sgn, fb[1] * sgn, fb[2] * sgn, desc_host_[irk], work_dev_, grid_ctas_, stream));
+        CU(launch_cg_stage(fb[0] * sgn, fb[1] * sgn, fb[2] * sgn, desc_host_[irk], work_dev_, grid_ctas_, stream,
+                           halo_out_));
         kernel_launches += 1;
         static const int wout[4] = {1, 2, 1, 0};
         cur_ = wout[irk];

@@ -40,6 +40,16 @@ struct HBox {
 };
 
 // --------------------------------------------------------- CGFDM stage
+// Where a part's stage kernel stores the interior layers next to one face:
+// the neighbour's output buffer of the same stage (its halo on the facing
+// side), that buffer's layout, and the shift from this part's padded index
+// along the face's axis to the neighbour's.  base null: no neighbour.
+struct HaloOut {
+    float *base;
+    long long plane, fstride;
+    int pitch, xoff, shift;
+};
+
 struct CgStageArgs {
     DevGrid g;
     HBox hbox;           // layout of hstore
@@ -66,6 +76,7 @@ struct CgStageArgs {
     int fs_on;           // the traction free surface in the top three layers
     int kchunk;
     float rDH, DT;
+    HaloOut ho[6];       // faces x-low x-high y-low y-high z-low z-high (halo-out launches only)
 };
 // TMA descriptors (CUtensorMap, 128 bytes each) used by one stage launch:
 // the stencil input with its halo box, and 32x8 point boxes of the metric,
@@ -85,7 +96,7 @@ struct alignas(64) CgStageDesc {
 };
 // One session's stage, its descriptor passed as a kernel parameter.
 cudaError_t launch_cg_stage(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,
-                            cudaStream_t st);
+                            cudaStream_t st, bool halo_out = false);
 // A batch: session s owns work items item_start[s] .. item_start[s+1]-1, its
 // descriptor is descs[s] in device memory; all advance with the same FB
 // signs and stage number.

@@ -370,6 +370,7 @@ void Session::stage_desc(int irk, CgStageDesc &d) const
     a.DT = (float)m.p.DT;
     a.err = err_dev_;
     a.ntiles_x = ntx_, a.ntiles_y = nty_, a.nchunk = nchunk_;
+    for (int f = 0; f < 6; f++) a.ho[f] = ho_[irk][f];
     std::memcpy(d.tmW, maps_[win_map[irk]].win, 128);
     std::memcpy(d.tmC, maps_[win_map[irk]].cjm, 128);
     std::memcpy(d.tmM, maps_[win_map[irk]].wm, 128);

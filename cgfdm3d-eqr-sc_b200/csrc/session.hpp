@@ -36,6 +36,10 @@ public:
     int part_advance(int *phase_done);
     long long halo_count(int face, int which) const;      // floats; which 0 wavefield, 1 metric (13 fields)
     int halo_copy(int face, int which, float *dev, bool pack);
+    // the stage kernel stores the layers next to `face` into the neighbour
+    // part's halo directly (same device, or peer memory): the halo exchange
+    // of phases 1..4 folded into the stages
+    int link_halo(int face, const Session &nbr);
     int run_timed(int nsteps, float *ms, float *stage_ms);
     int profile_stages(int nsteps, float *mean_stage_ms);
     double algo_bytes_per_step() const;
@@ -80,6 +84,8 @@ public:
     int it = 0;  // steps completed
     bool is_part_ = false;  // a part of a decomposition: stepped by part_advance
     int phase_ = 0, cur_ = 0;
+    bool halo_out_ = false;
+    HaloOut ho_[4][6] = {};  // per stage and face
     bool counted_ = false;  // registered with the device's gradient scratch
     int nst = 0;
     cudaStream_t stream = nullptr;

@@ -93,6 +93,12 @@ int cgfdm_create_part(const char *run_dir, const char *options_json, const int *
 int cgfdm_part_info(const cgfdm_session *s, int *lo, int *n, int *top);
 int cgfdm_part_station_ids(const cgfdm_session *s, int *ids, int count);
 int cgfdm_part_advance(cgfdm_session *s, int *phase);
+/* Folds the exchanges after phases 1..4 into the stage kernel: part s's
+ * stages store the interior layers next to `face` straight into the halo of
+ * neighbour part nbr (a session in the same process, on the same device or
+ * one whose memory s's device can address).  All parts must finish a phase
+ * before any starts the next; the exchange after phase 0 stays explicit. */
+int cgfdm_part_link(cgfdm_session *s, int face, const cgfdm_session *nbr);
 long long cgfdm_halo_count(const cgfdm_session *s, int face, int which);
 int cgfdm_halo_pack(cgfdm_session *s, int face, int which, float *d_buf);
 int cgfdm_halo_unpack(cgfdm_session *s, int face, int which, const float *d_buf);

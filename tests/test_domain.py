@@ -133,15 +133,19 @@ def _case():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("parts", [(2, 1, 2), (1, 2, 1), (2, 2, 2)])
-def test_decomposed_run_matches_single_domain(tmp_path, parts):
+@pytest.mark.parametrize("parts,fused", [((2, 1, 2), False), ((1, 2, 1), False), ((2, 2, 2), False),
+                                         ((2, 1, 2), True), ((2, 2, 2), True), ((3, 1, 1), True)])
+def test_decomposed_run_matches_single_domain(tmp_path, parts, fused):
+    """fused: the stage kernels store their boundary layers into the
+    neighbours' halos (cgfdm_part_link); only the exchange after the source
+    stays explicit."""
     c = _case()
     d = cases.write_case(c, str(tmp_path / "run"))
     with Session(d) as s:
         s.run(s.info.NT)
         ref = (s.wavefield()[3:-3, 3:-3, 3:-3], s.stations(), s.pgv()[..., :2])
         assert s.info.n_fault_cells > 1
-    got = domain.run_local(d, parts)
+    got = domain.run_local(d, parts, fused=fused)
     for a, b in zip(got, ref):
         np.testing.assert_array_equal(a, b)
     assert np.abs(got[0]).max() > 0
