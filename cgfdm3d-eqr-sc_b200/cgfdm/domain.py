@@ -105,6 +105,8 @@ class Part(Session):
         L.cgfdm_part_station_ids.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.cgfdm_part_advance.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
         L.cgfdm_part_link.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.cgfdm_part_handle.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong]
+        L.cgfdm_part_link_handle.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong]
         L.cgfdm_halo_count.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.cgfdm_halo_count.restype = ctypes.c_longlong
         L.cgfdm_halo_pack.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
@@ -132,6 +134,18 @@ class Part(Session):
     def link(self, face: int, nbr: "Part") -> None:
         """Stages store the layers next to `face` into nbr's halo directly."""
         self._check(self.L.cgfdm_part_link(self._h, face, nbr._h))
+
+    HANDLE_BYTES = 512
+
+    def handle(self) -> bytes:
+        """This part's stage buffers for a neighbour in another process."""
+        buf = ctypes.create_string_buffer(self.HANDLE_BYTES)
+        self._check(self.L.cgfdm_part_handle(self._h, buf, self.HANDLE_BYTES))
+        return buf.raw
+
+    def link_handle(self, face: int, handle: bytes) -> None:
+        buf = ctypes.create_string_buffer(handle, len(handle))
+        self._check(self.L.cgfdm_part_link_handle(self._h, face, buf, len(handle)))
 
     def halo_count(self, face: int, which: int) -> int:
         return int(self.L.cgfdm_halo_count(self._h, face, which))
@@ -234,10 +248,39 @@ def torch_transport(group, parts, coord):
     return move
 
 
+def link_neighbours(part, coord, parts, group=None) -> None:
+    """Every rank publishes its part's handle; each part links the handles
+    of its face neighbours (the stages then write their halos directly)."""
+    import torch.distributed as dist
+
+    handles = [None] * dist.get_world_size(group)
+    dist.all_gather_object(handles, part.handle(), group=group)
+    for f in range(FACES):
+        q = neighbour(parts, coord, f)
+        if q is not None:
+            part.link_handle(f, handles[rank_of(parts, q)])
+
+
+def step_distributed(part, coord, parts, nsteps: int, move, barrier, fused: bool, sync=lambda: None) -> None:
+    """nsteps steps of one part: the five phases, after each either the
+    exchange (phase 0 always; 1..3 unless fused) or, when fused, a barrier
+    so that no part starts a phase before its neighbours' stores landed."""
+    for _ in range(nsteps):
+        for phase in range(5):
+            part.advance()
+            sync()
+            if phase == 0 or (phase < 4 and not fused):
+                exchange(part, coord, parts, 0, move)
+            elif fused:
+                barrier()
+
+
 def run_distributed(run_dir: str, parts: Sequence[int], nsteps: Optional[int] = None,
-                    options: Optional[str] = None, group=None):
+                    options: Optional[str] = None, group=None, fused: bool = False):
     """One part per rank (rank r holds coord_of(parts, r), on cuda:LOCAL_RANK);
-    returns this part's session after the steps, for its outputs."""
+    returns this part's session after the steps, for its outputs.  fused:
+    neighbours' buffers are linked through CUDA IPC and the stage kernels
+    store into them over NVLink."""
     import os
 
     import torch
@@ -250,11 +293,9 @@ def run_distributed(run_dir: str, parts: Sequence[int], nsteps: Optional[int] = 
     p = Part(run_dir, parts, coord, options, dev)
     move = torch_transport(group, parts, coord)
     exchange(p, coord, parts, 1, move)
+    if fused:
+        link_neighbours(p, coord, parts, group)
     NT = p.info.NT
-    for _ in range(NT if nsteps is None else min(nsteps, NT)):
-        for phase in range(5):
-            p.advance()
-            if phase < 4:
-                torch.cuda.synchronize(dev)
-                exchange(p, coord, parts, 0, move)
+    step_distributed(p, coord, parts, NT if nsteps is None else min(nsteps, NT), move,
+                     lambda: dist.barrier(group), fused, lambda: torch.cuda.synchronize(dev))
     return p

@@ -105,6 +105,18 @@ int cgfdm_part_link(cgfdm_session *s, int face, const cgfdm_session *nbr)
     return s->s.link_halo(face, nbr->s);
 }
 
+int cgfdm_part_handle(cgfdm_session *s, void *out, long long bytes)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.part_handle(out, bytes);
+}
+
+int cgfdm_part_link_handle(cgfdm_session *s, int face, const void *handle, long long bytes)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.link_halo_handle(face, handle, bytes);
+}
+
 long long cgfdm_halo_count(const cgfdm_session *s, int face, int which)
 {
     if (!s) return -1;

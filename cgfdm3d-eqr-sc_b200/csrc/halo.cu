@@ -9,6 +9,7 @@
 // padded extent of the other two axes, so edge and corner halos are filled
 // too.  The same exchange refreshes the metric fields after set-up.
 #include <algorithm>
+#include <cstring>
 
 #include "device.cuh"
 #include "kernels.cuh"
@@ -84,18 +85,18 @@ int Session::halo_copy(int face, int which, float *dev, bool pack)
     return ST_OK;
 }
 
-int Session::link_halo(int face, const Session &nbr)
+int Session::link_halo_to(int face, float *const nw[3], const DevGrid &ng)
 {
-    if (face < 0 || face > 5 || nbr.m.p.scheme != SCHEME_CGFDM || m.p.scheme != SCHEME_CGFDM) {
-        err = "bad face or scheme for a halo link";
+    if (face < 0 || face > 5 || m.p.scheme != SCHEME_CGFDM || !nw[0] || !nw[1] || !nw[2]) {
+        err = "bad face, scheme or buffers for a halo link";
         return ST_ARG;
     }
     const int axis = face / 2;
     const int n_self = axis == 0 ? g.nx : axis == 1 ? g.ny : g.nz;
-    const int n_nbr = axis == 0 ? nbr.g.nx : axis == 1 ? nbr.g.ny : nbr.g.nz;
+    const int n_nbr = axis == 0 ? ng.nx : axis == 1 ? ng.ny : ng.nz;
     // the other two axes must match (a tensor-product decomposition)
     const int os[2] = {axis == 0 ? g.nyp : g.nxp, axis == 2 ? g.nyp : g.nzp};
-    const int on[2] = {axis == 0 ? nbr.g.nyp : nbr.g.nxp, axis == 2 ? nbr.g.nyp : nbr.g.nzp};
+    const int on[2] = {axis == 0 ? ng.nyp : ng.nxp, axis == 2 ? ng.nyp : ng.nzp};
     if (os[0] != on[0] || os[1] != on[1]) {
         err = "the neighbour's grid does not match on the shared face";
         return ST_ARG;
@@ -103,15 +104,73 @@ int Session::link_halo(int face, const Session &nbr)
     static const int wout[4] = {1, 2, 1, 0};   // output buffer of RK stage irk
     for (int irk = 0; irk < 4; irk++) {
         HaloOut &h = ho_[irk][face];
-        h.base = nbr.W_[wout[irk]];
-        h.plane = nbr.g.plane, h.fstride = nbr.g.fstride;
-        h.pitch = nbr.g.pitch, h.xoff = nbr.g.xoff;
+        h.base = nw[wout[irk]];
+        h.plane = ng.plane, h.fstride = ng.fstride;
+        h.pitch = ng.pitch, h.xoff = ng.xoff;
         // high face: interior n_self..n_self+2 -> neighbour halo 0..2;
         // low face: interior 3..5 -> neighbour halo n_nbr+3..n_nbr+5
         h.shift = (face & 1) ? -n_self : n_nbr;
     }
     halo_out_ = true;
     return build_stage_descs();
+}
+
+int Session::link_halo(int face, const Session &nbr)
+{
+    if (nbr.m.p.scheme != SCHEME_CGFDM) {
+        err = "the neighbour is not a CGFDM part";
+        return ST_ARG;
+    }
+    float *const nw[3] = {nbr.W_[0], nbr.W_[1], nbr.W_[2]};
+    return link_halo_to(face, nw, nbr.g);
+}
+
+// A part's stage buffers for a neighbour in another process: CUDA IPC
+// handles of buffers A, B, C and their layout.
+struct PartHandle {
+    cudaIpcMemHandle_t w[3];
+    DevGrid g;
+    long long magic;
+};
+static const long long PART_HANDLE_MAGIC = 0x48545241504d4447LL;
+
+int Session::part_handle(void *out, long long bytes)
+{
+    static_assert(sizeof(PartHandle) <= 512, "handle size");
+    if (!out || bytes < (long long)sizeof(PartHandle) || m.p.scheme != SCHEME_CGFDM) {
+        err = "handle buffer too small or not a CGFDM part";
+        return ST_ARG;
+    }
+    PartHandle h;
+    std::memset(&h, 0, sizeof h);
+    for (int b = 0; b < 3; b++) CU(cudaIpcGetMemHandle(&h.w[b], W_[b]));
+    h.g = g;
+    h.magic = PART_HANDLE_MAGIC;
+    std::memcpy(out, &h, sizeof h);
+    return ST_OK;
+}
+
+int Session::link_halo_handle(int face, const void *handle, long long bytes)
+{
+    PartHandle h;
+    if (!handle || bytes < (long long)sizeof h) {
+        err = "bad part handle";
+        return ST_ARG;
+    }
+    std::memcpy(&h, handle, sizeof h);
+    if (h.magic != PART_HANDLE_MAGIC) {
+        err = "bad part handle";
+        return ST_ARG;
+    }
+    CU(cudaSetDevice(device));
+    float *nw[3];
+    for (int b = 0; b < 3; b++) {
+        void *p = nullptr;
+        CU(cudaIpcOpenMemHandle(&p, h.w[b], cudaIpcMemLazyEnablePeerAccess));
+        ipc_open_.push_back(p);
+        nw[b] = (float *)p;
+    }
+    return link_halo_to(face, nw, h.g);
 }
 
 int Session::create_part(const std::string &dir, const std::string &options, const int parts[3],

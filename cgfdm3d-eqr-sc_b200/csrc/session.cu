@@ -88,6 +88,7 @@ Session::~Session()
     if (graph8_src_) cudaGraphDestroy(graph8_src_);
     for (auto &e : ev_)
         if (e) cudaEventDestroy(e);
+    for (void *p : ipc_open_) cudaIpcCloseMemHandle(p);
     for (void *p : allocs_) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
 }

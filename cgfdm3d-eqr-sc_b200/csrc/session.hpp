@@ -40,6 +40,10 @@ public:
     // part's halo directly (same device, or peer memory): the halo exchange
     // of phases 1..4 folded into the stages
     int link_halo(int face, const Session &nbr);
+    int link_halo_to(int face, float *const nbr_w[3], const DevGrid &nbr_g);
+    // the same across processes: CUDA IPC handles of the stage buffers
+    int part_handle(void *out, long long bytes);
+    int link_halo_handle(int face, const void *handle, long long bytes);
     int run_timed(int nsteps, float *ms, float *stage_ms);
     int profile_stages(int nsteps, float *mean_stage_ms);
     double algo_bytes_per_step() const;
@@ -86,6 +90,7 @@ public:
     int phase_ = 0, cur_ = 0;
     bool halo_out_ = false;
     HaloOut ho_[4][6] = {};  // per stage and face
+    std::vector<void *> ipc_open_;  // neighbours' buffers opened from IPC handles
     bool counted_ = false;  // registered with the device's gradient scratch
     int nst = 0;
     cudaStream_t stream = nullptr;

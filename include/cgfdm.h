@@ -99,6 +99,14 @@ int cgfdm_part_advance(cgfdm_session *s, int *phase);
  * one whose memory s's device can address).  All parts must finish a phase
  * before any starts the next; the exchange after phase 0 stays explicit. */
 int cgfdm_part_link(cgfdm_session *s, int face, const cgfdm_session *nbr);
+/* The same between processes (one part per GPU): cgfdm_part_handle writes
+ * CGFDM_PART_HANDLE_BYTES describing the part's stage buffers (CUDA IPC
+ * handles and layout) for its neighbours; cgfdm_part_link_handle(face)
+ * opens a neighbour's handle (peer access over NVLink) and links it.  A
+ * barrier between phases then replaces the halo exchange of phases 1..4. */
+#define CGFDM_PART_HANDLE_BYTES 512
+int cgfdm_part_handle(cgfdm_session *s, void *out, long long bytes);
+int cgfdm_part_link_handle(cgfdm_session *s, int face, const void *handle, long long bytes);
 long long cgfdm_halo_count(const cgfdm_session *s, int face, int which);
 int cgfdm_halo_pack(cgfdm_session *s, int face, int which, float *d_buf);
 int cgfdm_halo_unpack(cgfdm_session *s, int face, int which, const float *d_buf);

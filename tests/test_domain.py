@@ -13,6 +13,7 @@ CPU: the decomposition's arithmetic, and the exchange orchestration between
 two gloo ranks with array-backed parts: each rank's halos must equal its
 neighbour's interior layers afterwards."""
 
+import datetime
 import os
 import socket
 
@@ -126,6 +127,61 @@ def test_exchange_between_gloo_ranks(tmp_path, parts):
             np.testing.assert_array_equal(got, (Z * shape[1] + Y) * shape[0] + X)
 
 
+class LinkPart(ArrayPart):
+    """An array-backed part that records its links, phases and exchanges."""
+
+    def __init__(self, shape, parts, coord, rank):
+        super().__init__(shape, parts, coord)
+        self.rank, self.links, self.phases, self.packs = rank, {}, 0, 0
+
+    def handle(self):
+        return f"part-of-rank-{self.rank}".encode().ljust(32, b"\0")
+
+    def link_handle(self, face, handle):
+        self.links[face] = handle.rstrip(b"\0").decode()
+
+    def advance(self):
+        self.phases += 1
+
+    def pack(self, face, which, buf):
+        self.packs += 1
+        super().pack(face, which, buf)
+
+
+def _link_worker(rank, world, port, shape, parts, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        coord = domain.coord_of(parts, rank)
+        p = LinkPart(shape, parts, coord, rank)
+        domain.link_neighbours(p, coord, parts)
+        barriers = []
+        domain.step_distributed(p, coord, parts, 3, domain.torch_transport(None, parts, coord),
+                                lambda: (barriers.append(1), dist.barrier()), True)
+        np.save(os.path.join(out, f"r{rank}.npy"),
+                np.array([p.phases, p.packs, len(barriers)] + sorted(p.links)))
+        with open(os.path.join(out, f"r{rank}.txt"), "w") as f:
+            f.write(",".join(p.links[k] for k in sorted(p.links)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_fused_orchestration_between_gloo_ranks(tmp_path):
+    """Handles reach the face neighbours; with the stores fused, a step is
+    five phases, one exchange (after the source) and four barriers."""
+    shape, parts = (14, 9, 12), (3, 1, 1)
+    mp.spawn(_link_worker, args=(3, _free_port(), shape, parts, str(tmp_path)), nprocs=3, join=True)
+    expect_links = {0: [1], 1: [0, 1], 2: [0]}
+    for r in range(3):
+        v = np.load(tmp_path / f"r{r}.npy")
+        nfaces = len(expect_links[r])
+        assert v[0] == 15 and v[1] == 3 * nfaces and v[2] == 12
+        assert list(v[3:]) == expect_links[r]
+        names = open(tmp_path / f"r{r}.txt").read().split(",")
+        nb = [domain.rank_of(parts, domain.neighbour(parts, domain.coord_of(parts, r), f)) for f in expect_links[r]]
+        assert names == [f"part-of-rank-{q}" for q in nb]
+
+
 def _case():
     c = pu.multi_fault(steps=24, courant=0.45)
     c.gauss_hill = 1
@@ -149,6 +205,68 @@ def test_decomposed_run_matches_single_domain(tmp_path, parts, fused):
     for a, b in zip(got, ref):
         np.testing.assert_array_equal(a, b)
     assert np.abs(got[0]).max() > 0
+
+
+def _staged_transport(parts, coord):
+    """send/recv of device buffers through host memory (gloo moves CPU
+    tensors only)."""
+    def move(send, recv):
+        cs = {f: b.cpu() for f, b in send.items()}
+        cr = {f: torch.empty(b.numel()) for f, b in recv.items()}
+        peer = lambda f: domain.rank_of(parts, domain.neighbour(parts, coord, f))
+        ops = [dist.P2POp(dist.isend, cs[f], peer(f)) for f in cs] + [dist.P2POp(dist.irecv, cr[f], peer(f)) for f in cr]
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+        for f, b in recv.items():
+            b.copy_(cr[f])
+    return move
+
+
+def _ipc_worker(rank, world, port, run_dir, parts, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        coord = domain.coord_of(parts, rank)
+        p = domain.Part(run_dir, parts, coord, device=0)
+        move = _staged_transport(parts, coord)
+        domain.exchange(p, coord, parts, 1, move)
+        domain.link_neighbours(p, coord, parts)
+        domain.step_distributed(p, coord, parts, p.info.NT, move, dist.barrier, True, torch.cuda.synchronize)
+        np.savez(os.path.join(out, f"part{rank}.npz"), W=p.wavefield()[3:-3, 3:-3, 3:-3], st=p.stations(),
+                 pgv=p.pgv()[..., :2], lo=p.lo, n=p.n, ids=np.array(p.station_ids, int), top=p.top)
+        dist.barrier()   # no part unmaps its buffers while a neighbour may still use them
+        p.close()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_fused_parts_in_two_processes_match_single_domain(tmp_path):
+    """Two processes, one part each, on one GPU: the neighbours' stage
+    buffers linked through CUDA IPC handles, the stage kernels storing their
+    boundary layers into the other process's memory, host barriers between
+    phases (no kernel waits on another).  Bit-identical to one session."""
+    c = _case()
+    d = cases.write_case(c, str(tmp_path / "run"))
+    parts = (2, 1, 1)
+    mp.spawn(_ipc_worker, args=(2, _free_port(), d, parts, str(tmp_path)), nprocs=2, join=True)
+    with Session(d) as s:
+        s.run(s.info.NT)
+        ref = (s.wavefield()[3:-3, 3:-3, 3:-3], s.stations(), s.pgv()[..., :2])
+    W = np.zeros_like(ref[0])
+    st = np.zeros_like(ref[1])
+    pgv = np.zeros_like(ref[2])
+    for r in range(2):
+        z = np.load(tmp_path / f"part{r}.npz")
+        (x0, y0, z0), (lx, ly, lz) = z["lo"], z["n"]
+        W[z0:z0 + lz, y0:y0 + ly, x0:x0 + lx] = z["W"]
+        if len(z["ids"]):
+            st[z["ids"]] = z["st"]
+        if z["top"]:
+            pgv[y0:y0 + ly, x0:x0 + lx] = z["pgv"]
+    for a, b in zip((W, st, pgv), ref):
+        np.testing.assert_array_equal(a, b)
 
 
 @pytest.mark.gpu
