@@ -195,12 +195,14 @@ def _assemble(ps: Dict, shape, nst_total: int, NT: int):
 
 
 def run_local(run_dir: str, parts: Sequence[int], nsteps: Optional[int] = None, options: Optional[str] = None,
-              device: int = 0, flavor: str = "fast", fused: bool = False):
+              device: int = 0, flavor: str = "fast", fused: bool = False, write_outputs: bool = False):
     """Every part on one GPU; returns the interior wavefield [nz][ny][nx][9],
     the station traces [n][NT][9] in the run's station order and the PGV
     [ny][nx][2], assembled from the parts.  fused: the stages store their
     boundary layers into the neighbours' halos (cgfdm_part_link), leaving
-    one explicit exchange per step, after the source."""
+    one explicit exchange per step, after the source.  write_outputs: every
+    part writes its station and PGV files under its rank coordinates, as
+    the reference's ranks do."""
     parts = tuple(parts)
     ps = {}
     try:
@@ -225,6 +227,9 @@ def run_local(run_dir: str, parts: Sequence[int], nsteps: Optional[int] = None, 
                     _exchange_all_local(ps, parts, 0)
         shape = tuple(max(p.lo[a] + p.n[a] for p in ps.values()) for a in range(3))
         nst_total = 1 + max([max(p.station_ids) for p in ps.values() if p.station_ids], default=-1)
+        if write_outputs:
+            for p in ps.values():
+                p.write_outputs()
         return _assemble(ps, shape, nst_total, NT)
     finally:
         for p in ps.values():

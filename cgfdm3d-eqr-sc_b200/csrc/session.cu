@@ -699,6 +699,15 @@ std::string Session::out_dir() const
     return out;
 }
 
+// "_mpi_X_Y_Z": the rank coordinates in every output file name
+// (src/station.cpp:426, src/PGV.cpp:181, src/data_io.cpp:368-424); a part of a
+// decomposed grid writes under its own coordinates.
+static std::string rank_tag(const Model &m)
+{
+    return "_mpi_" + std::to_string(m.part_coord[0]) + "_" + std::to_string(m.part_coord[1]) + "_" +
+           std::to_string(m.part_coord[2]);
+}
+
 // ---------------------------------------------------------------- snapshots
 bool Session::snapshots_on() const
 {
@@ -709,8 +718,8 @@ bool Session::snapshots_on() const
 }
 
 // Velocity slices after step `step` (data2D_XYZ_out, src/data_io.cpp:485-560):
-// OUT/V{x,y,z}_<step>_{X,Y,Z}_mpi_0_0_0.bin at the configured slices and,
-// with sliceFreeSurf, OUT/FreeSurfV{x,y,z}_<step>_Z_mpi_0_0_0.bin of the top
+// OUT/V{x,y,z}_<step>_{X,Y,Z}_mpi_X_Y_Z.bin at the configured slices and,
+// with sliceFreeSurf, OUT/FreeSurfV{x,y,z}_<step>_Z_mpi_X_Y_Z.bin of the top
 // layer; with displacement on, OUT/FreeSurfU{x,y,z}_<step>_Z_... as well
 // (src/data_io.cpp:613-626).
 int Session::write_snapshots(int step)
@@ -726,7 +735,7 @@ int Session::write_snapshots(int step)
         CU(cudaMemcpyAsync(host.data(), slice_dev_, sizeof(float) * n0 * n1, cudaMemcpyDeviceToHost, stream));
         CU(cudaStreamSynchronize(stream));
         const char ax = "XYZ"[axis];
-        std::string path = out + "/" + name + "_" + ax + "_mpi_0_0_0.bin";
+        std::string path = out + "/" + name + "_" + ax + rank_tag(m) + ".bin";
         FILE *fp = std::fopen(path.c_str(), "wb");
         if (!fp) {
             err = "cannot write " + path;
@@ -768,7 +777,9 @@ int Session::write_snapshots(int step)
 static int write_model_slices(const Model &m, const std::string &out)
 {
     const Grid &G = m.g;
-    const int idx[3] = {m.p.sliceX + HALO, m.p.sliceY + HALO, m.p.sliceZ + HALO};
+    // global slice index to this part's padded index (src/data_io.cpp:26-60)
+    const int idx[3] = {m.p.sliceX + HALO - m.part_lo[0], m.p.sliceY + HALO - m.part_lo[1],
+                        m.p.sliceZ + HALO - m.part_lo[2]};
     const int lim[3] = {G._nx, G._ny, G._nz};
     const char *names[6] = {"coordX", "coordY", "coordZ", "Vs", "Vp", "rho"};
     for (int v = 0; v < 6; v++) {
@@ -787,7 +798,7 @@ static int write_model_slices(const Model &m, const std::string &out)
                     const long long p = ((long long)k * G._ny_ + j) * G._nx_ + i;
                     buf[(size_t)a1 * n0 + a0] = src[p * 3 + (v % 3)];
                 }
-            std::string path = out + "/" + names[v] + "_" + "XYZ"[axis] + "_mpi_0_0_0.bin";
+            std::string path = out + "/" + names[v] + "_" + "XYZ"[axis] + rank_tag(m) + ".bin";
             FILE *fp = std::fopen(path.c_str(), "wb");
             if (!fp) return ST_IO;
             std::fwrite(buf.data(), sizeof(float), buf.size(), fp);
@@ -813,7 +824,7 @@ static int write_projection(const Model &m, const std::string &out)
         }
     const std::pair<const char *, const std::vector<float> *> files[3] = {{"lon", &lon}, {"lat", &lat}, {"terrain", &h}};
     for (auto &f : files) {
-        std::string path = out + "/" + f.first + "_mpi_0_0_0.bin";
+        std::string path = out + "/" + f.first + rank_tag(m) + ".bin";
         FILE *fp = std::fopen(path.c_str(), "wb");
         if (!fp) return ST_IO;
         std::fwrite(f.second->data(), sizeof(float), f.second->size(), fp);
@@ -834,18 +845,18 @@ int Session::write_outputs() const
         std::vector<float> w((size_t)nst * m.NT * 9);
         int st = get_stations(w.data());
         if (st) return st;
-        std::string path = out + "/station_mpi_0_0_0.bin";
+        std::string path = out + "/station" + rank_tag(m) + ".bin";
         FILE *fp = std::fopen(path.c_str(), "wb");
         if (!fp) return ST_IO;
         std::fwrite(m.stations_global.data(), sizeof(int), (size_t)nst * 3, fp);
         std::fwrite(w.data(), sizeof(float), w.size(), fp);
         std::fclose(fp);
     }
-    {
+    if (m.fs_top) {   // the ranks holding the free surface (src/propagate.cpp:108-118, 347-353)
         std::vector<float> p((size_t)m.g.nx * m.g.ny * pgv_fields());
         int st = get_pgv(p.data());
         if (st) return st;
-        std::string path = out + "/PGV_Z_mpi_0_0_0.bin";
+        std::string path = out + "/PGV_Z" + rank_tag(m) + ".bin";
         FILE *fp = std::fopen(path.c_str(), "wb");
         if (!fp) return ST_IO;
         std::fwrite(p.data(), sizeof(float), p.size(), fp);

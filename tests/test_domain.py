@@ -270,6 +270,50 @@ def test_fused_parts_in_two_processes_match_single_domain(tmp_path):
 
 
 @pytest.mark.gpu
+def test_parts_write_per_rank_files(tmp_path):
+    """Each part writes station_mpi_X_Y_Z.bin (its stations' global indices
+    and traces) and, in the top parts, PGV_Z_mpi_X_Y_Z.bin; together they
+    hold exactly the single-domain run's files."""
+    c = _case()
+    d = cases.write_case(c, str(tmp_path / "run"))
+    with Session(d) as s:
+        s.run(s.info.NT)
+        s.write_outputs()
+        NT, NX, NY = s.info.NT, s.info.nx, s.info.ny
+    out = os.path.join(d, "output")
+    ref_st = np.fromfile(os.path.join(out, "station_mpi_0_0_0.bin"), np.uint8)
+    ref_pgv = np.fromfile(os.path.join(out, "PGV_Z_mpi_0_0_0.bin"), np.float32).reshape(NY, NX, 2)
+    os.remove(os.path.join(out, "station_mpi_0_0_0.bin"))
+    os.remove(os.path.join(out, "PGV_Z_mpi_0_0_0.bin"))
+    parts = (2, 1, 2)
+    domain.run_local(d, parts, write_outputs=True)
+    rows = {}
+    pgv = np.zeros_like(ref_pgv)
+    for p in domain.plan((NX, NY, c.NZ), parts):
+        tag = "_mpi_%d_%d_%d.bin" % p["coord"]
+        f = os.path.join(out, "station" + tag)
+        if os.path.exists(f):
+            raw = np.fromfile(f, np.uint8)
+            n = raw.size // (12 + NT * 36)
+            xyz = np.frombuffer(raw[: n * 12].tobytes(), np.int32).reshape(n, 3)
+            tr = np.frombuffer(raw[n * 12:].tobytes(), np.float32).reshape(n, NT, 9)
+            for a, b in zip(xyz, tr):
+                rows[tuple(a)] = b
+        g = os.path.join(out, "PGV_Z" + tag)
+        assert os.path.exists(g) == p["top"]
+        if p["top"]:
+            (x0, y0, _), (lx, ly, _) = p["lo"], p["n"]
+            pgv[y0:y0 + ly, x0:x0 + lx] = np.fromfile(g, np.float32).reshape(ly, lx, 2)
+    n = ref_st.size // (12 + NT * 36)
+    xyz = np.frombuffer(ref_st[: n * 12].tobytes(), np.int32).reshape(n, 3)
+    tr = np.frombuffer(ref_st[n * 12:].tobytes(), np.float32).reshape(n, NT, 9)
+    assert len(rows) == n
+    for a, b in zip(xyz, tr):
+        np.testing.assert_array_equal(rows[tuple(a)], b)
+    np.testing.assert_array_equal(pgv, ref_pgv)
+
+
+@pytest.mark.gpu
 def test_part_refuses_plain_run(tmp_path):
     from cgfdm import CgfdmError
 
