@@ -6,16 +6,48 @@
 #include "model.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <thread>
+#ifdef __linux__
+#include <sched.h>
+#endif
 
 #include "aeqd.h"
 
 namespace cgfdm {
+
+// f(k) for k = 0 .. n-1 on the host's cores: the model's per-plane loops
+// (every point's value depends on its own inputs only, so the result does
+// not depend on the split).
+template <class F>
+static void par_for(int n, F f)
+{
+    unsigned T = std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+#ifdef __linux__
+    {
+        cpu_set_t set;   // the cores this process may run on, not all the machine's
+        if (sched_getaffinity(0, sizeof set, &set) == 0) T = std::max(1u, std::min(T, (unsigned)CPU_COUNT(&set)));
+    }
+#endif
+    if (n < 2 || T == 1) {
+        for (int k = 0; k < n; k++) f(k);
+        return;
+    }
+    std::atomic<int> next(0);
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < std::min<unsigned>(T, (unsigned)n); t++)
+        th.emplace_back([&] {
+            for (int k; (k = next++) < n;) f(k);
+        });
+    for (auto &x : th) x.join();
+}
+
 
 // Constants as the reference defines them (src/macro.h:70-73): PI is a float
 // literal, DEGREE2RADIAN is PI converted to double over 180.0.
@@ -168,7 +200,7 @@ static void build_coords(Model &m)
     const int NZ = g.NZ;
     m.coord.assign((size_t)g.npad() * 3, 0.f);
     m.terrain.assign((size_t)g._nx_ * g._ny_, 0.f);
-    for (int k = 0; k < g._nz_; k++)
+    par_for(g._nz_, [&](int k) {
         for (int j = 0; j < g._ny_; j++)
             for (int i = 0; i < g._nx_; i++) {
                 long long id = g.idx(i, j, k) * 3;
@@ -178,12 +210,13 @@ static void build_coords(Model &m)
                 m.coord[id + 1] = (J - HALO) * DH - g.originalY * DH;
                 m.coord[id + 2] = (K - HALO + 1) * DH - NZ * DH;
             }
+    });
 }
 
 static void terrain_following_z(Model &m, float cal_depth)
 {
     const Grid &g = m.g;
-    for (int k = 0; k < g._nz_; k++)
+    par_for(g._nz_, [&](int k) {
         for (int j = 0; j < g._ny_; j++)
             for (int i = 0; i < g._nx_; i++) {
                 long long id = g.idx(i, j, k);
@@ -192,6 +225,7 @@ static void terrain_following_z(Model &m, float cal_depth)
                 float DZ = (float)(double(height + std::fabs(cal_depth)) / double(g.NZ - 1));
                 m.coord[id * 3 + 2] = -std::fabs(cal_depth) + DZ * K;
             }
+    });
 }
 
 static void gauss_hill(Model &m)
@@ -418,13 +452,14 @@ static void terrain_z_double(Model &m)
 {
     const Grid &g = m.g;
     const double Depth = m.p.Depth * 1e3;
-    for (int k = 0; k < g._nz_; k++)
+    par_for(g._nz_, [&](int k) {
         for (int j = 0; j < g._ny_; j++)
             for (int i = 0; i < g._nx_; i++) {
                 const int K = k - HALO;
                 const double DZ = double(m.terrain[(size_t)i + (size_t)j * g._nx_] + std::fabs(Depth)) / double(g.NZ - 1);
                 m.coord[g.idx(i, j, k) * 3 + 2] = (float)(-std::fabs(Depth) + DZ * K);
             }
+    });
 }
 
 // ----------------------------------------------------------------- medium
@@ -681,11 +716,14 @@ static int build_medium(Model &m, const std::string &run_dir, std::string &err)
 {
     const Grid &g = m.g;
     m.medium.resize((size_t)g.npad() * 3);
-    for (long long n = 0; n < g.npad(); n++) {
-        m.medium[n * 3 + 0] = 3300.0f;
-        m.medium[n * 3 + 1] = 5716.0f;
-        m.medium[n * 3 + 2] = 2700.0f;
-    }
+    const long long plane = (long long)g._nx_ * g._ny_;
+    par_for(g._nz_, [&](int k) {
+        for (long long n = k * plane; n < (k + 1) * plane; n++) {
+            m.medium[n * 3 + 0] = 3300.0f;
+            m.medium[n * 3 + 1] = 5716.0f;
+            m.medium[n * 3 + 2] = 2700.0f;
+        }
+    });
     if (!m.p.useMedium) return ST_OK;
     if (m.p.Crust_1Model)
         if (int st = crust_medium(m, run_dir, err)) return st;
@@ -719,7 +757,7 @@ static int build_medium(Model &m, const std::string &run_dir, std::string &err)
         rhod[F] = v[3] * 1000.f;
     }
     const float tolerance = 1.0f;
-    for (int k = 0; k < g._nz_; k++)
+    par_for(g._nz_, [&](int k) {
         for (int j = 0; j < g._ny_; j++)
             for (int i = 0; i < g._nx_; i++) {
                 long long id = g.idx(i, j, k);
@@ -736,6 +774,7 @@ static int build_medium(Model &m, const std::string &run_dir, std::string &err)
                     if ((h2 - tolerance) > coordz) md[0] = vsd[F], md[1] = vpd[F], md[2] = rhod[F];
                 }
             }
+    });
     return ST_OK;
 }
 
@@ -758,13 +797,26 @@ static int medium_file(Model &m, const std::string &path, std::string &err)
 static void value_ranges(Model &m)
 {
     // src/calc_CFL.cpp:165-180,283-285: ranges over the whole padded grid
+    // min and max per plane, then over planes (the order does not matter)
+    const int nz = m.g._nz_;
+    const long long plane = (long long)m.g._nx_ * m.g._ny_;
+    std::vector<float> pmn((size_t)nz * 3, 1.0e20f), pmx((size_t)nz * 3, -1.0e20f);
+    par_for(nz, [&](int k) {
+        float lo[3] = {1.0e20f, 1.0e20f, 1.0e20f}, hi[3] = {-1.0e20f, -1.0e20f, -1.0e20f};
+        const float *md = m.medium.data();
+        for (long long q = k * plane; q < (k + 1) * plane; q++)
+            for (int c = 0; c < 3; c++) {
+                float v = md[q * 3 + c];
+                if (v < lo[c]) lo[c] = v;
+                if (v > hi[c]) hi[c] = v;
+            }
+        for (int c = 0; c < 3; c++) pmn[k * 3 + c] = lo[c], pmx[k * 3 + c] = hi[c];
+    });
     float mn[3] = {1.0e20f, 1.0e20f, 1.0e20f}, mx[3] = {-1.0e20f, -1.0e20f, -1.0e20f};
-    const long long n = m.g.npad();
-    for (long long q = 0; q < n; q++)
+    for (int k = 0; k < nz; k++)
         for (int c = 0; c < 3; c++) {
-            float v = m.medium[q * 3 + c];
-            if (v < mn[c]) mn[c] = v;
-            if (v > mx[c]) mx[c] = v;
+            if (pmn[k * 3 + c] < mn[c]) mn[c] = pmn[k * 3 + c];
+            if (pmx[k * 3 + c] > mx[c]) mx[c] = pmx[k * 3 + c];
         }
     m.Vs_min = mn[0], m.Vs_max = mx[0];
     m.Vp_min = mn[1], m.Vp_max = mx[1];
@@ -1141,7 +1193,8 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
         return ST_OPTIONS;
     }
     if (p.PX != 1 || p.PY != 1 || p.PZ != 1) {
-        // single-GPU library: the decomposition is ignored, the whole grid runs on one device
+        // a session runs the whole grid on one device; a decomposition is
+        // explicit (cgfdm_create_part, partition.cpp)
         p.PX = p.PY = p.PZ = 1;
     }
     // src/modelChecking.cpp:17-61
@@ -1186,9 +1239,13 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
             if ((st = srtm_terrain(m, run_dir, err))) return st;
         terrain_z_double(m);
     }
-    if ((st = build_medium(m, run_dir, err))) return st;
-    if (!p.mediumFile.empty())
+    if (p.mediumFile.empty()) {
+        if ((st = build_medium(m, run_dir, err))) return st;
+    } else {
+        // a raw volume replaces whatever the switches would build
+        m.medium.resize((size_t)g.npad() * 3);
         if ((st = medium_file(m, join(run_dir, p.mediumFile), err))) return st;
+    }
     value_ranges(m);
     build_pml(m);
     build_point_source(m);
