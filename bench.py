@@ -479,6 +479,55 @@ def bench_adjoint(args, world, rank, local_rank):
 
 
 # ------------------------------------------------------------------- main
+def bench_parts(args, world, rank, local_rank):
+    """The workload decomposed into parts, all on this GPU: every phase of a
+    step on every part, halos refreshed between phases (stored by the stage
+    kernels with --exchange fused).  The parts synchronise with the host
+    after every phase, so the time is wall clock around the timed steps
+    (after a device synchronisation), against the same workload as one
+    session, device-timed."""
+    import torch
+
+    from cgfdm import Session, domain
+
+    if world != 1:
+        print(json.dumps({"metric": METRIC, "unavailable": "--parts runs every part on one GPU; N = 1 only"}))
+        return
+    parts = tuple(int(x) for x in args.parts.split(","))
+    total = args.warmup + args.steps + 8
+    d = os.path.join(WORK, f"{args.workload}_{total}")
+    make_workload(args.workload, total, d)
+    s = Session(d, device=local_rank)
+    pts = s.info.nx * s.info.ny * s.info.nz
+    s.run(args.warmup)
+    ms_one = s.run_timed(args.steps)
+    s.close()
+    dom = domain.LocalDomain(d, parts, device=local_rank, fused=args.exchange == "fused")
+    dom.step(args.warmup)
+    torch.cuda.synchronize(local_rank)
+    with ClockSampler(local_rank) as clk:
+        t0 = time.perf_counter()
+        dom.step(args.steps)
+        torch.cuda.synchronize(local_rank)
+        wall = time.perf_counter() - t0
+    nparts = len(dom.ps)
+    dom.close()
+    value = pts * args.steps / wall / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall * 1e3 / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "scheme": "CGFDM",
+        "timing": "wall clock around the timed steps (the parts synchronise with the host after every phase)",
+        "config": {"workload": workload_desc(args.workload), "points": pts, "parts": parts,
+                   "exchange": args.exchange, "l2": "inputs larger than L2",
+                   "parallelism": f"{nparts} parts on one GPU",
+                   "one_session_Mpts_step_s": pts * args.steps / (ms_one * 1e-3) / 1e6},
+        "gpu_launches": int(args.steps * nparts * (4 + 1)),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -490,6 +539,10 @@ def main():
     ap.add_argument("--checkpoint-every", type=int, default=100, help="adjoint workload: checkpoint interval")
     ap.add_argument("--store-segments", type=int, default=0,
                     help="adjoint workload: cap on segments stored during the first forward (0: memory decides)")
+    ap.add_argument("--parts", default="",
+                    help="CGFDM workloads, one GPU: run the grid as PX,PY,PZ parts (domain decomposition)")
+    ap.add_argument("--exchange", default="fused", choices=["fused", "explicit"],
+                    help="with --parts: halos stored by the stage kernels, or packed and copied per phase")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -518,6 +571,8 @@ def main():
 
     import torch
 
+    if args.parts:
+        return bench_parts(args, world, rank, local_rank)
     if args.workload.startswith("batch"):
         return bench_batch(args, world, rank, local_rank)
     if args.workload.startswith("adjoint"):

@@ -104,6 +104,8 @@ class Part(Session):
         L.cgfdm_part_info.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 3
         L.cgfdm_part_station_ids.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.cgfdm_part_advance.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        L.cgfdm_part_launch.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        L.cgfdm_part_finish.argtypes = [ctypes.c_void_p]
         L.cgfdm_part_link.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         L.cgfdm_part_handle.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong]
         L.cgfdm_part_link_handle.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_longlong]
@@ -130,6 +132,15 @@ class Part(Session):
         ph = ctypes.c_int()
         self._check(self.L.cgfdm_part_advance(self._h, ctypes.byref(ph)))
         return ph.value
+
+    def launch(self) -> int:
+        """Enqueue the next phase (finish() waits for it)."""
+        ph = ctypes.c_int()
+        self._check(self.L.cgfdm_part_launch(self._h, ctypes.byref(ph)))
+        return ph.value
+
+    def finish(self) -> None:
+        self._check(self.L.cgfdm_part_finish(self._h))
 
     def link(self, face: int, nbr: "Part") -> None:
         """Stages store the layers next to `face` into nbr's halo directly."""
@@ -194,6 +205,60 @@ def _assemble(ps: Dict, shape, nst_total: int, NT: int):
     return W, st, pgv
 
 
+class LocalDomain:
+    """Every part of a decomposition in this process on one GPU, halos moved
+    by device copies (or, fused, stored by the stage kernels)."""
+
+    def __init__(self, run_dir: str, parts: Sequence[int], options: Optional[str] = None, device: int = 0,
+                 flavor: str = "fast", fused: bool = False):
+        self.parts, self.fused = tuple(parts), fused
+        self.ps: Dict = {}
+        try:
+            for r in range(parts[0] * parts[1] * parts[2]):
+                c = coord_of(self.parts, r)
+                self.ps[c] = Part(run_dir, self.parts, c, options, device, flavor)
+            _exchange_all_local(self.ps, self.parts, 1)      # metric and medium halos
+            if fused:
+                for c, p in self.ps.items():
+                    for f in range(FACES):
+                        q = neighbour(self.parts, c, f)
+                        if q is not None:
+                            p.link(f, self.ps[q])
+        except Exception:
+            self.close()
+            raise
+        any_part = next(iter(self.ps.values()))
+        self.NT = any_part.info.NT
+        self.it = 0
+        self.shape = tuple(max(p.lo[a] + p.n[a] for p in self.ps.values()) for a in range(3))
+
+    def step(self, n: int) -> None:
+        n = min(n, self.NT - self.it)
+        for _ in range(n):
+            for phase in range(5):
+                for p in self.ps.values():        # the parts' kernels run concurrently
+                    assert p.launch() == phase
+                for p in self.ps.values():
+                    p.finish()
+                if phase == 0 or (phase < 4 and not self.fused):
+                    _exchange_all_local(self.ps, self.parts, 0)
+        self.it += n
+
+    def outputs(self):
+        """Interior wavefield, station traces in the run's order, PGV."""
+        nst_total = 1 + max([max(p.station_ids) for p in self.ps.values() if p.station_ids], default=-1)
+        return _assemble(self.ps, self.shape, nst_total, self.NT)
+
+    def write_outputs(self) -> None:
+        for p in self.ps.values():
+            p.write_outputs()
+
+    def close(self) -> None:
+        for p in self.ps.values():
+            p.close()
+        self.ps = {}
+
+
 def run_local(run_dir: str, parts: Sequence[int], nsteps: Optional[int] = None, options: Optional[str] = None,
               device: int = 0, flavor: str = "fast", fused: bool = False, write_outputs: bool = False):
     """Every part on one GPU; returns the interior wavefield [nz][ny][nx][9],
@@ -203,37 +268,14 @@ def run_local(run_dir: str, parts: Sequence[int], nsteps: Optional[int] = None, 
     one explicit exchange per step, after the source.  write_outputs: every
     part writes its station and PGV files under its rank coordinates, as
     the reference's ranks do."""
-    parts = tuple(parts)
-    ps = {}
+    dom = LocalDomain(run_dir, parts, options, device, flavor, fused)
     try:
-        for r in range(parts[0] * parts[1] * parts[2]):
-            c = coord_of(parts, r)
-            ps[c] = Part(run_dir, parts, c, options, device, flavor)
-        _exchange_all_local(ps, parts, 1)           # metric and medium halos
-        if fused:
-            for c, p in ps.items():
-                for f in range(FACES):
-                    q = neighbour(parts, c, f)
-                    if q is not None:
-                        p.link(f, ps[q])
-        any_part = next(iter(ps.values()))
-        NT = any_part.info.NT
-        steps = NT if nsteps is None else min(nsteps, NT)
-        for _ in range(steps):
-            for phase in range(5):
-                for p in ps.values():
-                    assert p.advance() == phase
-                if phase == 0 or (phase < 4 and not fused):
-                    _exchange_all_local(ps, parts, 0)
-        shape = tuple(max(p.lo[a] + p.n[a] for p in ps.values()) for a in range(3))
-        nst_total = 1 + max([max(p.station_ids) for p in ps.values() if p.station_ids], default=-1)
+        dom.step(dom.NT if nsteps is None else nsteps)
         if write_outputs:
-            for p in ps.values():
-                p.write_outputs()
-        return _assemble(ps, shape, nst_total, NT)
+            dom.write_outputs()
+        return dom.outputs()
     finally:
-        for p in ps.values():
-            p.close()
+        dom.close()
 
 
 def torch_transport(group, parts, coord):

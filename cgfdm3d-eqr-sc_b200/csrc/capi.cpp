@@ -99,6 +99,18 @@ int cgfdm_part_advance(cgfdm_session *s, int *phase)
     return s->s.part_advance(phase);
 }
 
+int cgfdm_part_launch(cgfdm_session *s, int *phase)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.part_launch(phase);
+}
+
+int cgfdm_part_finish(cgfdm_session *s)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.part_finish();
+}
+
 int cgfdm_part_link(cgfdm_session *s, int face, const cgfdm_session *nbr)
 {
     if (!s || !nbr) return CGFDM_E_ARG;

@@ -197,6 +197,20 @@ int Session::create_part(const std::string &dir, const std::string &options, con
 // wrote, the one the halo exchange refreshes.
 int Session::part_advance(int *phase_done)
 {
+    if (int st = part_launch(phase_done)) return st;
+    return part_finish();
+}
+
+int Session::part_finish()
+{
+    CU(cudaStreamSynchronize(stream));
+    return check_device_error();
+}
+
+// The launches of the next phase, not waited for (part_finish waits): the
+// parts of one GPU then run their phases concurrently.
+int Session::part_launch(int *phase_done)
+{
     if (m.p.scheme != SCHEME_CGFDM) {
         err = "part stepping is built for the CGFDM scheme";
         return ST_OPTIONS;
@@ -227,8 +241,7 @@ int Session::part_advance(int *phase_done)
     }
     phase_ = (ph + 1) % 5;
     if (phase_done) *phase_done = ph;
-    CU(cudaStreamSynchronize(stream));
-    return check_device_error();
+    return ST_OK;
 }
 
 }  // namespace cgfdm

@@ -33,7 +33,9 @@ public:
     // step in five phases with a halo exchange after each of the first four
     int create_part(const std::string &run_dir, const std::string &options, const int parts[3], const int coord[3],
                     int device);
-    int part_advance(int *phase_done);
+    int part_advance(int *phase_done);    // part_launch + part_finish
+    int part_launch(int *phase_done);
+    int part_finish();
     long long halo_count(int face, int which) const;      // floats; which 0 wavefield, 1 metric (13 fields)
     int halo_copy(int face, int which, float *dev, bool pack);
     // the stage kernel stores the layers next to `face` into the neighbour

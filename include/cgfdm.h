@@ -93,6 +93,12 @@ int cgfdm_create_part(const char *run_dir, const char *options_json, const int *
 int cgfdm_part_info(const cgfdm_session *s, int *lo, int *n, int *top);
 int cgfdm_part_station_ids(const cgfdm_session *s, int *ids, int count);
 int cgfdm_part_advance(cgfdm_session *s, int *phase);
+/* cgfdm_part_advance in two halves: cgfdm_part_launch enqueues the next
+ * phase and returns; cgfdm_part_finish waits for it and checks the device
+ * error word.  Parts sharing a GPU launch their phase together and then
+ * finish, so their kernels run concurrently. */
+int cgfdm_part_launch(cgfdm_session *s, int *phase);
+int cgfdm_part_finish(cgfdm_session *s);
 /* Folds the exchanges after phases 1..4 into the stage kernel: part s's
  * stages store the interior layers next to `face` straight into the halo of
  * neighbour part nbr (a session in the same process, on the same device or
