@@ -232,6 +232,16 @@ class Session:
     def write_outputs(self) -> None:
         self._check(self.L.cgfdm_write_outputs(self._h))
 
+    def check_finite(self):
+        """(count, first) of NaN/Inf values in the state (cgfdm_check_finite):
+        first = ((k * ny + j) * nx + i) * 9 + field over interior indices, -1
+        when count is 0."""
+        self.L.cgfdm_check_finite.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                                              ctypes.POINTER(ctypes.c_longlong)]
+        c, f = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.L.cgfdm_check_finite(self._h, ctypes.byref(c), ctypes.byref(f)))
+        return c.value, f.value
+
     def set_wavefield(self, w: np.ndarray) -> None:
         """Overwrites the wavefield, [nzp][nyp][nxp][9] (cgfdm_set_wavefield)."""
         w = np.ascontiguousarray(w, np.float32)

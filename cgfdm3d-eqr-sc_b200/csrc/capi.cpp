@@ -194,6 +194,12 @@ int cgfdm_model_coord(const char *run_dir, const char *options_json, float *terr
     return CGFDM_OK;
 }
 
+int cgfdm_check_finite(cgfdm_session *s, long long *count, long long *first)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.check_finite(count, first);
+}
+
 int cgfdm_run(cgfdm_session *s, int nsteps)
 {
     if (!s) return CGFDM_E_ARG;

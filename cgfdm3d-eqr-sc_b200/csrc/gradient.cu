@@ -14,6 +14,8 @@
 //
 // Point sources do not depend on the medium; a finite-fault table (scaled
 // by mu at its cells) is refused.  The gradient is zero in the PML layers.
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -474,6 +476,16 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
     //    RHS on the way, so they need no second run
     grad_ms[0] = grad_ms[1] = grad_ms[2] = 0.0f;
     CU(cudaEventRecord(ev[0], stream));
+    nvtxRangePushA("gradient: forward with checkpoints");
+    struct NvtxPop {
+        bool on = true;
+        void pop()
+        {
+            if (on) nvtxRangePop();
+            on = false;
+        }
+        ~NvtxPop() { pop(); }
+    } nvtx_fwd;
     for (int s = 0; s < nseg; s++) {
         if (int st = save_state(ckpt + sb * s)) return st;
         const int n = std::min(K, NT - it);
@@ -486,6 +498,7 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
     }
     if (int st = save_state(final_state)) return st;
     if (int st = lap(&grad_ms[0])) return st;
+    nvtx_fwd.pop();
     if (int st = check_device_error()) return st;
 
     // residuals and misfit
@@ -517,6 +530,8 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
         }
     for (int s = nseg - 1; s >= 0; s--) {
         const int n0 = s * K, n1 = std::min(NT, n0 + K);
+        nvtxRangePushA("gradient: segment");
+        NvtxPop nvtx_seg;
         if (s < nseg - R) {
             // forward again from the segment's checkpoint, storing each stage's RHS
             if (int st = load_state(ckpt + sb * s)) return st;

@@ -8,6 +8,8 @@
 // Faces are exchanged axis by axis, x then y then z, each over the full
 // padded extent of the other two axes, so edge and corner halos are filled
 // too.  The same exchange refreshes the metric fields after set-up.
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <cstring>
 
@@ -220,6 +222,11 @@ int Session::part_launch(int *phase_done)
         return ST_STATE;
     }
     const int ph = phase_;
+    static const char *names[5] = {"part: source", "part: stage 0", "part: stage 1", "part: stage 2", "part: stage 3"};
+    nvtxRangePushA(names[ph]);
+    struct Pop {
+        ~Pop() { nvtxRangePop(); }
+    } pop;
     if (ph == 0) {
         if (int st = launch_sources_on(stream)) return st;
         cur_ = 0;

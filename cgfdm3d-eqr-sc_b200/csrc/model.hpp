@@ -31,6 +31,7 @@ enum Status : int {
     ST_TIMEOUT = 20002,
     ST_ARG = 20003,
     ST_STATE = 20004,
+    ST_NONFINITE = 20005,
 };
 
 enum Scheme { SCHEME_CGFDM = 0, SCHEME_SCFDM = 1 };
@@ -76,6 +77,7 @@ struct Params {
     int adj_fused = 0;               // options "adjointKernel": "two-pass" (default) | "fused"
     int adj_store_max = 0;           // options "adjointStoreSegments": cap on segments kept from the forward (0: memory decides)
     std::string storage = "fp32";    // "storage": "fp32" | "fp16" | "bf16"
+    int check_finite = 0;            // "checkFinite": scan the wavefield for NaN/Inf every K steps (0: never)
     // extension inputs (raw arrays the reference has no reader for)
     std::string terrainFile;         // float32 [_ny_][_nx_] surface height (m)
     std::string mediumFile;          // float32 [_nz_][_ny_][_nx_][3] Vs, Vp, rho

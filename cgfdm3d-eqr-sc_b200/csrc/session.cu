@@ -542,26 +542,29 @@ int Session::run(int nsteps)
         return ST_STATE;
     }
     int n = std::min(nsteps, m.NT - it);
-    if (!snapshots_on()) {
-        int st = run_plain(n);
-        if (st) return st;
-    } else {
-        // snapshots after every step s with s % IT_SKIP == 0 (src/propagate.cpp:289-309)
-        const int end = it + n;
-        while (it < end) {
-            int next = (it + m.p.IT_SKIP - 1) / m.p.IT_SKIP * m.p.IT_SKIP;  // first snapshot step >= it
-            int stop = std::min(end, next + 1);
-            int st = run_plain(stop - it);
-            if (st) return st;
-            if (stop == next + 1) {
-                st = write_snapshots(next);
-                if (st) return st;
-            }
-        }
-    }
+    if (int st = run_checked(n)) return st;   // csrc/health.cu
     CU(cudaStreamSynchronize(stream));
     CU(cudaGetLastError());
     return check_device_error();
+}
+
+// n steps from `it`, with the snapshots that fall among them.
+int Session::run_span(int n)
+{
+    if (!snapshots_on()) return run_plain(n);
+    // snapshots after every step s with s % IT_SKIP == 0 (src/propagate.cpp:289-309)
+    const int end = it + n;
+    while (it < end) {
+        int next = (it + m.p.IT_SKIP - 1) / m.p.IT_SKIP * m.p.IT_SKIP;  // first snapshot step >= it
+        int stop = std::min(end, next + 1);
+        int st = run_plain(stop - it);
+        if (st) return st;
+        if (stop == next + 1) {
+            st = write_snapshots(next);
+            if (st) return st;
+        }
+    }
+    return ST_OK;
 }
 
 // A stage kernel whose bounded wait gave up leaves a bit in the error word.

@@ -29,6 +29,9 @@ public:
     ~Session();
     int create(const std::string &run_dir, const std::string &options, int device);
     int run(int nsteps);
+    int run_span(int n);                             // n steps with their snapshots
+    int run_checked(int n);                          // with the "checkFinite" scans (csrc/health.cu)
+    int check_finite(long long *count, long long *first);  // non-finite values in the state
     // a part of a decomposed grid (csrc/partition.cpp, csrc/halo.cu): the
     // step in five phases with a halo exchange after each of the first four
     int create_part(const std::string &run_dir, const std::string &options, const int parts[3], const int coord[3],

@@ -37,6 +37,7 @@ extern "C" {
 #define CGFDM_E_TIMEOUT 20002   /* a bounded device wait gave up */
 #define CGFDM_E_ARG 20003       /* bad argument */
 #define CGFDM_E_STATE 20004     /* call not valid in the session's state */
+#define CGFDM_E_NONFINITE 20005 /* NaN or Inf in the wavefield ("checkFinite") */
 
 typedef struct cgfdm_session cgfdm_session;
 
@@ -65,7 +66,8 @@ typedef struct cgfdm_info {
  * `options_json` (may be NULL) overrides run-time switches with the
  * reference's flag names: {"scheme": "CGFDM"|"SCFDM", "PML": 0|1,
  * "EXP_DECAY": 0|1, "SOLVE_DISPLACEMENT": 0|1, "SOLVE_PGA": 0|1, "metricPrecision":
- * "fp32"|"fp64", "OUT": "..."}. */
+ * "fp32"|"fp64", "OUT": "..."} and this library's own keys ("checkFinite": K,
+ * "adjointKernel", "adjointStoreSegments"). */
 int cgfdm_create(const char *run_dir, const char *options_json, int device, cgfdm_session **out);
 
 /* ---- Domain decomposition (the reference's MPI layout, src/init_grid.cpp) ----
@@ -144,6 +146,13 @@ int cgfdm_model_coord(const char *run_dir, const char *options_json, float *terr
  * writes the size in bytes to *bytes; otherwise *bytes is the capacity of
  * `out` on entry and the size on return. */
 int cgfdm_get_array(cgfdm_session *s, const char *name, void *out, long long *bytes);
+
+/* Health check: the number of NaN / Inf values in the state at the last step
+ * boundary over the interior points (`count`), and the first of them as
+ * ((k * ny + j) * nx + i) * 9 + field (`first`, -1 when none).  With the
+ * option "checkFinite": K, cgfdm_run scans after every K steps and returns
+ * CGFDM_E_NONFINITE, naming the step and point, when one is found. */
+int cgfdm_check_finite(cgfdm_session *s, long long *count, long long *first);
 
 /* Advances up to `nsteps` time steps (clamped to NT).  One step is the body
  * of the time loop, src/propagate.cpp:186-321: source term into W, the RK
