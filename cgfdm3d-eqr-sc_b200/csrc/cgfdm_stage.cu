@@ -50,6 +50,26 @@
 #ifndef CG_PREFETCH_MT
 #define CG_PREFETCH_MT 1
 #endif
+// Cache policy of the point streams (used once per stage): 1 marks the
+// stage-output and RK-sum stores evict-first, 2 also the metric, step-start
+// and RK-sum loads, so L2 keeps the plane ring the neighbouring tiles share.
+#ifndef CG_STREAM_HINTS
+#define CG_STREAM_HINTS 1
+#endif
+// 1: the plane-ring TMA loads carry an L2 evict-last policy
+#ifndef CG_RING_EVICT_LAST
+#define CG_RING_EVICT_LAST 0
+#endif
+#if CG_STREAM_HINTS >= 1
+#define CG_ST(p, v) __stcs(&(p), (v))
+#else
+#define CG_ST(p, v) ((p) = (v))
+#endif
+#if CG_STREAM_HINTS >= 2
+#define CG_LD(p) __ldcs(&(p))
+#else
+#define CG_LD(p) (p)
+#endif
 
 namespace cgfdm {
 
@@ -114,6 +134,22 @@ __device__ __forceinline__ void tma_load_4d(unsigned dst, const void *tmap, int 
         : "memory");
 }
 
+// the same with an L2 cache policy (createpolicy) on the loaded lines
+__device__ __forceinline__ void tma_load_4d_hint(unsigned dst, const void *tmap, int x, int y, int z, int f,
+                                                 unsigned bar, unsigned long long policy)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], "
+        "[%1, {%2, %3, %4, %5}], [%6], %7;\n" ::"r"(dst),
+        "l"((unsigned long long)tmap), "r"(x), "r"(y), "r"(z), "r"(f), "r"(bar), "l"(policy)
+        : "memory");
+}
+__device__ __forceinline__ unsigned long long l2_evict_last_policy()
+{
+    unsigned long long p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
 __device__ __forceinline__ void tma_prefetch_4d(const void *tmap, int x, int y, int z, int f)
 {
     asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];\n" ::"l"(
@@ -283,7 +319,10 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         unsigned bar = smem_u32(&bars[s]);
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         mbar_expect_tx(bar, SLOT_BYTES);
-        tma_load_4d(smem_u32(ring + s * SLOT_F), tmW, tx0, ty0, kk, 0, bar);
+        if (CG_RING_EVICT_LAST)
+            tma_load_4d_hint(smem_u32(ring + s * SLOT_F), tmW, tx0, ty0, kk, 0, bar, l2_evict_last_policy());
+        else
+            tma_load_4d(smem_u32(ring + s * SLOT_F), tmW, tx0, ty0, kk, 0, bar);
     };
     // point operands of plane kk into L2 ahead of their plain loads
     auto prefetch_points = [&](int kk) {
@@ -330,16 +369,19 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         float mu = 0, lam = 0, buo = 0, bz = 1;
         float mv[9], tv[9];
         if (active) {
-            xi_x = a.cjm[C_XI_X * F + q], xi_y = a.cjm[C_XI_Y * F + q], xi_z = a.cjm[C_XI_Z * F + q];
-            et_x = a.cjm[C_ET_X * F + q], et_y = a.cjm[C_ET_Y * F + q], et_z = a.cjm[C_ET_Z * F + q];
-            zt_x = a.cjm[C_ZT_X * F + q], zt_y = a.cjm[C_ZT_Y * F + q], zt_z = a.cjm[C_ZT_Z * F + q];
-            mu = a.cjm[C_MU * F + q], lam = a.cjm[C_LAMBDA * F + q];
-            buo = a.cjm[C_BUOY * F + q] * 1.0f;  // buoyancy *= Crho (= 1)
+            xi_x = CG_LD(a.cjm[C_XI_X * F + q]), xi_y = CG_LD(a.cjm[C_XI_Y * F + q]);
+            xi_z = CG_LD(a.cjm[C_XI_Z * F + q]);
+            et_x = CG_LD(a.cjm[C_ET_X * F + q]), et_y = CG_LD(a.cjm[C_ET_Y * F + q]);
+            et_z = CG_LD(a.cjm[C_ET_Z * F + q]);
+            zt_x = CG_LD(a.cjm[C_ZT_X * F + q]), zt_y = CG_LD(a.cjm[C_ZT_Y * F + q]);
+            zt_z = CG_LD(a.cjm[C_ZT_Z * F + q]);
+            mu = CG_LD(a.cjm[C_MU * F + q]), lam = CG_LD(a.cjm[C_LAMBDA * F + q]);
+            buo = CG_LD(a.cjm[C_BUOY * F + q]) * 1.0f;  // buoyancy *= Crho (= 1)
             bz = a.pml_beta_z[k];
             if (a.irk == 1 || a.irk == 2)
-                for (int f = 0; f < 9; f++) mv[f] = a.Wm[f * F + q];
+                for (int f = 0; f < 9; f++) mv[f] = CG_LD(a.Wm[f * F + q]);
             if (a.irk != 0)
-                for (int f = 0; f < 9; f++) tv[f] = a.T[f * F + q];
+                for (int f = 0; f < 9; f++) tv[f] = CG_LD(a.T[f * F + q]);
         }
         const int kk_new = k - za + 4;
         if (!mbar_wait_bounded(smem_u32(&bars[slot_of(kk_new)]), parity_of(kk_new))) {
@@ -496,19 +538,19 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         if (a.irk == 0) {
 #pragma unroll
             for (int f = 0; f < 9; f++) {
-                a.T[f * F + q] = mv[f] + RK_BETA1 * h[f];
+                CG_ST(a.T[f * F + q], mv[f] + RK_BETA1 * h[f]);
                 wout[f] = mv[f] + RK_ALPHA2 * h[f];
             }
         } else if (a.irk == 1) {
 #pragma unroll
             for (int f = 0; f < 9; f++) {
-                a.T[f * F + q] = tv[f] + RK_BETA2 * h[f];
+                CG_ST(a.T[f * F + q], tv[f] + RK_BETA2 * h[f]);
                 wout[f] = mv[f] + RK_ALPHA3 * h[f];
             }
         } else if (a.irk == 2) {
 #pragma unroll
             for (int f = 0; f < 9; f++) {
-                a.T[f * F + q] = tv[f] + RK_BETA3 * h[f];
+                CG_ST(a.T[f * F + q], tv[f] + RK_BETA3 * h[f]);
                 wout[f] = mv[f] + h[f];
             }
         } else {
@@ -516,7 +558,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
             for (int f = 0; f < 9; f++) wout[f] = tv[f] + RK_BETA4 * h[f];
         }
 #pragma unroll
-        for (int f = 0; f < 9; f++) a.Wout[f * F + q] = wout[f];
+        for (int f = 0; f < 9; f++) CG_ST(a.Wout[f * F + q], wout[f]);
         if (HOUT) {
             // a part of a decomposed grid: the interior layers next to a face
             // shared with a neighbour go straight into the neighbour's halo
