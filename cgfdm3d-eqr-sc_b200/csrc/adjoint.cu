@@ -56,6 +56,17 @@
 #define ADJ_BOUNDS_GATHER __launch_bounds__(32 * ADJ_TY)
 #endif
 
+// 1: the two-pass kernels' stores (Phi, the next mu, lambda, the gradient)
+// evict-first: each is read back by a later launch, after L2 has turned over
+#ifndef ADJ_STREAM_HINTS
+#define ADJ_STREAM_HINTS 0
+#endif
+#if ADJ_STREAM_HINTS
+#define AD_ST(p, v) __stcs(&(p), (v))
+#else
+#define AD_ST(p, v) ((p) = (v))
+#endif
+
 namespace cgfdm {
 
 // dir_rhs^T: the 9-vector adjoint of the nine scaled derivatives along one
@@ -220,7 +231,7 @@ __global__ void ADJ_BOUNDS_PRE k_adj_pre(const __grid_constant__ AdjStageArgs a)
         float phi[9];
         dir_rhs_t(mt[d][0], mt[d][1], mt[d][2], nu[d], mu, lam, buo, phi);
         for (int c = 0; c < 3; c++) phi[c] += extra[d][c];
-        for (int f = 0; f < 9; f++) a.Phi[(d * 9 + f) * F + q] = phi[f];
+        for (int f = 0; f < 9; f++) AD_ST(a.Phi[(d * 9 + f) * F + q], phi[f]);
     }
 
     if (fs) {
@@ -353,8 +364,8 @@ __global__ void ADJ_BOUNDS_GATHER k_adj_gather(const __grid_constant__ AdjStageA
     const float alpha = irk == 3 ? 1.0f : irk == 2 ? RK_ALPHA3 : RK_ALPHA2;
 #pragma unroll
     for (int f = 0; f < 9; f++) {
-        if (irk != 0) a.M[f * F + q] = beta * lp[f] + alpha * nu[f];
-        a.Lam[f * F + q] = (irk == 3 ? lp[f] : lm[f]) + nu[f];
+        if (irk != 0) AD_ST(a.M[f * F + q], beta * lp[f] + alpha * nu[f]);
+        AD_ST(a.Lam[f * F + q], (irk == 3 ? lp[f] : lm[f]) + nu[f]);
     }
 
     if (!grad) return;
@@ -383,9 +394,9 @@ __global__ void ADJ_BOUNDS_GATHER k_adj_gather(const __grid_constant__ AdjStageA
             else gl += acc;
         }
     }
-    a.grad[0 * F + q] = g3[0] + gm;
-    a.grad[1 * F + q] = g3[1] + gl;
-    a.grad[2 * F + q] = g3[2] + gb;
+    AD_ST(a.grad[0 * F + q], g3[0] + gm);
+    AD_ST(a.grad[1 * F + q], g3[1] + gl);
+    AD_ST(a.grad[2 * F + q], g3[2] + gb);
 }
 
 cudaError_t launch_adj_stage(const AdjStageArgs &a, cudaStream_t st)

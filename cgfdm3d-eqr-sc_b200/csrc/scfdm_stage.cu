@@ -44,6 +44,17 @@
 #include "kernels.cuh"
 #include "sc_ops.cuh"
 
+// 1: the passes' RHS and stage-output stores evict-first (each is read back
+// by a later pass or stage, long after L2 has turned over)
+#ifndef SC_STREAM_HINTS
+#define SC_STREAM_HINTS 1
+#endif
+#if SC_STREAM_HINTS
+#define SC_ST(p, v) __stcs(&(p), (v))
+#else
+#define SC_ST(p, v) ((p) = (v))
+#endif
+
 namespace cgfdm {
 
 namespace {
@@ -216,10 +227,10 @@ __device__ __forceinline__ void epilogue(const ScDirArgs &a, long long q, int i,
     const long long F = a.g.fstride;
     if (DIR == 0) {
 #pragma unroll
-        for (int v = 0; v < 9; v++) a.H[v * F + q] = val[v];
+        for (int v = 0; v < 9; v++) SC_ST(a.H[v * F + q], val[v]);
     } else if (DIR == 1) {
 #pragma unroll
-        for (int v = 0; v < 9; v++) a.H[v * F + q] = a.H[v * F + q] + val[v];
+        for (int v = 0; v < 9; v++) SC_ST(a.H[v * F + q], a.H[v * F + q] + val[v]);
     } else {
         const int _nz = a.g.nzp - CGFDM_HALO;
         const bool decay = a.decay != nullptr && k < _nz - 4;
@@ -240,7 +251,7 @@ __device__ __forceinline__ void epilogue(const ScDirArgs &a, long long q, int i,
                                                 __dmul_rn(2.0 / 3.0, (double)h)));
             }
             if (decay) o = decay_apply(o, i, j, k, a.g, a.decay, a.ndecay);
-            a.Wout[v * F + q] = o;
+            SC_ST(a.Wout[v * F + q], o);
         }
         if (a.copy_halo && k == _nz - 1)
             for (int h = 1; h <= CGFDM_HALO; h++)
