@@ -54,6 +54,12 @@
 #else
 #define SC_ST(p, v) ((p) = (v))
 #endif
+// 2: also the single-use loads of the RHS, the step-start state and DT rDH / J
+#if SC_STREAM_HINTS >= 2
+#define SC_LD(p) __ldcs(&(p))
+#else
+#define SC_LD(p) (p)
+#endif
 
 namespace cgfdm {
 
@@ -230,23 +236,23 @@ __device__ __forceinline__ void epilogue(const ScDirArgs &a, long long q, int i,
         for (int v = 0; v < 9; v++) SC_ST(a.H[v * F + q], val[v]);
     } else if (DIR == 1) {
 #pragma unroll
-        for (int v = 0; v < 9; v++) SC_ST(a.H[v * F + q], a.H[v * F + q] + val[v]);
+        for (int v = 0; v < 9; v++) SC_ST(a.H[v * F + q], SC_LD(a.H[v * F + q]) + val[v]);
     } else {
         const int _nz = a.g.nzp - CGFDM_HALO;
         const bool decay = a.decay != nullptr && k < _nz - 4;
 #pragma unroll
         for (int v = 0; v < 9; v++) {
-            const float h = a.H[v * F + q] + val[v];
+            const float h = SC_LD(a.H[v * F + q]) + val[v];
             const float w = a.W[v * F + q];
             float o;
             if (a.irk == 0) {
                 o = w + h;
             } else if (a.irk == 1) {
-                const double m = a.Wm[v * F + q];
+                const double m = SC_LD(a.Wm[v * F + q]);
                 o = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(0.75, m), __dmul_rn(0.25, (double)w)),
                                                 __dmul_rn(0.25, (double)h)));
             } else {
-                const double m = a.Wm[v * F + q];
+                const double m = SC_LD(a.Wm[v * F + q]);
                 o = __double2float_rn(__dadd_rn(__dadd_rn(__dmul_rn(1.0 / 3.0, m), __dmul_rn(2.0 / 3.0, (double)w)),
                                                 __dmul_rn(2.0 / 3.0, (double)h)));
             }
@@ -379,7 +385,7 @@ __global__ void __launch_bounds__(SC_THREADS, SC_TILE_MIN_CTAS) k_sc_tile(const 
         int i, j, k;
         coords(p, lane, i, j, k);
         const long long q = g.at(i, j, k);
-        const float coef = a.sjac[q];  // DT * rDH / J
+        const float coef = SC_LD(a.sjac[q]);  // DT * rDH / J
         float val[9];
         if (k >= _nz - 3) {
             float Fp[9], Fm[9];
