@@ -50,6 +50,10 @@
 #ifndef CG_PREFETCH_MT
 #define CG_PREFETCH_MT 1
 #endif
+// how many planes ahead the point operands are prefetched
+#ifndef CG_PREFETCH_DIST
+#define CG_PREFETCH_DIST 1
+#endif
 // Cache policy of the point streams (used once per stage): 1 marks the
 // stage-output and RK-sum stores evict-first, 2 also the metric, step-start
 // and RK-sum loads, so L2 keeps the plane ring the neighbouring tiles share.
@@ -334,7 +338,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     const int klast = ke - za + 3;          // last plane of the last window
     if (tid == 0) {
         for (int kk = kf; kk <= min(kf + NSLOT - 1, klast); kk++) issue(kk);
-        for (int kk = kb; kk < min(kb + 2, ke); kk++) prefetch_points(kk);
+        for (int kk = kb; kk < min(kb + CG_PREFETCH_DIST, ke); kk++) prefetch_points(kk);
     }
     int issued = min(kf + NSLOT - 1, klast);  // same value in every thread
     // the first window: planes kf .. kf+3 (kf+4 is waited for in the loop)
@@ -360,7 +364,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
             issued = want;
         }
         if (tid == 0) {
-            if (k + 2 < ke) prefetch_points(k + 2);
+            if (k + CG_PREFETCH_DIST < ke) prefetch_points(k + CG_PREFETCH_DIST);
             if (want + 2 <= klast) tma_prefetch_4d(tmW, tx0, ty0, want + 2, 0);
         }
         const long long q = g.at(i, j, k);
