@@ -54,6 +54,11 @@
 #ifndef CG_PREFETCH_DIST
 #define CG_PREFETCH_DIST 1
 #endif
+// how many planes beyond the newest ring fill the stencil planes are
+// prefetched into L2 (0: none)
+#ifndef CG_RING_PREFETCH_DIST
+#define CG_RING_PREFETCH_DIST 0
+#endif
 // Cache policy of the point streams (used once per stage): 1 marks the
 // stage-output and RK-sum stores evict-first, 2 also the metric, step-start
 // and RK-sum loads, so L2 keeps the plane ring the neighbouring tiles share.
@@ -365,7 +370,8 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         }
         if (tid == 0) {
             if (k + CG_PREFETCH_DIST < ke) prefetch_points(k + CG_PREFETCH_DIST);
-            if (want + 2 <= klast) tma_prefetch_4d(tmW, tx0, ty0, want + 2, 0);
+            if (CG_RING_PREFETCH_DIST > 0 && want + CG_RING_PREFETCH_DIST <= klast)
+                tma_prefetch_4d(tmW, tx0, ty0, want + CG_RING_PREFETCH_DIST, 0);
         }
         const long long q = g.at(i, j, k);
         // point-wise operands, loaded before the ring wait
