@@ -61,6 +61,23 @@ def peaks():
     return 6650.0, "fallback"
 
 
+# ME-AWENO arithmetic per interior point and step (54 WENO5 reconstructions
+# of about 90 flops and 4 divides, Lax-Friedrichs fluxes, flux differences
+# with their corrections, three TVD stages): about 19.4 kflop.
+SC_FLOP_PER_PT_STEP = 19.4e3
+
+
+def fp32_peak_tflops():
+    """FP32 (non-tensor) peak: 148 SMs x 128 FP32 lanes x 2 flop x the
+    maximum SM clock.  Nominal: no measured FP32 figure is provided."""
+    mhz = 1965.0
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            mhz = float(json.load(f).get("sm_max_mhz", mhz))
+    return 148 * 128 * 2 * mhz * 1e6 / 1e12
+
+
 def traffic_ratio():
     """DRAM traffic of the stage kernel over its algorithmic bytes, from the
     committed ncu summary (profiles/cg_stage_traffic.txt), or None."""
@@ -638,12 +655,21 @@ def main():
                    "l2": "inputs larger than L2 (model + wavefield %.1f GB resident)" % (info.device_bytes / 1e9),
                    "parallelism": f"replicas x{world}"},
         "hbm_gbs_algorithmic": algo_step * args.steps / (ms_max * 1e-3) / 1e9,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "peak_kind": peak_kind,
-                     "traffic": (tr * algo_launch if tr and not sc else None),
-                     "traffic_source": None if sc else "ncu ratio on terrain_fault_256x256x128 x algorithmic bytes of this launch",
-                     "kernel": "k_sc_dir x3 (one TVD stage)" if sc else "k_cg_stage",
-                     "algo_bytes_per_launch": algo_launch, "mean_launch_ms": stage_ms},
+        "roofline": ({"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                      "frac": achieved / hbm_peak, "peak_kind": peak_kind,
+                      "traffic": (tr * algo_launch if tr else None),
+                      "traffic_source": "ncu ratio on terrain_fault_256x256x128 x algorithmic bytes of this launch",
+                      "kernel": "k_cg_stage",
+                      "algo_bytes_per_launch": algo_launch, "mean_launch_ms": stage_ms}
+                     if not sc else
+                     {"bound": "fp32", "unit": "TFLOP/s",
+                      "achieved": SC_FLOP_PER_PT_STEP / 3 * pts / (stage_ms * 1e-3) / 1e12,
+                      "peak": fp32_peak_tflops(), "peak_kind": "nominal (148 SMs x 128 lanes x 2 x max SM clock)",
+                      "frac": SC_FLOP_PER_PT_STEP / 3 * pts / (stage_ms * 1e-3) / 1e12 / fp32_peak_tflops(),
+                      "algo_flop_per_pt_step": SC_FLOP_PER_PT_STEP, "traffic": None,
+                      "kernel": "k_sc_tile x3 (one TVD stage: x, y, z passes)",
+                      "hbm_achieved_gbs": achieved, "hbm_frac": achieved / hbm_peak,
+                      "algo_bytes_per_launch": algo_launch, "mean_launch_ms": stage_ms}),
         "e2e": {"value": world * pts * args.steps / e2e_s / 1e6, "unit": METRIC,
                 "h2d_bytes_per_step": i2.h2d_bytes / args.steps, "d2h_bytes_per_step": st.nbytes / args.steps,
                 "seconds": e2e_s, "path": "cgfdm_create(run dir) + cgfdm_run(K) + cgfdm_get_stations + destroy"},

@@ -280,6 +280,33 @@ class Session:
                                           ctypes.byref(ms)))
         return kc.value, ct.value, ms.value
 
+    def run_precise(self, nsteps: int, bits: int = 64, wavefield: bool = False):
+        """The time loop from step 0 in reference form with state and
+        arithmetic in FP64 (``bits`` 64) or FP32 (32) on this session's model
+        (cgfdm_run_precise).  Returns (stations [n][nsteps][9], pgv
+        [ny][nx][2], wavefield [nzp][nyp][nxp][9] or None), all float64."""
+        i = self.info
+        dp = ctypes.POINTER(ctypes.c_double)
+        self.L.cgfdm_run_precise.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp, ctypes.c_longlong, dp,
+                                             ctypes.c_longlong, dp, ctypes.c_longlong]
+        st = np.zeros((i.n_stations, int(nsteps), 9), np.float64)
+        pgv = np.zeros((i.ny, i.nx, 2), np.float64)
+        W = np.zeros((i.nzp, i.nyp, i.nxp, 9), np.float64) if wavefield else None
+
+        def p(a):
+            return a.ctypes.data_as(dp) if a is not None and a.size else None
+
+        self._check(self.L.cgfdm_run_precise(self._h, int(nsteps), int(bits), p(st), st.size, p(pgv), pgv.size,
+                                             p(W), W.size if W is not None else 0))
+        return st, pgv, W
+
+    def test_stall(self, item: int, fill: int, wait_cycles: int) -> None:
+        """Test hook (cgfdm_test_stall): the next stage launch's work item
+        ``item`` leaves plane copy ``fill`` unissued, once, and the stage
+        kernel's bounded waits give up after ``wait_cycles`` clocks."""
+        self.L.cgfdm_test_stall.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_longlong]
+        self._check(self.L.cgfdm_test_stall(self._h, int(item), int(fill), int(wait_cycles)))
+
     def set_tiling(self, kchunk: int, ctas: int) -> None:
         self._check(self.L.cgfdm_set_tiling(self._h, int(kchunk), int(ctas)))
 

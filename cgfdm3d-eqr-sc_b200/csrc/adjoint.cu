@@ -778,12 +778,9 @@ __global__ void __launch_bounds__(ADJF_NT) k_adj_fused(const __grid_constant__ A
 
 cudaError_t launch_adj_stage_fused(const AdjStageArgs &a, cudaStream_t st)
 {
-    static bool attr = false;
+    // per device and lost with a device reset: set on every launch
     const size_t smem = sizeof(float) * ADJF_SMEM_FLOATS;
-    if (!attr) {
-        CUDA_TRY(cudaFuncSetAttribute(k_adj_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = true;
-    }
+    CUDA_TRY(cudaFuncSetAttribute(k_adj_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 b(32, ADJF_TY), gr((a.g.nx + 31) / 32, (a.g.ny + ADJF_TY - 1) / ADJF_TY, a.nchunk);
     k_adj_fused<<<gr, b, smem, st>>>(a);
     return cudaGetLastError();

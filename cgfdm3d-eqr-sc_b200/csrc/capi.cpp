@@ -343,6 +343,26 @@ int cgfdm_autotune(cgfdm_session *s, int trial_steps, int *kchunk, int *ctas, fl
     return s->s.autotune(trial_steps, kchunk, ctas, ms_per_step);
 }
 
+int cgfdm_run_precise(cgfdm_session *s, int nsteps, int bits, double *stations, long long n_stations,
+                      double *pgv, long long n_pgv, double *wavefield, long long n_wavefield)
+{
+    if (!s) return CGFDM_E_ARG;
+    const cgfdm::Model &m = s->s.m;
+    const long long need_st = (long long)s->s.nst * nsteps * 9, need_pgv = (long long)m.g.nx * m.g.ny * 2;
+    const long long need_w = m.g.npad() * 9;
+    if ((stations && n_stations < need_st) || (pgv && n_pgv < need_pgv) || (wavefield && n_wavefield < need_w)) {
+        s->s.err = "cgfdm_run_precise: output buffer too small";
+        return CGFDM_E_ARG;
+    }
+    return s->s.run_precise(nsteps, bits, stations, pgv, wavefield);
+}
+
+int cgfdm_test_stall(cgfdm_session *s, int item, int fill, long long wait_cycles)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.test_stall(item, fill, wait_cycles);
+}
+
 int cgfdm_set_tiling(cgfdm_session *s, int kchunk, int ctas)
 {
     if (!s) return CGFDM_E_ARG;

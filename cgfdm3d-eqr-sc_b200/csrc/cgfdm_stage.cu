@@ -125,13 +125,14 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity)
         : "memory");
     return ok != 0;
 }
-// Bounded wait: gives up after ~2^31 clock cycles (about a second).
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity)
+// Bounded wait: gives up after `limit` clock cycles (2^31, about a second,
+// unless a test shortens it).
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity, long long limit)
 {
     if (mbar_try_wait(bar, parity)) return true;
     long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > (1LL << 31)) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 __device__ __forceinline__ void tma_load_4d(unsigned dst, const void *tmap, int x, int y, int z, int f, unsigned bar)
@@ -326,6 +327,9 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     auto issue = [&](int kk) {
         int s = slot_of(kk);
         unsigned bar = smem_u32(&bars[s]);
+        // test hook: leave this plane's slot without a copy (and without the
+        // arrival that would complete its barrier phase), once
+        if (a.stall && gitem == a.stall_item && kk - kf == a.stall_fill && atomicExch(a.stall, 0) == 1) return;
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         mbar_expect_tx(bar, SLOT_BYTES);
         if (CG_RING_EVICT_LAST)
@@ -340,6 +344,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         if (CG_PREFETCH_MT && a.irk != 0) tma_prefetch_4d(tmT, px0, j0, kk, 0);
     };
 
+    const long long wlim = a.wait_limit > 0 ? a.wait_limit : (1LL << 31);
     const int klast = ke - za + 3;          // last plane of the last window
     if (tid == 0) {
         for (int kk = kf; kk <= min(kf + NSLOT - 1, klast); kk++) issue(kk);
@@ -348,7 +353,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     int issued = min(kf + NSLOT - 1, klast);  // same value in every thread
     // the first window: planes kf .. kf+3 (kf+4 is waited for in the loop)
     bool ok = true;
-    for (int kk = kf; kk < kf + 4; kk++) ok = ok && mbar_wait_bounded(smem_u32(&bars[slot_of(kk)]), parity_of(kk));
+    for (int kk = kf; kk < kf + 4; kk++) ok = ok && mbar_wait_bounded(smem_u32(&bars[slot_of(kk)]), parity_of(kk), wlim);
     if (!ok) {
         s_abort = 1;
         atomicOr(a.err, 1);
@@ -394,7 +399,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
                 for (int f = 0; f < 9; f++) tv[f] = CG_LD(a.T[f * F + q]);
         }
         const int kk_new = k - za + 4;
-        if (!mbar_wait_bounded(smem_u32(&bars[slot_of(kk_new)]), parity_of(kk_new))) {
+        if (!mbar_wait_bounded(smem_u32(&bars[slot_of(kk_new)]), parity_of(kk_new), wlim)) {
             s_abort = 1;
             atomicOr(a.err, 1);
             continue;
@@ -608,7 +613,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         // no copy may still be landing in shared memory when the CTA exits
         if (tid == 0)
             for (int kk = max(kf, issued - NSLOT + 1); kk <= issued; kk++)
-                if (!mbar_wait_bounded(smem_u32(&bars[slot_of(kk)]), parity_of(kk))) atomicOr(a.err, 2);
+                if (!mbar_wait_bounded(smem_u32(&bars[slot_of(kk)]), parity_of(kk), wlim)) atomicOr(a.err, 2);
         break;
     }
     seq0 += (unsigned)(issued - kf + 1);
@@ -635,12 +640,11 @@ template <int FB1, int FB2, int FB3, bool BATCH, bool HOUT>
 static cudaError_t launch_t(const CgStageDesc &d1, const CgStageDesc *descs, const int *item_start, int nsess,
                             int *work, int ctas, cudaStream_t st)
 {
-    static bool attr = false;
-    if (!attr) {
-        CUDA_TRY(cudaFuncSetAttribute(k_cg_stage<FB1, FB2, FB3, BATCH, HOUT>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cg_stage_smem_bytes()));
-        attr = true;
-    }
+    // The shared-memory limit is an attribute of the kernel on the current
+    // device (and is lost with a device reset), so it is set on every launch:
+    // a host-side call of about a microsecond, legal during stream capture.
+    CUDA_TRY(cudaFuncSetAttribute(k_cg_stage<FB1, FB2, FB3, BATCH, HOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)cg_stage_smem_bytes()));
     k_cg_stage<FB1, FB2, FB3, BATCH, HOUT>
         <<<ctas, dim3(TX, TY, 1), cg_stage_smem_bytes(), st>>>(d1, descs, item_start, nsess, work);
     return cudaGetLastError();

@@ -67,7 +67,15 @@ struct CgStageArgs {
     float *dis;          // displacement, 3 fields in the W layout, stage 3 only
     float *hstore;       // or null: receives this stage's RHS h for the adjoint (9 fields, HBox layout)
     float *vdstore;      // or null: receives the surface layer's xi/eta velocity derivatives (6 x plane)
-    int *err;            // device error word: bit 0 = a bounded wait gave up
+    int *err;            // device error word: bit 0 = a bounded wait gave up, bit 1 = the drain after it did
+    // Test hook (null in normal runs): while *stall is 1, the CTA that takes
+    // work item stall_item does not issue the copy of its plane number
+    // stall_fill (counted from the item's first plane) and clears *stall, so
+    // the wait for that plane runs out.  wait_limit: clock cycles a bounded
+    // wait spins before it gives up (0: 2^31, about a second).
+    int *stall;
+    int stall_item, stall_fill;
+    long long wait_limit;
     int ntiles_x, ntiles_y, nchunk;  // work items: tiles x tiles x z-chunks
     int irk;
     int FB1, FB2, FB3;

@@ -20,7 +20,11 @@
 //
 // In host code the name g_hrange_scratch only stands for the device
 // variable; the device address is looked up with cudaGetSymbolAddress once
-// per device, with that device current, on the first call made there.
+// per device, with that device current, on the first call made there, and
+// again whenever the device's context has changed since (a cudaDeviceReset
+// destroys the context that held the old address).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -38,8 +42,10 @@ constexpr int BX = 32, BY = 8, ZCHUNK = 16;  // one block: 32 x 8 columns, 16 pl
 static __device__ __align__(256) double g_hrange_scratch[2 * NOALLOC_MAX_BLOCKS];
 
 constexpr int MAX_DEVICES = 64;
-std::mutex g_mu;
+std::mutex g_mu;      // guards the per-device address cache
+std::mutex g_fn_mu;   // guards the driver entry points
 double *g_scratch_addr[MAX_DEVICES] = {};
+unsigned long long g_scratch_ctx[MAX_DEVICES] = {};  // context the address belongs to
 thread_local std::string g_noalloc_error;
 
 // Point-to-plane distances of one point to the six diagonal-neighbour planes
@@ -129,8 +135,45 @@ __global__ void __launch_bounds__(1024) k_hrange_final(const double *__restrict_
     }
 }
 
+// Unique id of the context current on this thread (cuCtxGetId, through the
+// runtime's driver entry points), 0 when none is current yet (the runtime
+// binds its primary context on its first real call).  The id of a context
+// created after a device reset differs from the old one's.
+int current_context_id(unsigned long long *id)
+{
+    static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+    static PFN_cuCtxGetId_v12000 get_id = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_fn_mu);
+        if (!get_current || !get_id) {
+            cudaDriverEntryPointQueryResult q1, q2;
+            void *f1 = nullptr, *f2 = nullptr;
+            if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+                cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+                q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+                g_noalloc_error = "cuCtxGetCurrent / cuCtxGetId not available from the driver";
+                return CGFDM_E_CUDA;
+            }
+            get_current = (PFN_cuCtxGetCurrent_v4000)f1;
+            get_id = (PFN_cuCtxGetId_v12000)f2;
+        }
+    }
+    CUcontext c = nullptr;
+    unsigned long long v = 0;
+    if (get_current(&c) != CUDA_SUCCESS) {
+        g_noalloc_error = "cuCtxGetCurrent failed";
+        return CGFDM_E_CUDA;
+    }
+    if (c && get_id(c, &v) != CUDA_SUCCESS) {
+        g_noalloc_error = "cuCtxGetId failed";
+        return CGFDM_E_CUDA;
+    }
+    *id = v;
+    return CGFDM_OK;
+}
+
 // Device address of g_hrange_scratch on the current device, looked up once
-// per device.
+// per device and context.
 int scratch_for_current_device(double **out)
 {
     int dev = 0;
@@ -143,15 +186,20 @@ int scratch_for_current_device(double **out)
         g_noalloc_error = "device ordinal out of range";
         return CGFDM_E_ARG;
     }
+    unsigned long long ctx = 0;
+    if (int st = current_context_id(&ctx)) return st;
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
+    if (!g_scratch_addr[dev] || ctx == 0 || g_scratch_ctx[dev] != ctx) {
         double *p = nullptr;
-        e = cudaGetSymbolAddress((void **)&p, g_hrange_scratch);
+        e = cudaGetSymbolAddress((void **)&p, g_hrange_scratch);   // binds the primary context if none is
         if (e != cudaSuccess || !p) {
             g_noalloc_error = std::string("cudaGetSymbolAddress(g_hrange_scratch): ") + cudaGetErrorString(e);
             return CGFDM_E_CUDA;
         }
+        if (ctx == 0)
+            if (int st = current_context_id(&ctx)) return st;
         g_scratch_addr[dev] = p;
+        g_scratch_ctx[dev] = ctx;
     }
     *out = g_scratch_addr[dev];
     return CGFDM_OK;
@@ -169,6 +217,11 @@ int cgfdm_hrange_noalloc(const float *d_coord, int nx, int ny, int nz, double *d
     }
     const long long gx = (nx + BX - 1) / BX, gy = (ny + BY - 1) / BY, gz = (nz + ZCHUNK - 1) / ZCHUNK;
     const long long nblocks = gx * gy * gz;
+    if (gy > 65535 || gz > 65535) {
+        g_noalloc_error = "cgfdm_hrange_noalloc: grid needs " + std::to_string(gy) + " x " + std::to_string(gz) +
+                          " thread blocks along y x z; a launch allows at most 65535 each";
+        return CGFDM_E_ARG;
+    }
     if (nblocks > NOALLOC_MAX_BLOCKS) {
         g_noalloc_error = "cgfdm_hrange_noalloc: grid needs " + std::to_string(nblocks) +
                           " thread blocks of 32x8x16 points; the static scratch holds " +
@@ -180,12 +233,15 @@ int cgfdm_hrange_noalloc(const float *d_coord, int nx, int ny, int nz, double *d
     int st = scratch_for_current_device(&scratch);
     if (st) return st;
     cudaStream_t s = (cudaStream_t)stream;
-    k_hrange_partial<<<dim3((unsigned)gx, (unsigned)gy, (unsigned)gz), dim3(BX, BY, 1), 0, s>>>(d_coord, nx, ny, nz,
-                                                                                              scratch);
-    cudaError_t e = cudaGetLastError();
+    // cudaLaunchKernel returns this launch's own status, not an error an
+    // earlier launch of the caller left pending
+    int nx_ = nx, ny_ = ny, nz_ = nz, nb = (int)nblocks;
+    void *args1[] = {(void *)&d_coord, &nx_, &ny_, &nz_, &scratch};
+    cudaError_t e = cudaLaunchKernel((const void *)k_hrange_partial, dim3((unsigned)gx, (unsigned)gy, (unsigned)gz),
+                                     dim3(BX, BY, 1), args1, 0, s);
     if (e == cudaSuccess) {
-        k_hrange_final<<<1, 1024, 0, s>>>(scratch, (int)nblocks, d_out);
-        e = cudaGetLastError();
+        void *args2[] = {&scratch, &nb, &d_out};
+        e = cudaLaunchKernel((const void *)k_hrange_final, dim3(1), dim3(1024), args2, 0, s);
     }
     if (e != cudaSuccess) {
         g_noalloc_error = std::string("cgfdm_hrange_noalloc launch: ") + cudaGetErrorString(e);

@@ -371,6 +371,10 @@ void Session::stage_desc(int irk, CgStageDesc &d) const
     a.rDH = m.g.rDH;
     a.DT = (float)m.p.DT;
     a.err = err_dev_;
+    a.stall = stall_item_ >= 0 ? stall_dev_ : nullptr;
+    a.stall_item = stall_item_;
+    a.stall_fill = stall_fill_;
+    a.wait_limit = wait_limit_;
     a.ntiles_x = ntx_, a.ntiles_y = nty_, a.nchunk = nchunk_;
     for (int f = 0; f < 6; f++) a.ho[f] = ho_[irk][f];
     std::memcpy(d.tmW, maps_[win_map[irk]].win, 128);
@@ -577,6 +581,30 @@ int Session::check_device_error()
         err = "a stage kernel's bounded wait for its plane copies gave up (device error word " + std::to_string(e) + ")";
         return ST_TIMEOUT;
     }
+    return ST_OK;
+}
+
+int Session::test_stall(int item, int fill, long long wait_cycles)
+{
+    if (m.p.scheme != SCHEME_CGFDM) {
+        err = "the stall hook applies to the CGFDM stage kernel";
+        return ST_OPTIONS;
+    }
+    if (item < 0 || item >= stage_items() || fill < 0 || wait_cycles < 0) {
+        err = "stall hook: item, fill or wait_cycles out of range";
+        return ST_ARG;
+    }
+    if (!stall_dev_) ALLOC(stall_dev_, int, 1);
+    static const int one = 1;
+    CU(cudaMemcpyAsync(stall_dev_, &one, sizeof one, cudaMemcpyHostToDevice, stream));
+    CU(cudaStreamSynchronize(stream));
+    stall_item_ = item, stall_fill_ = fill, wait_limit_ = wait_cycles;
+    if (int st = build_stage_descs()) return st;
+    // the captured steps hold the old descriptors
+    if (graph8_) cudaGraphExecDestroy(graph8_);
+    if (graph8_src_) cudaGraphDestroy(graph8_src_);
+    graph8_ = nullptr;
+    graph8_src_ = nullptr;
     return ST_OK;
 }
 

@@ -84,6 +84,12 @@ public:
     int tune_save(char *dev);
     int tune_load(const char *dev);
     int time_steps(int nsteps, float *ms);          // direct launches from `it`, `it` unchanged
+    // The time loop from step 0 in reference form with state and arithmetic
+    // in FP64 (bits 64) or FP32 (bits 32) on the session's model
+    // (csrc/precise.cu); buffers of its own, the session's state untouched.
+    // stations [nst][nsteps][9], pgv [ny][nx][2], wavefield
+    // [_nz_][_ny_][_nx_][9], each optional.
+    int run_precise(int nsteps, int bits, double *stations, double *pgv, double *wavefield);
 
     Model m;
     DevGrid g;
@@ -136,8 +142,17 @@ private:
     ScTiling sct_ = {};
     static constexpr int SC_DECAY_LAYERS = 20;       // src/exp_decay_absorb.cpp:109
     int check_device_error();
+    template <class R>
+    int run_precise_t(int nsteps, double *stations, double *pgv, double *wavefield);
+    int *stall_dev_ = nullptr;                       // test hook of the stage kernel's bounded waits
+    int stall_item_ = -1, stall_fill_ = 0;
+    long long wait_limit_ = 0;
 
 public:
+    // Test hook: the next stage launch's work item `item` leaves its plane
+    // copy number `fill` unissued, once, and every bounded wait of the stage
+    // kernel gives up after `wait_cycles` clocks (0: the default limit).
+    int test_stall(int item, int fill, long long wait_cycles);
     // the stage descriptor of RK stage irk, and the stage's work items (batches use these)
     void stage_desc(int irk, CgStageDesc &d) const;
     int stage_items() const;

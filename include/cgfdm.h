@@ -302,6 +302,34 @@ int cgfdm_destroy(cgfdm_session *s);
  * cgfdm_create in this thread when s is NULL). */
 const char *cgfdm_last_error(const cgfdm_session *s);
 
+/* The session's time loop from step 0 in reference form with the state and
+ * all arithmetic in FP64 (bits = 64) or FP32 (bits = 32), on the session's
+ * model (metric, medium, free-surface matrices, PML profiles, sources,
+ * stations: FP32, promoted in FP64 as the reference's FP32 model is
+ * promoted).  No counterpart in the reference, which computes in float
+ * throughout (src/propagate.cpp:186-321 with src/wave_deriv.cpp:187-283's
+ * float locals): bits = 64 is the FP64 run every FP32 or reduced-storage
+ * result states its error against; bits = 32 reproduces cgfdm_run (bit for
+ * bit in the "exact" build).  One thread per point, buffers of its own for
+ * the call (the session's state, step counter and outputs are untouched).
+ * Outputs (each optional, NULL to skip; n_* their lengths in doubles):
+ * stations [n_stations][nsteps][9] as cgfdm_get_stations records them, pgv
+ * [ny][nx][2], wavefield [_nz_][_ny_][_nx_][9] after the last step. */
+int cgfdm_run_precise(cgfdm_session *s, int nsteps, int bits, double *stations, long long n_stations,
+                      double *pgv, long long n_pgv, double *wavefield, long long n_wavefield);
+
+/* Test hook of the stage kernel's bounded waits.  No counterpart in the
+ * reference, whose CHECK macro prints a CUDA error and carries on
+ * (src/macro.h:94-103): here every wait of the CGFDM stage kernel for its
+ * plane copies is bounded, and a wait that gives up sets a device error word
+ * that the next cgfdm_run reports as CGFDM_E_TIMEOUT.  After this call the
+ * next stage launch's work item `item` leaves its plane copy number `fill`
+ * (counted from the item's first plane) unissued, once, and every bounded
+ * wait gives up after `wait_cycles` clock cycles (0: the default, 2^31).  The
+ * kernel then drains the copies it did issue and returns; the session's
+ * state is not usable afterwards, the device is.  For tests only. */
+int cgfdm_test_stall(cgfdm_session *s, int item, int fill, long long wait_cycles);
+
 /* Allocation-free grid-spacing reduction.  No counterpart in the reference:
  * it offers the smallest and largest point-to-plane distance of the CFL
  * check (the quantity cgfdm_create computes as H_min, after
@@ -317,12 +345,14 @@ const char *cgfdm_last_error(const cgfdm_session *s);
  * the default stream; the call only enqueues work on it.
  *
  * Scratch lives in a static device array of CGFDM_NOALLOC_MAX_BLOCKS (min,
- * max) pairs, 1 MiB, one pair per block of 32 x 8 x 16 points; larger grids
- * are rejected with CGFDM_E_ARG and a message from
- * cgfdm_noalloc_last_error().  The array is shared by every call on a device
- * and keeps the last call's contents, so calls that overlap on the GPU race.
- * The first call on each device looks up the array's device address with
- * that device current. */
+ * max) pairs, 1 MiB, one pair per block of 32 x 8 x 16 points; grids that
+ * need more blocks, or more than 65535 blocks along y or z, are rejected
+ * with CGFDM_E_ARG and a message from cgfdm_noalloc_last_error().  The array
+ * is shared by every call on a device and keeps the last call's contents, so
+ * calls that overlap on the GPU race.  The first call on each device looks
+ * up the array's device address with that device current; a later call
+ * looks it up again if the device's context has changed (after a
+ * cudaDeviceReset). */
 #define CGFDM_NOALLOC_MAX_BLOCKS 65536
 int cgfdm_hrange_noalloc(const float *d_coord, int nx, int ny, int nz, double *d_out, void *stream);
 const char *cgfdm_noalloc_last_error(void);

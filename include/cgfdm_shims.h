@@ -2,9 +2,10 @@
  * Per-function entry points of libcgfdm.so: the reference's step drivers
  * (called from propagate(), src/propagate.cpp:186-309 of CGFDM3D-EQR-SC)
  * with the same names, argument meanings and effects, on arrays the caller
- * owns.  A copy of propagate.cpp whose drivers forward here runs the
- * reference's own time loop on this library's kernels; INTEGRATION.md shows
- * the forwarding wrappers.  The session API (cgfdm.h) is the fast path: it
+ * owns.  A copy of propagate.cpp whose drivers forward here (each driver's
+ * body replaced by a call of the cgfdm_ entry point of the same name) runs
+ * the reference's own time loop on this library's kernels.  The session API
+ * (cgfdm.h) is the fast path: it
  * fuses one RK stage into one kernel over its own layout.
  *
  * Arrays are DEVICE pointers in the reference's layouts (XFAST, src/axis.h:73):
