@@ -142,6 +142,36 @@ def workload_desc(name):
     return name
 
 
+def fp64_error(run_dir, steps, device, options=None):
+    """Error of an FP32 run (the session, as benched) against the FP64 run
+    of the same model (cgfdm_run_precise, bits 64) after ``steps`` steps:
+    relative L2 of the station velocity traces (None while they are all
+    zero) and of the final wavefield."""
+    import numpy as np
+
+    from cgfdm import Session
+
+    with Session(run_dir, options=options, device=device) as s:
+        steps = min(steps, s.info.NT)
+        t0 = time.perf_counter()
+        s.run(steps)
+        t32 = time.perf_counter() - t0
+        st32 = s.stations()[:, :steps, :3].astype(np.float64)
+        w32 = s.wavefield().astype(np.float64)
+        t0 = time.perf_counter()
+        st64, _, w64 = s.run_precise(steps, bits=64, wavefield=True)
+        t64 = time.perf_counter() - t0
+    st64 = st64[:, :, :3]
+
+    def rel(a, b):
+        nb = float(np.linalg.norm(b))
+        return float(np.linalg.norm(a - b)) / nb if nb > 0 else None
+
+    return {"steps": steps, "stations_velocity_rel_l2": rel(st32, st64), "wavefield_rel_l2": rel(w32, w64),
+            "against": "cgfdm_run_precise bits=64: the same time loop, state and arithmetic in FP64",
+            "options": options, "fp32_run_s": t32, "fp64_run_s": t64}
+
+
 def is_scfdm(name):
     return name.startswith("aweno")
 
@@ -545,6 +575,27 @@ def bench_parts(args, world, rank, local_rank):
     print(json.dumps(line))
 
 
+FULL_STEPS = {"terrain_fault": 3000, "aweno_basin": 4000, "halfspace": 1000}
+
+
+def session_options(args):
+    return None if args.storage == "fp32" else json.dumps({"storage": args.storage})
+
+
+def bench_fp64_check(args, local_rank):
+    """One JSON line: the benched path (FP32 or mixed storage) against the
+    FP64 run over the workload's steps (seismogram and wavefield relative L2)."""
+    steps = args.fp64_check
+    if steps < 0:
+        steps = args.full_steps or FULL_STEPS.get(args.workload, 1000)
+    d = os.path.join(WORK, f"{args.workload}_{steps}")
+    make_workload(args.workload, steps, d)
+    e = fp64_error(d, steps, local_rank, session_options(args))
+    print(json.dumps({"metric": "err_vs_fp64", "workload": workload_desc(args.workload), "storage": args.storage,
+                      **e}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -560,6 +611,15 @@ def main():
                     help="CGFDM workloads, one GPU: run the grid as PX,PY,PZ parts (domain decomposition)")
     ap.add_argument("--exchange", default="fused", choices=["fused", "explicit"],
                     help="with --parts: halos stored by the stage kernels, or packed and copied per phase")
+    ap.add_argument("--fp64-check", type=int, default=0, metavar="STEPS",
+                    help="only measure the FP32 run's error against the FP64 run over STEPS steps (-1: the "
+                         "workload's full length) and print it as one JSON line")
+    ap.add_argument("--full-steps", type=int, default=0,
+                    help="with --fp64-check -1: the workload's full length (default: 3000 for terrain_fault, "
+                         "4000 for aweno_basin, 1000 for halfspace)")
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
+                    help="wavefield storage of the CGFDM session: FP32, or FP16 stage and accumulator deltas "
+                         "from the FP32 step state (mixed precision)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -588,6 +648,8 @@ def main():
 
     import torch
 
+    if args.fp64_check:
+        return bench_fp64_check(args, local_rank)
     if args.parts:
         return bench_parts(args, world, rank, local_rank)
     if args.workload.startswith("batch"):
@@ -611,7 +673,7 @@ def main():
         dist.barrier()
 
     # ---- device-timed leg: inputs resident on the GPU
-    s = Session(d, device=local_rank)
+    s = Session(d, options=session_options(args), device=local_rank)
     info = s.info
     pts = info.nx * info.ny * info.nz
     s.run(args.warmup)
@@ -633,7 +695,7 @@ def main():
 
     # ---- end-to-end leg: run directory on disk -> C ABI -> stations on the host
     t0 = time.perf_counter()
-    s2 = Session(d, device=local_rank)
+    s2 = Session(d, options=session_options(args), device=local_rank)
     s2.run(args.steps)
     st = s2.stations()
     i2 = s2.info
@@ -650,6 +712,8 @@ def main():
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "storage": ("fp32" if args.storage == "fp32" else
+                    "fp16 stage/accumulator deltas (per-field scales) + fp32 step state; f32 arithmetic"),
         "scheme": "SCFDM" if sc else "CGFDM",
         "config": {"workload": workload_desc(args.workload), "points": pts, "DT": info.DT,
                    "l2": "inputs larger than L2 (model + wavefield %.1f GB resident)" % (info.device_bytes / 1e9),
@@ -676,6 +740,8 @@ def main():
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    # the result's error against the FP64 run over the timed steps
+    line["err_vs_fp64"] = fp64_error(d, args.steps, local_rank, session_options(args))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, why = cpu_reference_rate(args.workload, 2, 4, min(os.cpu_count() or 1, 32))
         line["cpu_baseline"] = cb if cb else {"unavailable": why}

@@ -108,6 +108,7 @@ int Session::time_steps(int nsteps, float *ms)
 
 int Session::autotune(int trial, int *best_kc, int *best_ctas, float *best_ms)
 {
+    if (int st = need_fp32_storage("autotune")) return st;
     if (m.p.scheme != SCHEME_CGFDM) {
         err = "the autotuner tunes the CGFDM stage kernel";
         return ST_OPTIONS;

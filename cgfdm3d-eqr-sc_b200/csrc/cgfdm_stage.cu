@@ -101,8 +101,14 @@ namespace cgfdm {
 #define SLOT_F (9 * PF)  // floats per slot
 #define SLOT_BYTES (SLOT_F * 4)
 #define NSLOT 6
+#define SLOT_HB (9 * PF * 2)  // mixed storage: bytes of a slot's FP16 delta box
+// Mixed storage: the ring also holds each plane's FP16 delta box, so a CTA
+// needs 104 KB and two fit on an SM.
+#ifndef CG_MIX_CTAS_PER_SM
+#define CG_MIX_CTAS_PER_SM 2
+#endif
 
-size_t cg_stage_smem_bytes() { return (size_t)NSLOT * SLOT_BYTES + NSLOT * 8; }
+size_t cg_stage_smem_bytes(bool mix) { return (size_t)NSLOT * (SLOT_BYTES + (mix ? SLOT_HB : 0)) + NSLOT * 8; }
 
 // ------------------------------------------------------------ TMA helpers
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -242,6 +248,69 @@ __device__ __forceinline__ void ljt_z(const float *__restrict__ W, const float *
     for (int c = 0; c < 3; c++) out[c] = lop(J[0][c], J[1][c], J[2][c], J[3][c], J[4][c], FB, rDH);
 }
 
+// Mixed storage: the stage's stencil input at a point, the FP32 step-start
+// state plus the FP16 delta times its inverse scale (stage 0: no delta).
+struct MixIn {
+    const float *W;
+    const __half *S;
+    const float *inv;
+    DevGrid g, gh;
+    __device__ __forceinline__ float operator()(int f, int i, int j, int k) const
+    {
+        const float v = W[f * g.fstride + g.at(i, j, k)];
+        return S ? v + __half2float(S[f * gh.fstride + gh.at(i, j, k)]) * inv[f] : v;
+    }
+};
+
+// jt_at, ljt_xy and ljt_z of the traction image on the mixed-storage input
+__device__ __forceinline__ void jt_at_m(const MixIn &w, const float *__restrict__ cjm, int i, int j, int k, int mdir,
+                                        float out[3])
+{
+    const long long F = w.g.fstride, q = w.g.at(i, j, k);
+    const float m0 = cjm[(3 * mdir + 0) * F + q], m1 = cjm[(3 * mdir + 1) * F + q], m2 = cjm[(3 * mdir + 2) * F + q];
+    const float jac = cjm[C_JAC * F + q];
+    const float Txx = w(3, i, j, k), Tyy = w(4, i, j, k), Tzz = w(5, i, j, k);
+    const float Txy = w(6, i, j, k), Txz = w(7, i, j, k), Tyz = w(8, i, j, k);
+    out[0] = ((m0 * Txx + m1 * Txy) + m2 * Txz) * jac;
+    out[1] = ((m0 * Txy + m1 * Tyy) + m2 * Tyz) * jac;
+    out[2] = ((m0 * Txz + m1 * Tyz) + m2 * Tzz) * jac;
+}
+
+__device__ __forceinline__ void ljt_xy_m(const MixIn &w, const float *__restrict__ cjm, int i, int j, int k, int dir,
+                                         int FB, float rDH, float out[3])
+{
+    float J[5][3];
+    for (int m = 0; m < 5; m++) {
+        const int o = (m - 1) * FB;
+        jt_at_m(w, cjm, dir == 0 ? i + o : i, dir == 1 ? j + o : j, k, dir, J[m]);
+    }
+    for (int c = 0; c < 3; c++) out[c] = lop(J[0][c], J[1][c], J[2][c], J[3][c], J[4][c], FB, rDH);
+}
+
+__device__ __forceinline__ void ljt_z_m(const MixIn &w, const float *__restrict__ cjm, int i, int j, int k, int ks_rel,
+                                        int FB, float rDH, float out[3])
+{
+    float J[5][3];
+    for (int m = 0; m < 5; m++) {
+        const int l = 3 + (m - 1) * FB;
+        int src = l, sign = 1;
+        if (l > ks_rel) src = 2 * ks_rel - l, sign = -1;
+        if (src == ks_rel) {
+            J[m][0] = J[m][1] = J[m][2] = 0.0f;
+        } else {
+            jt_at_m(w, cjm, i, j, k + src - 3, 2, J[m]);
+            if (sign < 0) J[m][0] = -J[m][0], J[m][1] = -J[m][1], J[m][2] = -J[m][2];
+        }
+    }
+    for (int c = 0; c < 3; c++) out[c] = lop(J[0][c], J[1][c], J[2][c], J[3][c], J[4][c], FB, rDH);
+}
+
+// a delta to its stored FP16 value (scaled, saturated)
+__device__ __forceinline__ __half to_h16(float x, float sc)
+{
+    return __float2half_rn(fminf(fmaxf(x * sc, -65504.0f), 65504.0f));
+}
+
 // ------------------------------------------------------------- the stage
 // Persistent CTAs (three per SM) take work items -- one 32 x 4 column tile
 // over one z-chunk -- from an atomic counter, chunks of a tile adjacent in
@@ -252,15 +321,24 @@ __device__ __forceinline__ void ljt_z(const float *__restrict__ W, const float *
 // and tensor maps in parameter space).  BATCH = true: the work items of
 // nsess sessions, their descriptors in global memory; a CTA copies the
 // arguments of the session its current item belongs to into shared memory.
-template <int FB1, int FB2, int FB3, bool BATCH, bool HOUT>
-__global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
+//
+// MIX = true: mixed-precision storage (see CgStageArgs).  Each slot also
+// receives the plane's FP16 delta box; when a plane arrives, the CTA adds the
+// delta into the FP32 box in place, so the taps read the stage's input as in
+// the FP32 kernel.
+template <int FB1, int FB2, int FB3, bool BATCH, bool HOUT, bool MIX = false>
+__global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER_SM)
     k_cg_stage(const __grid_constant__ CgStageDesc d1, const CgStageDesc *__restrict__ descs,
                const int *__restrict__ item_start, int nsess, int *work)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float *ring = reinterpret_cast<float *>(smem_raw);
-    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw + NSLOT * SLOT_BYTES);
+    __half *ring16 = reinterpret_cast<__half *>(smem_raw + NSLOT * SLOT_BYTES);
+    unsigned long long *bars =
+        reinterpret_cast<unsigned long long *>(smem_raw + NSLOT * (SLOT_BYTES + (MIX ? SLOT_HB : 0)));
     __shared__ int s_abort, s_item;
+    __shared__ float s_sc[MIX ? 9 : 1], s_inv[MIX ? 9 : 1];
+    __shared__ int s_par;
     __shared__ __align__(16) CgStageArgs s_args;
     const CgStageArgs &a = BATCH ? s_args : d1.a;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -274,8 +352,34 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         s_abort = 0;
         for (int s = 0; s < NSLOT; s++) mbar_init(smem_u32(&bars[s]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        if constexpr (MIX) {
+            // per-field scales of this step: the bound of field f maps below 2^13
+            const CgStageArgs &A0 = d1.a;
+            const int p = *A0.it_dev & 1;
+            s_par = p;
+            float M[9], Mv = 0.0f, Ms = 0.0f;
+            for (int f = 0; f < 9; f++) {
+                M[f] = __uint_as_float(A0.mx[p * 9 + f]);
+                if (f < 3 && M[f] > Mv) Mv = M[f];
+                if (f >= 3 && M[f] > Ms) Ms = M[f];
+            }
+            for (int f = 0; f < 9; f++) {
+                const float c = f < 3 ? Ms / A0.zs_min : Mv * A0.zp_max;
+                const float b = M[f] > c ? M[f] : c;
+                int e = 0;
+                if (b > 0.0f) frexpf(b, &e);
+                s_sc[f] = b > 0.0f ? ldexpf(1.0f, 13 - e) : 1.0f;
+                s_inv[f] = b > 0.0f ? ldexpf(1.0f, e - 13) : 1.0f;
+            }
+            // the next step's bounds start from zero; stage 3 raises them
+            if (A0.irk == 0 && blockIdx.x == 0)
+                for (int f = 0; f < 9; f++) A0.mx[(p ^ 1) * 9 + f] = 0u;
+        }
     }
     unsigned seq0 = 0;  // fills issued by this CTA before the current item
+    float rm[MIX ? 9 : 1];   // mixed storage, stage 3: running max |new state| per field
+#pragma unroll
+    for (int f = 0; f < (MIX ? 9 : 1); f++) rm[f] = 0.0f;
 
     for (;;) {
     __syncthreads();
@@ -302,6 +406,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     const CUtensorMap *tmC = reinterpret_cast<const CUtensorMap *>(D.tmC);
     const CUtensorMap *tmM = reinterpret_cast<const CUtensorMap *>(D.tmM);
     const CUtensorMap *tmT = reinterpret_cast<const CUtensorMap *>(D.tmT);
+    const CUtensorMap *tmS = reinterpret_cast<const CUtensorMap *>(D.tmS);
     const DevGrid g = a.g;
     const long long F = g.fstride;
     const int _nx = g.nxp - CGFDM_HALO, _ny = g.nyp - CGFDM_HALO, _nz = g.nzp - CGFDM_HALO;
@@ -320,6 +425,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     const int tx0 = g.xoff + i0 - 4;        // halo box origin column: a multiple of 4 (16 bytes)
     const int ty0 = j0 - hyL;
     const int px0 = g.xoff + i0;            // point box origin column: a multiple of 4
+    const int tx0h = MIX ? a.gh.xoff + i0 - 4 : 0;   // FP16 halo box origin: a multiple of 8 (16 bytes)
 
     // plane kk of this item is fill number seq0 + (kk - kf) of the CTA
     auto slot_of = [&](int kk) { return (int)((seq0 + (unsigned)(kk - kf)) % NSLOT); };
@@ -331,6 +437,13 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         // arrival that would complete its barrier phase), once
         if (a.stall && gitem == a.stall_item && kk - kf == a.stall_fill && atomicExch(a.stall, 0) == 1) return;
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        if constexpr (MIX) {
+            const bool hs = a.irk != 0;
+            mbar_expect_tx(bar, SLOT_BYTES + (hs ? SLOT_HB : 0));
+            tma_load_4d(smem_u32(ring + s * SLOT_F), tmW, tx0, ty0, kk, 0, bar);
+            if (hs) tma_load_4d(smem_u32(ring16 + s * (9 * PF)), tmS, tx0h, ty0, kk, 0, bar);
+            return;
+        }
         mbar_expect_tx(bar, SLOT_BYTES);
         if (CG_RING_EVICT_LAST)
             tma_load_4d_hint(smem_u32(ring + s * SLOT_F), tmW, tx0, ty0, kk, 0, bar, l2_evict_last_policy());
@@ -340,8 +453,24 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     // point operands of plane kk into L2 ahead of their plain loads
     auto prefetch_points = [&](int kk) {
         if (CG_PREFETCH_C) tma_prefetch_4d(tmC, px0, j0, kk, 0);
+        if constexpr (MIX) {
+            // the step-start state in stages 1-3, the FP16 accumulator (halo map) in 2-3
+            if (CG_PREFETCH_MT && a.irk != 0) tma_prefetch_4d(tmM, px0, j0, kk, 0);
+            if (CG_PREFETCH_MT && a.irk >= 2) tma_prefetch_4d(tmT, tx0h, ty0, kk, 0);
+            return;
+        }
         if (CG_PREFETCH_MT && (a.irk == 1 || a.irk == 2)) tma_prefetch_4d(tmM, px0, j0, kk, 0);
         if (CG_PREFETCH_MT && a.irk != 0) tma_prefetch_4d(tmT, px0, j0, kk, 0);
+    };
+    // mixed storage: the delta box of plane kk into its FP32 box, in place
+    auto convert = [&](int kk) {
+        float *r32 = ring + slot_of(kk) * SLOT_F;
+        const __half *r16 = ring16 + slot_of(kk) * (9 * PF);
+#pragma unroll 1
+        for (int f = 0; f < 9; f++) {
+            const float inv = s_inv[f];
+            for (int x = tid; x < PF; x += TX * TY) r32[f * PF + x] = r32[f * PF + x] + __half2float(r16[f * PF + x]) * inv;
+        }
     };
 
     const long long wlim = a.wait_limit > 0 ? a.wait_limit : (1LL << 31);
@@ -357,6 +486,13 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     if (!ok) {
         s_abort = 1;
         atomicOr(a.err, 1);
+    }
+    if constexpr (MIX) {
+        if (a.irk != 0) {
+            __syncthreads();   // every thread's outcome is in s_abort
+            if (!s_abort)
+                for (int kk = kf; kk < kf + 4; kk++) convert(kk);
+        }
     }
 
     const float bx = active ? a.pml_beta_x[i] : 1.0f, by = active ? a.pml_beta_y[j] : 1.0f;
@@ -393,17 +529,35 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
             mu = CG_LD(a.cjm[C_MU * F + q]), lam = CG_LD(a.cjm[C_LAMBDA * F + q]);
             buo = CG_LD(a.cjm[C_BUOY * F + q]) * 1.0f;  // buoyancy *= Crho (= 1)
             bz = a.pml_beta_z[k];
-            if (a.irk == 1 || a.irk == 2)
-                for (int f = 0; f < 9; f++) mv[f] = CG_LD(a.Wm[f * F + q]);
-            if (a.irk != 0)
-                for (int f = 0; f < 9; f++) tv[f] = CG_LD(a.T[f * F + q]);
+            if constexpr (MIX) {
+                if (a.irk != 0)
+                    for (int f = 0; f < 9; f++) mv[f] = a.Wm[f * F + q];
+                if (a.irk >= 2) {
+                    const long long qh = a.gh.at(i, j, k);
+                    for (int f = 0; f < 9; f++) tv[f] = __half2float(a.T16[f * a.gh.fstride + qh]) * s_inv[f];
+                }
+            } else {
+                if (a.irk == 1 || a.irk == 2)
+                    for (int f = 0; f < 9; f++) mv[f] = CG_LD(a.Wm[f * F + q]);
+                if (a.irk != 0)
+                    for (int f = 0; f < 9; f++) tv[f] = CG_LD(a.T[f * F + q]);
+            }
         }
         const int kk_new = k - za + 4;
-        if (!mbar_wait_bounded(smem_u32(&bars[slot_of(kk_new)]), parity_of(kk_new), wlim)) {
+        const bool okw = mbar_wait_bounded(smem_u32(&bars[slot_of(kk_new)]), parity_of(kk_new), wlim);
+        if (!okw) {
             s_abort = 1;
             atomicOr(a.err, 1);
-            continue;
         }
+        if constexpr (MIX) {
+            if (a.irk != 0) {
+                __syncthreads();   // every thread's outcome is in s_abort
+                if (s_abort) continue;
+                convert(kk_new);
+                __syncthreads();
+            }
+        }
+        if (!okw) continue;
         if (!active) continue;
 
         Taps<FB1, FB2, FB3> T;
@@ -438,9 +592,16 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
             // src/freeSurface.cpp:345-492
             const int ks_rel = (_nz - 1) - k + CGFDM_HALO;
             float jx[3], jy[3], jz[3];
-            ljt_xy(a.Win, a.cjm, g, i, j, k, 0, FB1, rDH, jx);
-            ljt_xy(a.Win, a.cjm, g, i, j, k, 1, FB2, rDH, jy);
-            ljt_z(a.Win, a.cjm, g, i, j, k, ks_rel, FB3, rDH, jz);
+            if constexpr (MIX) {
+                const MixIn w{a.Win, a.irk != 0 ? a.Sin : nullptr, s_inv, g, a.gh};
+                ljt_xy_m(w, a.cjm, i, j, k, 0, FB1, rDH, jx);
+                ljt_xy_m(w, a.cjm, i, j, k, 1, FB2, rDH, jy);
+                ljt_z_m(w, a.cjm, i, j, k, ks_rel, FB3, rDH, jz);
+            } else {
+                ljt_xy(a.Win, a.cjm, g, i, j, k, 0, FB1, rDH, jx);
+                ljt_xy(a.Win, a.cjm, g, i, j, k, 1, FB2, rDH, jy);
+                ljt_z(a.Win, a.cjm, g, i, j, k, ks_rel, FB3, rDH, jz);
+            }
             const float jinv = 1.0f / a.cjm[C_JAC * F + q];
             const float bj = buo * jinv;
             for (int c = 0; c < 3; c++) h[c] = (bj * ((jx[c] * bx + jy[c] * by) + jz[c])) * DT;
@@ -550,6 +711,36 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
 
         // ---- RK4 update of the wavefield (src/wave_rk.cpp:17-104)
         float wout[9];
+        if constexpr (MIX) {
+            // stage deltas d1 = h0 / 2, d2 = h1 / 2, d3 = h2 and the
+            // accumulator delta t - m (b1 h0 = d1 / 3, formed in stage 1)
+            const long long qh = a.gh.at(i, j, k), Fh = a.gh.fstride;
+            if (a.irk == 0) {
+#pragma unroll
+                for (int f = 0; f < 9; f++) a.Sout[f * Fh + qh] = to_h16(RK_ALPHA2 * h[f], s_sc[f]);
+            } else if (a.irk == 1) {
+                const __half *cur16 = ring16 + slot_of(k) * (9 * PF) + cell;
+#pragma unroll
+                for (int f = 0; f < 9; f++) {
+                    const float d1 = __half2float(cur16[f * PF]) * s_inv[f];
+                    a.T16[f * Fh + qh] = to_h16(d1 * 0.33333334f + RK_BETA2 * h[f], s_sc[f]);
+                    a.Sout[f * Fh + qh] = to_h16(RK_ALPHA3 * h[f], s_sc[f]);
+                }
+            } else if (a.irk == 2) {
+#pragma unroll
+                for (int f = 0; f < 9; f++) {
+                    a.T16[f * Fh + qh] = to_h16(tv[f] + RK_BETA3 * h[f], s_sc[f]);
+                    a.Sout[f * Fh + qh] = to_h16(h[f], s_sc[f]);
+                }
+            } else {
+#pragma unroll
+                for (int f = 0; f < 9; f++) {
+                    wout[f] = mv[f] + (tv[f] + RK_BETA4 * h[f]);
+                    CG_ST(a.Wout[f * F + q], wout[f]);
+                    rm[f] = fmaxf(rm[f], fabsf(wout[f]));
+                }
+            }
+        } else {
         if (a.irk == 0) {
 #pragma unroll
             for (int f = 0; f < 9; f++) {
@@ -574,6 +765,7 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
         }
 #pragma unroll
         for (int f = 0; f < 9; f++) CG_ST(a.Wout[f * F + q], wout[f]);
+        }
         if (HOUT) {
             // a part of a decomposed grid: the interior layers next to a face
             // shared with a neighbour go straight into the neighbour's halo
@@ -619,6 +811,16 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
     seq0 += (unsigned)(issued - kf + 1);
     }  // work items
 
+    if constexpr (MIX) {
+        // stage 3: raise the bounds of the next step with this CTA's maxima
+        if (d1.a.irk == 3)
+#pragma unroll 1
+            for (int f = 0; f < 9; f++) {
+                float v = rm[f];
+                for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+                if ((tid & 31) == 0 && v > 0.0f) atomicMax(&d1.a.mx[(s_par ^ 1) * 9 + f], __float_as_uint(v));
+            }
+    }
     // the last CTA out resets the work counter for the next launch
     __syncthreads();
     if (tid == 0) {
@@ -636,35 +838,92 @@ __global__ void __launch_bounds__(TX *TY, CG_CTAS_PER_SM)
 int cg_stage_ctas_per_sm() { return CG_CTAS_PER_SM; }
 int cg_stage_tile_y() { return TY; }
 
-template <int FB1, int FB2, int FB3, bool BATCH, bool HOUT>
+template <int FB1, int FB2, int FB3, bool BATCH, bool HOUT, bool MIX>
 static cudaError_t launch_t(const CgStageDesc &d1, const CgStageDesc *descs, const int *item_start, int nsess,
                             int *work, int ctas, cudaStream_t st)
 {
     // The shared-memory limit is an attribute of the kernel on the current
     // device (and is lost with a device reset), so it is set on every launch:
     // a host-side call of about a microsecond, legal during stream capture.
-    CUDA_TRY(cudaFuncSetAttribute(k_cg_stage<FB1, FB2, FB3, BATCH, HOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)cg_stage_smem_bytes()));
-    k_cg_stage<FB1, FB2, FB3, BATCH, HOUT>
-        <<<ctas, dim3(TX, TY, 1), cg_stage_smem_bytes(), st>>>(d1, descs, item_start, nsess, work);
+    CUDA_TRY(cudaFuncSetAttribute(k_cg_stage<FB1, FB2, FB3, BATCH, HOUT, MIX>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cg_stage_smem_bytes(MIX)));
+    k_cg_stage<FB1, FB2, FB3, BATCH, HOUT, MIX>
+        <<<ctas, dim3(TX, TY, 1), cg_stage_smem_bytes(MIX), st>>>(d1, descs, item_start, nsess, work);
     return cudaGetLastError();
 }
 
-template <bool BATCH, bool HOUT>
+template <bool BATCH, bool HOUT, bool MIX = false>
 static cudaError_t launch_b(int FB1, int FB2, int FB3, const CgStageDesc &d1, const CgStageDesc *descs,
                             const int *item_start, int nsess, int *work, int ctas, cudaStream_t st)
 {
     const int key = (FB1 > 0) * 4 + (FB2 > 0) * 2 + (FB3 > 0);
     switch (key) {
-    case 0: return launch_t<-1, -1, -1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
-    case 1: return launch_t<-1, -1, 1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
-    case 2: return launch_t<-1, 1, -1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
-    case 3: return launch_t<-1, 1, 1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
-    case 4: return launch_t<1, -1, -1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
-    case 5: return launch_t<1, -1, 1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
-    case 6: return launch_t<1, 1, -1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
-    default: return launch_t<1, 1, 1, BATCH, HOUT>(d1, descs, item_start, nsess, work, ctas, st);
+    case 0: return launch_t<-1, -1, -1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
+    case 1: return launch_t<-1, -1, 1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
+    case 2: return launch_t<-1, 1, -1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
+    case 3: return launch_t<-1, 1, 1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
+    case 4: return launch_t<1, -1, -1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
+    case 5: return launch_t<1, -1, 1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
+    case 6: return launch_t<1, 1, -1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
+    default: return launch_t<1, 1, 1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
     }
+}
+
+int cg_stage_mix_ctas_per_sm() { return CG_MIX_CTAS_PER_SM; }
+
+cudaError_t launch_cg_stage_mix(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int ctas, cudaStream_t st)
+{
+    return launch_b<false, false, true>(FB1, FB2, FB3, d, nullptr, nullptr, 1, work, ctas, st);
+}
+
+cudaError_t make_field_tmap16(void *out, const __half *base, const DevGrid &gh, int nf)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void *fn = nullptr;
+        CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    cuuint64_t dims[4] = {(cuuint64_t)gh.pitch, (cuuint64_t)gh.nyp, (cuuint64_t)gh.nzp, (cuuint64_t)nf};
+    cuuint64_t strides[3] = {(cuuint64_t)gh.pitch * 2, (cuuint64_t)gh.plane * 2, (cuuint64_t)gh.fstride * 2};
+    cuuint32_t box[4] = {(cuuint32_t)BXW, (cuuint32_t)BYW, 1, (cuuint32_t)nf};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = encode(reinterpret_cast<CUtensorMap *>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 4, (void *)base, dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CG_PROMO_HALO,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// Impedance bounds of the medium over the interior (float bits; the atomics
+// order non-negative floats as their bit patterns): min sqrt(mu / b) into
+// out[0], max sqrt((lambda + 2 mu) / b) into out[1].
+__global__ void k_impedance_bounds(const float *__restrict__ cjm, DevGrid g, unsigned *out)
+{
+    const int i = blockIdx.x * 32 + threadIdx.x + CGFDM_HALO, j = blockIdx.y * 4 + threadIdx.y + CGFDM_HALO;
+    const int k = blockIdx.z + CGFDM_HALO;
+    float zs = 3.4e38f, zp = 0.0f;
+    if (i < g.nxp - CGFDM_HALO && j < g.nyp - CGFDM_HALO) {
+        const long long F = g.fstride, q = g.at(i, j, k);
+        const float mu = cjm[C_MU * F + q], lam = cjm[C_LAMBDA * F + q], b = cjm[C_BUOY * F + q];
+        zs = __fsqrt_rn(__fdiv_rn(mu, b));
+        zp = __fsqrt_rn(__fdiv_rn(__fadd_rn(lam, __fmul_rn(2.0f, mu)), b));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        zs = fminf(zs, __shfl_xor_sync(0xffffffffu, zs, o));
+        zp = fmaxf(zp, __shfl_xor_sync(0xffffffffu, zp, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&out[0], __float_as_uint(zs));
+        atomicMax(&out[1], __float_as_uint(zp));
+    }
+}
+
+cudaError_t launch_impedance_bounds(const float *cjm, DevGrid g, unsigned *out, cudaStream_t st)
+{
+    k_impedance_bounds<<<dim3((g.nx + 31) / 32, (g.ny + 3) / 4, g.nz), dim3(32, 4), 0, st>>>(cjm, g, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_cg_stage(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int ctas, cudaStream_t st,

@@ -89,6 +89,7 @@ int Session::load_state(const char *src)
 
 int Session::set_wavefield(const float *host)
 {
+    if (int st = need_fp32_storage("set_wavefield")) return st;
     const long long npad = m.g.npad();
     float *d = nullptr;
     CU(cudaMalloc(&d, sizeof(float) * npad * 9));
@@ -102,6 +103,7 @@ int Session::set_wavefield(const float *host)
 
 int Session::set_medium(const float *host)
 {
+    if (int st = need_fp32_storage("set_medium")) return st;
     if (m.p.scheme != SCHEME_CGFDM) {
         err = "set_medium takes CGFDM sessions";
         return ST_OPTIONS;
@@ -263,6 +265,7 @@ int Session::adj_step(int n, float *const *h4, float *const *vd4)
 
 int Session::adjoint_apply(int nsteps, float *host)
 {
+    if (int st = need_fp32_storage("adjoint_apply")) return st;
     if (nsteps < 0 || nsteps > it) {
         err = "adjoint_apply covers steps the session has run: 0 <= nsteps <= steps completed";
         return ST_ARG;
@@ -351,6 +354,7 @@ void arena_session_remove(int device)
 
 int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
 {
+    if (int st = need_fp32_storage("gradient")) return st;
     if (it != 0) {
         err = "gradient starts from step 0 (set_medium returns a session there)";
         return ST_STATE;

@@ -89,6 +89,7 @@ int Session::halo_copy(int face, int which, float *dev, bool pack)
 
 int Session::link_halo_to(int face, float *const nw[3], const DevGrid &ng)
 {
+    if (int st = need_fp32_storage("link_halo_to")) return st;
     if (face < 0 || face > 5 || m.p.scheme != SCHEME_CGFDM || !nw[0] || !nw[1] || !nw[2]) {
         err = "bad face, scheme or buffers for a halo link";
         return ST_ARG;
@@ -138,6 +139,7 @@ static const long long PART_HANDLE_MAGIC = 0x48545241504d4447LL;
 
 int Session::part_handle(void *out, long long bytes)
 {
+    if (int st = need_fp32_storage("part_handle")) return st;
     static_assert(sizeof(PartHandle) <= 512, "handle size");
     if (!out || bytes < (long long)sizeof(PartHandle) || m.p.scheme != SCHEME_CGFDM) {
         err = "handle buffer too small or not a CGFDM part";
@@ -184,6 +186,10 @@ int Session::create_part(const std::string &dir, const std::string &options, con
     int st = build_model(dir, options, G, err);
     if (st) return st;
     if ((st = slice_model(G, parts, coord, m, err))) return st;
+    if (m.p.storage != "fp32") {
+        err = "a part of a decomposed grid stores its wavefield in FP32";
+        return ST_OPTIONS;
+    }
     is_part_ = parts[0] * parts[1] * parts[2] > 1;
     CU(cudaSetDevice(dev));
     arena_session_add(dev);

@@ -49,7 +49,7 @@ int Session::check_finite(long long *count, long long *first)
     CU(cudaMemcpyAsync(d, init, sizeof init, cudaMemcpyHostToDevice, stream));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    k_count_nonfinite<<<sms * 4, 256, 0, stream>>>(W_[0], g, d, d + 1);
+    k_count_nonfinite<<<sms * 4, 256, 0, stream>>>(state(), g, d, d + 1);
     CU(cudaGetLastError());
     unsigned long long h[2];
     CU(cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, stream));

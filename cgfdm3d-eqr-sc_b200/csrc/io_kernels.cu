@@ -19,9 +19,10 @@ __device__ __forceinline__ void decode_ref(long long c, const DevGrid &g, int &i
 // 262-377).  SCFDM stores strain, so the moment rate is converted with the
 // local compliance first (:217-238).
 __global__ void k_fault(float *W, const float *__restrict__ cjm, DevGrid g, FaultDev f, const int *it_dev, float DT,
-                        int scheme)
+                        int scheme, float *Walt, unsigned *mx)
 {
     const int it = *it_dev;
+    if (Walt && (it & 1)) W = Walt;   // mixed storage: this step's state buffer
     const float tmpT = __fmul_rn((float)it + 0.0f, DT);
     const int srcIt = (int)__fdiv_rn(tmpT, f.dt);
     if (srcIt + 1 >= f.nt) return;  // end of table: the reference stops injecting
@@ -52,7 +53,11 @@ __global__ void k_fault(float *W, const float *__restrict__ cjm, DevGrid g, Faul
             e[5] = __fdiv_rn(s[3], mu);
             for (int c = 0; c < 6; c++) W[(3 + c) * F + q] = __fsub_rn(W[(3 + c) * F + q], __fmul_rn(e[c], DT));
         } else {
-            for (int c = 0; c < 6; c++) W[(3 + c) * F + q] = __fsub_rn(W[(3 + c) * F + q], __fmul_rn(s[c], DT));
+            for (int c = 0; c < 6; c++) {
+                const float v = __fsub_rn(W[(3 + c) * F + q], __fmul_rn(s[c], DT));
+                W[(3 + c) * F + q] = v;
+                if (mx) atomicMax(&mx[(it & 1) * 9 + 3 + c], __float_as_uint(fabsf(v)));
+            }
         }
     }
 }
@@ -62,11 +67,18 @@ __global__ void k_fault(float *W, const float *__restrict__ cjm, DevGrid g, Faul
 // receive the value in the stage buffers (B, C), because the reference's RK
 // update keeps halo cells at their step-start value through all stages.
 __global__ void k_point(float *W, float *Wb, float *Wc, const float *__restrict__ cjm, DevGrid g, PointDev p,
-                        const int *it_dev, float DT, float DH, int scheme)
+                        const int *it_dev, float DT, float DH, int scheme, float *Walt, unsigned *mx)
 {
     const int t = threadIdx.x;
     if (t >= 343 || !p.inside) return;
     const int it = *it_dev;
+    if (Walt) {
+        // mixed storage: the state of this step is one of two buffers; halo
+        // cells, which no stage updates, get the value in both
+        Wb = (it & 1) ? W : Walt;
+        W = (it & 1) ? Walt : W;
+        Wc = nullptr;
+    }
     const int di = t % 7 - 3, dj = (t / 7) % 7 - 3, dk = t / 49 - 3;
     const int i = p.X + di, j = p.Y + dj, k = p.Z + dk;
     const long long F = g.fstride;
@@ -118,26 +130,29 @@ __global__ void k_point(float *W, float *Wb, float *Wc, const float *__restrict_
         if (halo) {
             if (Wb) Wb[(3 + c) * F + q] = v;
             if (Wc) Wc[(3 + c) * F + q] = v;
+        } else if (mx) {
+            atomicMax(&mx[(it & 1) * 9 + 3 + c], __float_as_uint(fabsf(v)));
         }
     }
 }
 
 cudaError_t launch_sources(float *W, const float *cjm, DevGrid g, const FaultDev &f, const PointDev &p,
-                           const int *it_dev, float DT, float DH, int scheme, cudaStream_t st)
+                           const int *it_dev, float DT, float DH, int scheme, cudaStream_t st, float *Walt,
+                           unsigned *mx)
 {
     if (f.npts > 0) {
         int nb = (int)std::min<long long>((f.npts + 255) / 256, 1024);
-        k_fault<<<nb, 256, 0, st>>>(W, cjm, g, f, it_dev, DT, scheme);
+        k_fault<<<nb, 256, 0, st>>>(W, cjm, g, f, it_dev, DT, scheme, Walt, mx);
         CUDA_TRY(cudaGetLastError());
     }
     return cudaSuccess;
 }
 
 cudaError_t launch_point(float *W, float *Wb, float *Wc, const float *cjm, DevGrid g, const PointDev &p,
-                         const int *it_dev, float DT, float DH, int scheme, cudaStream_t st)
+                         const int *it_dev, float DT, float DH, int scheme, cudaStream_t st, float *Walt, unsigned *mx)
 {
     if (p.kind == 0 || !p.inside) return cudaSuccess;
-    k_point<<<1, 352, 0, st>>>(W, Wb, Wc, cjm, g, p, it_dev, DT, DH, scheme);
+    k_point<<<1, 352, 0, st>>>(W, Wb, Wc, cjm, g, p, it_dev, DT, DH, scheme, Walt, mx);
     return cudaGetLastError();
 }
 
@@ -146,9 +161,11 @@ cudaError_t launch_point(float *W, float *Wb, float *Wc, const float *cjm, DevGr
 // the conserved state (:336-365).  One block; thread 0 then advances the
 // step counter for the next step's source term.
 __global__ void k_stations(const float *__restrict__ W, const float *__restrict__ cjm, DevGrid g,
-                           const int *__restrict__ idx, int nst, int NT, float *out, int *it_dev, int scheme)
+                           const int *__restrict__ idx, int nst, int NT, float *out, int *it_dev, int scheme,
+                           const float *__restrict__ Walt)
 {
     const int it = *it_dev;
+    if (Walt && ((it + 1) & 1)) W = Walt;   // mixed storage: the state after step it
     const long long F = g.fstride;
     for (int s = threadIdx.x; s < nst; s += blockDim.x) {
         const long long q = g.at(idx[s * 3 + 0], idx[s * 3 + 1], idx[s * 3 + 2]);
@@ -177,9 +194,9 @@ __global__ void k_stations(const float *__restrict__ W, const float *__restrict_
 }
 
 cudaError_t launch_stations(const float *W, const float *cjm, DevGrid g, const int *st_idx, int nst, int NT,
-                            float *out, int *it_dev, int scheme, cudaStream_t st)
+                            float *out, int *it_dev, int scheme, cudaStream_t st, const float *Walt)
 {
-    k_stations<<<1, 256, 0, st>>>(W, cjm, g, st_idx, nst, NT, out, it_dev, scheme);
+    k_stations<<<1, 256, 0, st>>>(W, cjm, g, st_idx, nst, NT, out, it_dev, scheme, Walt);
     return cudaGetLastError();
 }
 

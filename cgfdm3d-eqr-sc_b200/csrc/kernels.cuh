@@ -1,6 +1,7 @@
 // Kernel launch interfaces (host side).
 #pragma once
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "device.cuh"
@@ -76,6 +77,22 @@ struct CgStageArgs {
     int *stall;
     int stall_item, stall_fill;
     long long wait_limit;
+    // Mixed-precision storage ("storage": "fp16"; the MIX instantiation).
+    // The step-start state stays FP32 and alternates between two buffers
+    // with the step's parity (Wm = this step's, Wout in stage 3 = the
+    // next's); each stage's delta from it (Sout; the next stage's stencil
+    // input is Wm + Sin) and the RK accumulator's delta (T16) are FP16 values
+    // times a per-field power-of-two scale, in the FP16 layout gh.  The
+    // scales come from mx[parity][9], the bounds of |Wm| at the step start
+    // (float bits: stage 3 and the source kernels raise them with atomicMax),
+    // coupled between velocity and stress through the medium's impedance
+    // bounds zs_min, zp_max.
+    DevGrid gh;
+    const __half *Sin;
+    __half *Sout, *T16;
+    unsigned *mx;
+    const int *it_dev;
+    float zs_min, zp_max;
     int ntiles_x, ntiles_y, nchunk;  // work items: tiles x tiles x z-chunks
     int irk;
     int FB1, FB2, FB3;
@@ -100,6 +117,7 @@ struct CgStageMaps {
 // work: the launch's work-counter pair, zero between launches.
 struct alignas(64) CgStageDesc {
     unsigned char tmW[128], tmC[128], tmM[128], tmT[128];
+    unsigned char tmS[128];   // mixed storage: the FP16 stencil-input delta, halo box
     CgStageArgs a;
 };
 // One session's stage, its descriptor passed as a kernel parameter.
@@ -110,7 +128,17 @@ cudaError_t launch_cg_stage(int FB1, int FB2, int FB3, const CgStageDesc &d, int
 // signs and stage number.
 cudaError_t launch_cg_stage_batch(int FB1, int FB2, int FB3, const CgStageDesc *descs, const int *item_start,
                                   int nsess, int *work, int grid_ctas, cudaStream_t st);
-size_t cg_stage_smem_bytes();
+size_t cg_stage_smem_bytes(bool mix = false);
+// Mixed-precision storage: one session's stage (the MIX instantiation).
+cudaError_t launch_cg_stage_mix(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,
+                                cudaStream_t st);
+int cg_stage_mix_ctas_per_sm();
+// FP16 counterpart of make_field_tmap (halo box), for arrays in the layout gh.
+cudaError_t make_field_tmap16(void *out, const __half *base, const DevGrid &gh, int nf);
+// Smallest S and largest P impedance, sqrt(mu / b) and sqrt((lambda + 2 mu) / b),
+// over the interior, into out[0], out[1] (float bits; the caller sets out[0]
+// to +inf bits and out[1] to 0 first).
+cudaError_t launch_impedance_bounds(const float *cjm, DevGrid g, unsigned *out, cudaStream_t st);
 // Encodes the 4-D tensor map (x, y, z, field) of an nf-field buffer, with a
 // halo box (40 x (tile rows + 4) x 1 x nf) or a point box (32 x tile rows x 1 x nf); out must hold
 // 128 bytes.
@@ -212,13 +240,19 @@ struct PointDev {
 };
 // Adds the source terms of step *it_dev to W (stage-0 time), as the
 // reference does before the RK stages (src/propagate.cpp:198-210).
+// Mixed storage (Walt given): the step-start state of step n is W for even
+// n, Walt for odd n, and the injected values raise the bounds mx[n & 1].
 cudaError_t launch_sources(float *W, const float *cjm, DevGrid g, const FaultDev &f, const PointDev &p,
-                           const int *it_dev, float DT, float DH, int scheme, cudaStream_t st);
+                           const int *it_dev, float DT, float DH, int scheme, cudaStream_t st,
+                           float *Walt = nullptr, unsigned *mx = nullptr);
 cudaError_t launch_point(float *W, float *Wb, float *Wc, const float *cjm, DevGrid g, const PointDev &p,
-                         const int *it_dev, float DT, float DH, int scheme, cudaStream_t st);
+                         const int *it_dev, float DT, float DH, int scheme, cudaStream_t st, float *Walt = nullptr,
+                         unsigned *mx = nullptr);
 // Records 9 components per station at step *it_dev, then advances *it_dev.
+// Mixed storage (Walt given): the state after step n is in W or Walt by the
+// parity of n + 1.
 cudaError_t launch_stations(const float *W, const float *cjm, DevGrid g, const int *st_idx, int nst, int NT,
-                            float *out, int *it_dev, int scheme, cudaStream_t st);
+                            float *out, int *it_dev, int scheme, cudaStream_t st, const float *Walt = nullptr);
 // Peak ground acceleration [ny][nx][2] (PGAh, PGA) after a step whose index
 // *it_dev is a multiple of 10 (the reference's SOLVE_PGA).
 cudaError_t launch_pga(const float *W, const float *cjm, DevGrid g, const int *it_dev, float DT, int scheme,

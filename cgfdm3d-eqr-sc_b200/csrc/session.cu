@@ -130,6 +130,19 @@ int Session::create(const std::string &dir, const std::string &options, int dev)
         err = "EXP_DECAY is only available with the SCFDM scheme";
         return ST_OPTIONS;
     }
+    if (m.p.storage != "fp32" && m.p.storage != "fp16") {
+        err = "storage must be \"fp32\" or \"fp16\"";
+        return ST_OPTIONS;
+    }
+    mix_ = m.p.storage == "fp16";
+    if (mix_ && m.p.scheme != SCHEME_CGFDM) {
+        err = "FP16 storage is built for the CGFDM scheme";
+        return ST_OPTIONS;
+    }
+    if (mix_ && m.p.solve_pga) {
+        err = "SOLVE_PGA is not available with FP16 storage";
+        return ST_OPTIONS;
+    }
     if (m.p.scheme == SCHEME_SCFDM && m.g.nz < 8) {
         err = "the SCFDM scheme needs NZ >= 8";
         return ST_OPTIONS;
@@ -189,10 +202,33 @@ int Session::setup_device()
     CU(launch_setup(d_coord, d_med, cjm_, rdz_, g, G.rDH, m.p.scheme, m.p.metric_fp64, stream));
 
     // wavefield buffers: A (step start / final), B, C (stage values), T (RK4 sum)
-    for (int b = 0; b < (cg ? 4 : 3); b++) ALLOC(W_[b], float, F * 9);
+    if (mix_) {
+        // FP16 arrays: first interior column on a 16-byte boundary in the TMA
+        // halo box (xoff 33: column i0 - 4 = 32 + 32 n), rows of 16 bytes
+        gh_ = make_devgrid(G.nx, G.ny, G.nz, 33);
+        gh_.pitch = (gh_.pitch + 7) / 8 * 8;
+        gh_.plane = (long long)gh_.nyp * gh_.pitch;
+        gh_.fstride = ((long long)gh_.nzp * gh_.plane + 63) / 64 * 64;
+        ALLOC(W_[0], float, F * 9);
+        ALLOC(Walt_, float, F * 9);
+        ALLOC(Sb_, __half, gh_.fstride * 9);
+        ALLOC(Sc_, __half, gh_.fstride * 9);
+        ALLOC(T16_, __half, gh_.fstride * 9);
+        ALLOC(mx_, unsigned, 20);   // [2][9] bounds, then the two impedance bounds
+        const unsigned init[2] = {0x7f800000u, 0u};
+        CU(cudaMemcpyAsync(mx_ + 18, init, sizeof init, cudaMemcpyHostToDevice, stream));
+        CU(launch_impedance_bounds(cjm_, g, mx_ + 18, stream));
+        unsigned zb[2];
+        CU(cudaMemcpyAsync(zb, mx_ + 18, sizeof zb, cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        std::memcpy(&zs_min_, &zb[0], 4);
+        std::memcpy(&zp_max_, &zb[1], 4);
+    } else {
+        for (int b = 0; b < (cg ? 4 : 3); b++) ALLOC(W_[b], float, F * 9);
+    }
     ALLOC(err_dev_, int, 1);
     ALLOC(work_dev_, int, 2);
-    if (cg)
+    if (cg && !mix_)
         for (int b = 0; b < 3; b++) {
             CU(make_field_tmap(maps_[b].win, W_[b], g, 9, true));
             CU(make_field_tmap(maps_[b].cjm, cjm_, g, 13, false));
@@ -314,7 +350,7 @@ int Session::setup_device()
     ntx_ = (G.nx + 31) / 32;
     nty_ = (G.ny + cg_stage_tile_y() - 1) / cg_stage_tile_y();
     const long long tiles = (long long)ntx_ * nty_;
-    const int ctas = dev_sms * cg_stage_ctas_per_sm();
+    const int ctas = dev_sms * (mix_ ? cg_stage_mix_ctas_per_sm() : cg_stage_ctas_per_sm());
     nchunk_ = std::max(1, (G.nz + 7) / 8);
     while (tiles * nchunk_ < 4LL * ctas && G.nz / (nchunk_ + 1) >= 12) nchunk_++;
     kchunk_ = (G.nz + nchunk_ - 1) / nchunk_;
@@ -395,8 +431,46 @@ int Session::pml_faces() const
 
 int Session::build_stage_descs()
 {
+    if (mix_) {
+        for (int p = 0; p < 2; p++)
+            for (int irk = 0; irk < 4; irk++) stage_desc_mix(p, irk, desc_mix_[p][irk]);
+        return ST_OK;
+    }
     for (int irk = 0; irk < 4; irk++) stage_desc(irk, desc_host_[irk]);
     return ST_OK;
+}
+
+// Mixed storage: stage irk of a step of the given parity.  The state A is
+// read (with the delta of the previous stage as stencil input) and, in
+// stage 3, the next state written to the other buffer; deltas go Sb -> Sc -> Sb.
+void Session::stage_desc_mix(int parity, int irk, CgStageDesc &d) const
+{
+    stage_desc(irk, d);   // the common arguments; buffers and maps replaced below
+    CgStageArgs &a = d.a;
+    float *A = parity ? Walt_ : W_[0], *An = parity ? W_[0] : Walt_;
+    a.gh = gh_;
+    a.Win = A;
+    a.Wm = A;
+    a.T = nullptr;
+    a.Wout = irk == 3 ? An : nullptr;
+    a.Sin = irk == 0 ? nullptr : irk == 2 ? Sc_ : Sb_;
+    a.Sout = irk == 0 ? Sb_ : irk == 1 ? Sc_ : irk == 2 ? Sb_ : nullptr;
+    a.T16 = T16_;
+    a.mx = mx_;
+    a.it_dev = it_dev_;
+    a.zs_min = zs_min_, a.zp_max = zp_max_;
+    make_field_tmap(d.tmW, A, g, 9, true);
+    make_field_tmap(d.tmC, cjm_, g, 13, false);
+    make_field_tmap(d.tmM, A, g, 9, false);
+    make_field_tmap16(d.tmT, T16_, gh_, 9);
+    make_field_tmap16(d.tmS, irk == 2 ? Sc_ : Sb_, gh_, 9);
+}
+
+int Session::need_fp32_storage(const char *what)
+{
+    if (!mix_) return ST_OK;
+    err = std::string(what) + " is not available with FP16 storage";
+    return ST_OPTIONS;
 }
 
 // ----------------------------------------------------------------- step
@@ -409,7 +483,10 @@ int Session::launch_step(int step, bool timed_stages)
     if (cg) {
         for (int irk = 0; irk < 4; irk++) {
             if (timed_stages) CU(cudaEventRecord(ev_[2], stream));
-            CU(launch_cg_stage(FB1, FB2, FB3, desc_host_[irk], work_dev_, grid_ctas_, stream));
+            if (mix_)
+                CU(launch_cg_stage_mix(FB1, FB2, FB3, desc_mix_[step & 1][irk], work_dev_, grid_ctas_, stream));
+            else
+                CU(launch_cg_stage(FB1, FB2, FB3, desc_host_[irk], work_dev_, grid_ctas_, stream));
             if (timed_stages) {
                 CU(cudaEventRecord(ev_[3], stream));
                 CU(cudaEventSynchronize(ev_[3]));
@@ -465,6 +542,11 @@ int Session::launch_step(int step, bool timed_stages)
 int Session::launch_sources_on(cudaStream_t st)
 {
     const float DT = (float)m.p.DT;
+    if (mix_) {
+        CU(launch_point(W_[0], nullptr, nullptr, cjm_, g, point_, it_dev_, DT, m.g.DH, m.p.scheme, st, Walt_, mx_));
+        CU(launch_sources(W_[0], cjm_, g, fault_, point_, it_dev_, DT, m.g.DH, m.p.scheme, st, Walt_, mx_));
+        return ST_OK;
+    }
     CU(launch_point(W_[0], W_[1], W_[2], cjm_, g, point_, it_dev_, DT, m.g.DH, m.p.scheme, st));
     CU(launch_sources(W_[0], cjm_, g, fault_, point_, it_dev_, DT, m.g.DH, m.p.scheme, st));
     return ST_OK;
@@ -482,7 +564,7 @@ int Session::launch_pga_on(cudaStream_t st)
 // Station traces of the step just completed; advances *it_dev_.
 int Session::launch_stations_on(cudaStream_t st)
 {
-    CU(launch_stations(W_[0], cjm_, g, st_idx_, nst, m.NT, st_out_, it_dev_, m.p.scheme, st));
+    CU(launch_stations(W_[0], cjm_, g, st_idx_, nst, m.NT, st_out_, it_dev_, m.p.scheme, st, mix_ ? Walt_ : nullptr));
     return ST_OK;
 }
 
@@ -652,6 +734,15 @@ double Session::algo_bytes_per_step() const
     // SCFDM: W_n + 13 metric/medium fields -> W1 (31 fields), then two stages
     // reading the stage value, the metric and W_n and writing W (40 each)
     if (m.p.scheme == SCHEME_SCFDM) return 4.0 * 111.0 * n;
+    // FP16 storage: 4-byte state and metric fields, 2-byte deltas; stage 0
+    // reads A and 12 metric fields and writes the delta (84 + 18 B), stage 1
+    // adds the delta in and writes the accumulator and the next delta (102 +
+    // 36), stages 2-3 also read the accumulator (120 + 36); stage 3 writes
+    // the 4-byte state (120 + 36): 552 B per point and step
+    if (mix_) {
+        if (m.p.pml) faces = (double)G.nPML * (2.0 * G.ny * G.nz + 2.0 * G.nx * G.nz + (double)G.nx * G.ny);
+        return 552.0 * n + 4.0 * 144.0 * faces;
+    }
     if (m.p.pml && m.p.scheme == SCHEME_CGFDM)
         faces = (double)G.nPML * (2.0 * G.ny * G.nz + 2.0 * G.nx * G.nz + (double)G.nx * G.ny);
     return 4.0 * (192.0 * n + 144.0 * faces);
@@ -665,7 +756,7 @@ int Session::get_wavefield(float *host) const
     float *d = nullptr;
     long long npad = m.g.npad();
     if (cudaMalloc(&d, sizeof(float) * npad * 9) != cudaSuccess) return ST_ALLOC;
-    cudaError_t e = launch_to_aos(W_[0], 9, g, d, stream);
+    cudaError_t e = launch_to_aos(state(), 9, g, d, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(host, d, sizeof(float) * npad * 9, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     cudaFree(d);
@@ -784,12 +875,12 @@ int Session::write_snapshots(int step)
     for (int c = 0; c < 3; c++)
         for (int axis = 0; axis < 3; axis++)
             if (idx[axis] >= HALO && idx[axis] < lim[axis]) {
-                int st = one(W_[0], m.p.scheme, axis, idx[axis], c, std::string(comp_name[c]) + "_" + s);
+                int st = one(state(), m.p.scheme, axis, idx[axis], c, std::string(comp_name[c]) + "_" + s);
                 if (st) return st;
             }
     if (m.p.sliceFreeSurf) {
         for (int c = 0; c < 3; c++) {
-            int st = one(W_[0], m.p.scheme, 2, G._nz - 1, c, std::string("FreeSurf") + comp_name[c] + "_" + s);
+            int st = one(state(), m.p.scheme, 2, G._nz - 1, c, std::string("FreeSurf") + comp_name[c] + "_" + s);
             if (st) return st;
         }
         if (dis_) {
@@ -932,6 +1023,7 @@ size_t Session::checkpoint_bytes() const
 
 int Session::checkpoint(void *host, size_t bytes)
 {
+    if (int st = need_fp32_storage("checkpoint")) return st;
     if (bytes < checkpoint_bytes()) {
         err = "checkpoint buffer too small";
         return ST_ARG;
@@ -954,6 +1046,7 @@ int Session::checkpoint(void *host, size_t bytes)
 
 int Session::restore(const void *host, size_t bytes)
 {
+    if (int st = need_fp32_storage("restore")) return st;
     std::vector<std::pair<void *, size_t>> parts;
     ckpt_parts(parts);
     const long long *h = (const long long *)host;

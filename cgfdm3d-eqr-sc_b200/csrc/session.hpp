@@ -144,11 +144,27 @@ private:
     int check_device_error();
     template <class R>
     int run_precise_t(int nsteps, double *stations, double *pgv, double *wavefield);
+    // mixed-precision storage ("storage": "fp16", CGFDM; see CgStageArgs):
+    // step states W_[0] / Walt_ by step parity, stage deltas Sb_ / Sc_ and
+    // the accumulator delta T16_ in the FP16 layout gh_, bounds mx_[2][9]
+    bool mix_ = false;
+    float *Walt_ = nullptr;
+    __half *Sb_ = nullptr, *Sc_ = nullptr, *T16_ = nullptr;
+    unsigned *mx_ = nullptr;
+    DevGrid gh_{};
+    float zs_min_ = 0, zp_max_ = 0;
+    CgStageDesc desc_mix_[2][4] = {};
+    void stage_desc_mix(int parity, int irk, CgStageDesc &d) const;
     int *stall_dev_ = nullptr;                       // test hook of the stage kernel's bounded waits
     int stall_item_ = -1, stall_fill_ = 0;
     long long wait_limit_ = 0;
 
 public:
+    // The wavefield at the current step boundary (mixed storage alternates two buffers).
+    float *state() const { return mix_ && (it & 1) ? Walt_ : W_[0]; }
+    bool mixed() const { return mix_; }
+    // ST_OPTIONS with a message when the session stores FP16 deltas
+    int need_fp32_storage(const char *what);
     // Test hook: the next stage launch's work item `item` leaves its plane
     // copy number `fill` unissued, once, and every bounded wait of the stage
     // kernel gives up after `wait_cycles` clocks (0: the default limit).

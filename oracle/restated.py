@@ -29,7 +29,7 @@ BUILD = os.path.join(HERE, "build")
 
 
 def binary(precision: str = "f32") -> str:
-    """f32, f64, or s11 / s8 (FP32 with the stored state rounded to 11 / 8 significand bits)."""
+    """f32, f64, or m16 (FP32 arithmetic with the mixed-precision storage of the CGFDM path)."""
     return os.path.join(BUILD, f"stepper_{precision}")
 
 

@@ -477,50 +477,110 @@ static void cg_deriv(int FB1, int FB2, int FB3)
 
 /* RK4 of the wavefield over every point (src/wave_rk.cpp:17-104; halo
  * points have a zero RHS) and of the PML auxiliaries (src/pml_rk.cpp:18-73) */
-/* Storage-precision experiment (STORE_MANT_BITS, see Makefile): every
- * value written to the stored state (wavefield, RK sum, step start, PML
- * auxiliaries) is rounded to that many significand bits (11 = FP16, 8 =
- * BF16), with the float exponent range kept: 16-bit storage with ideal
- * per-field scaling.  Off by default. */
-#ifndef STORE_MANT_BITS
-#define STORE_MANT_BITS 0
-#endif
-static real store(real x)
+/* Mixed-precision storage (MIX16, REAL = float): the oracle of the
+ * library's "storage": "fp16" CGFDM path.  The step-start state m stays
+ * FP32; each stage's delta from it (d1 = a2 h0, d2 = a3 h1, d3 = h2) and the
+ * RK accumulator's delta (t - m) are stored as FP16 values times a per-field
+ * power-of-two scale, and the next stage's stencil input is m + d as
+ * reconstructed from the stored value.  The accumulator after stage 0 is
+ * b1 h0 = d1 / 3, formed from the stored d1 in stage 1.  The scale of field
+ * f makes the bound M_f of its values at the step start map below 2^13:
+ * M_f = max(max |m_f|, coupled) over the interior, where the coupled bound
+ * is the stress maximum over the smallest S impedance for a velocity field
+ * and the velocity maximum times the largest P impedance for a stress
+ * field (a stage's delta can be non-zero where m_f still is, e.g. velocity
+ * next to a stress source at step 0).  The PML auxiliaries stay FP32. */
+#ifdef MIX16
+static float *S16, *T16;            /* stored deltas, as the values they stand for */
+static float mscale[9], minv[9];
+static float Zs_min, Zp_max;        /* impedance bounds of the medium */
+static double Mpre[9];              /* max |m_f| before the step's source term */
+
+static float q16(float x, int f)
 {
-#if STORE_MANT_BITS > 0
-    float f = (float)x;
-    uint32_t u;
-    memcpy(&u, &f, 4);
-    const int drop = 24 - STORE_MANT_BITS;
-    const uint32_t half = 1u << (drop - 1), mask = (1u << drop) - 1;
-    const uint32_t lsb = (u >> drop) & 1u;
-    u = (u + half - 1 + lsb) & ~mask; /* round to nearest, ties to even */
-    memcpy(&f, &u, 4);
-    return (real)f;
-#else
-    return x;
-#endif
+    float y = x * mscale[f];
+    if (y > 65504.0f) y = 65504.0f;
+    if (y < -65504.0f) y = -65504.0f;
+    return (float)(_Float16)y * minv[f];
 }
+
+static void interior_max(double *M)
+{
+    for (int f = 0; f < 9; f++) M[f] = 0.0;
+    for (int k = HALO; k < nzp - HALO; k++)
+        for (int j = HALO; j < nyp - HALO; j++)
+            for (int i = HALO; i < nxp - HALO; i++)
+                for (int f = 0; f < 9; f++) {
+                    const double a = fabs((double)W[IDX(i, j, k) * 9 + f]);
+                    if (a > M[f]) M[f] = a;
+                }
+}
+
+static void mix_setup(void)
+{
+    Zs_min = 3.4e38f, Zp_max = 0.0f;
+    for (int k = HALO; k < nzp - HALO; k++)
+        for (int j = HALO; j < nyp - HALO; j++)
+            for (int i = HALO; i < nxp - HALO; i++) {
+                const long long q = IDX(i, j, k);
+                const float mu = CJM[q * ncjm + 10], lam = CJM[q * ncjm + 11], b = CJM[q * ncjm + 12];
+                const float zs = sqrtf(mu / b), zp = sqrtf((lam + 2.0f * mu) / b);
+                if (zs < Zs_min) Zs_min = zs;
+                if (zp > Zp_max) Zp_max = zp;
+            }
+    S16 = calloc(np_pad * 9, sizeof(float));
+    T16 = calloc(np_pad * 9, sizeof(float));
+}
+
+/* after the source term of a step: the scales of that step */
+static void mix_scales(void)
+{
+    double Mpost[9];
+    interior_max(Mpost);
+    float M[9], Mv = 0.0f, Ms = 0.0f;
+    for (int f = 0; f < 9; f++) {
+        M[f] = (float)(Mpre[f] > Mpost[f] ? Mpre[f] : Mpost[f]);
+        if (f < 3 && M[f] > Mv) Mv = M[f];
+        if (f >= 3 && M[f] > Ms) Ms = M[f];
+    }
+    for (int f = 0; f < 9; f++) {
+        const float c = f < 3 ? Ms / Zs_min : Mv * Zp_max;
+        const float b = M[f] > c ? M[f] : c;
+        int e = 0;
+        if (b > 0.0f) frexpf(b, &e);      /* 2^(e-1) <= b < 2^e */
+        mscale[f] = b > 0.0f ? ldexpf(1.0f, 13 - e) : 1.0f;
+        minv[f] = b > 0.0f ? ldexpf(1.0f, e - 13) : 1.0f;
+    }
+}
+#endif
 
 static void rk4(int irk)
 {
     const float b1 = 0.16666667f, b2 = 0.33333333f, b3 = 0.33333333f, b4 = 0.16666667f, a2 = 0.5f, a3 = 0.5f;
     for (long long n = 0; n < np_pad * 9; n++) {
         real h = Wh[n];
-        if (irk == 0) Wm[n] = W[n], Wt[n] = store(Wm[n] + b1 * h), W[n] = store(Wm[n] + a2 * h);
-        else if (irk == 1) Wt[n] = store(Wt[n] + b2 * h), W[n] = store(Wm[n] + a3 * h);
-        else if (irk == 2) Wt[n] = store(Wt[n] + b3 * h), W[n] = store(Wm[n] + h);
-        else W[n] = store(Wt[n] + b4 * h);
+#ifdef MIX16
+        const int f = (int)(n % 9);
+        if (irk == 0) Wm[n] = W[n], S16[n] = q16(a2 * h, f), W[n] = Wm[n] + S16[n];
+        else if (irk == 1) T16[n] = q16(S16[n] * 0.33333334f + b2 * h, f), S16[n] = q16(a3 * h, f), W[n] = Wm[n] + S16[n];
+        else if (irk == 2) T16[n] = q16(T16[n] + b3 * h, f), S16[n] = q16(h, f), W[n] = Wm[n] + S16[n];
+        else W[n] = Wm[n] + (T16[n] + b4 * h);
+#else
+        if (irk == 0) Wm[n] = W[n], Wt[n] = Wm[n] + b1 * h, W[n] = Wm[n] + a2 * h;
+        else if (irk == 1) Wt[n] = Wt[n] + b2 * h, W[n] = Wm[n] + a3 * h;
+        else if (irk == 2) Wt[n] = Wt[n] + b3 * h, W[n] = Wm[n] + h;
+        else W[n] = Wt[n] + b4 * h;
+#endif
     }
     if (pml_on)
         for (int fc = 0; fc < 5; fc++) {
             Face *F = &FACE[fc];
             for (long long n = 0; n < F->n * 9; n++) {
                 real h = F->h[n];
-                if (irk == 0) F->m[n] = F->A[n], F->t[n] = store(F->m[n] + b1 * h), F->A[n] = store(F->m[n] + a2 * h);
-                else if (irk == 1) F->t[n] = store(F->t[n] + b2 * h), F->A[n] = store(F->m[n] + a3 * h);
-                else if (irk == 2) F->t[n] = store(F->t[n] + b3 * h), F->A[n] = store(F->m[n] + h);
-                else F->A[n] = store(F->t[n] + b4 * h);
+                if (irk == 0) F->m[n] = F->A[n], F->t[n] = F->m[n] + b1 * h, F->A[n] = F->m[n] + a2 * h;
+                else if (irk == 1) F->t[n] = F->t[n] + b2 * h, F->A[n] = F->m[n] + a3 * h;
+                else if (irk == 2) F->t[n] = F->t[n] + b3 * h, F->A[n] = F->m[n] + h;
+                else F->A[n] = F->t[n] + b4 * h;
             }
         }
 }
@@ -626,9 +686,9 @@ static void tvd(int irk)
 {
     for (long long n = 0; n < np_pad * 9; n++) {
         real h = Wh[n];
-        if (irk == 0) Wm[n] = W[n], W[n] = store(Wm[n] + h);
-        else if (irk == 1) W[n] = store((real)(0.75 * Wm[n] + 0.25 * W[n] + 0.25 * h));
-        else W[n] = store((real)((1.0 / 3.0) * Wm[n] + (2.0 / 3.0) * W[n] + (2.0 / 3.0) * h));
+        if (irk == 0) Wm[n] = W[n], W[n] = Wm[n] + h;
+        else if (irk == 1) W[n] = (real)(0.75 * Wm[n] + 0.25 * W[n] + 0.25 * h);
+        else W[n] = (real)((1.0 / 3.0) * Wm[n] + (2.0 / 3.0) * W[n] + (2.0 / 3.0) * h);
     }
 }
 
@@ -904,9 +964,19 @@ int main(int argc, char **argv)
     }
     static const int FBT[8][3] = {{-1, -1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, -1, 1},
                                   {-1, 1, -1},  {1, -1, -1}, {1, -1, 1}, {-1, 1, 1}}; /* src/propagate.cpp:158-168 */
+#ifdef MIX16
+    if (scheme != 0) die("MIX16 covers the CGFDM scheme", NULL);
+    mix_setup();
+#endif
     for (int it = 0; it < NT; it++) {
+#ifdef MIX16
+        interior_max(Mpre);
+#endif
         if (src_kind == 1 || src_kind == 2) point_inject(it);
         if (src_kind == 3) fault_inject(it);
+#ifdef MIX16
+        mix_scales();
+#endif
         if (scheme == 0) {
             int FB1 = FBT[it % 8][0], FB2 = FBT[it % 8][1], FB3 = FBT[it % 8][2];
             for (int irk = 0; irk < 4; irk++) {
