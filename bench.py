@@ -617,6 +617,8 @@ def main():
     ap.add_argument("--full-steps", type=int, default=0,
                     help="with --fp64-check -1: the workload's full length (default: 3000 for terrain_fault, "
                          "4000 for aweno_basin, 1000 for halfspace)")
+    ap.add_argument("--kchunk", type=int, default=0,
+                    help="CGFDM: z planes per work item of the stage kernel (0: the session's default)")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
                     help="wavefield storage of the CGFDM session: FP32, or FP16 stage and accumulator deltas "
                          "from the FP32 step state (mixed precision)")
@@ -674,6 +676,9 @@ def main():
 
     # ---- device-timed leg: inputs resident on the GPU
     s = Session(d, options=session_options(args), device=local_rank)
+    if args.kchunk:
+        s.set_tiling(args.kchunk, s.tiling()[1])
+    tiling = s.tiling() if not is_scfdm(args.workload) else None
     info = s.info
     pts = info.nx * info.ny * info.nz
     s.run(args.warmup)
@@ -696,9 +701,12 @@ def main():
     # ---- end-to-end leg: run directory on disk -> C ABI -> stations on the host
     t0 = time.perf_counter()
     s2 = Session(d, options=session_options(args), device=local_rank)
+    if args.kchunk:
+        s2.set_tiling(args.kchunk, s2.tiling()[1])
     s2.run(args.steps)
     st = s2.stations()
     i2 = s2.info
+    create_prof = s2.create_profile()
     s2.close()
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{local_rank}")
@@ -716,6 +724,7 @@ def main():
                     "fp16 stage/accumulator deltas (per-field scales) + fp32 step state; f32 arithmetic"),
         "scheme": "SCFDM" if sc else "CGFDM",
         "config": {"workload": workload_desc(args.workload), "points": pts, "DT": info.DT,
+                   "stage_tiling": ({"tile": "32x4", "kchunk": tiling[0], "ctas": tiling[1]} if tiling else None),
                    "l2": "inputs larger than L2 (model + wavefield %.1f GB resident)" % (info.device_bytes / 1e9),
                    "parallelism": f"replicas x{world}"},
         "hbm_gbs_algorithmic": algo_step * args.steps / (ms_max * 1e-3) / 1e9,
@@ -736,7 +745,8 @@ def main():
                       "algo_bytes_per_launch": algo_launch, "mean_launch_ms": stage_ms}),
         "e2e": {"value": world * pts * args.steps / e2e_s / 1e6, "unit": METRIC,
                 "h2d_bytes_per_step": i2.h2d_bytes / args.steps, "d2h_bytes_per_step": st.nbytes / args.steps,
-                "seconds": e2e_s, "path": "cgfdm_create(run dir) + cgfdm_run(K) + cgfdm_get_stations + destroy"},
+                "seconds": e2e_s, "path": "cgfdm_create(run dir) + cgfdm_run(K) + cgfdm_get_stations + destroy",
+                "split_ms": create_prof},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }

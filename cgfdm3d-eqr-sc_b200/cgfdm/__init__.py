@@ -300,6 +300,14 @@ class Session:
                                              p(W), W.size if W is not None else 0))
         return st, pgv, W
 
+    def create_profile(self) -> dict:
+        """Host wall ms of the set-up (cgfdm_create_profile)."""
+        ms = (ctypes.c_double * 4)()
+        self.L.cgfdm_create_profile.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        self._check(self.L.cgfdm_create_profile(self._h, ms))
+        return {"model_from_files_ms": ms[0], "device_setup_ms": ms[1], "create_ms": ms[2],
+                "graph_capture_ms": ms[3]}
+
     def test_stall(self, item: int, fill: int, wait_cycles: int) -> None:
         """Test hook (cgfdm_test_stall): the next stage launch's work item
         ``item`` leaves plane copy ``fill`` unissued, once, and the stage

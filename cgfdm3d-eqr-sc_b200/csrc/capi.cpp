@@ -238,6 +238,14 @@ int cgfdm_info_get(const cgfdm_session *s, cgfdm_info *o)
     return CGFDM_OK;
 }
 
+int cgfdm_create_profile(const cgfdm_session *s, double *ms)
+{
+    if (!s || !ms) return CGFDM_E_ARG;
+    for (int i = 0; i < 3; i++) ms[i] = s->s.create_ms[i];
+    ms[3] = s->s.capture_ms;
+    return CGFDM_OK;
+}
+
 int cgfdm_profile_stages(cgfdm_session *s, int nsteps, float *mean_stage_ms)
 {
     if (!s || !mean_stage_ms || nsteps <= 0) return CGFDM_E_ARG;

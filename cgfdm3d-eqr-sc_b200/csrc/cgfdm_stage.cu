@@ -462,14 +462,19 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         if (CG_PREFETCH_MT && (a.irk == 1 || a.irk == 2)) tma_prefetch_4d(tmM, px0, j0, kk, 0);
         if (CG_PREFETCH_MT && a.irk != 0) tma_prefetch_4d(tmT, px0, j0, kk, 0);
     };
-    // mixed storage: the delta box of plane kk into its FP32 box, in place
+    // mixed storage: the delta box of plane kk into its FP32 box, in place,
+    // two values at a time (both boxes are [field][row][column], PF values a
+    // field, so pair e of one is pair e of the other)
     auto convert = [&](int kk) {
-        float *r32 = ring + slot_of(kk) * SLOT_F;
-        const __half *r16 = ring16 + slot_of(kk) * (9 * PF);
-#pragma unroll 1
-        for (int f = 0; f < 9; f++) {
-            const float inv = s_inv[f];
-            for (int x = tid; x < PF; x += TX * TY) r32[f * PF + x] = r32[f * PF + x] + __half2float(r16[f * PF + x]) * inv;
+        float2 *r32 = reinterpret_cast<float2 *>(ring + slot_of(kk) * SLOT_F);
+        const __half2 *r16 = reinterpret_cast<const __half2 *>(ring16 + slot_of(kk) * (9 * PF));
+        for (int e = tid; e < 9 * PF / 2; e += TX * TY) {
+            const float inv = s_inv[e / (PF / 2)];
+            const float2 d = __half22float2(r16[e]);
+            float2 w = r32[e];
+            w.x = w.x + d.x * inv;
+            w.y = w.y + d.y * inv;
+            r32[e] = w;
         }
     };
 
@@ -488,11 +493,9 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         atomicOr(a.err, 1);
     }
     if constexpr (MIX) {
-        if (a.irk != 0) {
-            __syncthreads();   // every thread's outcome is in s_abort
-            if (!s_abort)
-                for (int kk = kf; kk < kf + 4; kk++) convert(kk);
-        }
+        // (after a failed wait the values are unused: the loop head leaves)
+        if (a.irk != 0)
+            for (int kk = kf; kk < kf + 4; kk++) convert(kk);
     }
 
     const float bx = active ? a.pml_beta_x[i] : 1.0f, by = active ? a.pml_beta_y[j] : 1.0f;
@@ -551,10 +554,9 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         }
         if constexpr (MIX) {
             if (a.irk != 0) {
-                __syncthreads();   // every thread's outcome is in s_abort
-                if (s_abort) continue;
-                convert(kk_new);
+                convert(kk_new);   // unused if a wait failed: the loop head then leaves
                 __syncthreads();
+                if (s_abort) continue;
             }
         }
         if (!okw) continue;

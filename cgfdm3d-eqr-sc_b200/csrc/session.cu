@@ -11,6 +11,7 @@
 #include "session_util.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -113,12 +114,19 @@ void *Session::alloc(size_t bytes)
 }
 
 // --------------------------------------------------------------- create
+static double ms_since(std::chrono::steady_clock::time_point t0)
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
 int Session::create(const std::string &dir, const std::string &options, int dev)
 {
+    const auto t0 = std::chrono::steady_clock::now();
     run_dir = dir;
     device = dev;
     int st = build_model(dir, options, m, err);
     if (st) return st;
+    create_ms[0] = ms_since(t0);
     // the reference builds that exist: CGFDM with PML (Makefile_CGFDM), SCFDM
     // with the exponential sponge (Makefile_SCFDM); exp_decay_absorb.cpp only
     // compiles under SCFDM and the SCFDM flux kernels take no PML terms
@@ -152,7 +160,11 @@ int Session::create(const std::string &dir, const std::string &options, int dev)
     counted_ = true;
     CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     for (auto &e : ev_) CU(cudaEventCreate(&e));
-    return setup_device();
+    const auto t1 = std::chrono::steady_clock::now();
+    st = setup_device();
+    create_ms[1] = ms_since(t1);
+    create_ms[2] = ms_since(t0);
+    return st;
 }
 
 int Session::setup_device()
@@ -571,6 +583,7 @@ int Session::launch_stations_on(cudaStream_t st)
 int Session::launch_steps_graph(int n8)
 {
     if (!graph8_) {
+        const auto t0 = std::chrono::steady_clock::now();
         CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         long long kl = kernel_launches;
         int st = ST_OK;
@@ -582,6 +595,7 @@ int Session::launch_steps_graph(int n8)
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
         graph8_src_ = gsrc;
         CU(cudaGraphInstantiate(&graph8_, graph8_src_, 0));
+        capture_ms += ms_since(t0);
     }
     const int stage_launches = m.p.scheme == SCHEME_CGFDM ? 4 : 10;
     long long per8 = 8LL * (stage_launches + 1 + (fault_.npts > 0) + (point_.kind != 0 && point_.inside));

@@ -108,6 +108,10 @@ public:
     long long graph_launches = 0, kernel_launches = 0;
     size_t device_bytes = 0;
     double h2d_bytes = 0;
+    // host wall ms of cgfdm_create: model from the run directory (files,
+    // host arithmetic), device set-up (allocation, uploads, set-up kernels),
+    // whole create; and of capturing the eight-step CUDA graph
+    double create_ms[3] = {0, 0, 0}, capture_ms = 0;
 
 private:
     int cuda_fail(cudaError_t e, const char *what);

@@ -318,6 +318,13 @@ const char *cgfdm_last_error(const cgfdm_session *s);
 int cgfdm_run_precise(cgfdm_session *s, int nsteps, int bits, double *stations, long long n_stations,
                       double *pgv, long long n_pgv, double *wavefield, long long n_wavefield);
 
+/* Host wall milliseconds of the session's set-up: ms[0] the model from the
+ * run directory (file reads and host arithmetic, src/run.cpp:28-116's part
+ * before the time loop), ms[1] the device set-up (allocation, uploads,
+ * metric and CFL kernels), ms[2] all of cgfdm_create, ms[3] the capture of
+ * the eight-step CUDA graph (made by the first cgfdm_run of 8 or more steps). */
+int cgfdm_create_profile(const cgfdm_session *s, double ms[4]);
+
 /* Test hook of the stage kernel's bounded waits.  No counterpart in the
  * reference, whose CHECK macro prints a CUDA error and carries on
  * (src/macro.h:94-103): here every wait of the CGFDM stage kernel for its
