@@ -579,7 +579,12 @@ FULL_STEPS = {"terrain_fault": 3000, "aweno_basin": 4000, "halfspace": 1000}
 
 
 def session_options(args):
-    return None if args.storage == "fp32" else json.dumps({"storage": args.storage})
+    o = {}
+    if args.storage != "fp32":
+        o["storage"] = args.storage
+    if args.pipeline != "split":
+        o["stagePipeline"] = args.pipeline
+    return json.dumps(o) if o else None
 
 
 def bench_fp64_check(args, local_rank):
@@ -617,6 +622,9 @@ def main():
     ap.add_argument("--full-steps", type=int, default=0,
                     help="with --fp64-check -1: the workload's full length (default: 3000 for terrain_fault, "
                          "4000 for aweno_basin, 1000 for halfspace)")
+    ap.add_argument("--pipeline", default="split", choices=["ring", "split"],
+                    help="CGFDM FP32 stage kernel: the current plane's halo box with interior column boxes for the "
+                         "z window (default), or six full halo planes in a ring")
     ap.add_argument("--kchunk", type=int, default=0,
                     help="CGFDM: z planes per work item of the stage kernel (0: the session's default)")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
@@ -724,7 +732,9 @@ def main():
                     "fp16 stage/accumulator deltas (per-field scales) + fp32 step state; f32 arithmetic"),
         "scheme": "SCFDM" if sc else "CGFDM",
         "config": {"workload": workload_desc(args.workload), "points": pts, "DT": info.DT,
-                   "stage_tiling": ({"tile": "32x4", "kchunk": tiling[0], "ctas": tiling[1]} if tiling else None),
+                   "stage_tiling": ({"tile": "32x4", "kchunk": tiling[0], "ctas": tiling[1],
+                                     "pipeline": "ring" if args.storage == "fp16" else args.pipeline}
+                                    if tiling else None),
                    "l2": "inputs larger than L2 (model + wavefield %.1f GB resident)" % (info.device_bytes / 1e9),
                    "parallelism": f"replicas x{world}"},
         "hbm_gbs_algorithmic": algo_step * args.steps / (ms_max * 1e-3) / 1e9,

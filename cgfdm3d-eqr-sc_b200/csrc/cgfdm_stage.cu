@@ -65,6 +65,13 @@
 #ifndef CG_STREAM_HINTS
 #define CG_STREAM_HINTS 1
 #endif
+// PML points: their auxiliary values prefetched into L2 before the ring wait
+// (0: none, 1: this plane's, 2: this and the next plane's, 3: the next
+// plane's, the item's first plane in its prologue), so the loads in the PML
+// branch, after the stencil, find them in L2
+#ifndef CG_PML_PREFETCH
+#define CG_PML_PREFETCH 1
+#endif
 // 1: the plane-ring TMA loads carry an L2 evict-last policy
 #ifndef CG_RING_EVICT_LAST
 #define CG_RING_EVICT_LAST 0
@@ -101,6 +108,25 @@ namespace cgfdm {
 #define SLOT_F (9 * PF)  // floats per slot
 #define SLOT_BYTES (SLOT_F * 4)
 #define NSLOT 6
+// split pipeline: the current plane's halo box in a 2-slot ring, the
+// z-window's interior column boxes (32 x TY x 9) in a 6-slot ring, and the
+// point operands (13 metric/medium + 9 step-start + 9 RK-sum fields) of the
+// current plane in one slot
+#define CW (TX * TY)
+#define CSLOT_F (9 * CW)
+#define CSLOT_BYTES (CSLOT_F * 4)
+#ifndef CG_SPLIT_HSLOTS
+#define CG_SPLIT_HSLOTS 2   // halo ring: the current plane and CG_SPLIT_HSLOTS - 1 ahead
+#endif
+#ifndef CG_SPLIT_CSLOTS
+#define CG_SPLIT_CSLOTS 6   // column ring: the 5-plane window and CG_SPLIT_CSLOTS - 5 ahead
+#endif
+#ifndef CG_SPLIT_PTS
+#define CG_SPLIT_PTS 0      // 1: point operands staged by TMA, 0: plain loads as in the ring pipeline (measured 1 % faster)
+#endif
+#define NHSLOT CG_SPLIT_HSLOTS
+#define NCSLOT CG_SPLIT_CSLOTS
+#define PTS_F (CG_SPLIT_PTS ? 31 * CW : 0)
 #define SLOT_HB (9 * PF * 2)  // mixed storage: bytes of a slot's FP16 delta box
 // Mixed storage: the ring also holds each plane's FP16 delta box, so a CTA
 // needs 104 KB and two fit on an SM.
@@ -109,6 +135,7 @@ namespace cgfdm {
 #endif
 
 size_t cg_stage_smem_bytes(bool mix) { return (size_t)NSLOT * (SLOT_BYTES + (mix ? SLOT_HB : 0)) + NSLOT * 8; }
+size_t cg_stage2_smem_bytes() { return (size_t)NHSLOT * SLOT_BYTES + NCSLOT * CSLOT_BYTES + PTS_F * 4 + (NHSLOT + NCSLOT + 1) * 8; }
 
 // ------------------------------------------------------------ TMA helpers
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -166,6 +193,10 @@ __device__ __forceinline__ unsigned long long l2_evict_last_policy()
     asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
     return p;
 }
+__device__ __forceinline__ void l2_prefetch(const void *p)
+{
+    asm volatile("prefetch.global.L2 [%0];\n" ::"l"((unsigned long long)p));
+}
 __device__ __forceinline__ void tma_prefetch_4d(const void *tmap, int x, int y, int z, int f)
 {
     asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];\n" ::"l"(
@@ -174,30 +205,34 @@ __device__ __forceinline__ void tma_prefetch_4d(const void *tmap, int x, int y, 
                  : "memory");
 }
 
-// Stencil taps in the ring: zp[m] points at this thread's cell of plane
-// k + FB3*(m-1); pc = zp[1] is the current plane.
-template <int FB1, int FB2, int FB3>
+// Stencil taps: hc points at this thread's cell of the current plane's halo
+// box (x and y derivatives), zp[m] at its cell of plane k + FB3*(m-1) for the
+// z derivative, ZS floats a field apart (the halo box itself in the ring
+// pipeline, the interior column boxes in the split one).
+template <int FB1, int FB2, int FB3, int ZS = PF>
 struct Taps {
+    const float *hc;
     const float *zp[5];
     __device__ __forceinline__ float rx(int f, float rDH) const
     {
-        const float *c = zp[1] + f * PF;
+        const float *c = hc + f * PF;
         return lop(c[-FB1], c[0], c[FB1], c[2 * FB1], c[3 * FB1], FB1, rDH);
     }
     __device__ __forceinline__ float ry(int f, float rDH) const
     {
-        const float *c = zp[1] + f * PF;
+        const float *c = hc + f * PF;
         return lop(c[-FB2 * BXW], c[0], c[FB2 * BXW], c[2 * FB2 * BXW], c[3 * FB2 * BXW], FB2, rDH);
     }
     __device__ __forceinline__ float rz(int f, float rDH) const
     {
-        return lop(zp[0][f * PF], zp[1][f * PF], zp[2][f * PF], zp[3][f * PF], zp[4][f * PF], FB3, rDH);
+        return lop(zp[0][f * ZS], zp[1][f * ZS], zp[2][f * ZS], zp[3][f * ZS], zp[4][f * ZS], FB3, rDH);
     }
     __device__ __forceinline__ float rdir(int dir, int f, float rDH) const
     {
         return dir == 0 ? rx(f, rDH) : dir == 1 ? ry(f, rDH) : rz(f, rDH);
     }
-    __device__ __forceinline__ float c(int f) const { return zp[1][f * PF]; }
+    __device__ __forceinline__ float c(int f) const { return hc[f * PF]; }
+    __device__ __forceinline__ float z(int m, int f) const { return zp[m][f * ZS]; }
 };
 
 // J * (metric . traction) at a point, for the traction image
@@ -326,16 +361,30 @@ __device__ __forceinline__ __half to_h16(float x, float sc)
 // receives the plane's FP16 delta box; when a plane arrives, the CTA adds the
 // delta into the FP32 box in place, so the taps read the stage's input as in
 // the FP32 kernel.
-template <int FB1, int FB2, int FB3, bool BATCH, bool HOUT, bool MIX = false>
+//
+// V2 = true: the split pipeline (see CSLOT_F above).  Only the current plane
+// needs its x/y halo; the other planes of the z window need only the tile's
+// interior columns, so the shared memory left over holds the current plane's
+// point operands, brought in by TMA during the previous plane instead of
+// being loaded by every thread at the plane's start.
+template <int FB1, int FB2, int FB3, bool BATCH, bool HOUT, bool MIX = false, bool V2 = false>
 __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER_SM)
     k_cg_stage(const __grid_constant__ CgStageDesc d1, const CgStageDesc *__restrict__ descs,
                const int *__restrict__ item_start, int nsess, int *work)
 {
+    static_assert(!(V2 && (BATCH || HOUT || MIX)), "the split pipeline is a single-session FP32 variant");
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    float *ring = reinterpret_cast<float *>(smem_raw);
+    float *ring = reinterpret_cast<float *>(smem_raw);   // V2: the halo ring (2 slots)
     __half *ring16 = reinterpret_cast<__half *>(smem_raw + NSLOT * SLOT_BYTES);
-    unsigned long long *bars =
-        reinterpret_cast<unsigned long long *>(smem_raw + NSLOT * (SLOT_BYTES + (MIX ? SLOT_HB : 0)));
+    float *col = ring + NHSLOT * SLOT_F;                  // V2: column ring
+    float *pts = col + NCSLOT * CSLOT_F;                  // V2: point operands
+    constexpr int NCS = V2 ? NCSLOT : NSLOT;              // column (V2) or ring slots
+    constexpr bool SPTS = V2 && CG_SPLIT_PTS;             // point operands staged in shared memory
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(
+        V2 ? smem_raw + (NHSLOT * SLOT_F + NCSLOT * CSLOT_F + PTS_F) * 4
+           : smem_raw + NSLOT * (SLOT_BYTES + (MIX ? SLOT_HB : 0)));
+    // barrier of column (V2) or ring slot s
+    auto cbar = [&](int s) -> unsigned long long * { return V2 ? &bars[NHSLOT + s] : &bars[s]; };
     __shared__ int s_abort, s_item;
     __shared__ float s_sc[MIX ? 9 : 1], s_inv[MIX ? 9 : 1];
     __shared__ int s_par;
@@ -350,7 +399,7 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
 
     if (tid == 0) {
         s_abort = 0;
-        for (int s = 0; s < NSLOT; s++) mbar_init(smem_u32(&bars[s]), 1);
+        for (int s = 0; s < (V2 ? NHSLOT + NCSLOT + 1 : NSLOT); s++) mbar_init(smem_u32(&bars[s]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         if constexpr (MIX) {
             // per-field scales of this step: the bound of field f maps below 2^13
@@ -377,6 +426,7 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         }
     }
     unsigned seq0 = 0;  // fills issued by this CTA before the current item
+    unsigned hseq0 = 0, pseq0 = 0;   // V2: halo-ring and point-slot fills before the current item
     float rm[MIX ? 9 : 1];   // mixed storage, stage 3: running max |new state| per field
 #pragma unroll
     for (int f = 0; f < (MIX ? 9 : 1); f++) rm[f] = 0.0f;
@@ -407,6 +457,7 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
     const CUtensorMap *tmM = reinterpret_cast<const CUtensorMap *>(D.tmM);
     const CUtensorMap *tmT = reinterpret_cast<const CUtensorMap *>(D.tmT);
     const CUtensorMap *tmS = reinterpret_cast<const CUtensorMap *>(D.tmS);
+    const CUtensorMap *tmWc = reinterpret_cast<const CUtensorMap *>(D.tmWc);
     const DevGrid g = a.g;
     const long long F = g.fstride;
     const int _nx = g.nxp - CGFDM_HALO, _ny = g.nyp - CGFDM_HALO, _nz = g.nzp - CGFDM_HALO;
@@ -428,11 +479,31 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
     const int tx0h = MIX ? a.gh.xoff + i0 - 4 : 0;   // FP16 halo box origin: a multiple of 8 (16 bytes)
 
     // plane kk of this item is fill number seq0 + (kk - kf) of the CTA
-    auto slot_of = [&](int kk) { return (int)((seq0 + (unsigned)(kk - kf)) % NSLOT); };
-    auto parity_of = [&](int kk) { return ((seq0 + (unsigned)(kk - kf)) / NSLOT) & 1u; };
+    auto slot_of = [&](int kk) { return (int)((seq0 + (unsigned)(kk - kf)) % NCS); };
+    auto parity_of = [&](int kk) { return ((seq0 + (unsigned)(kk - kf)) / NCS) & 1u; };
+    // V2: halo box of plane kk (kb <= kk < ke) and point operands of plane kk
+    auto hslot_of = [&](int kk) { return (int)((hseq0 + (unsigned)(kk - kb)) % NHSLOT); };
+    auto hparity_of = [&](int kk) { return ((hseq0 + (unsigned)(kk - kb)) / NHSLOT) & 1u; };
+    auto pparity_of = [&](int kk) { return (pseq0 + (unsigned)(kk - kb)) & 1u; };
+    auto issue_halo = [&](int kk) {
+        const int hs = hslot_of(kk);
+        const unsigned bar = smem_u32(&bars[hs]);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(bar, SLOT_BYTES);
+        tma_load_4d(smem_u32(ring + hs * SLOT_F), tmW, tx0, ty0, kk, 0, bar);
+    };
+    auto issue_pts = [&](int kk) {
+        const unsigned bar = smem_u32(&bars[NHSLOT + NCSLOT]);
+        const bool wm = a.irk == 1 || a.irk == 2, wt = a.irk != 0;
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(bar, (13 + (wm ? 9 : 0) + (wt ? 9 : 0)) * CW * 4);
+        tma_load_4d(smem_u32(pts), tmC, px0, j0, kk, 0, bar);
+        if (wm) tma_load_4d(smem_u32(pts + 13 * CW), tmM, px0, j0, kk, 0, bar);
+        if (wt) tma_load_4d(smem_u32(pts + 22 * CW), tmT, px0, j0, kk, 0, bar);
+    };
     auto issue = [&](int kk) {
         int s = slot_of(kk);
-        unsigned bar = smem_u32(&bars[s]);
+        unsigned bar = smem_u32(cbar(s));
         // test hook: leave this plane's slot without a copy (and without the
         // arrival that would complete its barrier phase), once
         if (a.stall && gitem == a.stall_item && kk - kf == a.stall_fill && atomicExch(a.stall, 0) == 1) return;
@@ -442,6 +513,11 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
             mbar_expect_tx(bar, SLOT_BYTES + (hs ? SLOT_HB : 0));
             tma_load_4d(smem_u32(ring + s * SLOT_F), tmW, tx0, ty0, kk, 0, bar);
             if (hs) tma_load_4d(smem_u32(ring16 + s * (9 * PF)), tmS, tx0h, ty0, kk, 0, bar);
+            return;
+        }
+        if constexpr (V2) {
+            mbar_expect_tx(bar, CSLOT_BYTES);
+            tma_load_4d(smem_u32(col + s * CSLOT_F), tmWc, px0, j0, kk, 0, bar);
             return;
         }
         mbar_expect_tx(bar, SLOT_BYTES);
@@ -481,13 +557,24 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
     const long long wlim = a.wait_limit > 0 ? a.wait_limit : (1LL << 31);
     const int klast = ke - za + 3;          // last plane of the last window
     if (tid == 0) {
-        for (int kk = kf; kk <= min(kf + NSLOT - 1, klast); kk++) issue(kk);
-        for (int kk = kb; kk < min(kb + CG_PREFETCH_DIST, ke); kk++) prefetch_points(kk);
+        for (int kk = kf; kk <= min(kf + NCS - 1, klast); kk++) issue(kk);
+        if constexpr (V2) {
+            for (int kk = kb; kk < min(kb + NHSLOT, ke); kk++) issue_halo(kk);
+            if (SPTS) {
+                issue_pts(kb);
+                for (int kk = kb + 1; kk < min(kb + 3, ke); kk++) prefetch_points(kk);
+            } else {
+                for (int kk = kb; kk < min(kb + CG_PREFETCH_DIST, ke); kk++) prefetch_points(kk);
+            }
+        } else {
+            for (int kk = kb; kk < min(kb + CG_PREFETCH_DIST, ke); kk++) prefetch_points(kk);
+        }
     }
-    int issued = min(kf + NSLOT - 1, klast);  // same value in every thread
+    int issued = min(kf + NCS - 1, klast);  // same value in every thread
+    int hissued = min(kb + NHSLOT - 1, ke - 1), pissued = kb;  // V2
     // the first window: planes kf .. kf+3 (kf+4 is waited for in the loop)
     bool ok = true;
-    for (int kk = kf; kk < kf + 4; kk++) ok = ok && mbar_wait_bounded(smem_u32(&bars[slot_of(kk)]), parity_of(kk), wlim);
+    for (int kk = kf; kk < kf + 4; kk++) ok = ok && mbar_wait_bounded(smem_u32(cbar(slot_of(kk))), parity_of(kk), wlim);
     if (!ok) {
         s_abort = 1;
         atomicOr(a.err, 1);
@@ -506,13 +593,24 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
     for (int k = kb; k < ke; k++) {
         __syncthreads();                    // every thread is done with plane k - za - 1's slot
         if (s_abort) break;
-        // prefetch plane k - za + 5 into the slot plane k - za - 1 has left
-        const int want = k - za + 5;
+        // issue plane k - za - 1 + NCS into the slot plane k - za - 1 has left
+        const int want = k - za - 1 + NCS;
         if (want > issued && want <= klast) {
             if (tid == 0) issue(want);
             issued = want;
         }
-        if (tid == 0) {
+        if constexpr (V2) {
+            // the halo slot plane k - 1 has left takes plane k - 1 + NHSLOT
+            if (k > kb && k - 1 + NHSLOT < ke) {
+                if (tid == 0) issue_halo(k - 1 + NHSLOT);
+                hissued = k - 1 + NHSLOT;
+            }
+            if (SPTS) {
+                if (tid == 0 && k + 3 < ke) prefetch_points(k + 3);
+            } else {
+                if (tid == 0 && k + CG_PREFETCH_DIST < ke) prefetch_points(k + CG_PREFETCH_DIST);
+            }
+        } else if (tid == 0) {
             if (k + CG_PREFETCH_DIST < ke) prefetch_points(k + CG_PREFETCH_DIST);
             if (CG_RING_PREFETCH_DIST > 0 && want + CG_RING_PREFETCH_DIST <= klast)
                 tma_prefetch_4d(tmW, tx0, ty0, want + CG_RING_PREFETCH_DIST, 0);
@@ -522,7 +620,7 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         float xi_x = 0, xi_y = 0, xi_z = 0, et_x = 0, et_y = 0, et_z = 0, zt_x = 0, zt_y = 0, zt_z = 0;
         float mu = 0, lam = 0, buo = 0, bz = 1;
         float mv[9], tv[9];
-        if (active) {
+        if (!SPTS && active) {
             xi_x = CG_LD(a.cjm[C_XI_X * F + q]), xi_y = CG_LD(a.cjm[C_XI_Y * F + q]);
             xi_z = CG_LD(a.cjm[C_XI_Z * F + q]);
             et_x = CG_LD(a.cjm[C_ET_X * F + q]), et_y = CG_LD(a.cjm[C_ET_Y * F + q]);
@@ -546,9 +644,65 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
                     for (int f = 0; f < 9; f++) tv[f] = CG_LD(a.T[f * F + q]);
             }
         }
+        if (CG_PML_PREFETCH && active && (inx1 || iny1 || inx2 || iny2 || ((a.pml_on & 4) && k < CGFDM_HALO + nPML))) {
+            const int i0p = i - CGFDM_HALO, j0p = j - CGFDM_HALO;
+            const bool sel[5] = {inx1, iny1, (a.pml_on & 4) && k < CGFDM_HALO + nPML, inx2, iny2};
+#pragma unroll 1
+            for (int fc = 0; fc < 5; fc++) {
+                if (!sel[fc]) continue;
+                const PmlFace &P = a.face[fc];
+#pragma unroll 1
+                for (int dk = (CG_PML_PREFETCH == 3 && k > kb) ? 1 : 0; dk < (CG_PML_PREFETCH == 1 ? 1 : 2); dk++) {
+                    const int k0p = k + dk - CGFDM_HALO;
+                    if (k0p >= g.nz || (fc == 2 && k0p >= nPML)) break;
+                    long long pos;
+                    if (fc == 0 || fc == 3)
+                        pos = (long long)(i0p - (fc == 3 ? g.nx - nPML : 0)) + (long long)j0p * nPML +
+                              (long long)k0p * nPML * g.ny;
+                    else if (fc == 1 || fc == 4)
+                        pos = (long long)i0p + (long long)(j0p - (fc == 4 ? g.ny - nPML : 0)) * g.nx +
+                              (long long)k0p * g.nx * nPML;
+                    else
+                        pos = (long long)i0p + (long long)j0p * g.nx + (long long)k0p * g.nx * g.ny;
+                    // the buffers this stage reads: A (stage 0), B A T (1, 2), B T (3)
+                    const float *bufs[3] = {a.irk == 0 ? P.A : P.B, a.irk == 1 || a.irk == 2 ? P.A : nullptr,
+                                            a.irk != 0 ? P.T : nullptr};
+                    for (int b = 0; b < 3; b++)
+                        if (bufs[b])
+                            for (int f = 0; f < 9; f++) l2_prefetch(bufs[b] + f * P.count + pos);
+                }
+            }
+        }
         const int kk_new = k - za + 4;
-        const bool okw = mbar_wait_bounded(smem_u32(&bars[slot_of(kk_new)]), parity_of(kk_new), wlim);
-        if (!okw) {
+        bool okw = mbar_wait_bounded(smem_u32(cbar(slot_of(kk_new))), parity_of(kk_new), wlim);
+        if constexpr (V2) {
+            okw = okw && mbar_wait_bounded(smem_u32(&bars[hslot_of(k)]), hparity_of(k), wlim);
+        }
+        if constexpr (SPTS) {
+            okw = okw && mbar_wait_bounded(smem_u32(&bars[NHSLOT + NCSLOT]), pparity_of(k), wlim);
+            if (okw && active) {
+                const int cc = ty * TX + tx;
+                xi_x = pts[C_XI_X * CW + cc], xi_y = pts[C_XI_Y * CW + cc], xi_z = pts[C_XI_Z * CW + cc];
+                et_x = pts[C_ET_X * CW + cc], et_y = pts[C_ET_Y * CW + cc], et_z = pts[C_ET_Z * CW + cc];
+                zt_x = pts[C_ZT_X * CW + cc], zt_y = pts[C_ZT_Y * CW + cc], zt_z = pts[C_ZT_Z * CW + cc];
+                mu = pts[C_MU * CW + cc], lam = pts[C_LAMBDA * CW + cc];
+                buo = pts[C_BUOY * CW + cc] * 1.0f;  // buoyancy *= Crho (= 1)
+                bz = a.pml_beta_z[k];
+                if (a.irk == 1 || a.irk == 2)
+                    for (int f = 0; f < 9; f++) mv[f] = pts[(13 + f) * CW + cc];
+                if (a.irk != 0)
+                    for (int f = 0; f < 9; f++) tv[f] = pts[(22 + f) * CW + cc];
+            }
+            if (!okw) {
+                s_abort = 1;
+                atomicOr(a.err, 1);
+            }
+            __syncthreads();   // the point slot is free
+            if (!s_abort && k + 1 < ke) {
+                if (tid == 0) issue_pts(k + 1);
+                pissued = k + 1;
+            }
+        } else if (!okw) {
             s_abort = 1;
             atomicOr(a.err, 1);
         }
@@ -562,11 +716,12 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         if (!okw) continue;
         if (!active) continue;
 
-        Taps<FB1, FB2, FB3> T;
+        Taps<FB1, FB2, FB3, V2 ? CW : PF> T;
         for (int m = 0; m < 5; m++) {
             int kk = k + FB3 * (m - 1);
-            T.zp[m] = ring + slot_of(kk) * SLOT_F + cell;
+            T.zp[m] = V2 ? col + slot_of(kk) * CSLOT_F + ty * TX + tx : ring + slot_of(kk) * SLOT_F + cell;
         }
+        T.hc = V2 ? ring + hslot_of(k) * SLOT_F + cell : T.zp[1];
         if (a.irk == 0)
             for (int f = 0; f < 9; f++) mv[f] = T.c(f);
 
@@ -625,12 +780,12 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
                 }
             } else if (k == _nz - 2) {
                 // L2: plane k + FB3 is tap m = 2
-                for (int c = 0; c < 3; c++) vzt[c] = ((float)FB3 * (T.zp[2][c * PF] - T.zp[1][c * PF])) * rDH;
+                for (int c = 0; c < 3; c++) vzt[c] = ((float)FB3 * (T.z(2, c) - T.z(1, c))) * rDH;
             } else {
                 // L3: planes k, k + FB3, k + 2 FB3 are taps 1, 2, 3
                 for (int c = 0; c < 3; c++)
-                    vzt[c] = ((float)FB3 * ((CG_CF1 * T.zp[1][c * PF] + CG_CF2 * T.zp[2][c * PF]) +
-                                            CG_CF3 * T.zp[3][c * PF])) *
+                    vzt[c] = ((float)FB3 * ((CG_CF1 * T.z(1, c) + CG_CF2 * T.z(2, c)) +
+                                            CG_CF3 * T.z(3, c))) *
                              rDH;
             }
             float s1[9], s2[9], s3[9];
@@ -805,12 +960,22 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
     __syncthreads();
     if (s_abort) {
         // no copy may still be landing in shared memory when the CTA exits
-        if (tid == 0)
-            for (int kk = max(kf, issued - NSLOT + 1); kk <= issued; kk++)
-                if (!mbar_wait_bounded(smem_u32(&bars[slot_of(kk)]), parity_of(kk), wlim)) atomicOr(a.err, 2);
+        if (tid == 0) {
+            for (int kk = max(kf, issued - NCS + 1); kk <= issued; kk++)
+                if (!mbar_wait_bounded(smem_u32(cbar(slot_of(kk))), parity_of(kk), wlim)) atomicOr(a.err, 2);
+            if constexpr (V2) {
+                for (int kk = max(kb, hissued - NHSLOT + 1); kk <= hissued; kk++)
+                    if (!mbar_wait_bounded(smem_u32(&bars[hslot_of(kk)]), hparity_of(kk), wlim)) atomicOr(a.err, 2);
+            }
+            if constexpr (SPTS) {
+                if (!mbar_wait_bounded(smem_u32(&bars[NHSLOT + NCSLOT]), pparity_of(pissued), wlim)) atomicOr(a.err, 2);
+            }
+        }
         break;
     }
     seq0 += (unsigned)(issued - kf + 1);
+    hseq0 += (unsigned)(ke - kb);
+    pseq0 += (unsigned)(ke - kb);
     }  // work items
 
     if constexpr (MIX) {
@@ -840,38 +1005,45 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
 int cg_stage_ctas_per_sm() { return CG_CTAS_PER_SM; }
 int cg_stage_tile_y() { return TY; }
 
-template <int FB1, int FB2, int FB3, bool BATCH, bool HOUT, bool MIX>
+template <int FB1, int FB2, int FB3, bool BATCH, bool HOUT, bool MIX, bool V2>
 static cudaError_t launch_t(const CgStageDesc &d1, const CgStageDesc *descs, const int *item_start, int nsess,
                             int *work, int ctas, cudaStream_t st)
 {
     // The shared-memory limit is an attribute of the kernel on the current
     // device (and is lost with a device reset), so it is set on every launch:
     // a host-side call of about a microsecond, legal during stream capture.
-    CUDA_TRY(cudaFuncSetAttribute(k_cg_stage<FB1, FB2, FB3, BATCH, HOUT, MIX>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cg_stage_smem_bytes(MIX)));
-    k_cg_stage<FB1, FB2, FB3, BATCH, HOUT, MIX>
-        <<<ctas, dim3(TX, TY, 1), cg_stage_smem_bytes(MIX), st>>>(d1, descs, item_start, nsess, work);
+    const size_t smem = V2 ? cg_stage2_smem_bytes() : cg_stage_smem_bytes(MIX);
+    CUDA_TRY(cudaFuncSetAttribute(k_cg_stage<FB1, FB2, FB3, BATCH, HOUT, MIX, V2>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_cg_stage<FB1, FB2, FB3, BATCH, HOUT, MIX, V2>
+        <<<ctas, dim3(TX, TY, 1), smem, st>>>(d1, descs, item_start, nsess, work);
     return cudaGetLastError();
 }
 
-template <bool BATCH, bool HOUT, bool MIX = false>
+template <bool BATCH, bool HOUT, bool MIX = false, bool V2 = false>
 static cudaError_t launch_b(int FB1, int FB2, int FB3, const CgStageDesc &d1, const CgStageDesc *descs,
                             const int *item_start, int nsess, int *work, int ctas, cudaStream_t st)
 {
     const int key = (FB1 > 0) * 4 + (FB2 > 0) * 2 + (FB3 > 0);
     switch (key) {
-    case 0: return launch_t<-1, -1, -1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
-    case 1: return launch_t<-1, -1, 1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
-    case 2: return launch_t<-1, 1, -1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
-    case 3: return launch_t<-1, 1, 1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
-    case 4: return launch_t<1, -1, -1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
-    case 5: return launch_t<1, -1, 1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
-    case 6: return launch_t<1, 1, -1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
-    default: return launch_t<1, 1, 1, BATCH, HOUT, MIX>(d1, descs, item_start, nsess, work, ctas, st);
+    case 0: return launch_t<-1, -1, -1, BATCH, HOUT, MIX, V2>(d1, descs, item_start, nsess, work, ctas, st);
+    case 1: return launch_t<-1, -1, 1, BATCH, HOUT, MIX, V2>(d1, descs, item_start, nsess, work, ctas, st);
+    case 2: return launch_t<-1, 1, -1, BATCH, HOUT, MIX, V2>(d1, descs, item_start, nsess, work, ctas, st);
+    case 3: return launch_t<-1, 1, 1, BATCH, HOUT, MIX, V2>(d1, descs, item_start, nsess, work, ctas, st);
+    case 4: return launch_t<1, -1, -1, BATCH, HOUT, MIX, V2>(d1, descs, item_start, nsess, work, ctas, st);
+    case 5: return launch_t<1, -1, 1, BATCH, HOUT, MIX, V2>(d1, descs, item_start, nsess, work, ctas, st);
+    case 6: return launch_t<1, 1, -1, BATCH, HOUT, MIX, V2>(d1, descs, item_start, nsess, work, ctas, st);
+    default: return launch_t<1, 1, 1, BATCH, HOUT, MIX, V2>(d1, descs, item_start, nsess, work, ctas, st);
     }
 }
 
 int cg_stage_mix_ctas_per_sm() { return CG_MIX_CTAS_PER_SM; }
+
+cudaError_t launch_cg_stage_split(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int ctas,
+                                  cudaStream_t st)
+{
+    return launch_b<false, false, false, true>(FB1, FB2, FB3, d, nullptr, nullptr, 1, work, ctas, st);
+}
 
 cudaError_t launch_cg_stage_mix(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int ctas, cudaStream_t st)
 {

@@ -107,6 +107,7 @@ struct CgStageArgs {
 // the stencil input with its halo box, and 32x8 point boxes of the metric,
 // the step-start state and the RK accumulator for L2 prefetch.
 struct CgStageMaps {
+    alignas(64) unsigned char winp[128];   // the stencil input, point box (split pipeline)
     alignas(64) unsigned char win[128];
     alignas(64) unsigned char cjm[128];
     alignas(64) unsigned char wm[128];
@@ -118,6 +119,7 @@ struct CgStageMaps {
 struct alignas(64) CgStageDesc {
     unsigned char tmW[128], tmC[128], tmM[128], tmT[128];
     unsigned char tmS[128];   // mixed storage: the FP16 stencil-input delta, halo box
+    unsigned char tmWc[128];  // split pipeline: the stencil input, interior column box
     CgStageArgs a;
 };
 // One session's stage, its descriptor passed as a kernel parameter.
@@ -129,6 +131,11 @@ cudaError_t launch_cg_stage(int FB1, int FB2, int FB3, const CgStageDesc &d, int
 cudaError_t launch_cg_stage_batch(int FB1, int FB2, int FB3, const CgStageDesc *descs, const int *item_start,
                                   int nsess, int *work, int grid_ctas, cudaStream_t st);
 size_t cg_stage_smem_bytes(bool mix = false);
+size_t cg_stage2_smem_bytes();
+// The split pipeline (the current plane's halo box, interior column boxes for
+// the z window, TMA-staged point operands): one session's FP32 stage.
+cudaError_t launch_cg_stage_split(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,
+                                  cudaStream_t st);
 // Mixed-precision storage: one session's stage (the MIX instantiation).
 cudaError_t launch_cg_stage_mix(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,
                                 cudaStream_t st);

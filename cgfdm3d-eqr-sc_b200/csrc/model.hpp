@@ -78,6 +78,7 @@ struct Params {
     int adj_store_max = 0;           // options "adjointStoreSegments": cap on segments kept from the forward (0: memory decides)
     std::string storage = "fp32";    // "storage": "fp32" | "fp16" | "bf16"
     int check_finite = 0;            // "checkFinite": scan the wavefield for NaN/Inf every K steps (0: never)
+    int stage_split = 1;             // "stagePipeline": "split" (default) | "ring" (CGFDM FP32 stage kernel)
     // extension inputs (raw arrays the reference has no reader for)
     std::string terrainFile;         // float32 [_ny_][_nx_] surface height (m)
     std::string mediumFile;          // float32 [_nz_][_ny_][_nx_][3] Vs, Vp, rho

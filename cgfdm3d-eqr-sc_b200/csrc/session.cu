@@ -243,6 +243,7 @@ int Session::setup_device()
     if (cg && !mix_)
         for (int b = 0; b < 3; b++) {
             CU(make_field_tmap(maps_[b].win, W_[b], g, 9, true));
+            CU(make_field_tmap(maps_[b].winp, W_[b], g, 9, false));
             CU(make_field_tmap(maps_[b].cjm, cjm_, g, 13, false));
             CU(make_field_tmap(maps_[b].wm, W_[0], g, 9, false));
             CU(make_field_tmap(maps_[b].t, W_[3], g, 9, false));
@@ -429,6 +430,7 @@ void Session::stage_desc(int irk, CgStageDesc &d) const
     std::memcpy(d.tmC, maps_[win_map[irk]].cjm, 128);
     std::memcpy(d.tmM, maps_[win_map[irk]].wm, 128);
     std::memcpy(d.tmT, maps_[win_map[irk]].t, 128);
+    std::memcpy(d.tmWc, maps_[win_map[irk]].winp, 128);
 }
 
 int Session::stage_items() const { return ntx_ * nty_ * nchunk_; }
@@ -497,6 +499,8 @@ int Session::launch_step(int step, bool timed_stages)
             if (timed_stages) CU(cudaEventRecord(ev_[2], stream));
             if (mix_)
                 CU(launch_cg_stage_mix(FB1, FB2, FB3, desc_mix_[step & 1][irk], work_dev_, grid_ctas_, stream));
+            else if (m.p.stage_split)
+                CU(launch_cg_stage_split(FB1, FB2, FB3, desc_host_[irk], work_dev_, grid_ctas_, stream));
             else
                 CU(launch_cg_stage(FB1, FB2, FB3, desc_host_[irk], work_dev_, grid_ctas_, stream));
             if (timed_stages) {

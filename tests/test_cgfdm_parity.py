@@ -56,8 +56,8 @@ def ref_runs(tmp_path_factory):
     return {name: (d, refrun.read_outputs(d)) for name, d in dirs.items()}
 
 
-def _lib(d, flavor):
-    s = Session(d, flavor=flavor)
+def _lib(d, flavor, options=None):
+    s = Session(d, options=options, flavor=flavor)
     s.run(s.info.NT)
     res = {"stations": s.stations(), "W": s.wavefield(), "CJM": s.cjm(), "PGV": s.pgv(), "info": s.info}
     s.close()
@@ -90,3 +90,16 @@ def test_fast_tolerance(ref_runs, name):
     e_w = pu.rel_l2(lib["W"], ref["W"])
     assert e_st <= TOL_FAST, f"{name}: seismogram rel L2 {e_st:.3e}"
     assert e_w <= TOL_FAST, f"{name}: wavefield rel L2 {e_w:.3e}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_exact_bitwise_ring_pipeline(ref_runs, name):
+    """The ring stage pipeline (six full halo planes; the one batches, linked
+    parts and FP16 storage use) moves the data differently from the default
+    split pipeline and does the same arithmetic: bit-identical too."""
+    d, ref = ref_runs[name]
+    lib = _lib(d, "exact", '{"stagePipeline": "ring"}')
+    np.testing.assert_array_equal(lib["stations"], ref["stations"])
+    np.testing.assert_array_equal(lib["W"], ref["W"])
+    np.testing.assert_array_equal(lib["PGV"], ref["PGV"])
