@@ -37,10 +37,11 @@
 #ifndef ADJ_TY
 #define ADJ_TY 4            // block rows (the block is 32 x ADJ_TY points of one plane)
 #endif
-// minimum resident blocks per SM (a register cap) of each pass: 5 and 5
-// measured 3 % faster than the uncapped 4 and 5
+// minimum resident blocks per SM (a register cap) of each pass: 4 (no
+// spills) and 5; 5 and 5 spilled 156 bytes in the first pass and measured
+// 2 % slower in the adjoint steps; the uncapped 4 and 5, 3 % slower
 #ifndef ADJ_MINB_PRE
-#define ADJ_MINB_PRE 5
+#define ADJ_MINB_PRE 4
 #endif
 #ifndef ADJ_MINB_GATHER
 #define ADJ_MINB_GATHER 5

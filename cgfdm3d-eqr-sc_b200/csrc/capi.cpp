@@ -243,6 +243,8 @@ int cgfdm_create_profile(const cgfdm_session *s, double *ms)
     if (!s || !ms) return CGFDM_E_ARG;
     for (int i = 0; i < 3; i++) ms[i] = s->s.create_ms[i];
     ms[3] = s->s.capture_ms;
+    for (int i = 0; i < 5; i++) ms[4 + i] = s->s.m.phase_ms[i];
+    for (int i = 0; i < 3; i++) ms[9 + i] = s->s.setup_ms[i];
     return CGFDM_OK;
 }
 

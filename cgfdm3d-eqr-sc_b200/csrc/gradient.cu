@@ -109,7 +109,7 @@ int Session::set_medium(const float *host)
         return ST_OPTIONS;
     }
     const long long npad = m.g.npad();
-    std::vector<float> old = m.medium;
+    FieldVec old = m.medium;
     m.medium.assign(host, host + npad * 3);
     float vpmax = 0.0f;
     for (long long n = 0; n < npad; n++) vpmax = std::max(vpmax, m.medium[n * 3 + 1]);
@@ -466,7 +466,10 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
                 d.a.hbox = hb;
                 d.a.vdstore = vdptr(slot, n - n0, irk);
                 const int sgn = (irk & 1) ? -1 : 1;
-                CU(launch_cg_stage(FB[0] * sgn, FB[1] * sgn, FB[2] * sgn, d, work_dev_, grid_ctas_, stream));
+                if (m.p.stage_split)
+                    CU(launch_cg_stage_split(FB[0] * sgn, FB[1] * sgn, FB[2] * sgn, d, work_dev_, grid_ctas_, stream));
+                else
+                    CU(launch_cg_stage(FB[0] * sgn, FB[1] * sgn, FB[2] * sgn, d, work_dev_, grid_ctas_, stream));
             }
             if (first)
                 if (int st = launch_pga_on(stream)) return st;

@@ -6,6 +6,9 @@
 #include "model.hpp"
 
 #include <algorithm>
+#include <fcntl.h>
+#include <unistd.h>
+#include <chrono>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -198,7 +201,7 @@ static void build_coords(Model &m)
     const Grid &g = m.g;
     const float DH = g.DH;
     const int NZ = g.NZ;
-    m.coord.assign((size_t)g.npad() * 3, 0.f);
+    m.coord.resize((size_t)g.npad() * 3);   // every value written below
     m.terrain.assign((size_t)g._nx_ * g._ny_, 0.f);
     par_for(g._nz_, [&](int k) {
         for (int j = 0; j < g._ny_; j++)
@@ -779,15 +782,32 @@ static int build_medium(Model &m, const std::string &run_dir, std::string &err)
 }
 
 // Extension: raw float32 [_nz_][_ny_][_nx_][3] (Vs, Vp, rho) volume.
+// A raw float32 volume, read by the process's cores in plane-sized pieces
+// (pread at independent offsets), each piece landing in the pages that the
+// reading thread first touches.
 static int medium_file(Model &m, const std::string &path, std::string &err)
 {
-    std::ifstream f(path, std::ios::binary);
-    if (!f) {
+    const int fd = open(path.c_str(), O_RDONLY);
+    if (fd < 0) {
         err = "cannot open medium file " + path;
         return ST_IO;
     }
-    f.read((char *)m.medium.data(), (std::streamsize)(m.medium.size() * sizeof(float)));
-    if (!f) {
+    const long long plane_bytes = (long long)m.g._nx_ * m.g._ny_ * 3 * (long long)sizeof(float);
+    std::atomic<bool> short_read(false);
+    par_for(m.g._nz_, [&](int k) {
+        char *dst = (char *)m.medium.data() + (size_t)k * plane_bytes;
+        long long done = 0;
+        while (done < plane_bytes) {
+            const ssize_t r = pread(fd, dst + done, (size_t)(plane_bytes - done), (off_t)(k * plane_bytes + done));
+            if (r <= 0) {
+                short_read = true;
+                return;
+            }
+            done += r;
+        }
+    });
+    close(fd);
+    if (short_read) {
         err = "medium file too short: " + path;
         return ST_IO;
     }
@@ -1231,6 +1251,12 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
             return ST_PML_SIZE;
         }
     }
+    auto tick = std::chrono::steady_clock::now();
+    auto lap = [&](int ph) {
+        const auto now = std::chrono::steady_clock::now();
+        m.phase_ms[ph] = std::chrono::duration<double, std::milli>(now - tick).count();
+        tick = now;
+    };
     build_coords(m);
     if (p.gauss_hill) gauss_hill(m);
     else if (!p.terrainFile.empty()) {
@@ -1241,6 +1267,7 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
             if ((st = srtm_terrain(m, run_dir, err))) return st;
         terrain_z_double(m);
     }
+    lap(0);
     if (p.mediumFile.empty()) {
         if ((st = build_medium(m, run_dir, err))) return st;
     } else {
@@ -1248,12 +1275,16 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
         m.medium.resize((size_t)g.npad() * 3);
         if ((st = medium_file(m, join(run_dir, p.mediumFile), err))) return st;
     }
+    lap(1);
     value_ranges(m);
     build_pml(m);
+    lap(2);
     build_point_source(m);
     if (p.useMultiSource)
         if ((st = build_fault(m, run_dir, err))) return st;
+    lap(3);
     if ((st = read_stations(m, run_dir, err))) return st;
+    lap(4);
     return ST_OK;
 }
 

@@ -6,12 +6,42 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "json.hpp"
 
 namespace cgfdm {
+
+// An allocator whose value-less construct leaves the element uninitialised:
+// resize() of a FieldVec does not write the hundreds of megabytes of a
+// padded volume from one thread; the parallel loops that fill it first touch
+// its pages on the cores that use them.
+template <class T>
+struct DefaultInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = DefaultInitAlloc<U>;
+    };
+    DefaultInitAlloc() = default;
+    template <class U>
+    DefaultInitAlloc(const DefaultInitAlloc<U> &) noexcept {}
+    template <class U>
+    void construct(U *p) noexcept(std::is_nothrow_default_constructible<U>::value)
+    {
+        ::new ((void *)p) U;
+    }
+    template <class U, class... A>
+    void construct(U *p, A &&...args)
+    {
+        ::new ((void *)p) U(std::forward<A>(args)...);
+    }
+};
+using FieldVec = std::vector<float, DefaultInitAlloc<float>>;
+
 
 constexpr int HALO = 3;
 
@@ -127,10 +157,10 @@ struct Model {
     Params p;
     Grid g;
     int NT = 0;
-    std::vector<float> coord;        // [_nz_][_ny_][_nx_][3] (AoS, reference layout)
+    FieldVec coord;                  // [_nz_][_ny_][_nx_][3] (AoS, reference layout)
     std::vector<float> terrain;      // [_ny_][_nx_]
     std::vector<double> lon, lat;    // [_ny_][_nx_] column longitude, latitude (SRTM90 runs)
-    std::vector<float> medium;       // [_nz_][_ny_][_nx_][3] Vs Vp rho
+    FieldVec medium;                 // [_nz_][_ny_][_nx_][3] Vs Vp rho
     float H_min = 0, H_max = 0, Vs_min = 0, Vs_max = 0, Vp_min = 0, Vp_max = 0, rho_min = 0, rho_max = 0;
     float dtmax = 0;
     // PML profiles (src/init_pml_para.cpp:97-239): alpha, d/beta, 1/beta per axis
@@ -149,6 +179,9 @@ struct Model {
     int part_lo[3] = {0, 0, 0};
     int parts[3] = {1, 1, 1};
     int part_coord[3] = {0, 0, 0};
+    // host wall ms of build_model's phases: coordinates and terrain, medium,
+    // ranges and PML profiles, sources, stations
+    double phase_ms[5] = {0, 0, 0, 0, 0};
     bool fs_top = true;
     std::vector<int> station_ids;
 };

@@ -176,6 +176,7 @@ int Session::setup_device()
     const bool cg = m.p.scheme == SCHEME_CGFDM;
 
     // model arrays -> GPU, metrics on the GPU
+    const auto t0 = std::chrono::steady_clock::now();
     float *d_coord, *d_med;
     ALLOC(d_coord, float, npad * 3);
     ALLOC(d_med, float, npad * 3);
@@ -211,6 +212,7 @@ int Session::setup_device()
             return ST_CFL;
         }
     }
+    setup_ms[0] = ms_since(t0);   // allocation, uploads, CFL check (synchronised)
     CU(launch_setup(d_coord, d_med, cjm_, rdz_, g, G.rDH, m.p.scheme, m.p.metric_fp64, stream));
 
     // wavefield buffers: A (step start / final), B, C (stage values), T (RK4 sum)
@@ -375,7 +377,9 @@ int Session::setup_device()
         if (st) return st;
     }
 
+    setup_ms[1] = ms_since(t0) - setup_ms[0];   // state buffers, tables, descriptors (enqueued)
     CU(cudaStreamSynchronize(stream));
+    setup_ms[2] = ms_since(t0) - setup_ms[0] - setup_ms[1];   // the set-up kernels and copies finishing
     // coordinates and medium are not needed on the device any more
     for (auto it_ = allocs_.begin(); it_ != allocs_.end();) {
         if (*it_ == d_coord || *it_ == d_med) {
@@ -924,7 +928,7 @@ static int write_model_slices(const Model &m, const std::string &out)
     const int lim[3] = {G._nx, G._ny, G._nz};
     const char *names[6] = {"coordX", "coordY", "coordZ", "Vs", "Vp", "rho"};
     for (int v = 0; v < 6; v++) {
-        const std::vector<float> &src = v < 3 ? m.coord : m.medium;
+        const FieldVec &src = v < 3 ? m.coord : m.medium;
         if (src.empty()) continue;
         for (int axis = 0; axis < 3; axis++) {
             if (!(idx[axis] >= HALO && idx[axis] < lim[axis])) continue;

@@ -322,8 +322,11 @@ int cgfdm_run_precise(cgfdm_session *s, int nsteps, int bits, double *stations, 
  * run directory (file reads and host arithmetic, src/run.cpp:28-116's part
  * before the time loop), ms[1] the device set-up (allocation, uploads,
  * metric and CFL kernels), ms[2] all of cgfdm_create, ms[3] the capture of
- * the eight-step CUDA graph (made by the first cgfdm_run of 8 or more steps). */
-int cgfdm_create_profile(const cgfdm_session *s, double ms[4]);
+ * the eight-step CUDA graph (made by the first cgfdm_run of 8 or more steps),
+ * ms[4..8] the parts of ms[0]: coordinates and terrain, medium, value ranges
+ * and PML profiles, sources, stations; ms[9..11] the parts of ms[1]:
+ * allocation, uploads and the CFL check, the rest enqueued, its completion. */
+int cgfdm_create_profile(const cgfdm_session *s, double ms[12]);
 
 /* Test hook of the stage kernel's bounded waits.  No counterpart in the
  * reference, whose CHECK macro prints a CUDA error and carries on
