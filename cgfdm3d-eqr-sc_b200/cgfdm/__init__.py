@@ -302,14 +302,15 @@ class Session:
 
     def create_profile(self) -> dict:
         """Host wall ms of the set-up (cgfdm_create_profile)."""
-        ms = (ctypes.c_double * 12)()
+        ms = (ctypes.c_double * 14)()
         self.L.cgfdm_create_profile.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
         self._check(self.L.cgfdm_create_profile(self._h, ms))
         return {"model_from_files_ms": ms[0], "device_setup_ms": ms[1], "create_ms": ms[2],
                 "graph_capture_ms": ms[3],
                 "model_parts_ms": {"coordinates_terrain": ms[4], "medium": ms[5], "ranges_pml": ms[6],
                                    "sources": ms[7], "stations": ms[8]},
-                "device_setup_parts_ms": {"alloc_upload_cfl": ms[9], "enqueue_rest": ms[10], "complete": ms[11]}}
+                "device_setup_parts_ms": {"alloc_upload_cfl": ms[9], "enqueue_rest": ms[10], "complete": ms[11],
+                                          "of_which_alloc": ms[12], "of_which_upload": ms[13]}}
 
     def test_stall(self, item: int, fill: int, wait_cycles: int) -> None:
         """Test hook (cgfdm_test_stall): the next stage launch's work item

@@ -244,7 +244,7 @@ int cgfdm_create_profile(const cgfdm_session *s, double *ms)
     for (int i = 0; i < 3; i++) ms[i] = s->s.create_ms[i];
     ms[3] = s->s.capture_ms;
     for (int i = 0; i < 5; i++) ms[4 + i] = s->s.m.phase_ms[i];
-    for (int i = 0; i < 3; i++) ms[9 + i] = s->s.setup_ms[i];
+    for (int i = 0; i < 5; i++) ms[9 + i] = s->s.setup_ms[i];
     return CGFDM_OK;
 }
 

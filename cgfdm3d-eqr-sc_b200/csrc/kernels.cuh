@@ -11,6 +11,10 @@ namespace cgfdm {
 // ---------------------------------------------------------------- setup
 cudaError_t launch_setup(const float *d_coord, const float *d_medium, float *cjm, float *rdz, DevGrid g,
                          float rDH, int scheme, int fp64, cudaStream_t st);
+// The padded grid's coordinates from the surface height map (mode: 0 flat,
+// 1 terrain-following in float, 2 in double; see Model::coord_mode).
+cudaError_t launch_build_coords(float *coord, const float *terrain, int nxp, int nyp, int nzp, int mode, float DH,
+                                int originalX, int originalY, int NZ, float depth_f, double depth_d, cudaStream_t st);
 cudaError_t launch_scale_moment(float *rate, const long long *cell, long long npts, int nt, const float *cjm,
                                 DevGrid g, float DH, cudaStream_t st);
 

@@ -202,6 +202,7 @@ static void build_coords(Model &m)
     const float DH = g.DH;
     const int NZ = g.NZ;
     m.coord.resize((size_t)g.npad() * 3);   // every value written below
+    m.coord_mode = 0;
     m.terrain.assign((size_t)g._nx_ * g._ny_, 0.f);
     par_for(g._nz_, [&](int k) {
         for (int j = 0; j < g._ny_; j++)
@@ -219,6 +220,8 @@ static void build_coords(Model &m)
 static void terrain_following_z(Model &m, float cal_depth)
 {
     const Grid &g = m.g;
+    m.coord_mode = 1;
+    m.coord_depth_f = cal_depth;
     par_for(g._nz_, [&](int k) {
         for (int j = 0; j < g._ny_; j++)
             for (int i = 0; i < g._nx_; i++) {
@@ -455,6 +458,8 @@ static void terrain_z_double(Model &m)
 {
     const Grid &g = m.g;
     const double Depth = m.p.Depth * 1e3;
+    m.coord_mode = 2;
+    m.coord_depth_d = Depth;
     par_for(g._nz_, [&](int k) {
         for (int j = 0; j < g._ny_; j++)
             for (int i = 0; i < g._nx_; i++) {

@@ -158,6 +158,14 @@ struct Model {
     Grid g;
     int NT = 0;
     FieldVec coord;                  // [_nz_][_ny_][_nx_][3] (AoS, reference layout)
+    // how coord was made from the grid and the terrain, so the device can
+    // make it again instead of receiving it: 0 flat, 1 terrain-following in
+    // float (Gauss hill, terrain file; coord_depth_f = Depth * 1000), 2
+    // terrain-following in double (useTerrain; coord_depth_d = Depth * 1e3),
+    // -1 neither (a part of a decomposed grid: coord is uploaded)
+    int coord_mode = 0;
+    float coord_depth_f = 0;
+    double coord_depth_d = 0;
     std::vector<float> terrain;      // [_ny_][_nx_]
     std::vector<double> lon, lat;    // [_ny_][_nx_] column longitude, latitude (SRTM90 runs)
     FieldVec medium;                 // [_nz_][_ny_][_nx_][3] Vs Vp rho

@@ -69,6 +69,7 @@ int slice_model(const Model &G, const int parts[3], const int coord[3], Model &m
     // padded arrays: local padded (i, j, k) is global padded (i + lo_x, ...)
     const long long np = g.npad();
     m.coord.resize(np * 3);
+    m.coord_mode = -1;   // a sub-block of the global coordinates: uploaded
     m.medium.resize(np * 3);
     for (int k = 0; k < g._nz_; k++)
         for (int j = 0; j < g._ny_; j++)

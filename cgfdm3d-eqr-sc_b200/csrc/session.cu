@@ -180,9 +180,26 @@ int Session::setup_device()
     float *d_coord, *d_med;
     ALLOC(d_coord, float, npad * 3);
     ALLOC(d_med, float, npad * 3);
-    CU(cudaMemcpyAsync(d_coord, m.coord.data(), sizeof(float) * npad * 3, cudaMemcpyHostToDevice, stream));
+    CU(cudaStreamSynchronize(stream));
+    setup_ms[3] = ms_since(t0);   // allocation of the two upload buffers
+    if (m.coord_mode >= 0) {
+        // the coordinates are made again on the device from the height map
+        // (0.7 MB) instead of uploaded (12 bytes a point)
+        float *d_terrain;
+        ALLOC(d_terrain, float, (long long)G._nx_ * G._ny_);
+        CU(cudaMemcpyAsync(d_terrain, m.terrain.data(), sizeof(float) * G._nx_ * G._ny_, cudaMemcpyHostToDevice,
+                           stream));
+        CU(launch_build_coords(d_coord, d_terrain, G._nx_, G._ny_, G._nz_, m.coord_mode, G.DH, G.originalX,
+                               G.originalY, G.NZ, m.coord_depth_f, m.coord_depth_d, stream));
+        h2d_bytes += sizeof(float) * G._nx_ * G._ny_;
+    } else {
+        CU(cudaMemcpyAsync(d_coord, m.coord.data(), sizeof(float) * npad * 3, cudaMemcpyHostToDevice, stream));
+        h2d_bytes += sizeof(float) * npad * 3;
+    }
     CU(cudaMemcpyAsync(d_med, m.medium.data(), sizeof(float) * npad * 3, cudaMemcpyHostToDevice, stream));
-    h2d_bytes += 2.0 * sizeof(float) * npad * 3;
+    h2d_bytes += sizeof(float) * npad * 3;
+    CU(cudaStreamSynchronize(stream));
+    setup_ms[4] = ms_since(t0) - setup_ms[3];   // the uploads
     const int ncjm = cg ? 13 : 19;
     ALLOC(cjm_, float, F * ncjm);
     if (cg) ALLOC(rdz_, float, g.plane * 18);

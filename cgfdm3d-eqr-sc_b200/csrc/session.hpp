@@ -112,7 +112,7 @@ public:
     // host arithmetic), device set-up (allocation, uploads, set-up kernels),
     // whole create; and of capturing the eight-step CUDA graph
     double create_ms[3] = {0, 0, 0}, capture_ms = 0;
-    double setup_ms[3] = {0, 0, 0};   // parts of create_ms[1] (csrc/session.cu setup_device)
+    double setup_ms[5] = {0, 0, 0, 0, 0};   // parts of create_ms[1] (csrc/session.cu setup_device)
 
 private:
     int cuda_fail(cudaError_t e, const char *what);

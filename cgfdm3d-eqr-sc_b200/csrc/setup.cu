@@ -241,3 +241,50 @@ cudaError_t launch_scale_moment(float *rate, const long long *cell, long long np
 }
 
 }  // namespace cgfdm
+
+namespace cgfdm {
+
+// The coordinates of the padded grid [_nz_][_ny_][_nx_][3] from the grid and
+// the surface height map [_ny_][_nx_], with the host model's formulas
+// (csrc/model.cpp build_coords, terrain_following_z, terrain_z_double;
+// src/coord.cpp:130-132,228-234) in explicitly rounded operations, so they
+// equal the host's values in every build.
+__global__ void k_build_coords(float *__restrict__ coord, const float *__restrict__ terrain, int nxp, int nyp,
+                               int nzp, int mode, float DH, int originalX, int originalY, int NZ, float depth_f,
+                               double depth_d)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= nxp || j >= nyp) return;
+    const long long q = (((long long)k * nyp + j) * nxp + i) * 3;
+    coord[q + 0] = __fsub_rn(__fmul_rn((float)(i - CGFDM_HALO), DH), __fmul_rn((float)originalX, DH));
+    coord[q + 1] = __fsub_rn(__fmul_rn((float)(j - CGFDM_HALO), DH), __fmul_rn((float)originalY, DH));
+    const int K = k - CGFDM_HALO;
+    float z;
+    if (mode == 0) {
+        z = __fsub_rn(__fmul_rn((float)(K + 1), DH), __fmul_rn((float)NZ, DH));
+    } else {
+        const float h = terrain[(long long)j * nxp + i];
+        if (mode == 1) {
+            const float a = fabsf(depth_f);
+            const float DZ = __double2float_rn(__ddiv_rn((double)__fadd_rn(h, a), (double)(NZ - 1)));
+            z = __fadd_rn(-a, __fmul_rn(DZ, (float)K));
+        } else {
+            const double a = fabs(depth_d);
+            const double DZ = __ddiv_rn(__dadd_rn((double)h, a), (double)(NZ - 1));
+            z = __double2float_rn(__dadd_rn(-a, __dmul_rn(DZ, (double)K)));
+        }
+    }
+    coord[q + 2] = z;
+}
+
+cudaError_t launch_build_coords(float *coord, const float *terrain, int nxp, int nyp, int nzp, int mode, float DH,
+                                int originalX, int originalY, int NZ, float depth_f, double depth_d, cudaStream_t st)
+{
+    const dim3 b(32, 8, 1), gr((nxp + 31) / 32, (nyp + 7) / 8, nzp);
+    k_build_coords<<<gr, b, 0, st>>>(coord, terrain, nxp, nyp, nzp, mode, DH, originalX, originalY, NZ, depth_f,
+                                     depth_d);
+    return cudaGetLastError();
+}
+
+}  // namespace cgfdm

@@ -325,8 +325,9 @@ int cgfdm_run_precise(cgfdm_session *s, int nsteps, int bits, double *stations, 
  * the eight-step CUDA graph (made by the first cgfdm_run of 8 or more steps),
  * ms[4..8] the parts of ms[0]: coordinates and terrain, medium, value ranges
  * and PML profiles, sources, stations; ms[9..11] the parts of ms[1]:
- * allocation, uploads and the CFL check, the rest enqueued, its completion. */
-int cgfdm_create_profile(const cgfdm_session *s, double ms[12]);
+ * allocation, uploads and the CFL check, the rest enqueued, its completion;
+ * ms[12], ms[13] the allocation and the upload within ms[9]. */
+int cgfdm_create_profile(const cgfdm_session *s, double ms[14]);
 
 /* Test hook of the stage kernel's bounded waits.  No counterpart in the
  * reference, whose CHECK macro prints a CUDA error and carries on
