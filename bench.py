@@ -584,6 +584,8 @@ def session_options(args):
         o["storage"] = args.storage
     if args.pipeline != "split":
         o["stagePipeline"] = args.pipeline
+    if getattr(args, "tile", 0):
+        o["stageTile"] = args.tile
     return json.dumps(o) if o else None
 
 
@@ -625,6 +627,9 @@ def main():
     ap.add_argument("--pipeline", default="split", choices=["ring", "split"],
                     help="CGFDM FP32 stage kernel: the current plane's halo box with interior column boxes for the "
                          "z window (default), or six full halo planes in a ring")
+    ap.add_argument("--tile", type=int, default=0, choices=[0, 4, 8],
+                    help="CGFDM: rows of the stage kernel's 32-column tiles (0: the session's default, 8 on the "
+                         "FP32 split pipeline, 4 on the ring)")
     ap.add_argument("--kchunk", type=int, default=0,
                     help="CGFDM: z planes per work item of the stage kernel (0: the session's default)")
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"],
@@ -686,7 +691,7 @@ def main():
     s = Session(d, options=session_options(args), device=local_rank)
     if args.kchunk:
         s.set_tiling(args.kchunk, s.tiling()[1])
-    tiling = s.tiling() if not is_scfdm(args.workload) else None
+    tiling = s.tiling() + (s.stage_tile(),) if not is_scfdm(args.workload) else None
     info = s.info
     pts = info.nx * info.ny * info.nz
     s.run(args.warmup)
@@ -732,7 +737,7 @@ def main():
                     "fp16 stage/accumulator deltas (per-field scales) + fp32 step state; f32 arithmetic"),
         "scheme": "SCFDM" if sc else "CGFDM",
         "config": {"workload": workload_desc(args.workload), "points": pts, "DT": info.DT,
-                   "stage_tiling": ({"tile": "32x4", "kchunk": tiling[0], "ctas": tiling[1],
+                   "stage_tiling": ({"tile": f"32x{tiling[2]}", "kchunk": tiling[0], "ctas": tiling[1],
                                      "pipeline": "ring" if args.storage == "fp16" else args.pipeline}
                                     if tiling else None),
                    "l2": "inputs larger than L2 (model + wavefield %.1f GB resident)" % (info.device_bytes / 1e9),

@@ -88,6 +88,8 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
     L.cgfdm_autotune.argtypes = [vp, ctypes.c_int, ip, ip, ctypes.POINTER(ctypes.c_float)]
     L.cgfdm_set_tiling.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     L.cgfdm_get_tiling.argtypes = [vp, ip, ip]
+    L.cgfdm_set_stage_tile.argtypes = [vp, ctypes.c_int]
+    L.cgfdm_get_stage_tile.argtypes = [vp, ip]
     L.cgfdm_batch_autotune.argtypes = [vp, ctypes.c_int, ip, ip, ctypes.POINTER(ctypes.c_float)]
     L.cgfdm_gradient.argtypes = [vp, fp, ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(ctypes.c_double), fp,
                                  ctypes.c_longlong]
@@ -326,6 +328,16 @@ class Session:
         kc, ct = ctypes.c_int(), ctypes.c_int()
         self._check(self.L.cgfdm_get_tiling(self._h, ctypes.byref(kc), ctypes.byref(ct)))
         return kc.value, ct.value
+
+    def set_stage_tile(self, rows: int) -> None:
+        """Column-tile height of the CGFDM stage kernel (cgfdm_set_stage_tile):
+        4 or 8 rows of 32; 8 needs the FP32 split pipeline of a whole grid."""
+        self._check(self.L.cgfdm_set_stage_tile(self._h, int(rows)))
+
+    def stage_tile(self) -> int:
+        r = ctypes.c_int()
+        self._check(self.L.cgfdm_get_stage_tile(self._h, ctypes.byref(r)))
+        return r.value
 
     def gradient_profile(self):
         """Device ms of the last gradient's phases: forward with checkpoints,

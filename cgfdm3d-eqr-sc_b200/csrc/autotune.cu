@@ -1,4 +1,5 @@
-// Autotuner of the CGFDM stage launch: the work decomposition -- z planes
+// Autotuner of the CGFDM stage launch: the work decomposition -- the tile
+// height (4 or 8 rows of 32 columns, where the pipeline has both), z planes
 // per work item (the pencil a CTA marches through: longer pencils re-read
 // fewer chunk-edge planes, shorter ones balance the persistent CTAs better
 // on small or uneven grids) and the number of persistent CTAs -- is chosen
@@ -19,11 +20,11 @@ namespace cgfdm {
 // pencil lengths tried (clamped to the grid; the current one is added)
 static const int KCHUNK_CANDIDATES[] = {8, 12, 16, 20, 24, 32, 48, 64, 96, 128, 192, 256};
 
-static int device_full_ctas(int device)
+static int device_sms(int device)
 {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    return sms * cg_stage_ctas_per_sm();
+    return sms;
 }
 
 static std::vector<int> kchunk_candidates(int nz_max, int current)
@@ -51,7 +52,8 @@ int Session::set_tiling(int kc, int ctas)
     }
     kchunk_ = std::min(kc, m.g.nz);
     nchunk_ = (m.g.nz + kchunk_ - 1) / kchunk_;
-    grid_ctas_ = (int)std::min<long long>(std::min(ctas, device_full_ctas(device)), (long long)stage_items());
+    grid_ctas_ = (int)std::min<long long>(std::min(ctas, device_sms(device) * stage_ctas_per_sm()),
+                                          (long long)stage_items());
     if (int st = build_stage_descs()) return st;
     if (graph8_) cudaGraphExecDestroy(graph8_);
     if (graph8_src_) cudaGraphDestroy(graph8_src_);
@@ -125,26 +127,36 @@ int Session::autotune(int trial, int *best_kc, int *best_ctas, float *best_ms)
         ~Free() { cudaFree(p); }
     } fr{buf};
     if (int st = tune_save(buf)) return st;
-    const int full = device_full_ctas(device);
     // the current decomposition first; another one replaces it only when
     // it is faster by more than the trials' noise (1 %)
-    const int k0 = kchunk_, c0 = grid_ctas_;
-    int bk = k0, bc = c0;
+    const int t0 = tile_, k0 = kchunk_, c0 = grid_ctas_;
+    int bt = t0, bk = k0, bc = c0;
     float bms = 1e30f, ms0 = 1e30f;
-    std::vector<std::pair<int, int>> cand{{k0, c0}};
-    for (int kc : kchunk_candidates(m.g.nz, kchunk_))
-        for (int ctas : {full, full * 2 / 3}) cand.push_back({kc, ctas});
-    for (auto [kc, ctas] : cand) {
-        if (int st = set_tiling(kc, ctas)) return st;
+    struct Cand {
+        int rows, kc, ctas;
+    };
+    std::vector<Cand> cand{{t0, k0, c0}};
+    const bool both = m.p.stage_split && !mix_ && !part_session_;
+    for (int rows : {4, 8}) {
+        if (rows == 8 && !both) continue;
+        if (int st = set_tile(rows)) return st;
+        const int full = device_sms(device) * stage_ctas_per_sm();
+        for (int kc : kchunk_candidates(m.g.nz, kchunk_))
+            for (int ctas : {full, full * 2 / 3}) cand.push_back({rows, kc, ctas});
+    }
+    for (const Cand &c : cand) {
+        if (int st = set_tile(c.rows)) return st;
+        if (int st = set_tiling(c.kc, c.ctas)) return st;
         float ms = 0.0f;
         if (int st = tune_load(buf)) return st;
         if (int st = time_steps(1, &ms)) return st;   // first launch of this shape
         if (int st = tune_load(buf)) return st;
         if (int st = time_steps(trial, &ms)) return st;
-        if (kc == k0 && ctas == c0) ms0 = std::min(ms0, ms);
-        if (ms < bms) bms = ms, bk = kc, bc = ctas;
+        if (c.rows == t0 && c.kc == k0 && c.ctas == c0) ms0 = std::min(ms0, ms);
+        if (ms < bms) bms = ms, bt = c.rows, bk = c.kc, bc = c.ctas;
     }
-    if (bms > 0.99f * ms0) bk = k0, bc = c0, bms = ms0;
+    if (bms > 0.99f * ms0) bt = t0, bk = k0, bc = c0, bms = ms0;
+    if (int st = set_tile(bt)) return st;
     if (int st = set_tiling(bk, bc)) return st;
     if (int st = tune_load(buf)) return st;
     CU(cudaStreamSynchronize(stream));
@@ -224,7 +236,7 @@ int Batch::autotune(int trial, int *best_kc, int *best_ctas, float *best_ms)
     };
     int nz_max = 1;
     for (Session *x : s) nz_max = std::max(nz_max, x->m.g.nz);
-    const int full = device_full_ctas(device);
+    const int full = device_sms(device) * cg_stage_ctas_per_sm();
     // the current decomposition (each session's own pencil) first; a
     // uniform one replaces it only when faster by more than the trials'
     // noise (1 %)

@@ -72,6 +72,12 @@ int Batch::create(const std::vector<Session *> &sessions)
     }
     BCU(cudaSetDevice(device));
     for (Session *x : s) BCU(cudaStreamSynchronize(x->stream));
+    // the batched launch runs the 32 x 4 ring kernel
+    for (Session *x : s)
+        if (int st = x->set_tile(4)) {
+            err = x->err;
+            return st;
+        }
     BCU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     BCU(cudaEventCreate(&ev_[0]));
     BCU(cudaEventCreate(&ev_[1]));

@@ -387,6 +387,19 @@ int cgfdm_get_tiling(const cgfdm_session *s, int *kchunk, int *ctas)
     return CGFDM_OK;
 }
 
+int cgfdm_set_stage_tile(cgfdm_session *s, int rows)
+{
+    if (!s) return CGFDM_E_ARG;
+    return s->s.set_tile(rows);
+}
+
+int cgfdm_get_stage_tile(const cgfdm_session *s, int *rows)
+{
+    if (!s || !rows) return CGFDM_E_ARG;
+    *rows = s->s.tile();
+    return CGFDM_OK;
+}
+
 int cgfdm_batch_autotune(cgfdm_batch *b, int trial_steps, int *kchunk, int *ctas, float *ms_per_step)
 {
     if (!b || trial_steps < 1) return CGFDM_E_ARG;

@@ -87,7 +87,18 @@
 #define CG_LD(p) (p)
 #endif
 
+// The file is compiled once per tile height: CG_TILE_Y 4 (this object, an
+// inline namespace, so callers name its functions plainly) and 8
+// (cgfdm_stage_ty8.cu, namespace cgfdm::ty8); a session picks one.
+#ifndef CG_TILE_NS
+#define CG_TILE_NS ty4
+#define CG_TILE_NS_INLINE inline
+#else
+#define CG_TILE_NS_INLINE
+#endif
+
 namespace cgfdm {
+CG_TILE_NS_INLINE namespace CG_TILE_NS {
 
 // 32 x 4 tiles, three CTAs per SM (12 warps, 168 registers): 5 % faster on
 // the 400 x 400 x 200 workload than 32 x 8 tiles at two CTAs per SM, the
@@ -134,8 +145,23 @@ namespace cgfdm {
 #define CG_MIX_CTAS_PER_SM 2
 #endif
 
-size_t cg_stage_smem_bytes(bool mix) { return (size_t)NSLOT * (SLOT_BYTES + (mix ? SLOT_HB : 0)) + NSLOT * 8; }
-size_t cg_stage2_smem_bytes() { return (size_t)NHSLOT * SLOT_BYTES + NCSLOT * CSLOT_BYTES + PTS_F * 4 + (NHSLOT + NCSLOT + 1) * 8; }
+// Slot strides: a TMA copy's shared-memory destination must be 128-byte
+// aligned, so each slot starts on a 128-byte boundary whatever the box size
+// (a 40 x 6 x 9 float box, the 2-row tile's, is 8640 bytes).
+#define SLOT_SF ((SLOT_F + 31) / 32 * 32)          // floats between halo-box slots
+#define CSLOT_SF ((CSLOT_F + 31) / 32 * 32)        // floats between column-box slots
+#define SLOT_HSF ((9 * PF + 63) / 64 * 64)         // halves between FP16 delta-box slots
+static_assert(SLOT_SF % 32 == 0 && CSLOT_SF % 32 == 0 && SLOT_HSF % 64 == 0 && CW % 32 == 0,
+              "TMA destinations on 128-byte boundaries");
+
+size_t cg_stage_smem_bytes(bool mix)
+{
+    return (size_t)NSLOT * (SLOT_SF * 4 + (mix ? SLOT_HSF * 2 : 0)) + NSLOT * 8;
+}
+size_t cg_stage2_smem_bytes()
+{
+    return (size_t)(NHSLOT * SLOT_SF + NCSLOT * CSLOT_SF + PTS_F) * 4 + (NHSLOT + NCSLOT + 1) * 8;
+}
 
 // ------------------------------------------------------------ TMA helpers
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -375,14 +401,14 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
     static_assert(!(V2 && (BATCH || HOUT || MIX)), "the split pipeline is a single-session FP32 variant");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float *ring = reinterpret_cast<float *>(smem_raw);   // V2: the halo ring (2 slots)
-    __half *ring16 = reinterpret_cast<__half *>(smem_raw + NSLOT * SLOT_BYTES);
-    float *col = ring + NHSLOT * SLOT_F;                  // V2: column ring
-    float *pts = col + NCSLOT * CSLOT_F;                  // V2: point operands
+    __half *ring16 = reinterpret_cast<__half *>(smem_raw + NSLOT * SLOT_SF * 4);
+    float *col = ring + NHSLOT * SLOT_SF;                 // V2: column ring
+    float *pts = col + NCSLOT * CSLOT_SF;                 // V2: point operands
     constexpr int NCS = V2 ? NCSLOT : NSLOT;              // column (V2) or ring slots
     constexpr bool SPTS = V2 && CG_SPLIT_PTS;             // point operands staged in shared memory
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(
-        V2 ? smem_raw + (NHSLOT * SLOT_F + NCSLOT * CSLOT_F + PTS_F) * 4
-           : smem_raw + NSLOT * (SLOT_BYTES + (MIX ? SLOT_HB : 0)));
+        V2 ? smem_raw + (NHSLOT * SLOT_SF + NCSLOT * CSLOT_SF + PTS_F) * 4
+           : smem_raw + NSLOT * (SLOT_SF * 4 + (MIX ? SLOT_HSF * 2 : 0)));
     // barrier of column (V2) or ring slot s
     auto cbar = [&](int s) -> unsigned long long * { return V2 ? &bars[NHSLOT + s] : &bars[s]; };
     __shared__ int s_abort, s_item;
@@ -490,7 +516,7 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         const unsigned bar = smem_u32(&bars[hs]);
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         mbar_expect_tx(bar, SLOT_BYTES);
-        tma_load_4d(smem_u32(ring + hs * SLOT_F), tmW, tx0, ty0, kk, 0, bar);
+        tma_load_4d(smem_u32(ring + hs * SLOT_SF), tmW, tx0, ty0, kk, 0, bar);
     };
     auto issue_pts = [&](int kk) {
         const unsigned bar = smem_u32(&bars[NHSLOT + NCSLOT]);
@@ -511,20 +537,20 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         if constexpr (MIX) {
             const bool hs = a.irk != 0;
             mbar_expect_tx(bar, SLOT_BYTES + (hs ? SLOT_HB : 0));
-            tma_load_4d(smem_u32(ring + s * SLOT_F), tmW, tx0, ty0, kk, 0, bar);
-            if (hs) tma_load_4d(smem_u32(ring16 + s * (9 * PF)), tmS, tx0h, ty0, kk, 0, bar);
+            tma_load_4d(smem_u32(ring + s * SLOT_SF), tmW, tx0, ty0, kk, 0, bar);
+            if (hs) tma_load_4d(smem_u32(ring16 + s * SLOT_HSF), tmS, tx0h, ty0, kk, 0, bar);
             return;
         }
         if constexpr (V2) {
             mbar_expect_tx(bar, CSLOT_BYTES);
-            tma_load_4d(smem_u32(col + s * CSLOT_F), tmWc, px0, j0, kk, 0, bar);
+            tma_load_4d(smem_u32(col + s * CSLOT_SF), tmWc, px0, j0, kk, 0, bar);
             return;
         }
         mbar_expect_tx(bar, SLOT_BYTES);
         if (CG_RING_EVICT_LAST)
-            tma_load_4d_hint(smem_u32(ring + s * SLOT_F), tmW, tx0, ty0, kk, 0, bar, l2_evict_last_policy());
+            tma_load_4d_hint(smem_u32(ring + s * SLOT_SF), tmW, tx0, ty0, kk, 0, bar, l2_evict_last_policy());
         else
-            tma_load_4d(smem_u32(ring + s * SLOT_F), tmW, tx0, ty0, kk, 0, bar);
+            tma_load_4d(smem_u32(ring + s * SLOT_SF), tmW, tx0, ty0, kk, 0, bar);
     };
     // point operands of plane kk into L2 ahead of their plain loads
     auto prefetch_points = [&](int kk) {
@@ -542,8 +568,8 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
     // two values at a time (both boxes are [field][row][column], PF values a
     // field, so pair e of one is pair e of the other)
     auto convert = [&](int kk) {
-        float2 *r32 = reinterpret_cast<float2 *>(ring + slot_of(kk) * SLOT_F);
-        const __half2 *r16 = reinterpret_cast<const __half2 *>(ring16 + slot_of(kk) * (9 * PF));
+        float2 *r32 = reinterpret_cast<float2 *>(ring + slot_of(kk) * SLOT_SF);
+        const __half2 *r16 = reinterpret_cast<const __half2 *>(ring16 + slot_of(kk) * SLOT_HSF);
         for (int e = tid; e < 9 * PF / 2; e += TX * TY) {
             const float inv = s_inv[e / (PF / 2)];
             const float2 d = __half22float2(r16[e]);
@@ -719,9 +745,9 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         Taps<FB1, FB2, FB3, V2 ? CW : PF> T;
         for (int m = 0; m < 5; m++) {
             int kk = k + FB3 * (m - 1);
-            T.zp[m] = V2 ? col + slot_of(kk) * CSLOT_F + ty * TX + tx : ring + slot_of(kk) * SLOT_F + cell;
+            T.zp[m] = V2 ? col + slot_of(kk) * CSLOT_SF + ty * TX + tx : ring + slot_of(kk) * SLOT_SF + cell;
         }
-        T.hc = V2 ? ring + hslot_of(k) * SLOT_F + cell : T.zp[1];
+        T.hc = V2 ? ring + hslot_of(k) * SLOT_SF + cell : T.zp[1];
         if (a.irk == 0)
             for (int f = 0; f < 9; f++) mv[f] = T.c(f);
 
@@ -876,7 +902,7 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
 #pragma unroll
                 for (int f = 0; f < 9; f++) a.Sout[f * Fh + qh] = to_h16(RK_ALPHA2 * h[f], s_sc[f]);
             } else if (a.irk == 1) {
-                const __half *cur16 = ring16 + slot_of(k) * (9 * PF) + cell;
+                const __half *cur16 = ring16 + slot_of(k) * SLOT_HSF + cell;
 #pragma unroll
                 for (int f = 0; f < 9; f++) {
                     const float d1 = __half2float(cur16[f * PF]) * s_inv[f];
@@ -1135,4 +1161,5 @@ cudaError_t make_field_tmap(void *out, const float *base, const DevGrid &g, int 
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+}  // namespace CG_TILE_NS
 }  // namespace cgfdm

@@ -466,10 +466,7 @@ int Session::gradient(const float *obs, int K, double *misfit, float *grad_out)
                 d.a.hbox = hb;
                 d.a.vdstore = vdptr(slot, n - n0, irk);
                 const int sgn = (irk & 1) ? -1 : 1;
-                if (m.p.stage_split)
-                    CU(launch_cg_stage_split(FB[0] * sgn, FB[1] * sgn, FB[2] * sgn, d, work_dev_, grid_ctas_, stream));
-                else
-                    CU(launch_cg_stage(FB[0] * sgn, FB[1] * sgn, FB[2] * sgn, d, work_dev_, grid_ctas_, stream));
+                if (int st = launch_stage(FB[0] * sgn, FB[1] * sgn, FB[2] * sgn, d)) return st;
             }
             if (first)
                 if (int st = launch_pga_on(stream)) return st;

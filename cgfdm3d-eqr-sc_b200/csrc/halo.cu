@@ -191,6 +191,7 @@ int Session::create_part(const std::string &dir, const std::string &options, con
         return ST_OPTIONS;
     }
     is_part_ = parts[0] * parts[1] * parts[2] > 1;
+    part_session_ = true;
     CU(cudaSetDevice(dev));
     arena_session_add(dev);
     counted_ = true;

@@ -126,36 +126,47 @@ struct alignas(64) CgStageDesc {
     unsigned char tmWc[128];  // split pipeline: the stencil input, interior column box
     CgStageArgs a;
 };
-// One session's stage, its descriptor passed as a kernel parameter.
-cudaError_t launch_cg_stage(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,
-                            cudaStream_t st, bool halo_out = false);
-// A batch: session s owns work items item_start[s] .. item_start[s+1]-1, its
-// descriptor is descs[s] in device memory; all advance with the same FB
-// signs and stage number.
-cudaError_t launch_cg_stage_batch(int FB1, int FB2, int FB3, const CgStageDesc *descs, const int *item_start,
-                                  int nsess, int *work, int grid_ctas, cudaStream_t st);
-size_t cg_stage_smem_bytes(bool mix = false);
-size_t cg_stage2_smem_bytes();
-// The split pipeline (the current plane's halo box, interior column boxes for
-// the z window, TMA-staged point operands): one session's FP32 stage.
-cudaError_t launch_cg_stage_split(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,
-                                  cudaStream_t st);
-// Mixed-precision storage: one session's stage (the MIX instantiation).
-cudaError_t launch_cg_stage_mix(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,
-                                cudaStream_t st);
-int cg_stage_mix_ctas_per_sm();
-// FP16 counterpart of make_field_tmap (halo box), for arrays in the layout gh.
-cudaError_t make_field_tmap16(void *out, const __half *base, const DevGrid &gh, int nf);
-// Smallest S and largest P impedance, sqrt(mu / b) and sqrt((lambda + 2 mu) / b),
-// over the interior, into out[0], out[1] (float bits; the caller sets out[0]
-// to +inf bits and out[1] to 0 first).
-cudaError_t launch_impedance_bounds(const float *cjm, DevGrid g, unsigned *out, cudaStream_t st);
-// Encodes the 4-D tensor map (x, y, z, field) of an nf-field buffer, with a
-// halo box (40 x (tile rows + 4) x 1 x nf) or a point box (32 x tile rows x 1 x nf); out must hold
-// 128 bytes.
-cudaError_t make_field_tmap(void *out, const float *base, const DevGrid &g, int nf, bool halo_box);
-int cg_stage_ctas_per_sm();
-int cg_stage_tile_y();
+// The stage kernel's host functions, declared once per tile height: the
+// 32 x 4 build (inline namespace ty4: these names plainly) and the 32 x 8
+// build (cgfdm::ty8, csrc/cgfdm_stage_ty8.cu).
+//
+// launch_cg_stage: one session's stage (ring pipeline), its descriptor passed
+// as a kernel parameter.  launch_cg_stage_batch: session s owns work items
+// item_start[s] .. item_start[s+1]-1, its descriptor is descs[s] in device
+// memory; all advance with the same FB signs and stage number.
+// launch_cg_stage_split: the split pipeline (the current plane's halo box,
+// interior column boxes for the z window): one session's FP32 stage.
+// launch_cg_stage_mix: mixed-precision storage (the MIX instantiation).
+// make_field_tmap16: FP16 counterpart of make_field_tmap (halo box), for
+// arrays in the layout gh.  launch_impedance_bounds: smallest S and largest
+// P impedance, sqrt(mu / b) and sqrt((lambda + 2 mu) / b), over the interior,
+// into out[0], out[1] (float bits; the caller sets out[0] to +inf bits and
+// out[1] to 0 first).  make_field_tmap: the 4-D tensor map (x, y, z, field)
+// of an nf-field buffer, with a halo box (40 x (tile rows + 4) x 1 x nf) or a
+// point box (32 x tile rows x 1 x nf); out must hold 128 bytes.
+#define CG_STAGE_FUNCTIONS                                                                                         \
+    cudaError_t launch_cg_stage(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,      \
+                                cudaStream_t st, bool halo_out = false);                                         \
+    cudaError_t launch_cg_stage_batch(int FB1, int FB2, int FB3, const CgStageDesc *descs, const int *item_start, \
+                                      int nsess, int *work, int grid_ctas, cudaStream_t st);                     \
+    size_t cg_stage_smem_bytes(bool mix = false);                                                               \
+    size_t cg_stage2_smem_bytes();                                                                              \
+    cudaError_t launch_cg_stage_split(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,\
+                                      cudaStream_t st);                                                          \
+    cudaError_t launch_cg_stage_mix(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,  \
+                                    cudaStream_t st);                                                            \
+    int cg_stage_mix_ctas_per_sm();                                                                             \
+    cudaError_t make_field_tmap16(void *out, const __half *base, const DevGrid &gh, int nf);                    \
+    cudaError_t launch_impedance_bounds(const float *cjm, DevGrid g, unsigned *out, cudaStream_t st);           \
+    cudaError_t make_field_tmap(void *out, const float *base, const DevGrid &g, int nf, bool halo_box);         \
+    int cg_stage_ctas_per_sm();                                                                                 \
+    int cg_stage_tile_y();
+inline namespace ty4 {
+CG_STAGE_FUNCTIONS
+}
+namespace ty8 {
+CG_STAGE_FUNCTIONS
+}
 
 // ------------------------------------------------ SCFDM (ME-AWENO) stage
 // One directional pass of a TVD stage: x stores the RHS in H, y adds to it,

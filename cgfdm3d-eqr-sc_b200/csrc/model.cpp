@@ -1213,6 +1213,7 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
         if ((it = o.get("OUT")) && it->kind == JsonValue::String) m.p.OUT = it->str;
         if ((it = o.get("checkFinite"))) m.p.check_finite = std::max(0, it->as_int());
         if ((it = o.get("stagePipeline")) && it->kind == JsonValue::String) m.p.stage_split = it->str != "ring";
+        if ((it = o.get("stageTile"))) m.p.stage_tile = it->as_int();
     }
     Params &p = m.p;
     if (p.NX <= 0 || p.NY <= 0 || p.NZ <= 0 || p.DH <= 0 || p.DT <= 0) {

@@ -109,6 +109,7 @@ struct Params {
     std::string storage = "fp32";    // "storage": "fp32" | "fp16" | "bf16"
     int check_finite = 0;            // "checkFinite": scan the wavefield for NaN/Inf every K steps (0: never)
     int stage_split = 1;             // "stagePipeline": "split" (default) | "ring" (CGFDM FP32 stage kernel)
+    int stage_tile = 0;              // "stageTile": 4 | 8 rows of 32 columns (0: 8 for the FP32 split pipeline, else 4)
     // extension inputs (raw arrays the reference has no reader for)
     std::string terrainFile;         // float32 [_ny_][_nx_] surface height (m)
     std::string mediumFile;          // float32 [_nz_][_ny_][_nx_][3] Vs, Vp, rho

@@ -259,14 +259,22 @@ int Session::setup_device()
     }
     ALLOC(err_dev_, int, 1);
     ALLOC(work_dev_, int, 2);
-    if (cg && !mix_)
-        for (int b = 0; b < 3; b++) {
-            CU(make_field_tmap(maps_[b].win, W_[b], g, 9, true));
-            CU(make_field_tmap(maps_[b].winp, W_[b], g, 9, false));
-            CU(make_field_tmap(maps_[b].cjm, cjm_, g, 13, false));
-            CU(make_field_tmap(maps_[b].wm, W_[0], g, 9, false));
-            CU(make_field_tmap(maps_[b].t, W_[3], g, 9, false));
+    // tile height: 32 x 8 for the FP32 split pipeline of a whole grid
+    // (measured faster), 32 x 4 for the ring pipeline's users
+    if (cg) {
+        const bool eight_ok = m.p.stage_split && !mix_ && !part_session_;
+        if (m.p.stage_tile != 0 && m.p.stage_tile != 4 && m.p.stage_tile != 8) {
+            err = "\"stageTile\" is 4 or 8 (rows of 32-column stage tiles)";
+            return ST_OPTIONS;
         }
+        tile_ = m.p.stage_tile ? m.p.stage_tile : (eight_ok ? 8 : 4);
+        if (tile_ == 8 && !eight_ok) {
+            err = "32 x 8 stage tiles need the FP32 split pipeline of a whole grid";
+            return ST_OPTIONS;
+        }
+    }
+    if (cg && !mix_)
+        if (int st = build_maps()) return st;
 
     // SCFDM: RHS accumulator, DT * rDH / J, sponge factors, pass tiling
     if (!cg) {
@@ -380,9 +388,9 @@ int Session::setup_device()
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
     ntx_ = (G.nx + 31) / 32;
-    nty_ = (G.ny + cg_stage_tile_y() - 1) / cg_stage_tile_y();
+    nty_ = (G.ny + tile_ - 1) / tile_;
     const long long tiles = (long long)ntx_ * nty_;
-    const int ctas = dev_sms * (mix_ ? cg_stage_mix_ctas_per_sm() : cg_stage_ctas_per_sm());
+    const int ctas = dev_sms * stage_ctas_per_sm();
     nchunk_ = std::max(1, (G.nz + 7) / 8);
     while (tiles * nchunk_ < 4LL * ctas && G.nz / (nchunk_ + 1) >= 12) nchunk_++;
     kchunk_ = (G.nz + nchunk_ - 1) / nchunk_;
@@ -464,6 +472,63 @@ int Session::pml_faces() const
            (m.border[3] ? 16 : 0);
 }
 
+int Session::stage_ctas_per_sm() const
+{
+    return mix_ ? cg_stage_mix_ctas_per_sm() : tile_ == 8 ? ty8::cg_stage_ctas_per_sm() : cg_stage_ctas_per_sm();
+}
+
+int Session::build_maps()
+{
+    auto tmap = [&](void *out, const float *base, int nf, bool halo) {
+        return tile_ == 8 ? ty8::make_field_tmap(out, base, g, nf, halo) : make_field_tmap(out, base, g, nf, halo);
+    };
+    for (int b = 0; b < 3; b++) {
+        CU(tmap(maps_[b].win, W_[b], 9, true));
+        CU(tmap(maps_[b].winp, W_[b], 9, false));
+        CU(tmap(maps_[b].cjm, cjm_, 13, false));
+        CU(tmap(maps_[b].wm, W_[0], 9, false));
+        CU(tmap(maps_[b].t, W_[3], 9, false));
+    }
+    return ST_OK;
+}
+
+int Session::set_tile(int rows)
+{
+    if (rows != 4 && rows != 8) {
+        err = "stage tiles have 4 or 8 rows";
+        return ST_ARG;
+    }
+    if (m.p.scheme != SCHEME_CGFDM || rows == tile_) return ST_OK;
+    if (rows == 8 && !(m.p.stage_split && !mix_ && !part_session_)) {
+        err = "32 x 8 stage tiles need the FP32 split pipeline of a whole grid";
+        return ST_OPTIONS;
+    }
+    tile_ = rows;
+    nty_ = (m.g.ny + tile_ - 1) / tile_;
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
+    grid_ctas_ = (int)std::min<long long>((long long)dev_sms * stage_ctas_per_sm(), (long long)stage_items());
+    if (int st = build_maps()) return st;
+    if (int st = build_stage_descs()) return st;
+    if (graph8_) cudaGraphExecDestroy(graph8_);
+    if (graph8_src_) cudaGraphDestroy(graph8_src_);
+    graph8_ = nullptr;
+    graph8_src_ = nullptr;
+    return ST_OK;
+}
+
+int Session::launch_stage(int FB1, int FB2, int FB3, const CgStageDesc &d)
+{
+    cudaError_t e;
+    if (m.p.stage_split && !mix_)
+        e = tile_ == 8 ? ty8::launch_cg_stage_split(FB1, FB2, FB3, d, work_dev_, grid_ctas_, stream)
+                       : launch_cg_stage_split(FB1, FB2, FB3, d, work_dev_, grid_ctas_, stream);
+    else
+        e = launch_cg_stage(FB1, FB2, FB3, d, work_dev_, grid_ctas_, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "stage launch");
+    return ST_OK;
+}
+
 int Session::build_stage_descs()
 {
     if (mix_) {
@@ -520,10 +585,8 @@ int Session::launch_step(int step, bool timed_stages)
             if (timed_stages) CU(cudaEventRecord(ev_[2], stream));
             if (mix_)
                 CU(launch_cg_stage_mix(FB1, FB2, FB3, desc_mix_[step & 1][irk], work_dev_, grid_ctas_, stream));
-            else if (m.p.stage_split)
-                CU(launch_cg_stage_split(FB1, FB2, FB3, desc_host_[irk], work_dev_, grid_ctas_, stream));
-            else
-                CU(launch_cg_stage(FB1, FB2, FB3, desc_host_[irk], work_dev_, grid_ctas_, stream));
+            else if (int st = launch_stage(FB1, FB2, FB3, desc_host_[irk]))
+                return st;
             if (timed_stages) {
                 CU(cudaEventRecord(ev_[3], stream));
                 CU(cudaEventSynchronize(ev_[3]));

@@ -160,11 +160,23 @@ private:
     float zs_min_ = 0, zp_max_ = 0;
     CgStageDesc desc_mix_[2][4] = {};
     void stage_desc_mix(int parity, int irk, CgStageDesc &d) const;
+    int tile_ = 4;
+    int build_maps();                                // tensor maps of the stencil inputs for tile_
+    int stage_ctas_per_sm() const;
     int *stall_dev_ = nullptr;                       // test hook of the stage kernel's bounded waits
     int stall_item_ = -1, stall_fill_ = 0;
     long long wait_limit_ = 0;
 
 public:
+    // Column-tile height of the CGFDM stage kernel (4 or 8 rows of 32), the
+    // tensor maps and work items built for it; set_tile re-encodes them
+    // (8 only with the FP32 split pipeline of a whole-grid session)
+    int tile() const { return tile_; }
+    int set_tile(int rows);
+    // one RK stage of this session's CGFDM step, with the pipeline and tile
+    // height it uses
+    int launch_stage(int FB1, int FB2, int FB3, const CgStageDesc &d);
+    bool part_session_ = false;   // made by create_part: ring pipeline, 4-row tiles
     // The wavefield at the current step boundary (mixed storage alternates two buffers).
     float *state() const { return mix_ && (it & 1) ? Walt_ : W_[0]; }
     bool mixed() const { return mix_; }

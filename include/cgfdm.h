@@ -261,13 +261,17 @@ int cgfdm_adjoint_apply(cgfdm_session *s, int nsteps, float *state, long long co
 int cgfdm_gradient_profile(const cgfdm_session *s, float *ms3);
 
 /* Autotuner of the CGFDM stage launch (no counterpart in src/).  The stage
- * kernel's persistent CTAs take work items of 32 x 4 columns by `kchunk`
- * planes; cgfdm_autotune times candidate pencil lengths and CTA counts on
- * `trial_steps` steps each (from a device copy of the state, which is put
- * back: tuning does not advance the run), keeps the fastest and returns it
- * with its device time per step.  Results are bit-identical for every
- * tiling.  cgfdm_set_tiling / cgfdm_get_tiling set and read it directly
- * (ctas is clamped to the resident maximum and the work items).
+ * kernel's persistent CTAs take work items of 32 x `rows` columns by
+ * `kchunk` planes; cgfdm_autotune times candidate tile heights (4 and 8
+ * rows, where the session's pipeline has both), pencil lengths and CTA
+ * counts on `trial_steps` steps each (from a device copy of the state, which
+ * is put back: tuning does not advance the run), keeps the fastest and
+ * returns its pencil, CTA count and device time per step.  Results are
+ * bit-identical for every tiling.  cgfdm_set_tiling / cgfdm_get_tiling set
+ * and read the pencil and CTAs directly (ctas is clamped to the resident
+ * maximum and the work items); cgfdm_set_stage_tile / cgfdm_get_stage_tile
+ * the tile height (8 rows only with the FP32 split pipeline of a whole grid:
+ * CGFDM_E_OPTIONS otherwise; the default is 8 there and 4 elsewhere).
  * cgfdm_batch_autotune does the same for a batch's shared launch, trying
  * one pencil length for all its sessions against their own default ones
  * (*kchunk = 0 when those are kept).  A candidate replaces the current
@@ -275,6 +279,8 @@ int cgfdm_gradient_profile(const cgfdm_session *s, float *ms3);
 int cgfdm_autotune(cgfdm_session *s, int trial_steps, int *kchunk, int *ctas, float *ms_per_step);
 int cgfdm_set_tiling(cgfdm_session *s, int kchunk, int ctas);
 int cgfdm_get_tiling(const cgfdm_session *s, int *kchunk, int *ctas);
+int cgfdm_set_stage_tile(cgfdm_session *s, int rows);
+int cgfdm_get_stage_tile(const cgfdm_session *s, int *rows);
 
 /* Batches: several CGFDM sessions -- independent shots or media of uneven
  * grid sizes -- advanced together, every RK stage of all of them in one

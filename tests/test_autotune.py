@@ -8,7 +8,9 @@ import numpy as np
 import pytest
 
 import parity_util as pu
-from cgfdm import Batch, Session, cases, configs
+from cgfdm import Batch, CgfdmError, Session, cases, configs
+
+E_ARG, E_OPTIONS = 20003, 180
 
 
 @pytest.mark.gpu
@@ -32,6 +34,40 @@ def test_session_autotune_keeps_results(tmp_path):
         s2.run(s2.info.NT)
         np.testing.assert_array_equal(s2.stations(), ref[0])
         s2.close()
+
+
+@pytest.mark.gpu
+def test_stage_tile_heights(tmp_path):
+    """32 x 8 tiles by default on the FP32 split pipeline, 4 rows on the ring
+    pipeline and with FP16 storage (8 refused there); switching the height
+    in the middle of a run changes no number."""
+    d = cases.write_case(pu.multi_fault(steps=30), str(tmp_path / "run"))
+    with Session(d) as s:
+        assert s.stage_tile() == 8
+        s.run(s.info.NT)
+        ref = (s.stations(), s.wavefield(), s.pgv())
+    with Session(d) as s:
+        s.run(11)
+        s.set_stage_tile(4)
+        assert s.stage_tile() == 4
+        s.run(6)
+        s.set_stage_tile(8)
+        s.run(s.info.NT)
+        for a, r in zip((s.stations(), s.wavefield(), s.pgv()), ref):
+            np.testing.assert_array_equal(a, r)
+        with pytest.raises(CgfdmError) as e:
+            s.set_stage_tile(6)
+        assert e.value.code == E_ARG
+    for opts in ('{"stagePipeline": "ring"}', '{"storage": "fp16"}'):
+        with Session(d, options=opts) as s:
+            assert s.stage_tile() == 4
+            with pytest.raises(CgfdmError) as e:
+                s.set_stage_tile(8)
+            assert e.value.code == E_OPTIONS
+    for opts in ('{"stagePipeline": "ring", "stageTile": 8}', '{"stageTile": 6}'):
+        with pytest.raises(CgfdmError) as e:
+            Session(d, options=opts)
+        assert e.value.code == E_OPTIONS
 
 
 @pytest.mark.gpu
