@@ -113,8 +113,11 @@ def make_workload(name, steps, directory):
     if name == "terrain_fault":
         configs.terrain_fault(directory, steps=steps)
     elif name.startswith("terrain_fault_"):
-        nx, ny, nz = (int(v) for v in name.split("_")[-1].split("x"))
-        configs.terrain_fault(directory, steps=steps, NX=nx, NY=ny, NZ=nz)
+        # terrain_fault_<nx>x<ny>x<nz>[_pml<n>]
+        parts = name[len("terrain_fault_"):].split("_")
+        nx, ny, nz = (int(v) for v in parts[0].split("x"))
+        npml = int(parts[1][3:]) if len(parts) > 1 else 12
+        configs.terrain_fault(directory, steps=steps, NX=nx, NY=ny, NZ=nz, nPML=npml)
     elif name == "aweno_basin":
         configs.aweno_basin(directory, steps=steps)
     elif name.startswith("aweno_basin_"):
@@ -231,6 +234,21 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ CPU baseline
+def pml_point_fraction(nx, ny, nz, npml):
+    """Share of the grid's points inside the PML (x and y faces both sides,
+    the bottom z face; the top is the free surface)."""
+    return 1.0 - max(nx - 2 * npml, 0) * max(ny - 2 * npml, 0) * max(nz - npml, 0) / (nx * ny * nz)
+
+
+def sample_npml(sample, full=(400, 400, 200), npml_full=12):
+    """PML thickness of the CPU sample grid whose PML-point share is closest
+    to the full workload's: the reference's per-point cost is higher inside
+    the PML, so a sample with a thicker relative PML would understate its
+    rate on the full grid."""
+    f_full = pml_point_fraction(*full, npml_full)
+    return min(range(1, npml_full + 1), key=lambda n: abs(pml_point_fraction(*sample, n) - f_full))
+
+
 def cpu_reference_rate(name, warmup_steps, timed_steps, procs):
     """Reference CPU build on the sample grid: `procs` concurrent processes,
     wall time of (warmup + timed) steps minus (warmup) steps, aggregate rate."""
@@ -240,8 +258,10 @@ def cpu_reference_rate(name, warmup_steps, timed_steps, procs):
         return None, "reference CPU build (oracle/_ref) not built"
     sc = is_scfdm(name)
     nx, ny, nz = SAMPLE_GRID_SC if sc else SAMPLE_GRID
+    npml = None
     if name.startswith("terrain_fault"):
-        sample_name = f"terrain_fault_{nx}x{ny}x{nz}"
+        npml = sample_npml((nx, ny, nz))
+        sample_name = f"terrain_fault_{nx}x{ny}x{nz}_pml{npml}"
     elif sc:
         sample_name = f"aweno_basin_{nx}x{ny}x{nz}"
     else:
@@ -270,13 +290,21 @@ def cpu_reference_rate(name, warmup_steps, timed_steps, procs):
         if any(rcs):
             return None, f"reference CPU build failed with exit codes {sorted(set(rcs))}"
     dt = runs[warmup_steps + timed_steps] - runs[warmup_steps]
+    if dt <= 0:
+        return None, "reference CPU sample timing below its set-up noise (increase --steps)"
     pts = nx * ny * nz
     rate = procs * pts * timed_steps / max(dt, 1e-9) / 1e6
     sample = (f"reference CPU build ({scheme}, g++ {'-O3' if sc else '-O2'}, single-threaded as shipped), "
               f"{procs} concurrent processes pinned "
               f"one per core, each on the {nx}x{ny}x{nz} sub-grid of the workload (same generators), "
               f"{timed_steps} steps timed as wall({warmup_steps + timed_steps} steps) - wall({warmup_steps} steps)")
-    return {"value": rate, "unit": METRIC, "cores": procs, "kind": "reference", "sample": sample}, None
+    out = {"value": rate, "unit": METRIC, "cores": procs, "kind": "reference", "sample": sample}
+    if npml is not None:
+        out["sample"] += f", {npml}-layer PML so that its PML-point share matches the 400x400x200 workload's"
+        out["pml_point_fraction"] = {"sample": pml_point_fraction(nx, ny, nz, npml),
+                                     "workload": pml_point_fraction(400, 400, 200, 12),
+                                     "sample_with_12_layers": pml_point_fraction(nx, ny, nz, 12)}
+    return out, None
 
 
 def max_over_ranks(value, dist, device):
@@ -646,7 +674,7 @@ def main():
         if rank != 0:
             return 0
         procs = min(os.cpu_count() or 1, 32)
-        timed = max(1, min(args.steps, 4))
+        timed = max(2, min(args.steps, 4))   # one step is within the set-up time's noise
         cb, why = cpu_reference_rate(args.workload, args.warmup if args.warmup <= 4 else 2, timed, procs)
         if cb is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
