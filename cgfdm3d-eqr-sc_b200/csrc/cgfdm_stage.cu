@@ -67,10 +67,18 @@
 #endif
 // PML points: their auxiliary values prefetched into L2 before the ring wait
 // (0: none, 1: this plane's, 2: this and the next plane's, 3: the next
-// plane's, the item's first plane in its prologue), so the loads in the PML
-// branch, after the stencil, find them in L2
+// plane's, the item's first plane in its prologue).  With the face's loads
+// issued together (below) the prefetch costs more than it saves: 400x400x200
+// ran 7.80 ms per step without it and 8.02 ms with this plane's.
 #ifndef CG_PML_PREFETCH
-#define CG_PML_PREFETCH 1
+#define CG_PML_PREFETCH 0
+#endif
+// 1: a PML face's auxiliary, step-start and RK-sum values are all loaded
+// before its first store (0: each field's loads after the previous field's
+// stores, the order the compiler must keep for possibly aliasing pointers;
+// 8.24 ms per step on 400x400x200 against 8.02 with them first)
+#ifndef CG_PML_LOADS_FIRST
+#define CG_PML_LOADS_FIRST 1
 #endif
 // 1: the plane-ring TMA loads carry an L2 evict-last policy
 #ifndef CG_RING_EVICT_LAST
@@ -138,6 +146,17 @@ CG_TILE_NS_INLINE namespace CG_TILE_NS {
 #define NHSLOT CG_SPLIT_HSLOTS
 #define NCSLOT CG_SPLIT_CSLOTS
 #define PTS_F (CG_SPLIT_PTS ? 31 * CW : 0)
+// Split pipeline: the first PML face of each PML point has its operands
+// copied into a per-thread shared-memory stash by cp.async before the ring
+// wait, so they arrive during the stencil instead of after it: 9 floats a
+// thread (the auxiliary values), 18 (and the RK sum) or 27 (and the step
+// start); 0: none.  Measured on 400 x 400 x 200: 32 x 8 tiles 7.97 ms per
+// step without, 7.57 with 9, 8.30 with 18 (the larger carve-out leaves L1
+// too small for the point loads); 32 x 4 tiles 8.03 without, 7.98 with 27.
+#ifndef CG_PML_STASH
+#define CG_PML_STASH (TY == 8 ? 9 : 27)
+#endif
+#define STASH_F (CG_PML_STASH * CW)
 #define SLOT_HB (9 * PF * 2)  // mixed storage: bytes of a slot's FP16 delta box
 // Mixed storage: the ring also holds each plane's FP16 delta box, so a CTA
 // needs 104 KB and two fit on an SM.
@@ -160,11 +179,19 @@ size_t cg_stage_smem_bytes(bool mix)
 }
 size_t cg_stage2_smem_bytes()
 {
-    return (size_t)(NHSLOT * SLOT_SF + NCSLOT * CSLOT_SF + PTS_F) * 4 + (NHSLOT + NCSLOT + 1) * 8;
+    return (size_t)(NHSLOT * SLOT_SF + NCSLOT * CSLOT_SF + PTS_F + STASH_F) * 4 + (NHSLOT + NCSLOT + 1) * 8;
 }
 
 // ------------------------------------------------------------ TMA helpers
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+// one float from global to shared memory, asynchronously (cp.async); this
+// thread waits for its own copies with cp_async_wait_all
+__device__ __forceinline__ void cp_async4(float *dst, const float *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
 {
@@ -404,10 +431,12 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
     __half *ring16 = reinterpret_cast<__half *>(smem_raw + NSLOT * SLOT_SF * 4);
     float *col = ring + NHSLOT * SLOT_SF;                 // V2: column ring
     float *pts = col + NCSLOT * CSLOT_SF;                 // V2: point operands
+    float *stash = pts + PTS_F;                           // V2: PML operands of the first face
     constexpr int NCS = V2 ? NCSLOT : NSLOT;              // column (V2) or ring slots
     constexpr bool SPTS = V2 && CG_SPLIT_PTS;             // point operands staged in shared memory
+    constexpr bool STASH = V2 && CG_PML_STASH > 0;
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(
-        V2 ? smem_raw + (NHSLOT * SLOT_SF + NCSLOT * CSLOT_SF + PTS_F) * 4
+        V2 ? smem_raw + (NHSLOT * SLOT_SF + NCSLOT * CSLOT_SF + PTS_F + STASH_F) * 4
            : smem_raw + NSLOT * (SLOT_SF * 4 + (MIX ? SLOT_HSF * 2 : 0)));
     // barrier of column (V2) or ring slot s
     auto cbar = [&](int s) -> unsigned long long * { return V2 ? &bars[NHSLOT + s] : &bars[s]; };
@@ -489,6 +518,18 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
     const int _nx = g.nxp - CGFDM_HALO, _ny = g.nyp - CGFDM_HALO, _nz = g.nzp - CGFDM_HALO;
     const float rDH = a.rDH, DT = a.DT;
     const int nPML = a.nPML;
+    // position of point (ii, jj, kk) in the auxiliary arrays of PML face fc
+    // (x faces: [z][y][x of the layer]; y faces: [z][y of the layer][x];
+    // the z face: [z of the layer][y][x])
+    auto pml_pos = [&](int fc, int ii, int jj, int kk) -> long long {
+        const int ip = ii - CGFDM_HALO, jp = jj - CGFDM_HALO, kp = kk - CGFDM_HALO;
+        if (fc == 0 || fc == 3)
+            return (long long)(ip - (fc == 3 ? g.nx - nPML : 0)) + (long long)jp * nPML + (long long)kp * nPML * g.ny;
+        if (fc == 1 || fc == 4)
+            return (long long)ip + (long long)(jp - (fc == 4 ? g.ny - nPML : 0)) * g.nx +
+                   (long long)kp * g.nx * nPML;
+        return (long long)ip + (long long)jp * g.nx + (long long)kp * g.nx * g.ny;
+    };
     const int item = BATCH ? gitem - item_start[sess] : gitem;
     const int tile = item / a.nchunk, chunk = item - tile * a.nchunk;
     const int by_ = tile / a.ntiles_x, bx_ = tile - by_ * a.ntiles_x;
@@ -699,6 +740,24 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
                 }
             }
         }
+        // the first PML face of this point: its operands into the stash
+        int fc0 = -1;
+        if constexpr (STASH) {
+            const bool inz1p = (a.pml_on & 4) && k < CGFDM_HALO + nPML;
+            fc0 = !active ? -1 : inx1 ? 0 : iny1 ? 1 : inz1p ? 2 : inx2 ? 3 : iny2 ? 4 : -1;
+            if (fc0 >= 0) {
+                const PmlFace &P = a.face[fc0];
+                const long long pos = pml_pos(fc0, i, j, k);
+                float *st = stash + ty * TX + tx;
+                const float *cur = a.irk == 0 ? P.A : P.B;
+                for (int f = 0; f < 9; f++) cp_async4(st + f * CW, cur + f * P.count + pos);
+                if (CG_PML_STASH >= 18 && a.irk != 0)
+                    for (int f = 0; f < 9; f++) cp_async4(st + (9 + f) * CW, P.T + f * P.count + pos);
+                if (CG_PML_STASH >= 27 && (a.irk == 1 || a.irk == 2))
+                    for (int f = 0; f < 9; f++) cp_async4(st + (18 + f) * CW, P.A + f * P.count + pos);
+                cp_async_commit();
+            }
+        }
         const int kk_new = k - za + 4;
         bool okw = mbar_wait_bounded(smem_u32(cbar(slot_of(kk_new))), parity_of(kk_new), wlim);
         if constexpr (V2) {
@@ -824,22 +883,12 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         // ---- PML auxiliaries, faces in the reference's launch order x1 y1 z1 x2 y2
         const bool inz1 = (a.pml_on & 4) && k < CGFDM_HALO + nPML;
         if (inx1 || iny1 || inz1 || inx2 || iny2) {
-            const int i0p = i - CGFDM_HALO, j0p = j - CGFDM_HALO, k0p = k - CGFDM_HALO;
-            const int nx = g.nx, ny = g.ny;
             const bool sel[5] = {inx1, iny1, inz1, inx2, iny2};
             for (int fc = 0; fc < 5; fc++) {
                 if (!sel[fc]) continue;
                 const int dir = fc == 0 || fc == 3 ? 0 : fc == 1 || fc == 4 ? 1 : 2;
                 const PmlFace &P = a.face[fc];
-                long long pos;
-                if (dir == 0)
-                    pos = (long long)(i0p - (fc == 3 ? nx - nPML : 0)) + (long long)j0p * nPML +
-                          (long long)k0p * nPML * ny;
-                else if (dir == 1)
-                    pos = (long long)i0p + (long long)(j0p - (fc == 4 ? ny - nPML : 0)) * nx +
-                          (long long)k0p * nx * nPML;
-                else
-                    pos = (long long)i0p + (long long)j0p * nx + (long long)k0p * nx * ny;
+                const long long pos = pml_pos(fc, i, j, k);
                 const float *al = dir == 0 ? a.pml_alpha_x : dir == 1 ? a.pml_alpha_y : a.pml_alpha_z;
                 const float *be = dir == 0 ? a.pml_beta_x : dir == 1 ? a.pml_beta_y : a.pml_beta_z;
                 const float *dd = dir == 0 ? a.pml_d_x : dir == 1 ? a.pml_d_y : a.pml_d_z;
@@ -852,7 +901,29 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
                 for (int f = 0; f < 9; f++) d[f] = T.rdir(dir, f, rDH) * dval;
                 dir_rhs(m0, m1, m2, d, mu, lam, buo, rhs);
                 const float *cur = a.irk == 0 ? P.A : P.B;
-                for (int f = 0; f < 9; f++) aux[f] = cur[f * P.count + pos];
+                // every operand of this face loaded before the first store:
+                // the stores go through pointers the compiler cannot tell
+                // apart from the loads, which would otherwise wait for them
+                float xa[9], xt[9];
+                if (STASH && fc == fc0) {
+                    cp_async_wait_all();
+                    const float *st = stash + ty * TX + tx;
+                    for (int f = 0; f < 9; f++) aux[f] = st[f * CW];
+                    if (a.irk == 1 || a.irk == 2)
+                        for (int f = 0; f < 9; f++)
+                            xa[f] = CG_PML_STASH >= 27 ? st[(18 + f) * CW] : P.A[f * P.count + pos];
+                    if (a.irk != 0)
+                        for (int f = 0; f < 9; f++)
+                            xt[f] = CG_PML_STASH >= 18 ? st[(9 + f) * CW] : P.T[f * P.count + pos];
+                } else {
+                    for (int f = 0; f < 9; f++) aux[f] = cur[f * P.count + pos];
+                    if (CG_PML_LOADS_FIRST) {
+                        if (a.irk == 1 || a.irk == 2)
+                            for (int f = 0; f < 9; f++) xa[f] = P.A[f * P.count + pos];
+                        if (a.irk != 0)
+                            for (int f = 0; f < 9; f++) xt[f] = P.T[f * P.count + pos];
+                    }
+                }
                 for (int f = 0; f < 9; f++) hA[f] = (rhs[f] - alpha_d * aux[f]) * DT;
                 if (a.fs_on && k == _nz - 1 && dir < 2) {
                     // src/pml_freeSurface.cpp:90-125
@@ -874,13 +945,16 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
                     }
                 } else if (a.irk == 1 || a.irk == 2) {
                     for (int f = 0; f < 9; f++) {
-                        float mA = P.A[f * P.count + pos];
-                        float t = P.T[f * P.count + pos];
+                        float mA = CG_PML_LOADS_FIRST || (STASH && fc == fc0) ? xa[f] : P.A[f * P.count + pos];
+                        float t = CG_PML_LOADS_FIRST || (STASH && fc == fc0) ? xt[f] : P.T[f * P.count + pos];
                         P.T[f * P.count + pos] = t + (a.irk == 1 ? RK_BETA2 : RK_BETA3) * hA[f];
                         P.B[f * P.count + pos] = a.irk == 1 ? mA + RK_ALPHA3 * hA[f] : mA + hA[f];
                     }
                 } else {
-                    for (int f = 0; f < 9; f++) P.A[f * P.count + pos] = P.T[f * P.count + pos] + RK_BETA4 * hA[f];
+                    for (int f = 0; f < 9; f++)
+                        P.A[f * P.count + pos] =
+                            (CG_PML_LOADS_FIRST || (STASH && fc == fc0) ? xt[f] : P.T[f * P.count + pos]) +
+                            RK_BETA4 * hA[f];
                 }
             }
         }
@@ -999,6 +1073,9 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         }
         break;
     }
+    // no copy into the stash outlives the item (one may be pending after a
+    // failed wait)
+    if constexpr (STASH) cp_async_wait_all();
     seq0 += (unsigned)(issued - kf + 1);
     hseq0 += (unsigned)(ke - kb);
     pseq0 += (unsigned)(ke - kb);
