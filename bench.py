@@ -750,12 +750,18 @@ def main():
     s2 = Session(d, options=session_options(args), device=local_rank)
     if args.kchunk:
         s2.set_tiling(args.kchunk, s2.tiling()[1])
+    t1 = time.perf_counter()
     s2.run(args.steps)
+    t2 = time.perf_counter()
     st = s2.stations()
+    t3 = time.perf_counter()
     i2 = s2.info
     create_prof = s2.create_profile()
+    t4 = time.perf_counter()
     s2.close()
-    e2e_s = time.perf_counter() - t0
+    t5 = time.perf_counter()
+    e2e_s = t5 - t0
+    e2e_legs = {"create_s": t1 - t0, "run_s": t2 - t1, "stations_s": t3 - t2, "destroy_s": t5 - t4}
     e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{local_rank}")
 
     value = world * pts * args.steps / (ms_max * 1e-3) / 1e6
@@ -795,7 +801,7 @@ def main():
         "e2e": {"value": world * pts * args.steps / e2e_s / 1e6, "unit": METRIC,
                 "h2d_bytes_per_step": i2.h2d_bytes / args.steps, "d2h_bytes_per_step": st.nbytes / args.steps,
                 "seconds": e2e_s, "path": "cgfdm_create(run dir) + cgfdm_run(K) + cgfdm_get_stations + destroy",
-                "split_ms": create_prof},
+                "split_ms": create_prof, "legs": e2e_legs},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
