@@ -91,6 +91,7 @@ Session::~Session()
         if (e) cudaEventDestroy(e);
     for (void *p : ipc_open_) cudaIpcCloseMemHandle(p);
     for (void *p : allocs_) cudaFree(p);
+    if (arena_) cudaFree(arena_);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -103,6 +104,14 @@ int Session::cuda_fail(cudaError_t e, const char *what)
 void *Session::alloc(size_t bytes)
 {
     void *p = nullptr;
+    const size_t rounded = (bytes + 255) / 256 * 256;
+    if (arena_ && arena_used_ + rounded <= arena_size_) {
+        p = arena_ + arena_used_;
+        if (cudaMemsetAsync(p, 0, bytes, stream) != cudaSuccess) return nullptr;
+        arena_used_ += rounded;
+        device_bytes += bytes;
+        return p;
+    }
     if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
     if (cudaMemsetAsync(p, 0, bytes, stream) != cudaSuccess) {
         cudaFree(p);
@@ -167,6 +176,52 @@ int Session::create(const std::string &dir, const std::string &options, int dev)
     return st;
 }
 
+// Bytes of the arrays setup_device makes after its two upload buffers, each
+// rounded to 256 (the same list, in the same order).
+size_t Session::arena_estimate() const
+{
+    const Grid &G = m.g;
+    const bool cg = m.p.scheme == SCHEME_CGFDM;
+    const size_t F = (size_t)g.fstride;
+    size_t b = 0;
+    auto add = [&](size_t bytes) { b += (bytes + 255) / 256 * 256; };
+    add(sizeof(float) * (size_t)G._nx_ * G._ny_);                  // height map
+    add(sizeof(float) * F * (cg ? 13 : 19));                       // metric and medium
+    if (cg) add(sizeof(float) * (size_t)g.plane * 18);             // free-surface matrices
+    add(16);                                                       // spacing range
+    if (mix_) {
+        add(sizeof(float) * F * 9), add(sizeof(float) * F * 9);
+        for (int x = 0; x < 3; x++) add(2 * (size_t)gh_.fstride * 9);
+        add(80);
+    } else {
+        for (int x = 0; x < (cg ? 4 : 3); x++) add(sizeof(float) * F * 9);
+    }
+    add(4), add(8);
+    if (!cg) add(sizeof(float) * F * 9), add(sizeof(float) * F), add(sizeof(float) * 64);
+    if (cg) {
+        add(sizeof(float) * G._nx_), add(sizeof(float) * G._nx_), add(sizeof(float) * G._nx_);
+        add(sizeof(float) * G._ny_), add(sizeof(float) * G._ny_), add(sizeof(float) * G._ny_);
+        add(sizeof(float) * G._nz_), add(sizeof(float) * G._nz_), add(sizeof(float) * G._nz_);
+        if (m.p.pml) {
+            const size_t nP = (size_t)G.nPML;
+            const size_t cnt[5] = {nP * G.ny * G.nz, nP * G.nx * G.nz, nP * G.nx * G.ny, nP * G.ny * G.nz,
+                                   nP * G.nx * G.nz};
+            for (int fc = 0; fc < 5; fc++)
+                if (pml_faces() & (1 << fc))
+                    for (int x = 0; x < 3; x++) add(sizeof(float) * cnt[fc] * 9);
+        }
+    }
+    add(sizeof(float) * (size_t)G.nx * G.ny * 2);
+    if (m.p.solve_pga) add(sizeof(float) * (size_t)G.nx * G.ny * 2);
+    if (m.p.solve_displacement) add(sizeof(float) * F * 3);
+    const size_t ns = m.stations.size() / 3;
+    if (ns > 0) add(sizeof(int) * ns * 3), add(sizeof(float) * ns * std::max(m.NT, 1) * 9);
+    add(4);
+    if (m.fault.npts > 0) add(sizeof(long long) * m.fault.npts), add(sizeof(float) * m.fault.rate.size());
+    if (m.point.kind) add(sizeof(float) * m.point.amp.size()), add(sizeof(float) * std::max<size_t>(m.point.stf.size(), 1));
+    return b + 4096;
+}
+
 int Session::setup_device()
 {
     const Grid &G = m.g;
@@ -180,8 +235,30 @@ int Session::setup_device()
     float *d_coord, *d_med;
     ALLOC(d_coord, float, npad * 3);
     ALLOC(d_med, float, npad * 3);
+    if (mix_) {
+        // FP16 arrays: first interior column on a 16-byte boundary in the TMA
+        // halo box (xoff 33: column i0 - 4 = 32 + 32 n), rows of 16 bytes
+        gh_ = make_devgrid(G.nx, G.ny, G.nz, 33);
+        gh_.pitch = (gh_.pitch + 7) / 8 * 8;
+        gh_.plane = (long long)gh_.nyp * gh_.pitch;
+        gh_.fstride = ((long long)gh_.nzp * gh_.plane + 63) / 64 * 64;
+    }
+    if (!part_session_) {
+        // the long-lived arrays in one block (falls back to one allocation
+        // each if the block cannot be had).  Parts keep one allocation per
+        // array: a neighbour in another process maps their stage buffers by
+        // CUDA IPC, which maps whole allocations.
+        const size_t want = arena_estimate();
+        void *p = nullptr;
+        if (cudaMalloc(&p, want) == cudaSuccess) {
+            arena_ = (char *)p;
+            arena_size_ = want;
+        } else {
+            cudaGetLastError();
+        }
+    }
     CU(cudaStreamSynchronize(stream));
-    setup_ms[3] = ms_since(t0);   // allocation of the two upload buffers
+    setup_ms[3] = ms_since(t0);   // allocation of the two upload buffers and the block
     if (m.coord_mode >= 0) {
         // the coordinates are made again on the device from the height map
         // (0.7 MB) instead of uploaded (12 bytes a point)
@@ -234,12 +311,6 @@ int Session::setup_device()
 
     // wavefield buffers: A (step start / final), B, C (stage values), T (RK4 sum)
     if (mix_) {
-        // FP16 arrays: first interior column on a 16-byte boundary in the TMA
-        // halo box (xoff 33: column i0 - 4 = 32 + 32 n), rows of 16 bytes
-        gh_ = make_devgrid(G.nx, G.ny, G.nz, 33);
-        gh_.pitch = (gh_.pitch + 7) / 8 * 8;
-        gh_.plane = (long long)gh_.nyp * gh_.pitch;
-        gh_.fstride = ((long long)gh_.nzp * gh_.plane + 63) / 64 * 64;
         ALLOC(W_[0], float, F * 9);
         ALLOC(Walt_, float, F * 9);
         ALLOC(Sb_, __half, gh_.fstride * 9);

@@ -123,6 +123,13 @@ private:
     int launch_steps_graph(int n8);      // n8 full FB cycles via the captured graph
     void *alloc(size_t bytes);
     std::vector<void *> allocs_;
+    // One device block holds the session's long-lived arrays (sub-allocated
+    // on 256-byte boundaries): freeing some 30 separate arrays of an 8 GB
+    // session took 50-200 ms, one block 6 ms.  Arrays that do not fit (or
+    // that are made after set-up) get their own allocation.
+    char *arena_ = nullptr;
+    size_t arena_size_ = 0, arena_used_ = 0;
+    size_t arena_estimate() const;
     float *W_[4] = {nullptr, nullptr, nullptr, nullptr};  // A B C T
     float *cjm_ = nullptr, *rdz_ = nullptr;
     float *pml_[9] = {};
