@@ -89,6 +89,17 @@
 #else
 #define CG_ST(p, v) ((p) = (v))
 #endif
+// PML auxiliary stores: 1 evict-first like the stage outputs, 0 plain
+// (400x400x200: 7.57 ms per step with 1, 7.51-7.57 with 0; evict-first
+// loads as well, CG_STREAM_HINTS 2, took 8.32)
+#ifndef CG_PML_STORE_HINT
+#define CG_PML_STORE_HINT 0
+#endif
+#if CG_PML_STORE_HINT
+#define CG_PST(p, v) __stcs(&(p), (v))
+#else
+#define CG_PST(p, v) ((p) = (v))
+#endif
 #if CG_STREAM_HINTS >= 2
 #define CG_LD(p) __ldcs(&(p))
 #else
@@ -953,21 +964,21 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
                 // src/pml_rk.cpp:18-73
                 if (a.irk == 0) {
                     for (int f = 0; f < 9; f++) {
-                        P.T[f * P.count + pos] = aux[f] + RK_BETA1 * hA[f];
-                        P.B[f * P.count + pos] = aux[f] + RK_ALPHA2 * hA[f];
+                        CG_PST(P.T[f * P.count + pos], aux[f] + RK_BETA1 * hA[f]);
+                        CG_PST(P.B[f * P.count + pos], aux[f] + RK_ALPHA2 * hA[f]);
                     }
                 } else if (a.irk == 1 || a.irk == 2) {
                     for (int f = 0; f < 9; f++) {
                         float mA = CG_PML_LOADS_FIRST || (STASH && fc == fc0) ? xa[f] : P.A[f * P.count + pos];
                         float t = CG_PML_LOADS_FIRST || (STASH && fc == fc0) ? xt[f] : P.T[f * P.count + pos];
-                        P.T[f * P.count + pos] = t + (a.irk == 1 ? RK_BETA2 : RK_BETA3) * hA[f];
-                        P.B[f * P.count + pos] = a.irk == 1 ? mA + RK_ALPHA3 * hA[f] : mA + hA[f];
+                        CG_PST(P.T[f * P.count + pos], t + (a.irk == 1 ? RK_BETA2 : RK_BETA3) * hA[f]);
+                        CG_PST(P.B[f * P.count + pos], a.irk == 1 ? mA + RK_ALPHA3 * hA[f] : mA + hA[f]);
                     }
                 } else {
                     for (int f = 0; f < 9; f++)
-                        P.A[f * P.count + pos] =
-                            (CG_PML_LOADS_FIRST || (STASH && fc == fc0) ? xt[f] : P.T[f * P.count + pos]) +
-                            RK_BETA4 * hA[f];
+                        CG_PST(P.A[f * P.count + pos],
+                               (CG_PML_LOADS_FIRST || (STASH && fc == fc0) ? xt[f] : P.T[f * P.count + pos]) +
+                                   RK_BETA4 * hA[f]);
                 }
             }
         }
