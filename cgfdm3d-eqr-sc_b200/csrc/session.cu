@@ -9,6 +9,7 @@
 // captured once as a CUDA graph that is replayed.
 #include "session.hpp"
 #include "session_util.hpp"
+#include "upload.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -270,10 +271,10 @@ int Session::setup_device()
                                G.originalY, G.NZ, m.coord_depth_f, m.coord_depth_d, stream));
         h2d_bytes += sizeof(float) * G._nx_ * G._ny_;
     } else {
-        CU(cudaMemcpyAsync(d_coord, m.coord.data(), sizeof(float) * npad * 3, cudaMemcpyHostToDevice, stream));
+        CU(upload_h2d(d_coord, m.coord.data(), sizeof(float) * npad * 3, device, stream));
         h2d_bytes += sizeof(float) * npad * 3;
     }
-    CU(cudaMemcpyAsync(d_med, m.medium.data(), sizeof(float) * npad * 3, cudaMemcpyHostToDevice, stream));
+    CU(upload_h2d(d_med, m.medium.data(), sizeof(float) * npad * 3, device, stream));
     h2d_bytes += sizeof(float) * npad * 3;
     CU(cudaStreamSynchronize(stream));
     setup_ms[4] = ms_since(t0) - setup_ms[3];   // the uploads
