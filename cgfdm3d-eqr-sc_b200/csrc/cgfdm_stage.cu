@@ -174,6 +174,14 @@ CG_TILE_NS_INLINE namespace CG_TILE_NS {
 #define CG_PML_REST_PREFETCH 1
 #endif
 #define STASH_F (CG_PML_STASH * CW)
+// the same stash in the ring pipeline (batches, linked parts), FP32 only:
+// 9 floats took a 400x400x200 ring session from 8.25 to 8.04 ms per step but
+// batch32 from 34.6 to 35.5 ms (its small shots' L1 shrinks with the
+// carve-out), and batches are the ring's main users, so none by default
+#ifndef CG_PML_STASH_RING
+#define CG_PML_STASH_RING 0
+#endif
+#define STASH_RING_F (CG_PML_STASH_RING * TX * TY)
 #define SLOT_HB (9 * PF * 2)  // mixed storage: bytes of a slot's FP16 delta box
 // Mixed storage: the ring also holds each plane's FP16 delta box, so a CTA
 // needs 104 KB and two fit on an SM.
@@ -192,7 +200,7 @@ static_assert(SLOT_SF % 32 == 0 && CSLOT_SF % 32 == 0 && SLOT_HSF % 64 == 0 && C
 
 size_t cg_stage_smem_bytes(bool mix)
 {
-    return (size_t)NSLOT * (SLOT_SF * 4 + (mix ? SLOT_HSF * 2 : 0)) + NSLOT * 8;
+    return (size_t)NSLOT * (SLOT_SF * 4 + (mix ? SLOT_HSF * 2 : 0)) + (mix ? 0 : STASH_RING_F * 4) + NSLOT * 8;
 }
 size_t cg_stage2_smem_bytes()
 {
@@ -448,13 +456,16 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
     __half *ring16 = reinterpret_cast<__half *>(smem_raw + NSLOT * SLOT_SF * 4);
     float *col = ring + NHSLOT * SLOT_SF;                 // V2: column ring
     float *pts = col + NCSLOT * CSLOT_SF;                 // V2: point operands
-    float *stash = pts + PTS_F;                           // V2: PML operands of the first face
+    // PML operands of the first face (split: after the point slot; ring:
+    // after the ring)
+    float *stash = V2 ? pts + PTS_F : ring + NSLOT * SLOT_SF;
     constexpr int NCS = V2 ? NCSLOT : NSLOT;              // column (V2) or ring slots
     constexpr bool SPTS = V2 && CG_SPLIT_PTS;             // point operands staged in shared memory
-    constexpr bool STASH = V2 && CG_PML_STASH > 0;
+    constexpr int NSTASH = V2 ? CG_PML_STASH : MIX ? 0 : CG_PML_STASH_RING;
+    constexpr bool STASH = NSTASH > 0;
     unsigned long long *bars = reinterpret_cast<unsigned long long *>(
         V2 ? smem_raw + (NHSLOT * SLOT_SF + NCSLOT * CSLOT_SF + PTS_F + STASH_F) * 4
-           : smem_raw + NSLOT * (SLOT_SF * 4 + (MIX ? SLOT_HSF * 2 : 0)));
+           : smem_raw + NSLOT * (SLOT_SF * 4 + (MIX ? SLOT_HSF * 2 : 0)) + (MIX ? 0 : STASH_RING_F * 4));
     // barrier of column (V2) or ring slot s
     auto cbar = [&](int s) -> unsigned long long * { return V2 ? &bars[NHSLOT + s] : &bars[s]; };
     __shared__ int s_abort, s_item;
@@ -768,16 +779,16 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
                 float *st = stash + ty * TX + tx;
                 const float *cur = a.irk == 0 ? P.A : P.B;
                 for (int f = 0; f < 9; f++) cp_async4(st + f * CW, cur + f * P.count + pos);
-                if (CG_PML_STASH >= 18 && a.irk != 0)
+                if (NSTASH >= 18 && a.irk != 0)
                     for (int f = 0; f < 9; f++) cp_async4(st + (9 + f) * CW, P.T + f * P.count + pos);
-                if (CG_PML_STASH >= 27 && (a.irk == 1 || a.irk == 2))
+                if (NSTASH >= 27 && (a.irk == 1 || a.irk == 2))
                     for (int f = 0; f < 9; f++) cp_async4(st + (18 + f) * CW, P.A + f * P.count + pos);
                 cp_async_commit();
                 // the face's other operands (RK sum, step start) into L2
                 if (CG_PML_REST_PREFETCH) {
-                    if (CG_PML_STASH < 18 && a.irk != 0)
+                    if (NSTASH < 18 && a.irk != 0)
                         for (int f = 0; f < 9; f++) l2_prefetch(P.T + f * P.count + pos);
-                    if (CG_PML_STASH < 27 && (a.irk == 1 || a.irk == 2))
+                    if (NSTASH < 27 && (a.irk == 1 || a.irk == 2))
                         for (int f = 0; f < 9; f++) l2_prefetch(P.A + f * P.count + pos);
                 }
             }
@@ -935,10 +946,10 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
                     for (int f = 0; f < 9; f++) aux[f] = st[f * CW];
                     if (a.irk == 1 || a.irk == 2)
                         for (int f = 0; f < 9; f++)
-                            xa[f] = CG_PML_STASH >= 27 ? st[(18 + f) * CW] : P.A[f * P.count + pos];
+                            xa[f] = NSTASH >= 27 ? st[(18 + f) * CW] : P.A[f * P.count + pos];
                     if (a.irk != 0)
                         for (int f = 0; f < 9; f++)
-                            xt[f] = CG_PML_STASH >= 18 ? st[(9 + f) * CW] : P.T[f * P.count + pos];
+                            xt[f] = NSTASH >= 18 ? st[(9 + f) * CW] : P.T[f * P.count + pos];
                 } else {
                     for (int f = 0; f < 9; f++) aux[f] = cur[f * P.count + pos];
                     if (CG_PML_LOADS_FIRST) {
