@@ -352,6 +352,7 @@ def bench_batch(args, world, rank, local_rank):
     # the default decomposition, then the autotuner's choice (timed below)
     ms_default = b.run_timed(8)
     tuned = b.autotune(3)
+    tuned_tile = b.stage_tile()
     b.run(1)
     torch.cuda.synchronize(local_rank)
     with ClockSampler(local_rank) as clk:
@@ -386,7 +387,8 @@ def bench_batch(args, world, rank, local_rank):
                                "stage launch per RK stage for all shots, 8-step CUDA graphs",
                    "points": pts, "shots": n,
                    "alone_Mpts_step_s": pts * args.steps / (alone_ms * 1e-3) / 1e6,
-                   "autotuned": {"kchunk": tuned[0], "ctas": tuned[1], "trial_ms_per_step": tuned[2],
+                   "autotuned": {"tile": f"32x{tuned_tile}", "kchunk": tuned[0], "ctas": tuned[1],
+                                 "trial_ms_per_step": tuned[2],
                                  "default_ms_per_step": ms_default / 8},
                    "l2": "inputs larger than L2", "parallelism": "batch x1"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",

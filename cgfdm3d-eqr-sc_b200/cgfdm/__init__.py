@@ -90,6 +90,8 @@ def load(flavor: str = "fast") -> ctypes.CDLL:
     L.cgfdm_get_tiling.argtypes = [vp, ip, ip]
     L.cgfdm_set_stage_tile.argtypes = [vp, ctypes.c_int]
     L.cgfdm_get_stage_tile.argtypes = [vp, ip]
+    L.cgfdm_batch_set_stage_tile.argtypes = [vp, ctypes.c_int]
+    L.cgfdm_batch_get_stage_tile.argtypes = [vp, ip]
     L.cgfdm_batch_autotune.argtypes = [vp, ctypes.c_int, ip, ip, ctypes.POINTER(ctypes.c_float)]
     L.cgfdm_gradient.argtypes = [vp, fp, ctypes.c_longlong, ctypes.c_int, ctypes.POINTER(ctypes.c_double), fp,
                                  ctypes.c_longlong]
@@ -331,7 +333,7 @@ class Session:
 
     def set_stage_tile(self, rows: int) -> None:
         """Column-tile height of the CGFDM stage kernel (cgfdm_set_stage_tile):
-        4 or 8 rows of 32; 8 needs the FP32 split pipeline of a whole grid."""
+        4 or 8 rows of 32; 8 needs FP32 storage and a whole grid (not a part)."""
         self._check(self.L.cgfdm_set_stage_tile(self._h, int(rows)))
 
     def stage_tile(self) -> int:
@@ -397,6 +399,16 @@ class Batch:
         self._check(self.L.cgfdm_batch_autotune(self._h, int(trial_steps), ctypes.byref(kc), ctypes.byref(ct),
                                                 ctypes.byref(ms)))
         return kc.value, ct.value, ms.value
+
+    def set_stage_tile(self, rows: int) -> None:
+        """Rows (4 or 8) of the 32-column tiles of the batched stage launch
+        (cgfdm_batch_set_stage_tile)."""
+        self._check(self.L.cgfdm_batch_set_stage_tile(self._h, int(rows)))
+
+    def stage_tile(self) -> int:
+        r = ctypes.c_int()
+        self._check(self.L.cgfdm_batch_get_stage_tile(self._h, ctypes.byref(r)))
+        return r.value
 
     def close(self) -> None:
         if self._h:

@@ -136,7 +136,7 @@ int Session::autotune(int trial, int *best_kc, int *best_ctas, float *best_ms)
         int rows, kc, ctas;
     };
     std::vector<Cand> cand{{t0, k0, c0}};
-    const bool both = m.p.stage_split && !mix_ && !part_session_;
+    const bool both = !mix_ && !part_session_;
     for (int rows : {4, 8}) {
         if (rows == 8 && !both) continue;
         if (int st = set_tile(rows)) return st;
@@ -236,31 +236,35 @@ int Batch::autotune(int trial, int *best_kc, int *best_ctas, float *best_ms)
     };
     int nz_max = 1;
     for (Session *x : s) nz_max = std::max(nz_max, x->m.g.nz);
-    const int full = device_sms(device) * cg_stage_ctas_per_sm();
     // the current decomposition (each session's own pencil) first; a
     // uniform one replaces it only when faster by more than the trials'
     // noise (1 %)
     std::vector<int> k_orig;
     for (Session *x : s) k_orig.push_back(x->kchunk());
-    const int want_orig = want_ctas_;
+    const int want_orig = want_ctas_, t_orig = tile_;
     float ms0 = 0.0f;
     if (int st = load_all()) return st;
     if (int st = time_batch(1, &ms0)) return st;
     if (int st = load_all()) return st;
     if (int st = time_batch(trial, &ms0)) return st;
-    int bk = 0, bc = 0;
+    int bk = 0, bc = 0, bt = t_orig;
     float bms = 1e30f;
-    for (int kc : kchunk_candidates(nz_max, 0))
-        for (int ctas : {full, full * 2 / 3}) {
-            if (int st = set_tiling(kc, ctas)) return st;
-            float ms = 0.0f;
-            if (int st = load_all()) return st;
-            if (int st = time_batch(1, &ms)) return st;
-            if (int st = load_all()) return st;
-            if (int st = time_batch(trial, &ms)) return st;
-            if (ms < bms) bms = ms, bk = kc, bc = ctas;
-        }
+    for (int rows : {4, 8}) {
+        if (int st = set_tile(rows)) return st;
+        const int full = device_sms(device) * (rows == 8 ? ty8::cg_stage_ctas_per_sm() : cg_stage_ctas_per_sm());
+        for (int kc : kchunk_candidates(nz_max, 0))
+            for (int ctas : {full, full * 2 / 3}) {
+                if (int st = set_tiling(kc, ctas)) return st;
+                float ms = 0.0f;
+                if (int st = load_all()) return st;
+                if (int st = time_batch(1, &ms)) return st;
+                if (int st = load_all()) return st;
+                if (int st = time_batch(trial, &ms)) return st;
+                if (ms < bms) bms = ms, bk = kc, bc = ctas, bt = rows;
+            }
+    }
     if (bms > 0.99f * ms0) {
+        if (int st = set_tile(t_orig)) return st;
         for (size_t i = 0; i < s.size(); i++)
             if (int st = s[i]->set_tiling(k_orig[i], 1 << 30)) {
                 err = s[i]->err;
@@ -271,8 +275,9 @@ int Batch::autotune(int trial, int *best_kc, int *best_ctas, float *best_ms)
         drop_graph();
         bk = 0;   // per-session pencils kept
         bms = ms0;
-    } else if (int st = set_tiling(bk, bc)) {
-        return st;
+    } else {
+        if (int st = set_tile(bt)) return st;
+        if (int st = set_tiling(bk, bc)) return st;
     }
     if (int st = load_all()) return st;
     for (Session *x : s)

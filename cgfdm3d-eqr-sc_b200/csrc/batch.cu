@@ -72,9 +72,10 @@ int Batch::create(const std::vector<Session *> &sessions)
     }
     BCU(cudaSetDevice(device));
     for (Session *x : s) BCU(cudaStreamSynchronize(x->stream));
-    // the batched launch runs the 32 x 4 ring kernel
+    // the batched launch runs the ring kernel, 32 x 4 tiles unless set_tile
+    // chooses 8 rows
     for (Session *x : s)
-        if (int st = x->set_tile(4)) {
+        if (int st = x->set_tile(tile_)) {
             err = x->err;
             return st;
         }
@@ -106,8 +107,28 @@ int Batch::build_tables()
     BCU(cudaMemcpy(items_, items.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const int full = sms * cg_stage_ctas_per_sm();
+    const int full = sms * (tile_ == 8 ? ty8::cg_stage_ctas_per_sm() : cg_stage_ctas_per_sm());
     grid_ctas_ = std::min(want_ctas_ > 0 ? std::min(want_ctas_, full) : full, items[n]);
+    return ST_OK;
+}
+
+int Batch::set_tile(int rows)
+{
+    if (rows != 4 && rows != 8) {
+        err = "stage tiles have 4 or 8 rows";
+        return ST_ARG;
+    }
+    BCU(cudaSetDevice(device));
+    for (Session *x : s) BCU(cudaStreamSynchronize(x->stream));
+    BCU(cudaStreamSynchronize(stream));
+    for (Session *x : s)
+        if (int st = x->set_tile(rows)) {
+            err = x->err;
+            return st;
+        }
+    tile_ = rows;
+    if (int st = build_tables()) return st;
+    drop_graph();
     return ST_OK;
 }
 
@@ -132,7 +153,11 @@ int Batch::launch_step(int step)
         if (int st = x->launch_sources_on(stream)) return st;
     int FB1 = FB_BATCH[step % 8][0], FB2 = FB_BATCH[step % 8][1], FB3 = FB_BATCH[step % 8][2];
     for (int irk = 0; irk < 4; irk++) {
-        BCU(launch_cg_stage_batch(FB1, FB2, FB3, desc_[irk], items_, (int)s.size(), work_, grid_ctas_, stream));
+        if (tile_ == 8)
+            BCU(ty8::launch_cg_stage_batch(FB1, FB2, FB3, desc_[irk], items_, (int)s.size(), work_, grid_ctas_,
+                                           stream));
+        else
+            BCU(launch_cg_stage_batch(FB1, FB2, FB3, desc_[irk], items_, (int)s.size(), work_, grid_ctas_, stream));
         FB1 = -FB1, FB2 = -FB2, FB3 = -FB3;
     }
     for (Session *x : s)

@@ -20,6 +20,10 @@ public:
     // item (every session) and persistent CTAs
     int set_tiling(int kchunk, int ctas);
     int autotune(int trial_steps, int *kchunk, int *ctas, float *ms_per_step);
+    // rows of the column tiles of every session's stage (4 or 8; ring
+    // pipeline either way)
+    int set_tile(int rows);
+    int tile() const { return tile_; }
 
     std::vector<Session *> s;
     int device = 0;
@@ -34,6 +38,7 @@ private:
     int build_tables();                         // descriptor table, item prefix, CTA count
     void drop_graph();
     int want_ctas_ = 0;                         // requested persistent CTAs (0: all resident)
+    int tile_ = 4;
     CgStageDesc *desc_[4] = {};
     int *items_ = nullptr;
     int *work_ = nullptr;

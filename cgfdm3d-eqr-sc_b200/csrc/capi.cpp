@@ -406,6 +406,19 @@ int cgfdm_batch_autotune(cgfdm_batch *b, int trial_steps, int *kchunk, int *ctas
     return b->b.autotune(trial_steps, kchunk, ctas, ms_per_step);
 }
 
+int cgfdm_batch_set_stage_tile(cgfdm_batch *b, int rows)
+{
+    if (!b) return CGFDM_E_ARG;
+    return b->b.set_tile(rows);
+}
+
+int cgfdm_batch_get_stage_tile(const cgfdm_batch *b, int *rows)
+{
+    if (!b || !rows) return CGFDM_E_ARG;
+    *rows = b->b.tile();
+    return CGFDM_OK;
+}
+
 int cgfdm_gradient_profile(const cgfdm_session *s, float *ms3)
 {
     if (!s || !ms3) return CGFDM_E_ARG;

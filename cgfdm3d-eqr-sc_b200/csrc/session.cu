@@ -334,14 +334,13 @@ int Session::setup_device()
     // tile height: 32 x 8 for the FP32 split pipeline of a whole grid
     // (measured faster), 32 x 4 for the ring pipeline's users
     if (cg) {
-        const bool eight_ok = m.p.stage_split && !mix_ && !part_session_;
         if (m.p.stage_tile != 0 && m.p.stage_tile != 4 && m.p.stage_tile != 8) {
             err = "\"stageTile\" is 4 or 8 (rows of 32-column stage tiles)";
             return ST_OPTIONS;
         }
-        tile_ = m.p.stage_tile ? m.p.stage_tile : (eight_ok ? 8 : 4);
-        if (tile_ == 8 && !eight_ok) {
-            err = "32 x 8 stage tiles need the FP32 split pipeline of a whole grid";
+        tile_ = m.p.stage_tile ? m.p.stage_tile : (m.p.stage_split && !mix_ && !part_session_ ? 8 : 4);
+        if (tile_ == 8 && (mix_ || part_session_)) {
+            err = "32 x 8 stage tiles need FP32 storage and a whole grid";
             return ST_OPTIONS;
         }
     }
@@ -571,8 +570,8 @@ int Session::set_tile(int rows)
         return ST_ARG;
     }
     if (m.p.scheme != SCHEME_CGFDM || rows == tile_) return ST_OK;
-    if (rows == 8 && !(m.p.stage_split && !mix_ && !part_session_)) {
-        err = "32 x 8 stage tiles need the FP32 split pipeline of a whole grid";
+    if (rows == 8 && (mix_ || part_session_)) {
+        err = "32 x 8 stage tiles need FP32 storage and a whole grid";
         return ST_OPTIONS;
     }
     tile_ = rows;
@@ -596,7 +595,8 @@ int Session::launch_stage(int FB1, int FB2, int FB3, const CgStageDesc &d)
         e = tile_ == 8 ? ty8::launch_cg_stage_split(FB1, FB2, FB3, d, work_dev_, grid_ctas_, stream)
                        : launch_cg_stage_split(FB1, FB2, FB3, d, work_dev_, grid_ctas_, stream);
     else
-        e = launch_cg_stage(FB1, FB2, FB3, d, work_dev_, grid_ctas_, stream);
+        e = tile_ == 8 ? ty8::launch_cg_stage(FB1, FB2, FB3, d, work_dev_, grid_ctas_, stream)
+                       : launch_cg_stage(FB1, FB2, FB3, d, work_dev_, grid_ctas_, stream);
     if (e != cudaSuccess) return cuda_fail(e, "stage launch");
     return ST_OK;
 }

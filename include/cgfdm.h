@@ -270,12 +270,14 @@ int cgfdm_gradient_profile(const cgfdm_session *s, float *ms3);
  * bit-identical for every tiling.  cgfdm_set_tiling / cgfdm_get_tiling set
  * and read the pencil and CTAs directly (ctas is clamped to the resident
  * maximum and the work items); cgfdm_set_stage_tile / cgfdm_get_stage_tile
- * the tile height (8 rows only with the FP32 split pipeline of a whole grid:
- * CGFDM_E_OPTIONS otherwise; the default is 8 there and 4 elsewhere).
- * cgfdm_batch_autotune does the same for a batch's shared launch, trying
- * one pencil length for all its sessions against their own default ones
- * (*kchunk = 0 when those are kept).  A candidate replaces the current
- * decomposition only when faster by more than 1 %. */
+ * the tile height (8 rows only with FP32 storage on a whole grid, not a
+ * part: CGFDM_E_OPTIONS otherwise; the default is 8 on the split pipeline
+ * and 4 elsewhere).  cgfdm_batch_autotune does the same for a batch's
+ * shared launch, trying both tile heights and one pencil length for all its
+ * sessions against their own default ones (*kchunk = 0 when those are
+ * kept); cgfdm_batch_set_stage_tile / cgfdm_batch_get_stage_tile set and
+ * read the batch's tile height (4 by default).  A candidate replaces the
+ * current decomposition only when faster by more than 1 %. */
 int cgfdm_autotune(cgfdm_session *s, int trial_steps, int *kchunk, int *ctas, float *ms_per_step);
 int cgfdm_set_tiling(cgfdm_session *s, int kchunk, int ctas);
 int cgfdm_get_tiling(const cgfdm_session *s, int *kchunk, int *ctas);
@@ -298,6 +300,8 @@ int cgfdm_batch_run(cgfdm_batch *b, int nsteps);
 int cgfdm_batch_run_timed(cgfdm_batch *b, int nsteps, float *ms);
 int cgfdm_batch_destroy(cgfdm_batch *b);
 int cgfdm_batch_autotune(cgfdm_batch *b, int trial_steps, int *kchunk, int *ctas, float *ms_per_step);
+int cgfdm_batch_set_stage_tile(cgfdm_batch *b, int rows);
+int cgfdm_batch_get_stage_tile(const cgfdm_batch *b, int *rows);
 /* Last failure of b, or of the last failed cgfdm_batch_create in this
  * thread when b is NULL. */
 const char *cgfdm_batch_last_error(const cgfdm_batch *b);

@@ -58,13 +58,20 @@ def test_stage_tile_heights(tmp_path):
         with pytest.raises(CgfdmError) as e:
             s.set_stage_tile(6)
         assert e.value.code == E_ARG
-    for opts in ('{"stagePipeline": "ring"}', '{"storage": "fp16"}'):
-        with Session(d, options=opts) as s:
-            assert s.stage_tile() == 4
-            with pytest.raises(CgfdmError) as e:
-                s.set_stage_tile(8)
-            assert e.value.code == E_OPTIONS
-    for opts in ('{"stagePipeline": "ring", "stageTile": 8}', '{"stageTile": 6}'):
+    with Session(d, options='{"stagePipeline": "ring"}') as s:
+        # the ring pipeline runs 32 x 4 tiles unless asked for 8 rows
+        assert s.stage_tile() == 4
+        s.run(9)
+        s.set_stage_tile(8)
+        s.run(s.info.NT)
+        for a, r in zip((s.stations(), s.wavefield(), s.pgv()), ref):
+            np.testing.assert_array_equal(a, r)
+    with Session(d, options='{"storage": "fp16"}') as s:
+        assert s.stage_tile() == 4
+        with pytest.raises(CgfdmError) as e:
+            s.set_stage_tile(8)
+        assert e.value.code == E_OPTIONS
+    for opts in ('{"storage": "fp16", "stageTile": 8}', '{"stageTile": 6}'):
         with pytest.raises(CgfdmError) as e:
             Session(d, options=opts)
         assert e.value.code == E_OPTIONS
@@ -84,7 +91,9 @@ def test_batch_autotune_keeps_results(tmp_path):
         with Batch(sessions) as b:
             b.run(3)
             kc, ctas, ms = b.autotune(2)
-            assert kc >= 0 and ctas >= 1 and ms > 0
+            assert kc >= 0 and ctas >= 1 and ms > 0 and b.stage_tile() in (4, 8)
+            b.run(4)
+            b.set_stage_tile(12 - b.stage_tile())   # the other height, mid-run
             b.run(100)
         for s, ref in zip(sessions, alone):
             for a, r in zip((s.stations(), s.wavefield(), s.pgv()), ref):
