@@ -344,14 +344,15 @@ def bench_batch(args, world, rank, local_rank):
         configs.batch_shots(root, n=n, steps=total)
         open(marker, "w").close()
     dirs = sorted(os.path.join(root, d) for d in os.listdir(root) if d.startswith("shot_"))
-    sessions = [Session(d, device=local_rank) for d in dirs]
+    sessions = [Session(d, options=session_options(args), device=local_rank) for d in dirs]
     pts = sum(s.info.nx * s.info.ny * s.info.nz for s in sessions)
     algo = sum(s.info.algo_bytes_per_step for s in sessions)
     b = Batch(sessions)
     b.run(args.warmup)
     # the default decomposition, then the autotuner's choice (timed below)
     ms_default = b.run_timed(8)
-    tuned = b.autotune(3)
+    # (FP16 storage: no autotuner, whose trials restore a device copy of the state)
+    tuned = b.autotune(3) if args.storage == "fp32" else (0, None, ms_default / 8)
     tuned_tile = b.stage_tile()
     b.run(1)
     torch.cuda.synchronize(local_rank)
@@ -382,6 +383,8 @@ def bench_batch(args, world, rank, local_rank):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic", "scheme": "CGFDM",
+        "storage": ("fp32" if args.storage == "fp32" else
+                    "fp16 stage/accumulator deltas (per-field scales) + fp32 step state; f32 arithmetic"),
         "config": {"workload": f"{n} CGFDM shots of uneven sizes (64-256 x 64-256 x 64-128, DH=100 m), layered "
                                "media, terrain <= 1 km, random moment tensors, 32 stations each, one persistent "
                                "stage launch per RK stage for all shots, 8-step CUDA graphs",

@@ -195,6 +195,12 @@ int Batch::set_tiling(int kc, int ctas)
 
 int Batch::autotune(int trial, int *best_kc, int *best_ctas, float *best_ms)
 {
+    if (mix_) {
+        // its trials restore the state from a device copy, which FP16
+        // storage does not offer (as for a single session)
+        err = "autotune is not available with FP16 storage";
+        return ST_OPTIONS;
+    }
     trial = std::min(trial, remaining() - 1);
     if (trial < 1) {
         err = "too few steps left to tune on";

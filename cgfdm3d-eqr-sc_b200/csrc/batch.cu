@@ -34,8 +34,11 @@ Batch::~Batch()
 {
     if (graph8_) cudaGraphExecDestroy(graph8_);
     if (graph8_src_) cudaGraphDestroy(graph8_src_);
-    for (int irk = 0; irk < 4; irk++)
+    for (int irk = 0; irk < 4; irk++) {
         if (desc_[irk]) cudaFree(desc_[irk]);
+        for (int par = 0; par < 2; par++)
+            if (descm_[par][irk]) cudaFree(descm_[par][irk]);
+    }
     if (items_) cudaFree(items_);
     if (work_) cudaFree(work_);
     if (ev_[0]) cudaEventDestroy(ev_[0]);
@@ -69,7 +72,12 @@ int Batch::create(const std::vector<Session *> &sessions)
             err = "batch sessions cannot write snapshots";
             return ST_ARG;
         }
+        if (x->mixed() != s[0]->mixed()) {
+            err = "batch sessions must share one storage (FP32 or FP16)";
+            return ST_OPTIONS;
+        }
     }
+    mix_ = s[0]->mixed();
     BCU(cudaSetDevice(device));
     for (Session *x : s) BCU(cudaStreamSynchronize(x->stream));
     // the batched launch runs the ring kernel, 32 x 4 tiles unless set_tile
@@ -84,6 +92,9 @@ int Batch::create(const std::vector<Session *> &sessions)
     BCU(cudaEventCreate(&ev_[1]));
     const int n = (int)s.size();
     for (int irk = 0; irk < 4; irk++) BCU(cudaMalloc(&desc_[irk], sizeof(CgStageDesc) * n));
+    if (mix_)
+        for (int par = 0; par < 2; par++)
+            for (int irk = 0; irk < 4; irk++) BCU(cudaMalloc(&descm_[par][irk], sizeof(CgStageDesc) * n));
     BCU(cudaMalloc(&items_, sizeof(int) * (n + 1)));
     BCU(cudaMalloc(&work_, sizeof(int) * 2));
     BCU(cudaMemset(work_, 0, sizeof(int) * 2));
@@ -104,10 +115,17 @@ int Batch::build_tables()
         for (int i = 0; i < n; i++) s[i]->stage_desc(irk, d[i]);
         BCU(cudaMemcpy(desc_[irk], d.data(), sizeof(CgStageDesc) * n, cudaMemcpyHostToDevice));
     }
+    if (mix_)
+        for (int par = 0; par < 2; par++)
+            for (int irk = 0; irk < 4; irk++) {
+                for (int i = 0; i < n; i++) s[i]->stage_desc_mix(par, irk, d[i]);
+                BCU(cudaMemcpy(descm_[par][irk], d.data(), sizeof(CgStageDesc) * n, cudaMemcpyHostToDevice));
+            }
     BCU(cudaMemcpy(items_, items.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const int full = sms * (tile_ == 8 ? ty8::cg_stage_ctas_per_sm() : cg_stage_ctas_per_sm());
+    const int full =
+        sms * (mix_ ? cg_stage_mix_ctas_per_sm() : tile_ == 8 ? ty8::cg_stage_ctas_per_sm() : cg_stage_ctas_per_sm());
     grid_ctas_ = std::min(want_ctas_ > 0 ? std::min(want_ctas_, full) : full, items[n]);
     return ST_OK;
 }
@@ -153,7 +171,10 @@ int Batch::launch_step(int step)
         if (int st = x->launch_sources_on(stream)) return st;
     int FB1 = FB_BATCH[step % 8][0], FB2 = FB_BATCH[step % 8][1], FB3 = FB_BATCH[step % 8][2];
     for (int irk = 0; irk < 4; irk++) {
-        if (tile_ == 8)
+        if (mix_)
+            BCU(launch_cg_stage_batch_mix(FB1, FB2, FB3, descm_[step & 1][irk], items_, (int)s.size(), work_,
+                                          grid_ctas_, stream));
+        else if (tile_ == 8)
             BCU(ty8::launch_cg_stage_batch(FB1, FB2, FB3, desc_[irk], items_, (int)s.size(), work_, grid_ctas_,
                                            stream));
         else

@@ -39,6 +39,8 @@ private:
     void drop_graph();
     int want_ctas_ = 0;                         // requested persistent CTAs (0: all resident)
     int tile_ = 4;
+    bool mix_ = false;                          // FP16 storage (every session)
+    CgStageDesc *descm_[2][4] = {};             // mixed storage: per step parity
     CgStageDesc *desc_[4] = {};
     int *items_ = nullptr;
     int *work_ = nullptr;

@@ -439,10 +439,6 @@ int cgfdm_batch_create(cgfdm_session *const *sessions, int n, cgfdm_batch **out)
             g_create_error = "NULL session in batch";
             return CGFDM_E_ARG;
         }
-        if (sessions[i]->s.mixed()) {
-            g_create_error = "a batch advances FP32-storage sessions";
-            return CGFDM_E_OPTIONS;
-        }
         v.push_back(&sessions[i]->s);
     }
     cgfdm_batch *h = new (std::nothrow) cgfdm_batch;

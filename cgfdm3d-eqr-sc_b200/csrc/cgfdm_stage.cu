@@ -479,33 +479,49 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
     const int cell = (ty + hyL) * BXW + tx + 4;
     const int total = BATCH ? item_start[nsess] : d1.a.ntiles_x * d1.a.ntiles_y * d1.a.nchunk;
     int sess = -1;
+    // mixed storage (one thread): per-field scales of this step from the
+    // bounds of the session's step-start state -- the bound of field f
+    // maps below 2^13
+    auto mix_scales = [&](const CgStageArgs &A0) {
+        const int p = *A0.it_dev & 1;
+        s_par = p;
+        float M[9], Mv = 0.0f, Ms = 0.0f;
+        for (int f = 0; f < 9; f++) {
+            M[f] = __uint_as_float(A0.mx[p * 9 + f]);
+            if (f < 3 && M[f] > Mv) Mv = M[f];
+            if (f >= 3 && M[f] > Ms) Ms = M[f];
+        }
+        for (int f = 0; f < 9; f++) {
+            const float c = f < 3 ? Ms / A0.zs_min : Mv * A0.zp_max;
+            const float b = M[f] > c ? M[f] : c;
+            int e = 0;
+            if (b > 0.0f) frexpf(b, &e);
+            s_sc[f] = b > 0.0f ? ldexpf(1.0f, 13 - e) : 1.0f;
+            s_inv[f] = b > 0.0f ? ldexpf(1.0f, e - 13) : 1.0f;
+        }
+    };
+    // mixed storage, stage 3 (all threads): this CTA's maxima of the new
+    // state raise the bounds of the session's next step
+    auto mix_flush = [&](const CgStageArgs &A0, float *r) {
+        if (A0.irk != 3) return;
+#pragma unroll 1
+        for (int f = 0; f < 9; f++) {
+            float v = r[f];
+            for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+            if ((tid & 31) == 0 && v > 0.0f) atomicMax(&A0.mx[(s_par ^ 1) * 9 + f], __float_as_uint(v));
+            r[f] = 0.0f;
+        }
+    };
 
     if (tid == 0) {
         s_abort = 0;
         for (int s = 0; s < (V2 ? NHSLOT + NCSLOT + 1 : NSLOT); s++) mbar_init(smem_u32(&bars[s]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-        if constexpr (MIX) {
-            // per-field scales of this step: the bound of field f maps below 2^13
-            const CgStageArgs &A0 = d1.a;
-            const int p = *A0.it_dev & 1;
-            s_par = p;
-            float M[9], Mv = 0.0f, Ms = 0.0f;
-            for (int f = 0; f < 9; f++) {
-                M[f] = __uint_as_float(A0.mx[p * 9 + f]);
-                if (f < 3 && M[f] > Mv) Mv = M[f];
-                if (f >= 3 && M[f] > Ms) Ms = M[f];
-            }
-            for (int f = 0; f < 9; f++) {
-                const float c = f < 3 ? Ms / A0.zs_min : Mv * A0.zp_max;
-                const float b = M[f] > c ? M[f] : c;
-                int e = 0;
-                if (b > 0.0f) frexpf(b, &e);
-                s_sc[f] = b > 0.0f ? ldexpf(1.0f, 13 - e) : 1.0f;
-                s_inv[f] = b > 0.0f ? ldexpf(1.0f, e - 13) : 1.0f;
-            }
+        if constexpr (MIX && !BATCH) {
+            mix_scales(d1.a);
             // the next step's bounds start from zero; stage 3 raises them
-            if (A0.irk == 0 && blockIdx.x == 0)
-                for (int f = 0; f < 9; f++) A0.mx[(p ^ 1) * 9 + f] = 0u;
+            if (d1.a.irk == 0 && blockIdx.x == 0)
+                for (int f = 0; f < 9; f++) d1.a.mx[((s_par) ^ 1) * 9 + f] = 0u;
         }
     }
     unsigned seq0 = 0;  // fills issued by this CTA before the current item
@@ -525,11 +541,26 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
         int ns = 0;
         while (ns + 1 < nsess && gitem >= item_start[ns + 1]) ns++;
         if (ns != sess) {
+            if constexpr (MIX) {
+                // the previous session's maxima go to its bounds first
+                if (sess >= 0) mix_flush(s_args, rm);
+                __syncthreads();
+            }
             sess = ns;
             const int *src = reinterpret_cast<const int *>(&descs[sess].a);
             int *dst = reinterpret_cast<int *>(&s_args);
             for (int w = tid; w < (int)(sizeof(CgStageArgs) / 4); w += TX * TY) dst[w] = src[w];
             __syncthreads();
+            if constexpr (MIX) {
+                if (tid == 0) {
+                    mix_scales(s_args);
+                    // the CTA with the session's first item resets its next
+                    // step's bounds (stage 3, a later launch, raises them)
+                    if (s_args.irk == 0 && gitem == item_start[sess])
+                        for (int f = 0; f < 9; f++) s_args.mx[(s_par ^ 1) * 9 + f] = 0u;
+                }
+                __syncthreads();
+            }
         }
     } else {
         sess = 0;
@@ -1118,13 +1149,8 @@ __global__ void __launch_bounds__(TX *TY, MIX ? CG_MIX_CTAS_PER_SM : CG_CTAS_PER
 
     if constexpr (MIX) {
         // stage 3: raise the bounds of the next step with this CTA's maxima
-        if (d1.a.irk == 3)
-#pragma unroll 1
-            for (int f = 0; f < 9; f++) {
-                float v = rm[f];
-                for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-                if ((tid & 31) == 0 && v > 0.0f) atomicMax(&d1.a.mx[(s_par ^ 1) * 9 + f], __float_as_uint(v));
-            }
+        if (!BATCH) mix_flush(d1.a, rm);
+        else if (sess >= 0) mix_flush(s_args, rm);
     }
     // the last CTA out resets the work counter for the next launch
     __syncthreads();
@@ -1186,6 +1212,13 @@ cudaError_t launch_cg_stage_split(int FB1, int FB2, int FB3, const CgStageDesc &
 cudaError_t launch_cg_stage_mix(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int ctas, cudaStream_t st)
 {
     return launch_b<false, false, true>(FB1, FB2, FB3, d, nullptr, nullptr, 1, work, ctas, st);
+}
+
+cudaError_t launch_cg_stage_batch_mix(int FB1, int FB2, int FB3, const CgStageDesc *descs, const int *item_start,
+                                      int nsess, int *work, int ctas, cudaStream_t st)
+{
+    static const CgStageDesc unused{};
+    return launch_b<true, false, true>(FB1, FB2, FB3, unused, descs, item_start, nsess, work, ctas, st);
 }
 
 cudaError_t make_field_tmap16(void *out, const __half *base, const DevGrid &gh, int nf)

@@ -136,7 +136,8 @@ struct alignas(64) CgStageDesc {
 // memory; all advance with the same FB signs and stage number.
 // launch_cg_stage_split: the split pipeline (the current plane's halo box,
 // interior column boxes for the z window): one session's FP32 stage.
-// launch_cg_stage_mix: mixed-precision storage (the MIX instantiation).
+// launch_cg_stage_mix: mixed-precision storage (the MIX instantiation);
+// launch_cg_stage_batch_mix: the same for a batch of such sessions.
 // make_field_tmap16: FP16 counterpart of make_field_tmap (halo box), for
 // arrays in the layout gh.  launch_impedance_bounds: smallest S and largest
 // P impedance, sqrt(mu / b) and sqrt((lambda + 2 mu) / b), over the interior,
@@ -155,6 +156,9 @@ struct alignas(64) CgStageDesc {
                                       cudaStream_t st);                                                          \
     cudaError_t launch_cg_stage_mix(int FB1, int FB2, int FB3, const CgStageDesc &d, int *work, int grid_ctas,  \
                                     cudaStream_t st);                                                            \
+    cudaError_t launch_cg_stage_batch_mix(int FB1, int FB2, int FB3, const CgStageDesc *descs,                  \
+                                          const int *item_start, int nsess, int *work, int grid_ctas,           \
+                                          cudaStream_t st);                                                      \
     int cg_stage_mix_ctas_per_sm();                                                                             \
     cudaError_t make_field_tmap16(void *out, const __half *base, const DevGrid &gh, int nf);                    \
     cudaError_t launch_impedance_bounds(const float *cjm, DevGrid g, unsigned *out, cudaStream_t st);           \

@@ -166,7 +166,6 @@ private:
     DevGrid gh_{};
     float zs_min_ = 0, zp_max_ = 0;
     CgStageDesc desc_mix_[2][4] = {};
-    void stage_desc_mix(int parity, int irk, CgStageDesc &d) const;
     int tile_ = 4;
     int build_maps();                                // tensor maps of the stencil inputs for tile_
     int stage_ctas_per_sm() const;
@@ -177,7 +176,7 @@ private:
 public:
     // Column-tile height of the CGFDM stage kernel (4 or 8 rows of 32), the
     // tensor maps and work items built for it; set_tile re-encodes them
-    // (8 only with the FP32 split pipeline of a whole-grid session)
+    // (8 only with FP32 storage on a whole grid)
     int tile() const { return tile_; }
     int set_tile(int rows);
     // one RK stage of this session's CGFDM step, with the pipeline and tile
@@ -193,8 +192,11 @@ public:
     // copy number `fill` unissued, once, and every bounded wait of the stage
     // kernel gives up after `wait_cycles` clocks (0: the default limit).
     int test_stall(int item, int fill, long long wait_cycles);
-    // the stage descriptor of RK stage irk, and the stage's work items (batches use these)
+    // the stage descriptor of RK stage irk (with FP16 storage: for the
+    // step-start state of step parity `parity`), and the stage's work items
+    // (batches use these)
     void stage_desc(int irk, CgStageDesc &d) const;
+    void stage_desc_mix(int parity, int irk, CgStageDesc &d) const;
     int stage_items() const;
     int pml_faces() const;
     int launch_sources_on(cudaStream_t st);

@@ -288,7 +288,9 @@ int cgfdm_get_stage_tile(const cgfdm_session *s, int *rows);
  * grid sizes -- advanced together, every RK stage of all of them in one
  * persistent launch of the fused stage kernel, eight steps per replay of a
  * captured CUDA graph.  The sessions must be CGFDM, on one device, at the
- * same step, without snapshots; they stay owned by the caller and must
+ * same step, without snapshots, all with FP32 or all with FP16 storage
+ * ("storage": "fp16"; such a batch takes 32 x 4 tiles and no autotuning,
+ * CGFDM_E_OPTIONS otherwise); they stay owned by the caller and must
  * outlive the batch, and while batched they are stepped only through it
  * (cgfdm_batch_run advances each by min(nsteps, steps left to the shortest
  * NT)).  Results per session are those of running it alone, bit for bit.

@@ -49,3 +49,40 @@ def test_batch_detects_solo_step(tmp_path):
     finally:
         for s in sessions:
             s.close()
+
+
+@pytest.mark.gpu
+def test_fp16_storage_batch_matches_single_runs(tmp_path):
+    """Sessions with FP16 storage (FP32 step state, per-field-scaled FP16
+    stage and accumulator deltas) batched together: each shot's traces,
+    wavefield and PGV are bit-identical to its own run with the same
+    storage; the per-field scales and the bounds they come from stay per
+    session inside the shared launch.  A batch mixing both storages is
+    refused."""
+    fp16 = '{"storage": "fp16"}'
+    dirs = _shots(tmp_path)
+    alone = []
+    for d in dirs:
+        with Session(d, options=fp16) as s:
+            s.run(s.info.NT)
+            alone.append((s.stations(), s.wavefield(), s.pgv()))
+    sessions = [Session(d, options=fp16) for d in dirs]
+    try:
+        with Batch(sessions) as b:
+            b.run(5)
+            b.run(100)
+        for s, ref in zip(sessions, alone):
+            assert s.info.steps_done == s.info.NT
+            for a, r in zip((s.stations(), s.wavefield(), s.pgv()), ref):
+                np.testing.assert_array_equal(a, r)
+    finally:
+        for s in sessions:
+            s.close()
+    both = [Session(dirs[0], options=fp16), Session(dirs[1])]
+    try:
+        with pytest.raises(CgfdmError) as e:
+            Batch(both)
+        assert e.value.code == 180
+    finally:
+        for s in both:
+            s.close()
