@@ -185,6 +185,7 @@ int cgfdm_model_coord(const char *run_dir, const char *options_json, float *terr
         return st;
     }
     if (dims) dims[0] = m.g._nz_, dims[1] = m.g._ny_, dims[2] = m.g._nx_;
+    if (coord) cgfdm::materialize_coords(m);
     if ((terrain && terrain_count < (long long)m.terrain.size()) || (coord && coord_count < (long long)m.coord.size())) {
         g_create_error = "output array too small";
         return CGFDM_E_ARG;

@@ -120,6 +120,7 @@ int Session::set_medium(const float *host)
     }
     m.Vp_max = vpmax;
     m.dtmax = (float)(1.34 * m.H_min / m.Vp_max);
+    materialize_coords(m);   // the set-up kernels take the coordinate volume
     float *d_coord = nullptr, *d_med = nullptr;
     CU(cudaMalloc(&d_coord, sizeof(float) * npad * 3));
     cudaError_t e = cudaMalloc(&d_med, sizeof(float) * npad * 3);

@@ -185,6 +185,7 @@ int Session::create_part(const std::string &dir, const std::string &options, con
     Model G;
     int st = build_model(dir, options, G, err);
     if (st) return st;
+    materialize_coords(G);   // the part receives its slice of the volume
     if ((st = slice_model(G, parts, coord, m, err))) return st;
     if (m.p.storage != "fp32") {
         err = "a part of a decomposed grid stores its wavefield in FP32";

@@ -195,15 +195,61 @@ Grid make_grid(const Params &p)
 
 // ------------------------------------------------------------ coordinates
 // Flat grid (src/coord.cpp:99-134), single Gauss hill (:136-177) and the
-// terrain-following z of src/coord.cpp:204-255.
-static void build_coords(Model &m)
+// terrain-following z of src/coord.cpp:204-255.  Each coordinate is
+// computed by coord_at from the grid, the terrain and the mode, in the same
+// operations and types as the filled volume, so both ways give the same
+// floats.
+float Model::coord_at(int i, int j, int k, int c) const
+{
+    if (!coord_lazy) return coord[(size_t)g.idx(i, j, k) * 3 + c];
+    const float DH = g.DH;
+    const int NZ = g.NZ;
+    if (c == 0) return (i - HALO) * DH - g.originalX * DH;
+    if (c == 1) return (j - HALO) * DH - g.originalY * DH;
+    if (coord_mode == 0) return (k - HALO + 1) * DH - NZ * DH;
+    const int K = k - HALO;
+    if (coord_mode == 1) {
+        const float cal_depth = coord_depth_f;
+        const float height = terrain[(size_t)i + (size_t)j * g._nx_];
+        const float DZ = (float)(double(height + std::fabs(cal_depth)) / double(NZ - 1));
+        return -std::fabs(cal_depth) + DZ * K;
+    }
+    const double Depth = coord_depth_d;
+    const double DZ = double(terrain[(size_t)i + (size_t)j * g._nx_] + std::fabs(Depth)) / double(NZ - 1);
+    return (float)(-std::fabs(Depth) + DZ * K);
+}
+
+void materialize_coords(Model &m)
+{
+    if (!m.coord_lazy) return;
+    const Grid &g = m.g;
+    m.coord.resize((size_t)g.npad() * 3);   // every value written below
+    par_for(g._nz_, [&](int k) {
+        for (int j = 0; j < g._ny_; j++)
+            for (int i = 0; i < g._nx_; i++)
+                for (int c = 0; c < 3; c++) m.coord[(size_t)g.idx(i, j, k) * 3 + c] = m.coord_at(i, j, k, c);
+    });
+    m.coord_lazy = false;
+}
+
+// lazy: leave the volume to coord_at (the flat mode's terrain is still made)
+static void build_coords(Model &m, bool lazy)
 {
     const Grid &g = m.g;
     const float DH = g.DH;
     const int NZ = g.NZ;
-    m.coord.resize((size_t)g.npad() * 3);   // every value written below
     m.coord_mode = 0;
     m.terrain.assign((size_t)g._nx_ * g._ny_, 0.f);
+    if (lazy) {
+        const int K = NZ + HALO - 1;
+        for (int j = 0; j < g._ny_; j++)
+            for (int i = 0; i < g._nx_; i++) m.terrain[(size_t)i + (size_t)j * g._nx_] = (K - HALO + 1) * DH - NZ * DH;
+        m.coord.clear();
+        m.coord_lazy = true;
+        return;
+    }
+    m.coord.resize((size_t)g.npad() * 3);   // every value written below
+    m.coord_lazy = false;
     par_for(g._nz_, [&](int k) {
         for (int j = 0; j < g._ny_; j++)
             for (int i = 0; i < g._nx_; i++) {
@@ -222,6 +268,7 @@ static void terrain_following_z(Model &m, float cal_depth)
     const Grid &g = m.g;
     m.coord_mode = 1;
     m.coord_depth_f = cal_depth;
+    if (m.coord_lazy) return;
     par_for(g._nz_, [&](int k) {
         for (int j = 0; j < g._ny_; j++)
             for (int i = 0; i < g._nx_; i++) {
@@ -460,6 +507,7 @@ static void terrain_z_double(Model &m)
     const double Depth = m.p.Depth * 1e3;
     m.coord_mode = 2;
     m.coord_depth_d = Depth;
+    if (m.coord_lazy) return;
     par_for(g._nz_, [&](int k) {
         for (int j = 0; j < g._ny_; j++)
             for (int i = 0; i < g._nx_; i++) {
@@ -503,9 +551,8 @@ static int column_lonlat(const Model &m, float lonMin, float lonMax, float latMi
     const int k = g._nz - 1;
     for (int j = 0; j < g._ny_; j++)
         for (int i = 0; i < g._nx_; i++) {
-            const long long id = g.idx(i, j, k) * 3;
             double la, ph;
-            cgfdm_aeqd_inv(lon0, lat0, (double)m.coord[id + 0], (double)m.coord[id + 1], &la, &ph);
+            cgfdm_aeqd_inv(lon0, lat0, (double)m.coord_at(i, j, k, 0), (double)m.coord_at(i, j, k, 1), &la, &ph);
             lon[(size_t)i + (size_t)j * g._nx_] = la * r2d;
             lat[(size_t)i + (size_t)j * g._nx_] = ph * r2d;
         }
@@ -593,9 +640,9 @@ static int shen_medium(Model &m, const std::string &run_dir, std::string &err)
         for (int j = 0; j < g._ny_; j++)
             for (int i = 0; i < g._nx_; i++) {
                 const long long id = g.idx(i, j, k);
-                const double DZ = (double)(m.coord[g.idx(i, j, 4) * 3 + 2] - m.coord[g.idx(i, j, 3) * 3 + 2]);
+                const double DZ = (double)(m.coord_at(i, j, 4, 2) - m.coord_at(i, j, 3, 2));
                 const double top = DZ * double(NZ - 1) - std::fabs(DepthM);
-                int K = (int)((float)int(-((double)m.coord[id * 3 + 2] - top)) / p.MVeticalStep);
+                int K = (int)((float)int(-((double)m.coord_at(i, j, k, 2) - top)) / p.MVeticalStep);
                 if (K <= 0) K = 0;
                 if (K >= NLayer) {
                     err = "a grid point lies below the Shen model's deepest layer";
@@ -692,7 +739,7 @@ static int crust_medium(Model &m, const std::string &run_dir, std::string &err)
             for (int i = 0; i < g._nx_; i++) {
                 const long long id = g.idx(i, j, k);
                 const size_t c = (size_t)i + (size_t)j * g._nx_;
-                const float coordZ = m.coord[id * 3 + 2];
+                const float coordZ = m.coord_at(i, j, k, 2);
                 auto B = [&](int l) { return bnds[(size_t)l * plane + c]; };
                 // the layer above the first boundary at least 1 km below boundary `from`
                 auto take_below = [&](int from) {
@@ -770,7 +817,7 @@ static int build_medium(Model &m, const std::string &run_dir, std::string &err)
             for (int i = 0; i < g._nx_; i++) {
                 long long id = g.idx(i, j, k);
                 double terrain = m.terrain[(size_t)i + (size_t)j * g._nx_];
-                float coordz = m.coord[id * 3 + 2];
+                float coordz = m.coord_at(i, j, k, 2);
                 float *md = &m.medium[id * 3];
                 for (int F = 1; F < layers; ++F) {
                     float h0 = (float)(-hgt[0] + terrain);
@@ -1059,15 +1106,15 @@ static int build_fault(Model &m, const std::string &run_dir, std::string &err)
         int srcX = int(x[i] / DH + 0.5) + g.originalX + HALO;
         int srcY = int(y[i] / DH + 0.5) + g.originalY + HALO;
         if (srcX >= HALO && srcX < g._nx && srcY >= HALO && srcY < g._ny) {
-            double DZ = m.coord[g.idx(srcX, srcY, 4) * 3 + 2] - m.coord[g.idx(srcX, srcY, 3) * 3 + 2];
+            double DZ = m.coord_at(srcX, srcY, 4, 2) - m.coord_at(srcX, srcY, 3, 2);
             double terrain = DZ * double(g.NZ - 1) - std::fabs(Depth);
             z[i] = (float)(terrain + z[i]);
             for (int k = HALO; k < g._nz; k++) {
-                long long index1 = g.idx(srcX, srcY, k - 1), index2 = g.idx(srcX, srcY, k + 1);
                 long long index = g.idx(srcX, srcY, k);
-                double dz1 = (m.coord[index * 3 + 2] - m.coord[index1 * 3 + 2]) * 0.5;
-                double dz2 = (m.coord[index2 * 3 + 2] - m.coord[index * 3 + 2]) * 0.5;
-                if (m.coord[index * 3 + 2] - dz1 <= z[i] && z[i] < dz2 + m.coord[index * 3 + 2]) {
+                const float zk = m.coord_at(srcX, srcY, k, 2);
+                double dz1 = (zk - m.coord_at(srcX, srcY, k - 1, 2)) * 0.5;
+                double dz2 = (m.coord_at(srcX, srcY, k + 1, 2) - zk) * 0.5;
+                if (zk - dz1 <= z[i] && z[i] < dz2 + zk) {
                     point_index[i] = index;
                     pointNum++;
                 }
@@ -1263,7 +1310,7 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
         m.phase_ms[ph] = std::chrono::duration<double, std::milli>(now - tick).count();
         tick = now;
     };
-    build_coords(m);
+    build_coords(m, true);
     if (p.gauss_hill) gauss_hill(m);
     else if (!p.terrainFile.empty()) {
         if ((st = terrain_file(m, join(run_dir, p.terrainFile), err))) return st;

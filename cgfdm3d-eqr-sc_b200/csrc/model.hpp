@@ -167,6 +167,12 @@ struct Model {
     int coord_mode = 0;
     float coord_depth_f = 0;
     double coord_depth_d = 0;
+    // coord not filled: every coordinate follows from the grid, the terrain
+    // and coord_mode, and coord_at computes it (the host model build reads
+    // only a few columns and layers of it); materialize_coords fills coord
+    // for the readers of the whole volume
+    bool coord_lazy = false;
+    float coord_at(int i, int j, int k, int c) const;
     std::vector<float> terrain;      // [_ny_][_nx_]
     std::vector<double> lon, lat;    // [_ny_][_nx_] column longitude, latitude (SRTM90 runs)
     FieldVec medium;                 // [_nz_][_ny_][_nx_][3] Vs Vp rho
@@ -210,6 +216,8 @@ void point_moment(float strike, float dip, float rake, float Mw, float mom[6], f
 // faces at the global boundary only, the free surface in the top layer of
 // parts, sources and stations of the part's interior.  CGFDM only.
 int slice_model(const Model &G, const int parts[3], const int coord[3], Model &m, std::string &err);
+// fills m.coord if it was left to coord_at (no-op otherwise)
+void materialize_coords(Model &m);
 // interior offset and size of part c of n along an axis of N points
 void part_extent(int N, int n, int c, int *lo, int *len);
 

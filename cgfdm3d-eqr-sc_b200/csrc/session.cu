@@ -271,6 +271,7 @@ int Session::setup_device()
                                G.originalY, G.NZ, m.coord_depth_f, m.coord_depth_d, stream));
         h2d_bytes += sizeof(float) * G._nx_ * G._ny_;
     } else {
+        materialize_coords(m);
         CU(upload_h2d(d_coord, m.coord.data(), sizeof(float) * npad * 3, device, stream));
         h2d_bytes += sizeof(float) * npad * 3;
     }
@@ -1081,7 +1082,7 @@ static int write_model_slices(const Model &m, const std::string &out)
     const char *names[6] = {"coordX", "coordY", "coordZ", "Vs", "Vp", "rho"};
     for (int v = 0; v < 6; v++) {
         const FieldVec &src = v < 3 ? m.coord : m.medium;
-        if (src.empty()) continue;
+        if (src.empty() && !(v < 3 && m.coord_lazy)) continue;
         for (int axis = 0; axis < 3; axis++) {
             if (!(idx[axis] >= HALO && idx[axis] < lim[axis])) continue;
             const int n0 = axis == 0 ? G.ny : G.nx, n1 = axis == 2 ? G.ny : G.nz;
@@ -1093,7 +1094,7 @@ static int write_model_slices(const Model &m, const std::string &out)
                     else if (axis == 1) i = a0 + HALO, j = idx[1], k = a1 + HALO;
                     else i = a0 + HALO, j = a1 + HALO, k = idx[2];
                     const long long p = ((long long)k * G._ny_ + j) * G._nx_ + i;
-                    buf[(size_t)a1 * n0 + a0] = src[p * 3 + (v % 3)];
+                    buf[(size_t)a1 * n0 + a0] = v < 3 ? m.coord_at(i, j, k, v) : src[p * 3 + v % 3];
                 }
             std::string path = out + "/" + names[v] + "_" + "XYZ"[axis] + rank_tag(m) + ".bin";
             FILE *fp = std::fopen(path.c_str(), "wb");
