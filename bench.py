@@ -727,7 +727,9 @@ def main():
         dist.barrier()
 
     # ---- device-timed leg: inputs resident on the GPU
+    t_first = time.perf_counter()
     s = Session(d, options=session_options(args), device=local_rank)
+    first_create_s = time.perf_counter() - t_first   # the process's first session (includes one-time costs)
     if args.kchunk:
         s.set_tiling(args.kchunk, s.tiling()[1])
     tiling = s.tiling() + (s.stage_tile(),) if not is_scfdm(args.workload) else None
@@ -806,7 +808,8 @@ def main():
         "e2e": {"value": world * pts * args.steps / e2e_s / 1e6, "unit": METRIC,
                 "h2d_bytes_per_step": i2.h2d_bytes / args.steps, "d2h_bytes_per_step": st.nbytes / args.steps,
                 "seconds": e2e_s, "path": "cgfdm_create(run dir) + cgfdm_run(K) + cgfdm_get_stations + destroy",
-                "split_ms": create_prof, "legs": e2e_legs},
+                "split_ms": create_prof, "legs": e2e_legs,
+                "first_session_create_s": first_create_s},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
