@@ -1232,6 +1232,12 @@ static int read_stations(Model &m, const std::string &run_dir, std::string &err)
 // ------------------------------------------------------------------ model
 int build_model(const std::string &run_dir, const std::string &options_json, Model &m, std::string &err)
 {
+    return build_model(run_dir, options_json, m, err, {});
+}
+
+int build_model(const std::string &run_dir, const std::string &options_json, Model &m, std::string &err,
+                const std::function<void(const Model &)> &medium_ready)
+{
     int st = read_params(join(run_dir, "params.json"), m.p, err);
     if (st) return st;
     if (!options_json.empty()) {
@@ -1329,6 +1335,7 @@ int build_model(const std::string &run_dir, const std::string &options_json, Mod
         if ((st = medium_file(m, join(run_dir, p.mediumFile), err))) return st;
     }
     lap(1);
+    if (medium_ready) medium_ready(m);
     value_ranges(m);
     build_pml(m);
     lap(2);

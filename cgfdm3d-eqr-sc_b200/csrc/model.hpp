@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <string>
 #include <type_traits>
@@ -247,5 +248,9 @@ void part_extent(int N, int n, int c, int *lo, int *len);
 // PML profiles, sources and stations.  Metrics are computed on the GPU
 // (metrics.cu) from coord and medium.
 int build_model(const std::string &run_dir, const std::string &options_json, Model &m, std::string &err);
+// As above; medium_ready(m) is called once m.medium is complete (the rest of
+// the build only reads it), so a caller can start its upload meanwhile.
+int build_model(const std::string &run_dir, const std::string &options_json, Model &m, std::string &err,
+                const std::function<void(const Model &)> &medium_ready);
 
 }  // namespace cgfdm

@@ -85,6 +85,7 @@ __global__ void k_hrange(const float *__restrict__ coord, int nxp, int nyp, int 
 // ----------------------------------------------------------------- util
 Session::~Session()
 {
+    if (med_thread_.joinable()) med_thread_.join();
     if (counted_) arena_session_remove(device);
     if (graph8_) cudaGraphExecDestroy(graph8_);
     if (graph8_src_) cudaGraphDestroy(graph8_src_);
@@ -124,6 +125,9 @@ void *Session::alloc(size_t bytes)
 }
 
 // --------------------------------------------------------------- create
+#ifndef CG_MEDIUM_OVERLAP
+#define CG_MEDIUM_OVERLAP 1   // the medium upload overlaps the rest of the host model build
+#endif
 static double ms_since(std::chrono::steady_clock::time_point t0)
 {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -134,7 +138,31 @@ int Session::create(const std::string &dir, const std::string &options, int dev)
     const auto t0 = std::chrono::steady_clock::now();
     run_dir = dir;
     device = dev;
-    int st = build_model(dir, options, m, err);
+    // a large medium volume starts its way to the device as soon as it is
+    // read, while the host model build goes on (ranges, PML profiles,
+    // sources, stations)
+    auto medium_ready = [&](const Model &mm) {
+        if (!CG_MEDIUM_OVERLAP) return;
+        const size_t bytes = sizeof(float) * (size_t)mm.g.npad() * 3;
+        if (bytes < (size_t(64) << 20) || mm.medium.size() * sizeof(float) < bytes) return;
+        float *p = nullptr;
+        if (cudaSetDevice(dev) != cudaSuccess || cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return;   // setup_device uploads it then
+        }
+        pre_med_ = p;
+        allocs_.push_back(p);
+        device_bytes += bytes;
+        const float *src = mm.medium.data();
+        med_thread_ = std::thread([this, p, src, bytes, dev] {
+            cudaStream_t st = nullptr;
+            med_err_ = cudaSetDevice(dev);
+            if (med_err_ == cudaSuccess) med_err_ = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+            if (med_err_ == cudaSuccess) med_err_ = upload_h2d(p, src, bytes, dev, st);
+            if (st) cudaStreamDestroy(st);
+        });
+    };
+    int st = build_model(dir, options, m, err, medium_ready);
     if (st) return st;
     create_ms[0] = ms_since(t0);
     // the reference builds that exist: CGFDM with PML (Makefile_CGFDM), SCFDM
@@ -235,7 +263,10 @@ int Session::setup_device()
     const auto t0 = std::chrono::steady_clock::now();
     float *d_coord, *d_med;
     ALLOC(d_coord, float, npad * 3);
-    ALLOC(d_med, float, npad * 3);
+    if (pre_med_)
+        d_med = pre_med_;   // already on its way (Session::create)
+    else
+        ALLOC(d_med, float, npad * 3);
     if (mix_) {
         // FP16 arrays: first interior column on a 16-byte boundary in the TMA
         // halo box (xoff 33: column i0 - 4 = 32 + 32 n), rows of 16 bytes
@@ -275,7 +306,12 @@ int Session::setup_device()
         CU(upload_h2d(d_coord, m.coord.data(), sizeof(float) * npad * 3, device, stream));
         h2d_bytes += sizeof(float) * npad * 3;
     }
-    CU(upload_h2d(d_med, m.medium.data(), sizeof(float) * npad * 3, device, stream));
+    if (pre_med_) {
+        if (med_thread_.joinable()) med_thread_.join();
+        if (med_err_ != cudaSuccess) return cuda_fail(med_err_, "medium upload");
+    } else {
+        CU(upload_h2d(d_med, m.medium.data(), sizeof(float) * npad * 3, device, stream));
+    }
     h2d_bytes += sizeof(float) * npad * 3;
     CU(cudaStreamSynchronize(stream));
     setup_ms[4] = ms_since(t0) - setup_ms[3];   // the uploads

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "device.cuh"
@@ -127,6 +128,11 @@ private:
     // on 256-byte boundaries): freeing some 30 separate arrays of an 8 GB
     // session took 50-200 ms, one block 6 ms.  Arrays that do not fit (or
     // that are made after set-up) get their own allocation.
+    // the medium volume's upload, started while the host model build goes on
+    // (large volumes only): its device buffer, the thread and its status
+    float *pre_med_ = nullptr;
+    std::thread med_thread_;
+    cudaError_t med_err_ = cudaSuccess;
     char *arena_ = nullptr;
     size_t arena_size_ = 0, arena_used_ = 0;
     size_t arena_estimate() const;
