@@ -171,20 +171,22 @@ def _terrain_case(kind):
     c.stations = [(20, 20, c.NZ - 1), (40, 30, c.NZ - 1)]
     c.layers = ()
     c.center_lon, c.center_lat = 102.5, 32.5
-    c.extra = dict(c.extra, useTerrain=1, SRTM90=int(kind == "srtm"), TerrainDir="./terrain",
-                   lonStart=100, latStart=30, blockX=1, blockY=1)
-    if kind == "gauss":
+    c.extra = dict(c.extra, useTerrain=int(kind != "gauss_float"), SRTM90=int(kind == "srtm"),
+                   TerrainDir="./terrain", lonStart=100, latStart=30, blockX=1, blockY=1)
+    if kind in ("gauss", "gauss_float"):
         c.gauss_hill = 1
     return c
 
 
-@pytest.mark.parametrize("kind", ["flat", "gauss", "srtm"])
+@pytest.mark.parametrize("kind", ["flat", "gauss", "srtm", "gauss_float"])
 def test_terrain_host_matches_reference(tmp_path, kind):
     """useTerrain (src/coord.cpp:325-328, src/terrain.cpp:772-858) on the
     CPU: the SRTM90 surface (tiles read, despiked and smoothed around the
     model, interpolated to every column and smoothed again) and the
     terrain-following z of every point, against the reference's CPU build,
-    bit for bit; "flat" and "gauss" apply only the z mapping."""
+    bit for bit; "flat" and "gauss" apply only the z mapping, and
+    "gauss_float" the Gauss hill without useTerrain (the terrain-following z
+    in float, src/coord.cpp:204-255)."""
     from cgfdm import model_coord
 
     if not refrun.available("CGFDM"):
