@@ -255,7 +255,10 @@ int Batch::autotune(int trial, int *best_kc, int *best_ctas, float *best_ms)
     if (int st = time_batch(trial, &ms0)) return st;
     int bk = 0, bc = 0, bt = t_orig;
     float bms = 1e30f;
+    bool eight = true;   // every session can take 32 x 8 tiles (FP32 storage, whole grid)
+    for (Session *x : s) eight = eight && !x->mixed() && !x->part_session_;
     for (int rows : {4, 8}) {
+        if (rows == 8 && !eight) continue;
         if (int st = set_tile(rows)) return st;
         const int full = device_sms(device) * (rows == 8 ? ty8::cg_stage_ctas_per_sm() : cg_stage_ctas_per_sm());
         for (int kc : kchunk_candidates(nz_max, 0))

@@ -53,7 +53,14 @@ cudaError_t prepare(Staging &s, int device)
             for (int b = 0; b < 2; b++) {
                 void *p = nullptr;
                 cudaError_t e = cudaHostAlloc(&p, UP_CHUNK, cudaHostAllocPortable);
-                if (e != cudaSuccess) return e;
+                if (e != cudaSuccess) {
+                    // give back what was pinned; the caller copies plainly
+                    for (int u = 0; u < UP_THREADS; u++)
+                        for (int c = 0; c < 2; c++)
+                            if (s.slot[u][c]) cudaFreeHost(s.slot[u][c]), s.slot[u][c] = nullptr;
+                    cudaGetLastError();
+                    return e;
+                }
                 s.slot[t][b] = (char *)p;
             }
     }
